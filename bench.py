@@ -1,0 +1,348 @@
+"""Benchmark of the evora hydro update on B200.
+
+Workload (one "step" = one full hydro step of main.f90:109-155: primitive,
+ghost fill, CFL reduction, updatetime, predictor, three sweeps): the 3D
+Kelvin-Helmholtz instability on a 256^3 periodic grid, gamma = 5/3, HLLC,
+minmod, CFL 0.5 (the reference's default, parameter.f90:46), seeded vy
+perturbation (SplitMix64 seed 42, amplitude 0.01, modes k = 1..4), synthetic
+IC built on the host in FP64.
+
+Headline `value`: the FP32 form (FP32 state/slopes/fluxes, FP64 pressure
+recovery where kin > E/2, FP64 CFL reduction) in cell-updates/s, inputs
+resident in HBM.  The FP64 form is measured on the same workload and
+reported under "fp64", with the relative L1 density error of FP32 vs FP64
+after the same steps.  `e2e` is the same metric through the public C ABI
+with host buffers: every step uploads q(6,256,256,256) from pinned host
+memory, advances one step and reads q back.
+
+`--impl reference` times the CPU oracle (the C restatement of the
+reference's hot path; the reference is Fortran and no Fortran compiler exists
+on this image) on all host threads, on a bounded z-slab sample of the same
+workload.
+
+Multi-GPU: the single-grid path has no exchange (one grid per GPU, no domain
+decomposition), so N > 1 runs N independent replicas, one per rank
+("scaling": "weak"); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = NZ = 256
+GAMMA = 5.0 / 3.0
+CFL = 0.5
+METRIC = "cell-updates/s"
+BYTES_PER_CELL = {"f32": 40, "f64": 80}   # 5 fields read + written once
+WORKLOAD = "3D Kelvin-Helmholtz 256^3 periodic, gamma=5/3, HLLC, minmod, CFL 0.5"
+
+
+def kh_params(ev, nz=NZ):
+    return ev.default_params(nx=NX, ny=NY, nz=nz, g=GAMMA, cfl=CFL, boundtype=2, solver=2,
+                             limiter=1, tend=1.0e6)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch from a committed ncu summary (profiles/*.md):
+    a line 'traffic_bytes_per_launch: N'."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"evora_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_grid(ev, torch, q, precision, steps, warmup, stream):
+    """Device-timed resident steps; returns (ms_total, kernel timing, grid)."""
+    g = ev.Grid(kh_params(ev), precision)
+    g.set_stream(stream)
+    g.set_q(q)
+    g.step(warmup, sync=True)
+    torch.cuda.synchronize()
+    g.set_timing(True)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    g.step(steps, sync=False)
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    kt = g.timing()
+    st = g.status()
+    if st:
+        raise RuntimeError(f"grid status {st}")
+    return ms, kt, g
+
+
+def time_e2e(ev, torch, q_pinned, out_pinned, precision, steps):
+    """Per step: host->device q, one step, device->host q (public C ABI)."""
+    g = ev.Grid(kh_params(ev), precision)
+    g.set_q(q_pinned)
+    g.step(1)
+    g.get_q(out_pinned)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        g.set_q(q_pinned)
+        g.step(1, sync=True)
+        g.get_q(out_pinned)
+    el = time.perf_counter() - t0
+    g.close()
+    return el
+
+
+def cpu_baseline(steps_budget_s=20.0, threads=None):
+    """The oracle (C restatement, FP64) on all host threads, on a z-slab of
+    the workload (256 x 256 x nz_s, periodic; the KH IC is z-invariant, so
+    the per-cell work equals the full grid's)."""
+    from oracle.oracle import Oracle, make_params
+    o = Oracle(make_params(nx=NX, ny=NY, nz=8, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6))
+    if threads:
+        o.set_threads(threads)
+    cores = o.max_threads()
+    q = o.ic_kh3d(42, 0.01)
+    t0 = time.perf_counter()
+    o.run(q, 1)
+    per_cell = (time.perf_counter() - t0) / q[..., 0].size
+    nz_s = int(max(8, min(NZ, steps_budget_s / 3.0 / max(per_cell, 1e-12) / (NX * NY))))
+    o = Oracle(make_params(nx=NX, ny=NY, nz=nz_s, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6))
+    q = o.ic_kh3d(42, 0.01)
+    o.run(q, 1)   # warm
+    t0 = time.perf_counter()
+    r = o.run(q, 2)
+    el = time.perf_counter() - t0
+    cells = NX * NY * nz_s * r["steps"]
+    return {"value": cells / el, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"2 steps of a {NX}x{NY}x{nz_s} periodic slab of the workload, FP64, "
+                      f"OpenMP over pencils ({cores} threads), {el:.1f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle.oracle import Oracle, make_params
+    probe = Oracle(make_params(nx=NX, ny=NY, nz=4, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6))
+    cores = probe.max_threads()
+    q = probe.ic_kh3d(42, 0.01)
+    t0 = time.perf_counter()
+    probe.run(q, 1)
+    per_cell = (time.perf_counter() - t0) / q[..., 0].size
+    budget = 150.0 / max(1, args.steps + args.warmup)       # seconds per step
+    nz_s = int(max(4, min(NZ, budget / max(per_cell, 1e-12) / (NX * NY))))
+    o = Oracle(make_params(nx=NX, ny=NY, nz=nz_s, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6))
+    q = o.ic_kh3d(42, 0.01)
+    o.run(q, args.warmup)
+    t0 = time.perf_counter()
+    r = o.run(q, args.steps)
+    el = time.perf_counter() - t0
+    value = NX * NY * nz_s * r["steps"] / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(1, r["steps"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sample_nz": nz_s},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of a {NX}x{NY}x{nz_s} periodic slab of the "
+                                   f"workload (z-invariant IC), FP64, OpenMP over pencils"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import evora_b200 as ev
+
+    world, rank, local = dist_setup(args.gpus)
+    stream = torch.cuda.Stream()
+    p = kh_params(ev)
+    q = ev.ic.kh3d(p, seed=42, amp=0.01)
+    n = NX * NY * NZ
+
+    barrier(world)
+    with ClockSampler(local) as clk:
+        ms32, kt32, g32 = time_grid(ev, torch, q, ev.FP32, args.steps, args.warmup, stream)
+    clocks = clk.summary()
+    ms32 = max_over_ranks(world, ms32)
+    barrier(world)
+    ms64, kt64, g64 = time_grid(ev, torch, q, ev.FP64, args.steps, args.warmup, stream)
+    ms64 = max_over_ranks(world, ms64)
+    # accuracy of the FP32 form against FP64 after the same steps
+    r32 = g32.get_q()[..., 0]
+    r64 = g64.get_q()[..., 0]
+    l1 = float(np.abs(r32 - r64).sum() / np.abs(r64).sum())
+    g32.close()
+    g64.close()
+
+    peak, peak_kind = measured_peaks()
+    value32 = world * n * args.steps / (ms32 * 1e-3)
+    value64 = world * n * args.steps / (ms64 * 1e-3)
+
+    def roofline(kt, dtype, prof):
+        avg_ms = kt["update_ms"] / max(1, kt["steps"])
+        bytes_alg = n * BYTES_PER_CELL[dtype]
+        achieved = bytes_alg / (avg_ms * 1e-3) / 1e9
+        traffic = profile_traffic(prof)
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_fused (fused MUSCL-Hancock update)",
+                "kernel_ms": avg_ms, "cfl_kernel_ms": kt["cfl_ms"] / max(1, kt["steps"]),
+                "algorithmic_bytes_per_launch": bytes_alg}
+
+    line = {
+        "metric": METRIC, "value": value32, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": n, "form": "FP32 state, FP64 pressure recovery (kin>E/2) and "
+                   "CFL reduction", "l2": "inputs larger than L2 (335 MB FP32 / 671 MB FP64 state per copy)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline(kt32, "f32", "fused_update_kh256_fp32.md"),
+        "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
+                 "roofline": roofline(kt64, "f64", "fused_update_kh256_fp64.md")},
+        "fp32_over_fp64": value32 / value64,
+        "l1_density_fp32_vs_fp64": l1,
+        "gpu_launches": kt32["launches"],
+        "clocks": clocks,
+    }
+    if not args.no_e2e and rank == 0:
+        qp = torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy()
+        qp[...] = q
+        outp = torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy()
+        e2e_steps = max(3, min(args.steps, 10))
+        el = time_e2e(ev, torch, qp, outp, ev.FP32, e2e_steps)
+        line["e2e"] = {"value": n * e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": q.nbytes,
+                       "d2h_bytes_per_step": q.nbytes, "form": "FP32",
+                       "note": "per step: q(6,256^3) FP64 from pinned host -> set_q, 1 step, get_q -> host"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

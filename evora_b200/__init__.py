@@ -1,0 +1,11 @@
+"""evora_b200 -- the hydro update of evora (MUSCL-Hancock predictor and
+sweeps, HLL/HLLC fluxes, ghost-cell fill, CFL reduction) as hand-written
+CUDA kernels for B200 (sm_100a), behind a C ABI (include/evora_gpu.h)."""
+from ._native import LIB_PATH, EvoraError, lib
+from .hydro import (CARRY_ENTROPY, FP32, FP64, REFERENCE_KERNELS, STRICT, DropIn, EvoraDerived,
+                    EvoraParams, Grid, default_params, derived, shapes)
+from . import ic
+
+__all__ = ["LIB_PATH", "EvoraError", "lib", "CARRY_ENTROPY", "FP32", "FP64", "REFERENCE_KERNELS",
+           "STRICT", "DropIn", "EvoraDerived", "EvoraParams", "Grid", "default_params", "derived",
+           "shapes", "ic"]

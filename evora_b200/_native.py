@@ -1,0 +1,165 @@
+"""ctypes binding of libevora_b200.so (the C ABI of include/evora_gpu.h).
+
+The library is built in-tree (evora_b200/_lib/libevora_b200.so) by
+`python -m evora_b200.build`.  There is no fallback: if the library cannot be
+loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libevora_b200.so")
+
+c_int32 = ctypes.c_int32
+c_int64 = ctypes.c_int64
+c_double = ctypes.c_double
+c_void_p = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class EvoraParams(ctypes.Structure):
+    """evora_params: the hydro subset of namelist &para (parameter.f90:30-37)."""
+
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
+        ("solver", c_int32), ("limiter", c_int32), ("boundtype", c_int32),
+        ("secondorder", c_int32), ("dualenergy", c_int32), ("atomic", c_int32),
+        ("reserved", c_int32),
+        ("g", c_double), ("cfl", c_double), ("de_thresh", c_double),
+        ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
+        ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
+        ("tstart", c_double), ("tend", c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class EvoraDerived(ctypes.Structure):
+    """evora_derived: constants of compparameter (parameter.f90:164-265)."""
+
+    _fields_ = [(n, c_double) for n in (
+        "g", "g1", "g1inv", "gg1", "cfl", "de_thresh1", "dx", "dy", "dz",
+        "dxinv", "dyinv", "dzinv", "x0", "y0", "z0", "volume")] + [
+        ("onedimension", c_int32), ("twodimension", c_int32)]
+
+
+class EvoraError(RuntimeError):
+    """A nonzero status of the C ABI (bit mask of EVORA_ERR_*)."""
+
+    NAMES = {
+        1: "negative pressure (comp.f90:74-84)",
+        2: "unphysical Riemann pressure (riemann.f90:61-66,111-116)",
+        4: "no HLL branch (riemann.f90:87-90)",
+        8: "no HLLC branch (riemann.f90:148-150)",
+        16: "time step <= 0 (timestep.f90:51-55)",
+        32: "unknown slope limiter",
+        64: "unknown Riemann solver",
+        128: "invalid argument",
+        256: "CUDA error",
+        512: "device allocation failed",
+        1024: "timeout",
+    }
+
+    def __init__(self, status: int, where: str = ""):
+        self.status = int(status)
+        parts = [v for k, v in self.NAMES.items() if self.status & k]
+        msg = f"{where}: status {self.status} ({'; '.join(parts) or 'unknown'})"
+        if self.status & 256:
+            try:
+                msg += f" [{lib().evora_last_error().decode()}]"
+            except Exception:  # pragma: no cover
+                pass
+        super().__init__(msg)
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(L):
+    P = ctypes.POINTER(EvoraParams)
+    D = ctypes.POINTER(EvoraDerived)
+    G = c_void_p
+    sig = {
+        "evora_version": ([], ctypes.c_char_p),
+        "evora_last_error": ([], ctypes.c_char_p),
+        "evora_params_default": ([P], None),
+        "evora_compparameter": ([P, D], c_int32),
+        "evora_array_sizes": ([P, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64),
+                               ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], None),
+        "evora_set_params": ([P], c_int32),
+        "evora_set_strict": ([c_int32], c_int32),
+        "evora_primitive": ([c_void_p, c_void_p], c_int32),
+        "evora_bound": ([c_void_p], c_int32),
+        "evora_hydrostep": ([c_void_p, _dp], c_int32),
+        "evora_updatetime": ([ctypes.POINTER(c_int32)] * 3 + [_dp, _dp], c_int32),
+        "evora_compevo": ([c_void_p, c_void_p, c_void_p, c_double], c_int32),
+        "evora_sweep": ([c_void_p, c_void_p, c_void_p, c_void_p, c_double], c_int32),
+        "evora_grid_create": ([P, c_int32, c_int32, ctypes.POINTER(G)], c_int32),
+        "evora_grid_destroy": ([G], c_int32),
+        "evora_grid_set_stream": ([G, c_void_p], c_int32),
+        "evora_grid_set_q": ([G, c_void_p], c_int32),
+        "evora_grid_get_q": ([G, c_void_p], c_int32),
+        "evora_grid_step": ([G, c_int32, c_int32], c_int32),
+        "evora_grid_time": ([G, _dp, _dp, ctypes.POINTER(c_int32), ctypes.POINTER(c_int64)], c_int32),
+        "evora_grid_status": ([G], c_int32),
+        "evora_grid_totals": ([G, _dp], c_int32),
+        "evora_grid_set_timing": ([G, c_int32], c_int32),
+        "evora_grid_timing": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], c_int32),
+    }
+    optional = set()
+    for name, (args, res) in sig.items():
+        try:
+            fn = getattr(L, name)
+        except AttributeError:
+            if name in optional:
+                continue
+            raise
+        fn.argtypes = args
+        fn.restype = res
+    _declare_batch(L)
+    return L
+
+
+def _declare_batch(L):
+    """Batched-tube and no-allocation entry points (declared when present)."""
+    G = c_void_p
+    sig = {
+        "evora_batch_create": ([ctypes.POINTER(EvoraParams), c_int32, ctypes.POINTER(c_int32),
+                                c_int32, c_int32, ctypes.POINTER(G)], c_int32),
+        "evora_batch_destroy": ([G], c_int32),
+        "evora_batch_set_stream": ([G, c_void_p], c_int32),
+        "evora_batch_set_q": ([G, c_int32, c_void_p], c_int32),
+        "evora_batch_get_q": ([G, c_int32, c_void_p], c_int32),
+        "evora_batch_run": ([G, c_int32, c_int32], c_int32),
+        "evora_batch_info": ([G, c_int32, _dp, _dp, ctypes.POINTER(c_int32),
+                              ctypes.POINTER(c_int64), ctypes.POINTER(c_int32)], c_int32),
+        "evora_batch_steps_done": ([G, ctypes.POINTER(c_int64)], c_int32),
+    }
+    for name, (args, res) in sig.items():
+        if hasattr(L, name):
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+
+
+def lib():
+    """The loaded library; raises if it is not built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m evora_b200.build` "
+                    "(there is no CPU fallback)")
+            _lib = _declare(ctypes.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(status: int, where: str):
+    if status:
+        raise EvoraError(status, where)

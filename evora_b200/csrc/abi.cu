@@ -1,0 +1,349 @@
+// abi.cu -- host side of the C ABI: parameters (readparameter defaults,
+// compparameter), error reporting, and the drop-in layer entry points that
+// mirror primitive / bound / hydrostep / updatetime / compevo / sweep.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/evora_gpu.h"
+#include "common.h"
+#include "dropin_api.h"
+
+namespace evora {
+
+static thread_local char g_last_error[256] = "";
+
+void set_cuda_error(cudaError_t e, const char* where) {
+  std::snprintf(g_last_error, sizeof g_last_error, "%s: %s", where, cudaGetErrorString(e));
+}
+
+bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, int* status) {
+  evora_derived dd;
+  int rc = evora_compparameter(p, &dd);
+  if (status) *status = rc;
+  if (rc) return false;
+  if (d) *d = dd;
+  P->nx = p->nx; P->ny = p->ny; P->nz = p->nz;
+  P->solver = p->solver; P->limiter = p->limiter; P->boundtype = p->boundtype;
+  P->secondorder = p->secondorder != 0; P->dualenergy = p->dualenergy != 0;
+  P->onedimension = dd.onedimension; P->twodimension = dd.twodimension;
+  P->g = dd.g; P->g1 = dd.g1; P->g1inv = dd.g1inv; P->gg1 = dd.gg1; P->cfl = dd.cfl;
+  P->de_thresh1 = dd.de_thresh1;
+  P->dx = dd.dx; P->dy = dd.dy; P->dz = dd.dz;
+  P->dxinv = dd.dxinv; P->dyinv = dd.dyinv; P->dzinv = dd.dzinv;
+  return true;
+}
+
+bool is_device_pointer(const void* ptr) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace evora
+
+using namespace evora;
+
+extern "C" {
+
+const char* evora_version(void) { return "evora-b200 0.1 (sm_100a)"; }
+
+const char* evora_last_error(void) { return g_last_error; }
+
+void evora_params_default(evora_params* p) {
+  std::memset(p, 0, sizeof *p);
+  // parameter.f90:43-82 (hydro and grid subset)
+  p->secondorder = 1;
+  p->solver = 2;
+  p->limiter = 1;
+  p->cfl = 0.5;
+  p->g = (double)1.4f;  // default-real literal
+  p->atomic = 0;
+  p->nx = p->ny = p->nz = 32;
+  p->xmin = 0.0; p->xmax = 1.0;
+  p->ymin = 0.0; p->ymax = 1.0;
+  p->zmin = 0.0; p->zmax = 1.0;
+  p->boundtype = 2;
+  p->tstart = 0.0; p->tend = 1.0;
+  p->dualenergy = 0;
+  p->de_thresh = 0.0;
+}
+
+int evora_compparameter(const evora_params* p, evora_derived* d) {
+  if (!p || !d) return EVORA_ERR_ARG;
+  if (p->nx < 2 || p->ny < 1 || p->nz < 1) return EVORA_ERR_ARG;
+  if (p->nz > 1 && p->ny == 1) return EVORA_ERR_ARG;
+  if (p->solver != 1 && p->solver != 2) return EVORA_ERR_SOLVER;
+  if (p->limiter < 1 || p->limiter > 3) return EVORA_ERR_LIMITER;
+  if (p->boundtype < 1 || p->boundtype > 3) return EVORA_ERR_ARG;
+  // parameter.f90:164-265
+  double g = p->atomic ? (double)(5.0f / 3.0f) : p->g;
+  d->g = g;
+  d->cfl = p->cfl;
+  d->onedimension = (p->ny == 1 && p->nz == 1);
+  d->twodimension = (p->nz == 1);
+  double xmin = p->xmin, xmax = p->xmax, ymin = p->ymin, ymax = p->ymax;
+  double zmin = p->zmin, zmax = p->zmax;
+  d->dx = (xmax - xmin) / p->nx;
+  d->dy = (ymax - ymin) / p->ny;
+  d->dz = (zmax - zmin) / p->nz;
+  if (d->onedimension) {
+    d->dy = d->dx; d->dz = d->dx;
+    ymin = 0.0; ymax = d->dy; zmin = 0.0; zmax = d->dz;
+    d->dy = (ymax - ymin) / p->ny;
+    d->dz = (zmax - zmin) / p->nz;
+  }
+  if (d->twodimension) {
+    d->dz = d->dx;
+    zmin = 0.0; zmax = d->dz;
+    d->dz = (zmax - zmin) / p->nz;
+  }
+  d->dxinv = 1.0 / d->dx; d->dyinv = 1.0 / d->dy; d->dzinv = 1.0 / d->dz;
+  d->x0 = xmin + d->dx / 2; d->y0 = ymin + d->dy / 2; d->z0 = zmin + d->dz / 2;
+  d->volume = (xmax - xmin) * (ymax - ymin) * (zmax - zmin);
+  d->g1 = g - 1.0;
+  d->g1inv = 1.0 / d->g1;
+  d->gg1 = g / d->g1;
+  d->de_thresh1 = p->dualenergy ? 1.0 - p->de_thresh : 1.0;
+  if (!(d->dx > 0.0) || !(d->dy > 0.0) || !(d->dz > 0.0)) return EVORA_ERR_ARG;
+  return EVORA_OK;
+}
+
+void evora_array_sizes(const evora_params* p, int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
+  if (nq) *nq = (int64_t)EVORA_NQ * p->nx * p->ny * p->nz;
+  if (nw) *nw = (int64_t)EVORA_NW * (p->nx + 4) * (p->ny + 4) * (p->nz + 4);
+  if (ne) *ne = (int64_t)EVORA_NW * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+  if (ns) *ns = (int64_t)EVORA_NW * 3 * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- drop-in --
+namespace {
+
+struct DropinState {
+  std::mutex mu;
+  bool have_params = false;
+  evora_params params{};
+  HydroParams P{};
+  int strict = 0;
+  int device = -1;
+  unsigned* d_err = nullptr;
+  unsigned long long* d_smax = nullptr;
+  // staging buffers for host arrays: q, w, evo, s
+  double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t stage_bytes[4] = {0, 0, 0, 0};
+};
+
+DropinState& ds() {
+  static DropinState s;
+  return s;
+}
+
+enum { SLOT_Q = 0, SLOT_W = 1, SLOT_E = 2, SLOT_S = 3 };
+
+#define CU(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) {                       \
+      set_cuda_error(e_, #call);                   \
+      return EVORA_ERR_CUDA;                       \
+    }                                              \
+  } while (0)
+
+// Resolves a caller pointer to a device pointer: device memory is used in
+// place; host memory is copied into a cached staging buffer when copy_in.
+int resolve(DropinState& S, int slot, const double* ptr, size_t bytes, bool copy_in, double** out) {
+  if (!ptr) return EVORA_ERR_ARG;
+  if (is_device_pointer(ptr)) {
+    *out = const_cast<double*>(ptr);
+    return 0;
+  }
+  if (S.stage_bytes[slot] < bytes) {
+    if (S.stage[slot]) cudaFree(S.stage[slot]);
+    S.stage[slot] = nullptr;
+    S.stage_bytes[slot] = 0;
+    if (cudaMalloc(&S.stage[slot], bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return EVORA_ERR_NOMEM;
+    }
+    S.stage_bytes[slot] = bytes;
+  }
+  if (copy_in) CU(cudaMemcpy(S.stage[slot], ptr, bytes, cudaMemcpyHostToDevice));
+  *out = S.stage[slot];
+  return 0;
+}
+
+int copy_back(double* host, const double* dev, size_t bytes) {
+  if (host == dev) return 0;
+  CU(cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int begin(DropinState& S) {
+  if (!S.have_params) return EVORA_ERR_ARG;
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (S.device != dev || !S.d_err) {
+    if (S.d_err) cudaFree(S.d_err);
+    S.d_err = nullptr;
+    CU(cudaMalloc(&S.d_err, sizeof(unsigned) + 3 * sizeof(unsigned long long)));
+    S.d_smax = reinterpret_cast<unsigned long long*>(S.d_err + 2);
+    for (auto& b : S.stage) {
+      if (b) cudaFree(b);
+      b = nullptr;
+    }
+    for (auto& n : S.stage_bytes) n = 0;
+    S.device = dev;
+  }
+  CU(cudaMemset(S.d_err, 0, sizeof(unsigned)));
+  return 0;
+}
+
+int finish(DropinState& S) {
+  CU(cudaGetLastError());
+  CU(cudaDeviceSynchronize());
+  unsigned e = 0;
+  CU(cudaMemcpy(&e, S.d_err, sizeof e, cudaMemcpyDeviceToHost));
+  return (int)e;
+}
+
+const DropinOps& ops(const DropinState& S) { return S.strict ? evora::strict::kOps : evora::fast::kOps; }
+
+}  // namespace
+
+extern "C" {
+
+int evora_set_params(const evora_params* p) {
+  if (!p) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  HydroParams P;
+  int rc = 0;
+  if (!params_to_hydro(p, &P, nullptr, &rc)) return rc;
+  S.params = *p;
+  S.P = P;
+  S.have_params = true;
+  return 0;
+}
+
+int evora_set_strict(int32_t strict) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  S.strict = strict != 0;
+  return 0;
+}
+
+int evora_primitive(double* w, double* q) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  int rc = begin(S);
+  if (rc) return rc;
+  int64_t nq, nw;
+  evora_array_sizes(&S.params, &nq, &nw, nullptr, nullptr);
+  double *dq, *dw;
+  if ((rc = resolve(S, SLOT_Q, q, nq * 8, true, &dq))) return rc;
+  if ((rc = resolve(S, SLOT_W, w, nw * 8, true, &dw))) return rc;
+  ops(S).primitive(S.P, dw, dq, S.d_err, nullptr, 0);
+  int st = finish(S);
+  if (st & EVORA_ERR_CUDA) return st;
+  if ((rc = copy_back(w, dw, nw * 8))) return rc;
+  if (S.P.dualenergy && (rc = copy_back(q, dq, nq * 8))) return rc;
+  return st;
+}
+
+int evora_bound(double* w) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  int rc = begin(S);
+  if (rc) return rc;
+  int64_t nw;
+  evora_array_sizes(&S.params, nullptr, &nw, nullptr, nullptr);
+  double* dw;
+  if ((rc = resolve(S, SLOT_W, w, nw * 8, true, &dw))) return rc;
+  ops(S).bound(S.P, dw, nullptr, 0);
+  int st = finish(S);
+  if ((rc = copy_back(w, dw, nw * 8))) return rc;
+  return st;
+}
+
+int evora_hydrostep(const double* w, double* dt) {
+  if (!dt) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  int rc = begin(S);
+  if (rc) return rc;
+  int64_t nw;
+  evora_array_sizes(&S.params, nullptr, &nw, nullptr, nullptr);
+  double* dw;
+  if ((rc = resolve(S, SLOT_W, w, nw * 8, true, &dw))) return rc;
+  CU(cudaMemset(S.d_smax, 0, 3 * sizeof(unsigned long long)));
+  ops(S).cfl(S.P, dw, S.d_smax, nullptr, 0);
+  int st = finish(S);
+  if (st) return st;
+  unsigned long long bits[3];
+  CU(cudaMemcpy(bits, S.d_smax, sizeof bits, cudaMemcpyDeviceToHost));
+  double sm[3];
+  std::memcpy(sm, bits, sizeof sm);
+  unsigned e = 0;
+  *dt = cfl_dt(S.P, sm[0], sm[1], sm[2], *dt, e);
+  return (int)e;
+}
+
+int evora_updatetime(int32_t* go, int32_t* dump, int32_t* k, double* t, double* dt) {
+  (void)dump;
+  (void)k;
+  if (!go || !t || !dt) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  int g = *go;
+  update_time(S.params.tend, *t, *dt, g);
+  *go = g;
+  return 0;
+}
+
+int evora_compevo(const double* w, double* evo, double* s, double dt) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  int rc = begin(S);
+  if (rc) return rc;
+  int64_t nw, ne, ns;
+  evora_array_sizes(&S.params, nullptr, &nw, &ne, &ns);
+  double *dw, *de, *dss;
+  if ((rc = resolve(S, SLOT_W, w, nw * 8, true, &dw))) return rc;
+  if ((rc = resolve(S, SLOT_E, evo, ne * 8, true, &de))) return rc;
+  if ((rc = resolve(S, SLOT_S, s, ns * 8, true, &dss))) return rc;
+  ops(S).compevo(S.P, dw, de, dss, dt, nullptr, 0);
+  int st = finish(S);
+  if ((rc = copy_back(evo, de, ne * 8))) return rc;
+  if ((rc = copy_back(s, dss, ns * 8))) return rc;
+  return st;
+}
+
+int evora_sweep(const double* w, double* q, const double* evo, const double* s, double dt) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  int rc = begin(S);
+  if (rc) return rc;
+  int64_t nq, nw, ne, ns;
+  evora_array_sizes(&S.params, &nq, &nw, &ne, &ns);
+  double *dq, *dw, *de, *dss;
+  if ((rc = resolve(S, SLOT_Q, q, nq * 8, true, &dq))) return rc;
+  if ((rc = resolve(S, SLOT_W, w, nw * 8, true, &dw))) return rc;
+  if ((rc = resolve(S, SLOT_E, evo, ne * 8, true, &de))) return rc;
+  if ((rc = resolve(S, SLOT_S, s, ns * 8, true, &dss))) return rc;
+  ops(S).sweep(S.P, dw, dq, de, dss, dt, S.d_err, nullptr, 0);
+  int st = finish(S);
+  if ((rc = copy_back(q, dq, nq * 8))) return rc;
+  return st;
+}
+
+}  // extern "C"

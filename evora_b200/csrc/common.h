@@ -1,0 +1,20 @@
+// common.h -- host-side helpers shared by the ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/evora_gpu.h"
+#include "hydro_math.cuh"
+
+namespace evora {
+
+// Records a CUDA error for evora_last_error().
+void set_cuda_error(cudaError_t e, const char* where);
+
+// evora_params -> validated HydroParams (+ derived constants).
+bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, int* status);
+
+// True for device or managed memory.
+bool is_device_pointer(const void* ptr);
+
+}  // namespace evora

@@ -1,0 +1,182 @@
+// fused.cu -- planning, layout conversion and diagnostics of the fused
+// (structure-of-arrays) backend.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "../../include/evora_gpu.h"
+#include "common.h"
+#include "fused.h"
+
+namespace evora {
+
+int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* pl) {
+  *pl = FusedPlan{};
+  pl->P = P;
+  pl->precision = precision;
+  pl->nf = nf;
+  pl->strict = strict;
+  pl->dim = P.onedimension ? 1 : (P.twodimension ? 2 : 3);
+  pl->n = (int64_t)P.nx * P.ny * P.nz;
+  FusedLaunch (*pick)(int, int, int*, int*, int*, size_t*, int*);
+  if (precision == EVORA_FP32) {
+    pick = f32::pick;
+    pl->cfl = f32::cfl;
+  } else if (strict) {
+    pick = f64s::pick;
+    pl->cfl = f64s::cfl;
+  } else {
+    pick = f64::pick;
+    pl->cfl = f64::cfl;
+  }
+  pl->launch = pick(nf, pl->dim, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads);
+  if (pl->dim == 1) {
+    int64_t b = (P.nx + 127) / 128;
+    pl->grid = dim3((unsigned)(b < 1 ? 1 : b), 1, 1);
+  } else {
+    pl->grid = dim3((P.nx + pl->tx - 1) / pl->tx, (P.ny + pl->ty - 1) / pl->ty,
+                    pl->dim == 3 ? (P.nz + pl->zc - 1) / pl->zc : 1);
+  }
+  int64_t nb = (pl->n + 255) / 256;
+  pl->nblk_tot = (int)(nb > 148 * 4 ? 148 * 4 : nb);
+  if (cudaMalloc(&pl->partials, sizeof(double) * 6 * pl->nblk_tot) != cudaSuccess) {
+    cudaGetLastError();
+    return EVORA_ERR_NOMEM;
+  }
+  return 0;
+}
+
+void fused_plan_free(FusedPlan* pl) {
+  if (pl->partials) cudaFree(pl->partials);
+  pl->partials = nullptr;
+}
+
+void fused_cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st) { pl.cfl(pl, q, ctl, st); }
+
+void fused_update(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
+  pl.launch(pl, qin, qout, ctl, st);
+}
+
+namespace {
+
+template <typename T>
+__global__ void k_from_aos(const double* __restrict__ aos, T* __restrict__ q, int64_t n, int nf) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int f = 0; f < nf; ++f) q[f * n + i] = (T)aos[EVORA_NQ * i + f];
+}
+
+// Without the entropy field, q(6) = p / rho^(g-1) of the current state
+// (the value pressure() would resynchronise it to, comp.f90:66-68).
+template <typename T>
+__global__ void k_to_aos(const T* __restrict__ q, double* __restrict__ aos, int64_t n, int nf, double g1) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v[6];
+    for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+    if (nf == 5) {
+      double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
+      double kin = 0.5 * m2 / v[0];
+      double p = g1 * (v[4] - kin);
+      v[5] = p / pow(v[0], g1);
+    }
+    for (int f = 0; f < EVORA_NQ; ++f) aos[EVORA_NQ * i + f] = v[f];
+  }
+}
+
+// Deterministic two-pass sum of the six conserved fields.
+template <typename T>
+__global__ void k_totals_part(const T* __restrict__ q, int64_t n, int nf, int aos, double g1, double* part) {
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v[6];
+    for (int f = 0; f < 6; ++f) v[f] = 0.0;
+    if (aos) {
+      for (int f = 0; f < 6; ++f) v[f] = (double)q[6 * i + f];
+    } else {
+      for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+      if (nf == 5) {
+        double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
+        double p = g1 * (v[4] - 0.5 * m2 / v[0]);
+        v[5] = p / pow(v[0], g1);
+      }
+    }
+    for (int f = 0; f < 6; ++f) s[f] += v[f];
+  }
+  __shared__ double red[6][256];
+  for (int f = 0; f < 6; ++f) red[f][threadIdx.x] = s[f];
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int f = 0; f < 6; ++f) red[f][threadIdx.x] += red[f][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int f = 0; f < 6; ++f) part[6 * blockIdx.x + f] = red[f][0];
+}
+
+__global__ void k_totals_final(const double* part, int nb, double* out) {
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += part[6 * b + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+int grid_of(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
+}
+
+}  // namespace
+
+void fused_from_aos(const FusedPlan& pl, const double* aos, void* q, cudaStream_t st) {
+  if (pl.precision == EVORA_FP32) k_from_aos<float><<<grid_of(pl.n), 256, 0, st>>>(aos, (float*)q, pl.n, pl.nf);
+  else k_from_aos<double><<<grid_of(pl.n), 256, 0, st>>>(aos, (double*)q, pl.n, pl.nf);
+}
+
+void fused_to_aos(const FusedPlan& pl, const void* q, double* aos, cudaStream_t st) {
+  if (pl.precision == EVORA_FP32)
+    k_to_aos<float><<<grid_of(pl.n), 256, 0, st>>>((const float*)q, aos, pl.n, pl.nf, pl.P.g1);
+  else
+    k_to_aos<double><<<grid_of(pl.n), 256, 0, st>>>((const double*)q, aos, pl.n, pl.nf, pl.P.g1);
+}
+
+static int totals_run(const void* q, bool f32, int64_t n, int nf, int aos, double g1, double* part, int nb,
+                      double out[6], cudaStream_t st) {
+  double* dout = part + 6 * (nb - 1) + 6;  // not used: final goes to a small buffer below
+  (void)dout;
+  double* fin = nullptr;
+  if (cudaMalloc(&fin, 6 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return EVORA_ERR_NOMEM;
+  }
+  if (f32) k_totals_part<float><<<nb, 256, 0, st>>>((const float*)q, n, nf, aos, g1, part);
+  else k_totals_part<double><<<nb, 256, 0, st>>>((const double*)q, n, nf, aos, g1, part);
+  k_totals_final<<<1, 32, 0, st>>>(part, nb, fin);
+  cudaError_t e = cudaMemcpyAsync(out, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(fin);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "totals");
+    return EVORA_ERR_CUDA;
+  }
+  return 0;
+}
+
+int fused_totals(const FusedPlan& pl, const void* q, double out[6], cudaStream_t st) {
+  return totals_run(q, pl.precision == EVORA_FP32, pl.n, pl.nf, 0, pl.P.g1, pl.partials, pl.nblk_tot, out, st);
+}
+
+int fused_totals_aos(const double* aos, int64_t n, double out[6], cudaStream_t st) {
+  int64_t nb64 = (n + 255) / 256;
+  int nb = (int)(nb64 > 148 * 4 ? 148 * 4 : nb64);
+  double* part = nullptr;
+  if (cudaMalloc(&part, sizeof(double) * 6 * nb) != cudaSuccess) {
+    cudaGetLastError();
+    return EVORA_ERR_NOMEM;
+  }
+  int rc = totals_run(aos, false, n, 6, 1, 0.0, part, nb, out, st);
+  cudaFree(part);
+  return rc;
+}
+
+}  // namespace evora

@@ -1,0 +1,64 @@
+// fused.h -- host interface of the fused (structure-of-arrays) backend.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "hydro_math.cuh"
+
+namespace evora {
+
+struct FusedPlan;
+
+// Launches the fused update of one step, qin -> qout.
+typedef void (*FusedLaunch)(const FusedPlan& plan, const void* qin, void* qout, GridCtl* ctl,
+                            cudaStream_t st);
+
+struct FusedPlan {
+  HydroParams P{};
+  int precision = 0;   // EVORA_FP64 / EVORA_FP32
+  int nf = 5;          // advected fields
+  int strict = 0;
+  int dim = 3;         // 1, 2 or 3
+  int64_t n = 0;       // cells
+  int tx = 0, ty = 0, zc = 0;
+  size_t smem = 0;
+  dim3 grid{1, 1, 1};
+  int threads = 0;
+  FusedLaunch launch = nullptr;
+  void (*cfl)(const FusedPlan&, const void* q, GridCtl* ctl, cudaStream_t st) = nullptr;
+  double* partials = nullptr;  // device scratch of the totals reduction
+  int nblk_tot = 0;
+};
+
+// Chooses tiles and the kernel instantiation; allocates small scratch.
+int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* plan);
+void fused_plan_free(FusedPlan* plan);
+
+// hydrostep part 1: per-axis maxima of |u_d| + a into ctl->smax (FP64).
+void fused_cfl(const FusedPlan& plan, const void* q, GridCtl* ctl, cudaStream_t st);
+
+// The fused MUSCL-Hancock update (primitive, bound, compevo, sweep).
+void fused_update(const FusedPlan& plan, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st);
+
+// Layout conversions between the reference q(6, nx, ny, nz) (FP64) and the
+// resident SoA state.  Without the entropy field, q(6) is written as
+// p / rho^(g-1) of the current state.
+void fused_from_aos(const FusedPlan& plan, const double* aos, void* q, cudaStream_t st);
+void fused_to_aos(const FusedPlan& plan, const void* q, double* aos, cudaStream_t st);
+
+// Sums of q(1..6) over the grid in FP64, deterministic order (synchronises).
+int fused_totals(const FusedPlan& plan, const void* q, double out[6], cudaStream_t st);
+int fused_totals_aos(const double* aos, int64_t n, double out[6], cudaStream_t st);
+
+// Instantiation launchers (fused_f64.cu, fused_f64_strict.cu, fused_f32.cu).
+#define EVORA_DECLARE_FUSED_NS(ns)                                                           \
+  namespace ns {                                                                             \
+  FusedLaunch pick(int nf, int dim, int* tx, int* ty, int* zc, size_t* smem, int* threads);   \
+  void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st);                \
+  }
+EVORA_DECLARE_FUSED_NS(f64)
+EVORA_DECLARE_FUSED_NS(f64s)
+EVORA_DECLARE_FUSED_NS(f32)
+#undef EVORA_DECLARE_FUSED_NS
+
+}  // namespace evora

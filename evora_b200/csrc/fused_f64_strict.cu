@@ -1,0 +1,9 @@
+// Fused backend, FP64, strict arithmetic: compiled with --fmad=false so that
+// the result equals a gfortran -O3 x86-64 build of the reference bit for bit
+// on rho, m and E (the entropy field goes through pow).
+#define EVORA_FNS f64s
+#define EVORA_T double
+#define EVORA_TX 32
+#define EVORA_TY 4
+#define EVORA_ZC 32
+#include "fused_inst.cuh"

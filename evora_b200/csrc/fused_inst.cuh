@@ -1,0 +1,106 @@
+// fused_inst.cuh -- one arithmetic instantiation of the fused backend: the
+// update kernels for NF = 5/6 fields and 1, 2, 3 dimensions, and the CFL
+// kernel, compiled with this translation unit's floating-point flags.
+// Requires EVORA_FNS (namespace), EVORA_T (state type) and the tile shape
+// EVORA_TX, EVORA_TY, EVORA_ZC.
+#pragma once
+
+#include "fused.h"
+#include "fused_kernel.cuh"
+
+namespace evora {
+namespace EVORA_FNS {
+
+using TT = EVORA_T;
+constexpr int TX = EVORA_TX, TY = EVORA_TY, ZC = EVORA_ZC;
+
+template <int NF, int DIM>
+void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
+  FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n};
+  if constexpr (DIM == 1) {
+    k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
+  } else {
+    k_fused<TT, NF, DIM, TX, TY, ZC><<<pl.grid, pl.threads, pl.smem, st>>>(A);
+  }
+}
+
+template <int NF, int DIM>
+FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads) {
+  if constexpr (DIM == 1) {
+    *tx = 128; *ty = 1; *zc = 1; *smem = 0; *threads = 128;
+  } else {
+    *tx = TX; *ty = TY; *zc = DIM == 3 ? ZC : 1;
+    *smem = sizeof(FusedSmem<TT, NF, TX, TY>);
+    *threads = TX * TY;
+    cudaFuncSetAttribute(k_fused<TT, NF, DIM, TX, TY, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)*smem);
+  }
+  return &launch<NF, DIM>;
+}
+
+FusedLaunch pick(int nf, int dim, int* tx, int* ty, int* zc, size_t* smem, int* threads) {
+  if (nf == 5) {
+    if (dim == 1) return pick_one<5, 1>(tx, ty, zc, smem, threads);
+    if (dim == 2) return pick_one<5, 2>(tx, ty, zc, smem, threads);
+    return pick_one<5, 3>(tx, ty, zc, smem, threads);
+  }
+  if (dim == 1) return pick_one<6, 1>(tx, ty, zc, smem, threads);
+  if (dim == 2) return pick_one<6, 2>(tx, ty, zc, smem, threads);
+  return pick_one<6, 3>(tx, ty, zc, smem, threads);
+}
+
+// hydrostep part 1 on the SoA state: maxima of |u_d| + a in FP64 (the state
+// is widened to FP64 first; q2w as in primitive, comp.f90:26-85).
+template <int NF>
+__global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, GridCtl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const Gas<double> c = Gas<double>::make(P);
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  unsigned err = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double qv[6], w[5];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) qv[f] = (double)__ldg(q + f * n + i);
+    q2w(qv, w, c, P.dualenergy != 0, err);
+    double a = sqrt(P.g * w[4] / w[0]);
+    double s0 = fabs(w[1]) + a, s1 = fabs(w[2]) + a, s2 = fabs(w[3]) + a;
+    if (s0 > m0) m0 = s0;
+    if (s1 > m1) m1 = s1;
+    if (s2 > m2) m2 = s2;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    m0 = fmax2(m0, __shfl_xor_sync(0xffffffffu, m0, off));
+    m1 = fmax2(m1, __shfl_xor_sync(0xffffffffu, m1, off));
+    m2 = fmax2(m2, __shfl_xor_sync(0xffffffffu, m2, off));
+  }
+  __shared__ double red[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) { red[0][wid] = m0; red[1][wid] = m1; red[2][wid] = m2; }
+  __syncthreads();
+  if (wid == 0) {
+    m0 = lane < nw ? red[0][lane] : 0.0;
+    m1 = lane < nw ? red[1][lane] : 0.0;
+    m2 = lane < nw ? red[2][lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) {
+      m0 = fmax2(m0, __shfl_xor_sync(0xffffffffu, m0, off));
+      m1 = fmax2(m1, __shfl_xor_sync(0xffffffffu, m1, off));
+      m2 = fmax2(m2, __shfl_xor_sync(0xffffffffu, m2, off));
+    }
+    if (lane == 0) {
+      atomicMax(&ctl->smax[0], ordered_bits(m0));
+      atomicMax(&ctl->smax[1], ordered_bits(m1));
+      atomicMax(&ctl->smax[2], ordered_bits(m2));
+    }
+  }
+  if (err) atomicOr(&ctl->err, err);
+}
+
+void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st) {
+  int64_t blocks = (pl.n + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (pl.nf == 5) k_cfl_soa<5><<<(int)blocks, 256, 0, st>>>(pl.P, (const TT*)q, pl.n, ctl);
+  else k_cfl_soa<6><<<(int)blocks, 256, 0, st>>>(pl.P, (const TT*)q, pl.n, ctl);
+}
+
+}  // namespace EVORA_FNS
+}  // namespace evora

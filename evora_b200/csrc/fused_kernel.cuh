@@ -1,0 +1,490 @@
+// fused_kernel.cuh -- the whole hydro update of one step in one HBM pass.
+//
+// The reference computes primitives w, ghost cells, slopes s and the
+// half-step predictor evo into full-grid arrays, then sweeps x, y and z
+// (muscl.f90:26-290).  All three sweeps read the same start-of-step w, s and
+// evo and only add flux differences to q, in the order x, y, z per cell, so
+// the update of a cell is a pure function of the start-of-step state in a
+// radius-2 neighbourhood.  This kernel computes it tile by tile without
+// writing any intermediate to HBM:
+//
+//   CTA tile = TX x TY columns (x, y) marching over ZC planes in z.
+//   Per plane c:
+//     A  load q of plane c+1 over the tile plus a 2-cell halo, map ghost
+//        cells onto interior cells (periodic / zero-gradient mirror /
+//        reflecting upper x, boundary.f90:26-113), convert to primitives
+//        (q2w, comp.f90:26-85) into a 3-plane shared-memory ring;
+//     B  slopes in x, y, z (comp_slope, muscl.f90:115-169) and the predictor
+//        evo (muscl.f90:89-111) for the tile cells and the one-cell x/y ring,
+//        then the face states w -+ s/2 + evo (muscl.f90:208-209);
+//     C  one Riemann solve per x and y interface of the plane (riemann.f90)
+//        into shared memory, and per column the z interface c-1/2 in
+//        registers;
+//     D  per owned cell: q + dt/dx (Fx- - Fx+), then + dt/dy (Fy- - Fy+)
+//        (integration, muscl.f90:276-290); the z term of plane c-1 is added
+//        once the flux c-1/2 is known, and plane c-1 is written out.
+//
+// Ghost cells are never materialised: the boundary condition is an index
+// map applied when the halo is loaded.  The ping-pong output buffer keeps
+// neighbouring tiles reading the start-of-step state.
+//
+// The same source compiles for a host emulation (EVORA_HOST_EMU) in which the
+// threads of a CTA are std::threads meeting at a std::barrier, so the tile
+// logic can be checked against the CPU oracle without a GPU.
+#pragma once
+
+#include "hydro_math.cuh"
+
+#ifdef EVORA_HOST_EMU
+#include <algorithm>
+#include <atomic>
+#include <barrier>
+namespace evora_emu {
+extern thread_local std::barrier<>* tl_barrier;
+}
+#define EV_SYNC() ::evora_emu::tl_barrier->arrive_and_wait()
+#define EV_RESTRICT
+#else
+#define EV_SYNC() __syncthreads()
+#define EV_RESTRICT __restrict__
+#endif
+
+#ifndef EVORA_FNS
+#error "define EVORA_FNS (namespace of this instantiation) before including fused_kernel.cuh"
+#endif
+
+namespace evora {
+namespace EVORA_FNS {
+
+template <typename T>
+struct FusedArgs {
+  HydroParams P;
+  const T* qin;     // NF planes of n cells, x fastest (SoA)
+  T* qout;
+  GridCtl* ctl;     // dt, active flag, error mask
+  int64_t n;        // cells per field
+};
+
+// Boundary index map of one axis (0-based), boundary.f90:26-113: g in
+// [-2, n+1] maps onto the interior.  Periodic wraps; zero gradient mirrors
+// (ghost -1 <- cell 0, ghost -2 <- cell 1); boundtype 3 mirrors with all
+// velocity components negated at the upper x face.
+__device__ __forceinline__ int ghost_map(int g, int n, int bt, int axis, bool& flip) {
+  if (g >= 0 && g < n) return g;
+  if (bt == 2) return g < 0 ? g + n : g - n;
+  if (g < 0) return -g - 1;
+  if (bt == 3 && axis == 0) flip = true;
+  return 2 * n - g - 1;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p) {
+#if defined(__CUDACC__) && !defined(EVORA_HOST_EMU)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+
+// Primitive variables from conserved ones.  For FP64 this is q2w itself.
+// For FP32 state the pressure p = (g-1)(E - kin) is recovered in FP64 when
+// kin > E/2, where FP32 cancellation would lose more than one bit.
+template <typename T>
+__device__ __forceinline__ void prim(T* q, T* w, const Gas<T>& c, const HydroParams& P, bool de,
+                                     unsigned& err) {
+  if constexpr (sizeof(T) == 8) {
+    q2w(q, w, c, de, err);
+  } else {
+    T densinv = (T)1.0 / q[0];
+    w[0] = q[0];
+    w[1] = q[1] * densinv;
+    w[2] = q[2] * densinv;
+    w[3] = q[3] * densinv;
+    T m2 = (q[1] * q[1]) + (q[2] * q[2]) + (q[3] * q[3]);
+    T kin = (T)0.5 * m2 / q[0];
+    T press;
+    if (kin > (T)0.5 * q[4]) {
+      double dm2 = ((double)q[1] * q[1]) + ((double)q[2] * q[2]) + ((double)q[3] * q[3]);
+      double dkin = 0.5 * dm2 / (double)q[0];
+      press = (T)(P.g1 * ((double)q[4] - dkin));
+    } else {
+      press = c.g1 * (q[4] - kin);
+    }
+    if (press <= (T)0) err |= EVORA_ERR_PRESSURE;
+    w[4] = press;
+  }
+}
+
+// Shared-memory layout of one CTA (all arrays field-major).
+template <typename T, int NF, int TX, int TY>
+struct FusedSmem {
+  static constexpr int RX = TX + 4, RY = TY + 4;
+  T w[3][5][RY][RX];          // primitive ring: planes c-1, c, c+1 (+ halo 2)
+  T xf[2][5][TY][TX + 2];     // x face states of the tile + x ring: [0] lower, [1] upper
+  T yf[2][5][TY + 2][TX];     // y face states of the tile + y ring
+  T fx[NF][TY][TX + 1];       // x fluxes, interface i-1/2 at column i
+  T fy[NF][TY + 1][TX];       // y fluxes, interface j-1/2 at row j
+};
+
+// Slopes, predictor and face states of one cell of plane c.  (cx, cy) are
+// coordinates in the halo ring arrays.  DIM = 2 or 3 selects the 2D
+// (muscl.f90:70-88) or 3D (89-111) predictor.
+template <typename T, int DIM, int TX, int TY, typename Sm>
+__device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn, int cx, int cy,
+                                           const HydroParams& P, T dt2, T* wv, T (*face)[2][5]) {
+  T sx[5], sy[5], sz[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    wv[f] = sm.w[sc][f][cy][cx];
+    sx[f] = slope1(sm.w[sc][f][cy][cx - 1], wv[f], sm.w[sc][f][cy][cx + 1], P.limiter);
+    sy[f] = slope1(sm.w[sc][f][cy - 1][cx], wv[f], sm.w[sc][f][cy + 1][cx], P.limiter);
+    if (DIM == 3) sz[f] = slope1(sm.w[sp][f][cy][cx], wv[f], sm.w[sn][f][cy][cx], P.limiter);
+  }
+  if (!P.secondorder) {
+    // first-order Godunov: the face states are the cell averages (sweep,
+    // muscl.f90:198-201, 207-210)
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) face[d][0][f] = face[d][1][f] = wv[f];
+    return;
+  }
+  T a1[5], a2[5], a3[5], evo[5];
+  const T g = (T)P.g;
+  predictor_term(wv, sx, 1, g, a1);
+  predictor_term(wv, sy, 2, g, a2);
+  if (DIM == 3) predictor_term(wv, sz, 3, g, a3);
+  const T dxi = (T)P.dxinv, dyi = (T)P.dyinv, dzi = (T)P.dzinv;
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    if (DIM == 3) evo[f] = dt2 * (a1[f] * dxi + a2[f] * dyi + a3[f] * dzi);
+    else evo[f] = dt2 * (a1[f] * dxi + a2[f] * dyi);
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    face[0][0][f] = face_minus(wv[f], sx[f], evo[f]);
+    face[0][1][f] = face_plus(wv[f], sx[f], evo[f]);
+    face[1][0][f] = face_minus(wv[f], sy[f], evo[f]);
+    face[1][1][f] = face_plus(wv[f], sy[f], evo[f]);
+    if (DIM == 3) {
+      face[2][0][f] = face_minus(wv[f], sz[f], evo[f]);
+      face[2][1][f] = face_plus(wv[f], sz[f], evo[f]);
+    }
+  }
+}
+
+// The tile program of one CTA.  tid in [0, TX*TY); (bx, by, bz) its tile.
+template <typename T, int NF, int DIM, int TX, int TY, int ZC>
+__device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, NF, TX, TY>& sm,
+                                           int tid, int bx, int by, int bz) {
+  constexpr int NT = TX * TY;
+  constexpr int RX = TX + 4, RY = TY + 4;
+  const HydroParams& P = A.P;
+  const int nx = P.nx, ny = P.ny, nz = DIM == 3 ? P.nz : 1;
+  const int X0 = bx * TX, Y0 = by * TY, Z0 = DIM == 3 ? bz * ZC : 0;
+  const int xe = nx - X0 < TX ? nx - X0 : TX;
+  const int ye = ny - Y0 < TY ? ny - Y0 : TY;
+  const int ze = DIM == 3 ? (nz - Z0 < ZC ? nz - Z0 : ZC) : 1;
+  const int oi = tid % TX, oj = tid / TX;
+  const bool owned = oi < xe && oj < ye;
+  const int64_t n = A.n;
+  const Gas<T> c = Gas<T>::make(P);
+  const bool de = P.dualenergy != 0;
+  unsigned err = 0;
+
+  if (ctl_skip(A.ctl)) {
+    // Inactive step: pass the state through to the other buffer.
+    if (owned)
+      for (int z = Z0; z < Z0 + ze; ++z) {
+        const int64_t idx = ((int64_t)z * ny + (Y0 + oj)) * nx + (X0 + oi);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) A.qout[f * n + idx] = A.qin[f * n + idx];
+      }
+    return;
+  }
+
+  const double dtd = A.ctl->dt;
+  const T dt2 = (T)(-0.5 * dtd);
+  const T dtdx = (T)(dtd * P.dxinv), dtdy = (T)(dtd * P.dyinv), dtdz = (T)(dtd * P.dzinv);
+
+  // A: primitives of plane z (global index, may be a ghost plane) into slot.
+  auto load_plane = [&](int z, int slot) {
+    for (int it = tid; it < RX * RY; it += NT) {
+      const int lx = it % RX, ly = it / RX;
+      int gx = X0 - 2 + lx, gy = Y0 - 2 + ly;
+      // cells past the first two ghosts of a partial tile feed no owned
+      // cell; clamp them onto valid cells so they hold physical data
+      gx = gx > nx + 1 ? nx + 1 : gx;
+      gy = gy > ny + 1 ? ny + 1 : gy;
+      bool flip = false;
+      const int mx = ghost_map(gx, nx, P.boundtype, 0, flip);
+      const int my = ghost_map(gy, ny, P.boundtype, 1, flip);
+      const int mz = DIM == 3 ? ghost_map(z, nz, P.boundtype, 2, flip) : 0;
+      const int64_t idx = ((int64_t)mz * ny + my) * nx + mx;
+      T qv[6], wv[5];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
+      prim(qv, wv, c, P, de, err);
+      if (flip) {
+        wv[1] = -wv[1];
+        wv[2] = -wv[2];
+        wv[3] = -wv[3];
+      }
+#pragma unroll
+      for (int f = 0; f < 5; ++f) sm.w[slot][f][ly][lx] = wv[f];
+    }
+  };
+
+  // Per-column state carried across planes (registers of the owner).
+  T qacc[NF];       // plane c-1 after its x and y terms
+  T wzp_prev[5];    // upper z face state of plane c-1
+  T fz_prev[NF];    // z flux through c-3/2
+#pragma unroll
+  for (int f = 0; f < NF; ++f) { qacc[f] = (T)0; fz_prev[f] = (T)0; }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) wzp_prev[f] = (T)0;
+
+  const int zfirst = DIM == 3 ? Z0 - 1 : 0;
+  const int zlast = DIM == 3 ? Z0 + ze : 0;
+  auto slot_of = [&](int z) { return (z - (Z0 - 2)) % 3; };
+  if (DIM == 3) {
+    load_plane(Z0 - 2, slot_of(Z0 - 2));
+    load_plane(Z0 - 1, slot_of(Z0 - 1));
+  }
+
+  for (int cz = zfirst; cz <= zlast; ++cz) {
+    const bool inner = cz >= Z0 && cz < Z0 + ze;  // plane cz is updated by this tile
+    // ---- A
+    if (DIM == 3) load_plane(cz + 1, slot_of(cz + 1));
+    else load_plane(0, 1);
+    EV_SYNC();
+    const int sp = DIM == 3 ? slot_of(cz - 1) : 0;
+    const int sc = DIM == 3 ? slot_of(cz) : 1;
+    const int sn = DIM == 3 ? slot_of(cz + 1) : 2;
+    // ---- B
+    T wzm_cur[5], wzp_cur[5];
+    if (owned) {
+      T wv[5], face[3][2][5];
+      cell_faces<T, DIM, TX, TY>(sm, sp, sc, sn, oi + 2, oj + 2, P, dt2, wv, face);
+      if (inner) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+          sm.xf[0][f][oj][oi + 1] = face[0][0][f];
+          sm.xf[1][f][oj][oi + 1] = face[0][1][f];
+          sm.yf[0][f][oj + 1][oi] = face[1][0][f];
+          sm.yf[1][f][oj + 1][oi] = face[1][1][f];
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        wzm_cur[f] = face[2][0][f];
+        wzp_cur[f] = face[2][1][f];
+      }
+    }
+    if (inner) {
+      // ring cells: x ring at x = -1 and x = xe (rows 0..ye-1),
+      // y ring at y = -1 and y = ye (columns 0..xe-1)
+      const int nring = 2 * ye + 2 * xe;
+      for (int r = tid; r < nring; r += NT) {
+        int li, lj;
+        bool xring;
+        if (r < 2 * ye) {
+          xring = true;
+          lj = r >> 1;
+          li = (r & 1) ? xe : -1;
+        } else {
+          xring = false;
+          const int rr = r - 2 * ye;
+          li = rr >> 1;
+          lj = (rr & 1) ? ye : -1;
+        }
+        T wv[5], face[3][2][5];
+        cell_faces<T, DIM, TX, TY>(sm, sp, sc, sn, li + 2, lj + 2, P, dt2, wv, face);
+        if (xring) {
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            sm.xf[0][f][lj][li + 1] = face[0][0][f];
+            sm.xf[1][f][lj][li + 1] = face[0][1][f];
+          }
+        } else {
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            sm.yf[0][f][lj + 1][li] = face[1][0][f];
+            sm.yf[1][f][lj + 1][li] = face[1][1][f];
+          }
+        }
+      }
+    }
+    EV_SYNC();
+    // ---- C
+    if (inner) {
+      const int nxi = (xe + 1) * ye, nyi = xe * (ye + 1);
+      for (int it = tid; it < nxi + nyi; it += NT) {
+        T wl[5], wr[5], fv[NF];
+        if (it < nxi) {
+          const int i = it % (xe + 1), j = it / (xe + 1);
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            wl[f] = sm.xf[1][f][j][i];
+            wr[f] = sm.xf[0][f][j][i + 1];
+          }
+          riemann<T, NF>(wl, wr, fv, 1, P.solver, c, err);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) sm.fx[f][j][i] = fv[f];
+        } else {
+          const int r = it - nxi;
+          const int i = r % xe, j = r / xe;
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            wl[f] = sm.yf[1][f][j][i];
+            wr[f] = sm.yf[0][f][j + 1][i];
+          }
+          riemann<T, NF>(wl, wr, fv, 2, P.solver, c, err);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) sm.fy[f][j][i] = fv[f];
+        }
+      }
+    }
+    T fz[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) fz[f] = (T)0;
+    if (DIM == 3 && owned && cz > zfirst) riemann<T, NF>(wzp_prev, wzm_cur, fz, 3, P.solver, c, err);
+    EV_SYNC();
+    // ---- D
+    if (owned) {
+      if (DIM == 3 && cz - 1 >= Z0 && cz - 1 < Z0 + ze) {
+        // plane cz-1 gets its z term and is written out
+        const int64_t idx = ((int64_t)(cz - 1) * ny + (Y0 + oj)) * nx + (X0 + oi);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) A.qout[f * n + idx] = qacc[f] + dtdz * (fz_prev[f] - fz[f]);
+      }
+      if (inner) {
+        const int64_t idx = ((int64_t)cz * ny + (Y0 + oj)) * nx + (X0 + oi);
+        T qv[6], wdummy[5];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
+        if (de) {
+          unsigned e2 = 0;
+          prim(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdx * (sm.fx[f][oj][oi] - sm.fx[f][oj][oi + 1]);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdy * (sm.fy[f][oj][oi] - sm.fy[f][oj + 1][oi]);
+        if (DIM == 3) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) qacc[f] = qv[f];
+        } else {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) A.qout[f * n + idx] = qv[f];
+        }
+      }
+      if (DIM == 3) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) fz_prev[f] = fz[f];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) wzp_prev[f] = wzp_cur[f];
+      }
+    }
+  }
+  if (err) {
+#if defined(EVORA_HOST_EMU)
+    reinterpret_cast<std::atomic<unsigned>*>(&A.ctl->err)->fetch_or(err);
+#else
+    atomicOr(&A.ctl->err, err);
+#endif
+  }
+}
+
+// 1D grids: one thread per cell.  The cell rebuilds the primitives of its
+// radius-2 neighbourhood, the face states of cells i-1, i, i+1 with the 1D
+// predictor (muscl.f90:60-69) and solves its two interfaces.
+template <typename T, int NF>
+__device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
+  const HydroParams& P = A.P;
+  const int nx = P.nx;
+  const int64_t n = A.n;
+  if (ctl_skip(A.ctl)) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) A.qout[f * n + i] = A.qin[f * n + i];
+    return;
+  }
+  const Gas<T> c = Gas<T>::make(P);
+  const bool de = P.dualenergy != 0;
+  unsigned err = 0;
+  const double dtd = A.ctl->dt;
+  const T dt2 = (T)(-0.5 * dtd);
+  const T dtdx = (T)(dtd * P.dxinv);
+  const T dxi = (T)P.dxinv;
+  T w[5][5];
+#pragma unroll
+  for (int o = 0; o < 5; ++o) {
+    bool flip = false;
+    const int m = ghost_map(i - 2 + o, nx, P.boundtype, 0, flip);
+    T qv[6];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + m);
+    prim(qv, w[o], c, P, de, err);
+    if (flip) {
+      w[o][1] = -w[o][1];
+      w[o][2] = -w[o][2];
+      w[o][3] = -w[o][3];
+    }
+  }
+  T fm[3][5], fp[3][5];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (P.secondorder) {
+      T s[5], a[5];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) s[f] = slope1(w[k][f], w[k + 1][f], w[k + 2][f], P.limiter);
+      predictor_term(w[k + 1], s, 1, (T)P.g, a);
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        const T e = dt2 * a[f] * dxi;
+        fm[k][f] = face_minus(w[k + 1][f], s[f], e);
+        fp[k][f] = face_plus(w[k + 1][f], s[f], e);
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < 5; ++f) fm[k][f] = fp[k][f] = w[k + 1][f];
+    }
+  }
+  T flo[NF], fhi[NF];
+  riemann<T, NF>(fp[0], fm[1], flo, 1, P.solver, c, err);
+  riemann<T, NF>(fp[1], fm[2], fhi, 1, P.solver, c, err);
+  T qv[6], wd[5];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + i);
+  if (de) {
+    unsigned e2 = 0;
+    prim(qv, wd, c, P, de, e2);
+  }
+#pragma unroll
+  for (int f = 0; f < NF; ++f) A.qout[f * n + i] = qv[f] + dtdx * (flo[f] - fhi[f]);
+  if (err) {
+#if defined(EVORA_HOST_EMU)
+    reinterpret_cast<std::atomic<unsigned>*>(&A.ctl->err)->fetch_or(err);
+#else
+    atomicOr(&A.ctl->err, err);
+#endif
+  }
+}
+
+#if !defined(EVORA_HOST_EMU)
+template <typename T, int NF>
+__global__ void __launch_bounds__(128) k_fused1d(FusedArgs<T> A) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.P.nx; i += gridDim.x * blockDim.x)
+    fused_cell1d<T, NF>(A, i);
+}
+
+template <typename T, int NF, int DIM, int TX, int TY, int ZC>
+__global__ void __launch_bounds__(TX* TY) k_fused(FusedArgs<T> A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<FusedSmem<T, NF, TX, TY>*>(smem_raw);
+  fused_tile<T, NF, DIM, TX, TY, ZC>(A, sm, threadIdx.x, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+#endif
+
+}  // namespace EVORA_FNS
+}  // namespace evora

@@ -1,0 +1,369 @@
+// grid.cu -- the resident layer: a grid whose state stays in HBM across
+// steps.  One step is the hydro subset of the reference loop
+// (main.f90:109-155): primitive, bound, hydrostep, updatetime, compevo,
+// sweep.  The time scalars live in a device control block (GridCtl) so that a
+// step needs no host round trip and can be replayed from a CUDA graph.
+//
+// Two backends:
+//  * fused (default): the conserved state in structure-of-arrays form, one
+//    fused kernel per step (fused3d.cu) plus a CFL kernel; FP64 or FP32.
+//  * reference kernels (EVORA_REFERENCE_KERNELS): the drop-in layer kernels on
+//    device-resident arrays in the reference layouts; FP64 only.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/evora_gpu.h"
+#include "common.h"
+#include "dropin_api.h"
+#include "fused.h"
+
+using namespace evora;
+
+struct evora_grid {
+  evora_params params{};
+  evora_derived d{};
+  HydroParams P{};
+  int precision = EVORA_FP64;
+  int flags = 0;
+  int device = 0;
+  int nf = 5;  // advected fields (5, or 6 with the entropy)
+  cudaStream_t stream = nullptr;
+  GridCtl* ctl = nullptr;  // device
+  // reference-kernel backend
+  double* q_aos = nullptr;
+  double* w = nullptr;
+  double* evo = nullptr;
+  double* s = nullptr;
+  // fused backend: two SoA copies of the conserved state (ping-pong)
+  void* qbuf[2] = {nullptr, nullptr};
+  int cur = 0;
+  FusedPlan plan{};
+  double* aos_stage = nullptr;  // device staging for q in reference layout
+  // kernel timing
+  bool timing = false;
+  std::vector<cudaEvent_t> events;  // 4 per timed step
+  size_t ev_used = 0;
+  int64_t launches = 0;
+};
+
+namespace {
+
+#define CU(call)                 \
+  do {                           \
+    cudaError_t e_ = (call);     \
+    if (e_ != cudaSuccess) {     \
+      set_cuda_error(e_, #call); \
+      return EVORA_ERR_CUDA;     \
+    }                            \
+  } while (0)
+
+bool reference_backend(const evora_grid* g) { return (g->flags & EVORA_REFERENCE_KERNELS) != 0; }
+
+int64_t ncells(const evora_grid* g) { return (int64_t)g->P.nx * g->P.ny * g->P.nz; }
+
+size_t elem_size(const evora_grid* g) { return g->precision == EVORA_FP32 ? 4 : 8; }
+
+__global__ void k_step_begin(GridCtl* ctl) {
+  ctl->active = (ctl->go != 0 && ctl->err == 0) ? 1 : 0;
+  ctl->smax[0] = ctl->smax[1] = ctl->smax[2] = 0ull;
+}
+
+// hydrostep part 2 + updatetime (timestep.f90:26-57, 147-171).
+__global__ void k_step_time(HydroParams P, GridCtl* ctl) {
+  if (!ctl->active || ctl->err) {
+    ctl->active = 0;
+    return;
+  }
+  double sm[3];
+  for (int i = 0; i < 3; ++i) sm[i] = __longlong_as_double((long long)ctl->smax[i]);
+  unsigned e = 0;
+  double dt = cfl_dt(P, sm[0], sm[1], sm[2], 1e99, e);
+  if (e) {
+    ctl->err |= e;
+    ctl->active = 0;
+    return;
+  }
+  double t = ctl->t;
+  int go = ctl->go;
+  update_time(ctl->tend, t, dt, go);
+  ctl->t = t;
+  ctl->dt = dt;
+  ctl->go = go;
+}
+
+__global__ void k_step_end(GridCtl* ctl) {
+  if (ctl->active && ctl->err == 0) ctl->k += 1;
+}
+
+cudaEvent_t next_event(evora_grid* g) {
+  if (g->ev_used == g->events.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    g->events.push_back(e);
+  }
+  return g->events[g->ev_used++];
+}
+
+void mark(evora_grid* g) {
+  if (!g->timing) return;
+  cudaEvent_t e = next_event(g);
+  if (e) cudaEventRecord(e, g->stream);
+}
+
+int enqueue_reference_step(evora_grid* g) {
+  const DropinOps& o = (g->flags & EVORA_STRICT) ? evora::strict::kOps : evora::fast::kOps;
+  cudaStream_t st = g->stream;
+  const int nb = (g->P.nx != 1) + (g->P.ny != 1) + (g->P.nz != 1);
+  g->launches += 7 + nb;
+  k_step_begin<<<1, 1, 0, st>>>(g->ctl);
+  mark(g);
+  o.primitive(g->P, g->w, g->q_aos, &g->ctl->err, g->ctl, st);
+  o.bound(g->P, g->w, g->ctl, st);
+  o.cfl(g->P, g->w, g->ctl->smax, g->ctl, st);
+  mark(g);
+  k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
+  mark(g);
+  if (g->P.secondorder) o.compevo(g->P, g->w, g->evo, g->s, 0.0, g->ctl, st);
+  o.sweep(g->P, g->w, g->q_aos, g->evo, g->s, 0.0, &g->ctl->err, g->ctl, st);
+  mark(g);
+  k_step_end<<<1, 1, 0, st>>>(g->ctl);
+  CU(cudaGetLastError());
+  return 0;
+}
+
+int enqueue_fused_step(evora_grid* g) {
+  cudaStream_t st = g->stream;
+  g->launches += 5;
+  k_step_begin<<<1, 1, 0, st>>>(g->ctl);
+  mark(g);
+  fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
+  mark(g);
+  k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
+  mark(g);
+  fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
+  mark(g);
+  k_step_end<<<1, 1, 0, st>>>(g->ctl);
+  CU(cudaGetLastError());
+  // The swap is unconditional on the host; an inactive step copies q through
+  // unchanged (fused_update does that when the step is inactive).
+  g->cur ^= 1;
+  return 0;
+}
+
+void free_grid(evora_grid* g) {
+  if (!g) return;
+  for (cudaEvent_t e : g->events) cudaEventDestroy(e);
+  fused_plan_free(&g->plan);
+  cudaFree(g->ctl);
+  cudaFree(g->q_aos);
+  cudaFree(g->w);
+  cudaFree(g->evo);
+  cudaFree(g->s);
+  cudaFree(g->qbuf[0]);
+  cudaFree(g->qbuf[1]);
+  cudaFree(g->aos_stage);
+  delete g;
+}
+
+}  // namespace
+
+extern "C" {
+
+int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags, evora_grid** out) {
+  if (!p || !out) return EVORA_ERR_ARG;
+  *out = nullptr;
+  if (precision != EVORA_FP64 && precision != EVORA_FP32) return EVORA_ERR_ARG;
+  evora_grid* g = new (std::nothrow) evora_grid();
+  if (!g) return EVORA_ERR_NOMEM;
+  int rc = 0;
+  if (!params_to_hydro(p, &g->P, &g->d, &rc)) {
+    delete g;
+    return rc;
+  }
+  g->params = *p;
+  g->precision = precision;
+  g->flags = flags;
+  g->nf = (flags & EVORA_CARRY_ENTROPY) || p->dualenergy ? 6 : 5;
+  if (reference_backend(g) && precision != EVORA_FP64) {
+    delete g;
+    return EVORA_ERR_ARG;
+  }
+  if (!reference_backend(g) && p->dualenergy && precision == EVORA_FP32) {
+    delete g;
+    return EVORA_ERR_ARG;  // the dual-energy switch is evaluated in FP64 only
+  }
+  cudaGetDevice(&g->device);
+  if (cudaMalloc(&g->ctl, sizeof(GridCtl)) != cudaSuccess) goto nomem;
+  if (reference_backend(g)) {
+    int64_t nq, nw, ne, ns;
+    evora_array_sizes(p, &nq, &nw, &ne, &ns);
+    if (cudaMalloc(&g->q_aos, nq * 8) != cudaSuccess) goto nomem;
+    if (cudaMalloc(&g->w, nw * 8) != cudaSuccess) goto nomem;
+    if (cudaMalloc(&g->evo, ne * 8) != cudaSuccess) goto nomem;
+    if (cudaMalloc(&g->s, ns * 8) != cudaSuccess) goto nomem;
+    if (cudaMemset(g->w, 0, nw * 8) != cudaSuccess) goto nomem;
+    if (cudaMemset(g->evo, 0, ne * 8) != cudaSuccess) goto nomem;  // main.f90:76-77
+    if (cudaMemset(g->s, 0, ns * 8) != cudaSuccess) goto nomem;
+  } else {
+    size_t bytes = (size_t)g->nf * ncells(g) * elem_size(g);
+    if (cudaMalloc(&g->qbuf[0], bytes) != cudaSuccess) goto nomem;
+    if (cudaMalloc(&g->qbuf[1], bytes) != cudaSuccess) goto nomem;
+    rc = fused_plan(g->P, g->precision, g->nf, (flags & EVORA_STRICT) != 0, &g->plan);
+    if (rc) {
+      free_grid(g);
+      return rc;
+    }
+  }
+  {
+    GridCtl c{};
+    c.t = p->tstart;
+    c.tend = p->tend;
+    c.go = 1;
+    if (cudaMemcpy(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess) goto nomem;
+  }
+  *out = g;
+  return 0;
+nomem:
+  cudaGetLastError();
+  free_grid(g);
+  return EVORA_ERR_NOMEM;
+}
+
+int evora_grid_destroy(evora_grid* g) {
+  if (!g) return EVORA_ERR_ARG;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  else cudaDeviceSynchronize();
+  free_grid(g);
+  return 0;
+}
+
+int evora_grid_set_stream(evora_grid* g, void* stream) {
+  if (!g) return EVORA_ERR_ARG;
+  g->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int evora_grid_set_q(evora_grid* g, const double* q) {
+  if (!g || !q) return EVORA_ERR_ARG;
+  int64_t nq;
+  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
+  const bool dev = is_device_pointer(q);
+  if (reference_backend(g)) {
+    CU(cudaMemcpyAsync(g->q_aos, q, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       g->stream));
+  } else {
+    const double* src = q;
+    if (!dev) {
+      if (!g->aos_stage) CU(cudaMalloc(&g->aos_stage, nq * 8));
+      CU(cudaMemcpyAsync(g->aos_stage, q, nq * 8, cudaMemcpyHostToDevice, g->stream));
+      src = g->aos_stage;
+    }
+    g->cur = 0;
+    fused_from_aos(g->plan, src, g->qbuf[0], g->stream);
+  }
+  GridCtl c{};
+  c.t = g->params.tstart;
+  c.tend = g->params.tend;
+  c.go = 1;
+  CU(cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  return 0;
+}
+
+int evora_grid_get_q(evora_grid* g, double* q) {
+  if (!g || !q) return EVORA_ERR_ARG;
+  int64_t nq;
+  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
+  const bool dev = is_device_pointer(q);
+  if (reference_backend(g)) {
+    CU(cudaMemcpyAsync(q, g->q_aos, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       g->stream));
+  } else {
+    double* dst = q;
+    if (!dev) {
+      if (!g->aos_stage) CU(cudaMalloc(&g->aos_stage, nq * 8));
+      dst = g->aos_stage;
+    }
+    fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream);
+    if (!dev) CU(cudaMemcpyAsync(q, dst, nq * 8, cudaMemcpyDeviceToHost, g->stream));
+  }
+  CU(cudaStreamSynchronize(g->stream));
+  return 0;
+}
+
+int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync) {
+  if (!g || nsteps < 0) return EVORA_ERR_ARG;
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
+    if (rc) return rc;
+  }
+  if (sync) return evora_grid_status(g);
+  return 0;
+}
+
+int evora_grid_time(evora_grid* g, double* t, double* dt, int32_t* go, int64_t* k) {
+  if (!g) return EVORA_ERR_ARG;
+  GridCtl c;
+  CU(cudaMemcpyAsync(&c, g->ctl, sizeof c, cudaMemcpyDeviceToHost, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  if (t) *t = c.t;
+  if (dt) *dt = c.dt;
+  if (go) *go = c.go;
+  if (k) *k = c.k;
+  return 0;
+}
+
+int evora_grid_status(evora_grid* g) {
+  if (!g) return EVORA_ERR_ARG;
+  GridCtl c;
+  cudaError_t e = cudaMemcpyAsync(&c, g->ctl, sizeof c, cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "evora_grid_status");
+    return EVORA_ERR_CUDA;
+  }
+  return (int)c.err;
+}
+
+int evora_grid_set_timing(evora_grid* g, int32_t on) {
+  if (!g) return EVORA_ERR_ARG;
+  g->timing = on != 0;
+  g->ev_used = 0;
+  g->launches = 0;
+  return 0;
+}
+
+int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps, int64_t* launches) {
+  if (!g) return EVORA_ERR_ARG;
+  CU(cudaStreamSynchronize(g->stream));
+  double up = 0.0, cf = 0.0;
+  const size_t nstep = g->ev_used / 4;
+  for (size_t i = 0; i < nstep; ++i) {
+    float a = 0.f, b = 0.f;
+    CU(cudaEventElapsedTime(&a, g->events[4 * i + 0], g->events[4 * i + 1]));
+    CU(cudaEventElapsedTime(&b, g->events[4 * i + 2], g->events[4 * i + 3]));
+    cf += a;
+    up += b;
+  }
+  if (update_ms) *update_ms = up;
+  if (cfl_ms) *cfl_ms = cf;
+  if (steps) *steps = (int64_t)nstep;
+  if (launches) *launches = g->launches;
+  g->ev_used = 0;
+  g->launches = 0;
+  return 0;
+}
+
+int evora_grid_totals(evora_grid* g, double out[6]) {
+  if (!g || !out) return EVORA_ERR_ARG;
+  if (reference_backend(g)) {
+    return fused_totals_aos(g->q_aos, ncells(g), out, g->stream);
+  }
+  return fused_totals(g->plan, g->qbuf[g->cur], out, g->stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,307 @@
+// hydro_math.cuh -- device arithmetic of the evora hydro update.
+//
+// Every function states the reference routine it follows.  The association
+// of each floating-point expression is the Fortran one (left to right,
+// a*b*c = (a*b)*c, x**2 = x*x), so a build without FMA contraction
+// (--fmad=false) reproduces a gfortran -O3 x86-64 build of the reference
+// bit for bit wherever libm pow is not involved (pow only feeds the entropy
+// field S).  Fortran MIN/MAX are "take the next argument if it is
+// smaller/larger", written as selects rather than fmin/fmax so that ties of
+// signed zeros resolve the same way.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#if !defined(__CUDACC__)
+// Host compilation of the device arithmetic (used by the CPU emulation of the
+// fused kernel in the test suite): the CUDA qualifiers vanish.
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#define __global__
+#endif
+
+#include "../../include/evora_gpu.h"
+
+namespace evora {
+
+// Step control block of a resident grid, in device memory.  Kernels of a
+// step read dt from here and return at once when the step is inactive
+// (go was already false, or an error was raised earlier).
+struct GridCtl {
+  double t, dt, tend;
+  int go;        // updatetime's go flag
+  int active;    // the current step runs
+  long long k;   // steps completed
+  unsigned err;  // accumulated EVORA_ERR_* mask
+  unsigned pad;
+  unsigned long long smax[3];  // CFL maxima of |u_d| + a (ordered bits)
+};
+
+__device__ __forceinline__ bool ctl_skip(const GridCtl* ctl) {
+  return ctl != nullptr && (!ctl->active || ctl->err != 0);
+}
+
+// Parameters every kernel reads (module global after compparameter).
+struct HydroParams {
+  int nx, ny, nz;
+  int solver, limiter, boundtype, secondorder, dualenergy;
+  int onedimension, twodimension;
+  double g, g1, g1inv, gg1, cfl, de_thresh1;
+  double dx, dy, dz, dxinv, dyinv, dzinv;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ T fmin2(T a, T b) { return (b < a) ? b : a; }
+template <typename T>
+__host__ __device__ __forceinline__ T fmax2(T a, T b) { return (b > a) ? b : a; }
+
+__device__ __forceinline__ double dpow(double a, double b) { return std::pow(a, b); }
+__device__ __forceinline__ float dpow(float a, float b) { return std::pow(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return std::sqrt(a); }
+__device__ __forceinline__ float dsqrt(float a) { return std::sqrt(a); }
+
+// Gas constants in the working precision.
+template <typename T>
+struct Gas {
+  T g, g1, g1inv, gg1, de_thresh1;
+  __host__ __device__ static Gas make(const HydroParams& P) {
+    Gas c;
+    c.g = (T)P.g; c.g1 = (T)P.g1; c.g1inv = (T)P.g1inv; c.gg1 = (T)P.gg1;
+    c.de_thresh1 = (T)P.de_thresh1;
+    return c;
+  }
+};
+
+// pressure(q,press), comp.f90:45-85.  With dualenergy, writes q[4] (S system)
+// or q[5] (E system) back.  Raises EVORA_ERR_PRESSURE for p <= 0.
+template <typename T>
+__device__ __forceinline__ T pressure(T* q, const Gas<T>& c, bool dualenergy, unsigned& err) {
+  T m2 = (q[1] * q[1]) + (q[2] * q[2]) + (q[3] * q[3]);
+  T kin = (T)0.5 * m2 / q[0];
+  T press;
+  if (dualenergy) {
+    T ratio = kin / q[4];
+    if (ratio > c.de_thresh1) {
+      press = q[5] * dpow(q[0], c.g1);
+      q[4] = kin + press * c.g1inv;
+    } else {
+      press = c.g1 * (q[4] - kin);
+      q[5] = press / dpow(q[0], c.g1);
+    }
+  } else {
+    press = c.g1 * (q[4] - kin);
+  }
+  if (press <= (T)0) err |= EVORA_ERR_PRESSURE;
+  return press;
+}
+
+// q2w(q,w), comp.f90:26-43.
+template <typename T>
+__device__ __forceinline__ void q2w(T* q, T* w, const Gas<T>& c, bool dualenergy, unsigned& err) {
+  T densinv = (T)1.0 / q[0];
+  w[0] = q[0];
+  w[1] = q[1] * densinv;
+  w[2] = q[2] * densinv;
+  w[3] = q[3] * densinv;
+  w[4] = pressure(q, c, dualenergy, err);
+}
+
+// comp_slope for one field, muscl.f90:115-169.
+template <typename T>
+__device__ __forceinline__ T slope1(T wl, T w, T wr, int limiter) {
+  T dwl = w - wl;
+  T dwr = wr - w;
+  if (limiter == 1) {                       // minmod, 128-140
+    bool lp = dwl >= (T)0, rp = dwr >= (T)0;
+    if (lp != rp) return (T)0;
+    return rp ? fmin2(dwl, dwr) : fmax2(dwl, dwr);
+  } else if (limiter == 2) {                // monotonised central, 141-154
+    T dwc = (wr - wl) * (T)0.5;
+    bool lp = dwl >= (T)0, rp = dwr >= (T)0;
+    if (lp != rp) return (T)0;
+    if (rp) return fmin2(fmin2((T)2.0 * dwl, dwc), (T)2.0 * dwr);
+    return fmax2(fmax2((T)2.0 * dwl, dwc), (T)2.0 * dwr);
+  } else {                                  // van Leer, 155-163
+    T pro = dwl * dwr;
+    if (pro <= (T)0) return (T)0;
+    return (T)2.0 * pro / (dwr + dwl);
+  }
+}
+
+// The per-direction predictor term a(:,d) of compevo (muscl.f90:100-104 and
+// the 1D/2D copies 64-66, 78-84): a = u_d * s; a(5) += g p s(u_d);
+// a(u_d) += s(p) / rho.  d = 1..3.
+template <typename T>
+__device__ __forceinline__ void predictor_term(const T* w, const T* s, int d, T g, T* a) {
+#pragma unroll
+  for (int f = 0; f < 5; ++f) a[f] = w[d] * s[f];
+  a[4] = a[4] + g * w[4] * s[d];
+  a[d] = a[d] + s[4] / w[0];
+}
+
+// flux(w,f,dir), riemann.f90:157-205.  nf = 5 or 6 (the entropy flux).
+template <typename T, int NF>
+__device__ __forceinline__ void flux(const T* w, T* f, int dir, const Gas<T>& c) {
+  T u2 = w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
+  const T ud = w[dir];
+  f[0] = w[0] * ud;
+  if (dir == 1) {
+    f[1] = w[0] * (w[1] * w[1]) + w[4];
+    f[2] = w[0] * w[1] * w[2];
+    f[3] = w[0] * w[1] * w[3];
+  } else if (dir == 2) {
+    f[1] = w[0] * w[2] * w[1];
+    f[2] = w[0] * (w[2] * w[2]) + w[4];
+    f[3] = w[0] * w[2] * w[3];
+  } else {
+    f[1] = w[0] * w[3] * w[1];
+    f[2] = w[0] * w[3] * w[2];
+    f[3] = w[0] * (w[3] * w[3]) + w[4];
+  }
+  f[4] = ud * ((T)0.5 * w[0] * u2 + c.gg1 * w[4]);
+  if (NF == 6) f[NF - 1] = ud * w[4] / dpow(w[0], c.g1);
+}
+
+// state(w,q), riemann.f90:207-239.
+template <typename T, int NF>
+__device__ __forceinline__ void state(const T* w, T* q, const Gas<T>& c) {
+  q[0] = w[0];
+  q[1] = w[0] * w[1];
+  q[2] = w[0] * w[2];
+  q[3] = w[0] * w[3];
+  T u2 = (w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3]);
+  q[4] = (T)0.5 * w[0] * u2 + w[4] / c.g1;
+  if (NF == 6) q[NF - 1] = w[4] / dpow(w[0], c.g1);
+}
+
+// statex(w,qx,s,sm,dir), riemann.f90:241-288.
+template <typename T, int NF>
+__device__ __forceinline__ void statex(const T* w, T* qx, T s, T sm, int dir, const Gas<T>& c) {
+  const T wd = w[dir];
+  qx[0] = w[0] * (s - wd) / (s - sm);
+  qx[1] = (dir == 1 ? sm : w[1]) * qx[0];
+  qx[2] = (dir == 2 ? sm : w[2]) * qx[0];
+  qx[3] = (dir == 3 ? sm : w[3]) * qx[0];
+  T energy = (T)0.5 * w[0] * ((w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3])) + w[4] / c.g1;
+  qx[4] = qx[0] * (energy / w[0] + (sm - wd) * (sm + (w[4] / (w[0] * (s - wd)))));
+  if (NF == 6) qx[NF - 1] = qx[0] * w[4] / dpow(w[0], c.g);
+}
+
+// hll(wl,wr,f,dir), riemann.f90:47-92.
+template <typename T, int NF>
+__device__ __forceinline__ void hll(const T* wl, const T* wr, T* f, int dir, const Gas<T>& c,
+                                    unsigned& err) {
+  if (wl[4] <= (T)0 || wr[4] <= (T)0) err |= EVORA_ERR_RIEMANN_PRESSURE;
+  T al = dsqrt(c.g * wl[4] / wl[0]);
+  T ar = dsqrt(c.g * wr[4] / wr[0]);
+  T sl = fmin2(wl[dir] - al, wr[dir] - ar);
+  T sr = fmax2(wl[dir] + al, wr[dir] + ar);
+  if ((T)0 < sl) {
+    flux<T, NF>(wl, f, dir, c);
+  } else if ((T)0 > sr) {
+    flux<T, NF>(wr, f, dir, c);
+  } else if (sl <= (T)0 && (T)0 <= sr) {
+    T fl[NF], fr[NF], ql[NF], qr[NF];
+    flux<T, NF>(wl, fl, dir, c);
+    flux<T, NF>(wr, fr, dir, c);
+    state<T, NF>(wl, ql, c);
+    state<T, NF>(wr, qr, c);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) f[i] = (sr * fl[i] - sl * fr[i] + sl * sr * (qr[i] - ql[i])) / (sr - sl);
+  } else {
+    err |= EVORA_ERR_HLL;
+#pragma unroll
+    for (int i = 0; i < NF; ++i) f[i] = (T)0;
+  }
+}
+
+// hllc(wl,wr,f,dir), riemann.f90:96-153.
+template <typename T, int NF>
+__device__ __forceinline__ void hllc(const T* wl, const T* wr, T* f, int dir, const Gas<T>& c,
+                                     unsigned& err) {
+  if (wl[4] <= (T)0 || wr[4] <= (T)0) err |= EVORA_ERR_RIEMANN_PRESSURE;
+  T al = dsqrt(c.g * wl[4] / wl[0]);
+  T ar = dsqrt(c.g * wr[4] / wr[0]);
+  T sl = fmin2(wl[dir] - al, wr[dir] - ar);
+  T sr = fmax2(wl[dir] + al, wr[dir] + ar);
+  T facl = wl[0] * (sl - wl[dir]);
+  T facr = wr[0] * (sr - wr[dir]);
+  T sm = (wr[4] - wl[4] + facl * wl[dir] - facr * wr[dir]) / (facl - facr);
+  if ((T)0 < sl) {
+    flux<T, NF>(wl, f, dir, c);
+  } else if ((T)0 > sr) {
+    flux<T, NF>(wr, f, dir, c);
+  } else {
+    // The two star branches share one evaluation: side K with wave speed sk.
+    const bool left = (sl < (T)0 && (T)0 < sm);
+    const bool right = (sm <= (T)0 && (T)0 < sr);
+    if (!(left || right)) {
+      err |= EVORA_ERR_HLLC;
+#pragma unroll
+      for (int i = 0; i < NF; ++i) f[i] = (T)0;
+      return;
+    }
+    const T* wk = left ? wl : wr;
+    const T sk = left ? sl : sr;
+    T fk[NF], qk[NF], qx[NF];
+    flux<T, NF>(wk, fk, dir, c);
+    state<T, NF>(wk, qk, c);
+    statex<T, NF>(wk, qx, sk, sm, dir, c);
+#pragma unroll
+    for (int i = 0; i < NF; ++i) f[i] = fk[i] + sk * (qx[i] - qk[i]);
+  }
+}
+
+// riemannsolver(wl,wr,f,dir), riemann.f90:26-43.
+template <typename T, int NF>
+__device__ __forceinline__ void riemann(const T* wl, const T* wr, T* f, int dir, int solver,
+                                        const Gas<T>& c, unsigned& err) {
+  if (solver == 1) hll<T, NF>(wl, wr, f, dir, c, err);
+  else hllc<T, NF>(wl, wr, f, dir, c, err);
+}
+
+// Interface states of sweep (muscl.f90:199-200, 208-209): the state a cell
+// shows on its upper face, w + 0.5 s + evo, and on its lower face,
+// w - 0.5 s + evo.
+template <typename T>
+__device__ __forceinline__ T face_plus(T w, T s, T e) { return w + (T)0.5 * s + e; }
+template <typename T>
+__device__ __forceinline__ T face_minus(T w, T s, T e) { return w - (T)0.5 * s + e; }
+
+#if defined(__CUDACC__)
+// Positive doubles order like their bit patterns as unsigned integers; the
+// CFL reduction keeps maxima of signal speeds that way (atomicMax on u64).
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+#endif
+
+}  // namespace evora
+
+namespace evora {
+
+// hydrostep, timestep.f90:26-57, part 2: from the per-axis maxima of
+// |u_d| + a, v = min(1e6, dx/Sx, dy/Sy, dz/Sz) (equal to the reference's
+// running min over cells), dt = min(cfl * v, dt_in); EVORA_ERR_DT if <= 0.
+__host__ __device__ inline double cfl_dt(const HydroParams& P, double sx, double sy, double sz,
+                                         double dt_in, unsigned& err) {
+  double v = 1e6;
+  double vx = P.dx / sx, vy = P.dy / sy, vz = P.dz / sz;
+  v = fmin2(fmin2(fmin2(vx, vy), vz), v);
+  double dt = fmin2(P.cfl * v, dt_in);
+  if (dt <= 0.0) err |= EVORA_ERR_DT;
+  return dt;
+}
+
+// updatetime, timestep.f90:147-171, non-comoving branch.
+__host__ __device__ inline void update_time(double tend, double& t, double& dt, int& go) {
+  if (tend - t <= dt) {
+    dt = tend - t;
+    go = 0;
+  }
+  t = t + dt;
+}
+
+}  // namespace evora

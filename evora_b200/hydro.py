@@ -1,0 +1,219 @@
+"""Python front end of the evora hydro update on B200.
+
+Mirrors the reference's operator interface for the hydro path: the drop-in
+routines `primitive`, `bound`, `hydrostep`, `updatetime`, `compevo`, `sweep`
+(same names, arguments and array layouts as muscl.f90 / boundary.f90 /
+timestep.f90), and the resident `Grid` that advances whole steps on the
+device.  Arrays are numpy (host) or torch CUDA tensors (device), float64,
+C-contiguous, in the reference's column-major layouts read in C order:
+
+    q   (nz, ny, nx, 6)           q(6, nx, ny, nz)                  main.f90:72
+    w   (nz+4, ny+4, nx+4, 5)     w(5, -1:nx+2, -1:ny+2, -1:nz+2)   main.f90:73
+    evo (nz+2, ny+2, nx+2, 5)     evo(5, 0:nx+1, ...)               main.f90:74
+    s   (nz+2, ny+2, nx+2, 3, 5)  s(5, 3, 0:nx+1, ...)              main.f90:75
+
+Every call goes through libevora_b200.so; errors raise EvoraError with the
+reference condition that caused them.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._native import EvoraDerived, EvoraError, EvoraParams, check, lib
+
+FP64 = 0
+FP32 = 1
+CARRY_ENTROPY = 1
+STRICT = 2
+REFERENCE_KERNELS = 4
+
+
+# ------------------------------------------------------------- parameters --
+def default_params(**overrides) -> EvoraParams:
+    """readparameter defaults (parameter.f90:41-82), then keyword overrides."""
+    p = EvoraParams()
+    lib().evora_params_default(ctypes.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"unknown parameter {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def derived(p: EvoraParams) -> EvoraDerived:
+    """compparameter (parameter.f90:164-265)."""
+    d = EvoraDerived()
+    check(lib().evora_compparameter(ctypes.byref(p), ctypes.byref(d)), "compparameter")
+    return d
+
+
+def shapes(p: EvoraParams):
+    nx, ny, nz = p.nx, p.ny, p.nz
+    return dict(q=(nz, ny, nx, 6), w=(nz + 4, ny + 4, nx + 4, 5),
+                evo=(nz + 2, ny + 2, nx + 2, 5), s=(nz + 2, ny + 2, nx + 2, 3, 5))
+
+
+def _ptr(a, shape=None, writable=True):
+    """Address of a float64 C-contiguous numpy array or torch tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError("arrays must be float64 and C-contiguous")
+        if writable and not a.flags["WRITEABLE"]:
+            raise TypeError("array is read-only")
+        if shape is not None and a.shape != tuple(shape):
+            raise ValueError(f"shape {a.shape} != expected {tuple(shape)}")
+        return ctypes.c_void_p(a.ctypes.data)
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        raise TypeError("unsupported array type")
+    if isinstance(a, torch.Tensor):
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("tensors must be float64 and contiguous")
+        if shape is not None and tuple(a.shape) != tuple(shape):
+            raise ValueError(f"shape {tuple(a.shape)} != expected {tuple(shape)}")
+        return ctypes.c_void_p(a.data_ptr())
+    raise TypeError("unsupported array type")
+
+
+# ----------------------------------------------------------- drop-in layer --
+class DropIn:
+    """The drop-in routines for one set of module-global parameters."""
+
+    def __init__(self, params: EvoraParams, strict: bool = False):
+        self.params = params
+        self.shape = shapes(params)
+        check(lib().evora_set_params(ctypes.byref(params)), "set_params")
+        check(lib().evora_set_strict(1 if strict else 0), "set_strict")
+
+    def _activate(self):
+        check(lib().evora_set_params(ctypes.byref(self.params)), "set_params")
+
+    def primitive(self, w, q):
+        """primitive(w,q), muscl.f90:26-43."""
+        check(lib().evora_primitive(_ptr(w, self.shape["w"]), _ptr(q, self.shape["q"])), "primitive")
+
+    def bound(self, w):
+        """bound(w), boundary.f90:26-113."""
+        check(lib().evora_bound(_ptr(w, self.shape["w"])), "bound")
+
+    def hydrostep(self, w, dt: float = 1e99) -> float:
+        """hydrostep(w), timestep.f90:26-57; returns min(cfl*v, dt)."""
+        d = ctypes.c_double(dt)
+        check(lib().evora_hydrostep(_ptr(w, self.shape["w"], False), ctypes.byref(d)), "hydrostep")
+        return d.value
+
+    def updatetime(self, go: bool, t: float, dt: float, k: int = 1):
+        """updatetime(go,dump,k), timestep.f90:147-171; returns (go, t, dt)."""
+        g = ctypes.c_int32(1 if go else 0)
+        dump = ctypes.c_int32(0)
+        kk = ctypes.c_int32(k)
+        tt, dd = ctypes.c_double(t), ctypes.c_double(dt)
+        check(lib().evora_updatetime(ctypes.byref(g), ctypes.byref(dump), ctypes.byref(kk),
+                                     ctypes.byref(tt), ctypes.byref(dd)), "updatetime")
+        return bool(g.value), tt.value, dd.value
+
+    def compevo(self, w, evo, s, dt: float):
+        """compevo(w,evo,s), muscl.f90:45-113."""
+        check(lib().evora_compevo(_ptr(w, self.shape["w"], False), _ptr(evo, self.shape["evo"]),
+                                  _ptr(s, self.shape["s"]), float(dt)), "compevo")
+
+    def sweep(self, w, q, evo, s, dt: float):
+        """sweep(w,q,evo,s), muscl.f90:171-274."""
+        check(lib().evora_sweep(_ptr(w, self.shape["w"], False), _ptr(q, self.shape["q"]),
+                                _ptr(evo, self.shape["evo"], False), _ptr(s, self.shape["s"], False),
+                                float(dt)), "sweep")
+
+
+# ---------------------------------------------------------- resident grid --
+class Grid:
+    """A grid whose state stays on the current CUDA device across steps."""
+
+    def __init__(self, params: EvoraParams, precision: int = FP64, flags: int = 0, stream=None):
+        self.params = params
+        self.precision = precision
+        self.flags = flags
+        self.shape_q = shapes(params)["q"]
+        h = ctypes.c_void_p()
+        check(lib().evora_grid_create(ctypes.byref(params), precision, flags, ctypes.byref(h)),
+              "grid_create")
+        self._h = h
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().evora_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream):
+        """stream: a torch.cuda.Stream or a raw cudaStream_t integer."""
+        raw = getattr(stream, "cuda_stream", stream)
+        check(lib().evora_grid_set_stream(self._h, ctypes.c_void_p(int(raw))), "grid_set_stream")
+
+    def set_q(self, q):
+        check(lib().evora_grid_set_q(self._h, _ptr(q, self.shape_q, False)), "grid_set_q")
+
+    def get_q(self, out=None):
+        if out is None:
+            out = np.empty(self.shape_q)
+        check(lib().evora_grid_get_q(self._h, _ptr(out, self.shape_q)), "grid_get_q")
+        return out
+
+    def step(self, nsteps: int = 1, sync: bool = True):
+        st = lib().evora_grid_step(self._h, int(nsteps), 1 if sync else 0)
+        check(st, "grid_step")
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        go, k = ctypes.c_int32(), ctypes.c_int64()
+        check(lib().evora_grid_time(self._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(go),
+                                    ctypes.byref(k)), "grid_time")
+        return dict(t=t.value, dt=dt.value, go=bool(go.value), k=k.value)
+
+    def status(self) -> int:
+        return int(lib().evora_grid_status(self._h))
+
+    def totals(self):
+        out = (ctypes.c_double * 6)()
+        check(lib().evora_grid_totals(self._h, out), "grid_totals")
+        return np.array(out[:])
+
+    def set_timing(self, on: bool = True):
+        check(lib().evora_grid_set_timing(self._h, 1 if on else 0), "grid_set_timing")
+
+    def timing(self):
+        up, cf = ctypes.c_double(), ctypes.c_double()
+        n, la = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().evora_grid_timing(self._h, ctypes.byref(up), ctypes.byref(cf), ctypes.byref(n),
+                                      ctypes.byref(la)), "grid_timing")
+        return dict(update_ms=up.value, cfl_ms=cf.value, steps=n.value, launches=la.value)
+
+    def run(self, max_steps: int = 1 << 30, chunk: int = 64):
+        """Advances until updatetime clears go (or max_steps)."""
+        done = 0
+        while done < max_steps:
+            n = min(chunk, max_steps - done)
+            self.step(n, sync=True)
+            done += n
+            if not self.time()["go"]:
+                break
+        return self.time()
+
+
+__all__ = ["EvoraError", "EvoraParams", "EvoraDerived", "default_params", "derived", "shapes",
+           "DropIn", "Grid", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS"]

@@ -1,0 +1,218 @@
+/*
+ * evora_gpu.h -- C ABI of the B200 (sm_100a) hydro update of evora.
+ *
+ * The hot path of the reference is the hydro update that main.f90 drives
+ * once per step (main.f90:109-155):
+ *
+ *     call primitive(w,q)      muscl.f90:26-43   (q2w/pressure, comp.f90:26-85)
+ *     call bound(w)            boundary.f90:26-113
+ *     dt = 1d99
+ *     call hydrostep(w)        timestep.f90:26-57
+ *     call updatetime(go,..)   timestep.f90:147-171
+ *     call compevo(w,evo,s)    muscl.f90:45-113  (comp_slope 115-169)
+ *     call sweep(w,q,evo,s)    muscl.f90:171-274 (riemann.f90, integration)
+ *
+ * This header offers two layers over the same CUDA kernels:
+ *
+ *  1. The drop-in layer (evora_primitive ... evora_sweep): one entry point per
+ *     reference subroutine, same arguments, same array layouts (column-major
+ *     AoS, field index fastest, ghost frames as allocated in main.f90:72-75).
+ *     Parameters that the Fortran code reads from `module global` are set
+ *     once with evora_set_params(); time-step scalars are passed explicitly.
+ *     Array pointers may be device pointers (used in place) or host pointers
+ *     (staged through device buffers on every call).
+ *
+ *  2. The resident layer (evora_grid_*): the whole step fused on the device,
+ *     state kept in HBM across steps in structure-of-arrays form, FP64 or
+ *     FP32 arithmetic.  This is the fast path a driver uses between dumps.
+ *
+ * All entry points return a status: 0 on success, otherwise a bit mask of
+ * EVORA_ERR_* codes.  The reference prints a message and stops at each of
+ * these conditions; the library reports them and leaves the decision to the
+ * caller.  No entry point traps, and no device wait is unbounded.
+ */
+#ifndef EVORA_GPU_H
+#define EVORA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+enum evora_status {
+  EVORA_OK = 0,
+  EVORA_ERR_PRESSURE = 1,         /* p <= 0 recovering primitives, comp.f90:74-84 */
+  EVORA_ERR_RIEMANN_PRESSURE = 2, /* wl(5)<=0 or wr(5)<=0, riemann.f90:61-66,111-116 */
+  EVORA_ERR_HLL = 4,              /* no HLL branch taken, riemann.f90:87-90 */
+  EVORA_ERR_HLLC = 8,             /* no HLLC branch taken, riemann.f90:148-150 */
+  EVORA_ERR_DT = 16,              /* hydro step <= 0, timestep.f90:51-55 */
+  EVORA_ERR_LIMITER = 32,         /* unknown slope limiter, muscl.f90:164-167 */
+  EVORA_ERR_SOLVER = 64,          /* unknown Riemann solver, riemann.f90:38-41 */
+  EVORA_ERR_ARG = 128,            /* invalid argument, size or call order */
+  EVORA_ERR_CUDA = 256,           /* CUDA runtime error (see evora_last_error) */
+  EVORA_ERR_NOMEM = 512,          /* device allocation failed */
+  EVORA_ERR_TIMEOUT = 1024        /* a bounded host or device wait gave up */
+};
+
+/* Number of conserved / primitive / flux fields of the plain build
+ * (global.f90:35: nq=6, nf=6, nw=5).  Field order of q: rho, rho*u, rho*v,
+ * rho*w, E, S = p/rho^(g-1); of w: rho, u, v, w, p. */
+#define EVORA_NQ 6
+#define EVORA_NW 5
+
+/* ------------------------------------------------------------ parameters -- */
+/* The hydro subset of namelist &para (parameter.f90:30-37). */
+typedef struct evora_params {
+  int32_t nx, ny, nz;   /* cells per axis; ny = nz = 1 is 1D, nz = 1 is 2D   */
+  int32_t solver;       /* 1 = HLL, 2 = HLLC                                 */
+  int32_t limiter;      /* 1 = minmod, 2 = monotonised central, 3 = van Leer */
+  int32_t boundtype;    /* 1 = zero gradient, 2 = periodic,
+                           3 = zero gradient with reflecting upper x face    */
+  int32_t secondorder;  /* Fortran logical: MUSCL-Hancock predictor on       */
+  int32_t dualenergy;   /* Fortran logical: dual-energy pressure recovery    */
+  int32_t atomic;       /* Fortran logical: forces g = 5.0/3.0 (single prec) */
+  int32_t reserved;
+  double g, cfl, de_thresh;
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double tstart, tend;
+} evora_params;
+
+/* The derived constants of compparameter (parameter.f90:164-265) that the
+ * hydro path reads from module global. */
+typedef struct evora_derived {
+  double g, g1, g1inv, gg1, cfl, de_thresh1;
+  double dx, dy, dz, dxinv, dyinv, dzinv;
+  double x0, y0, z0, volume;
+  int32_t onedimension, twodimension;
+} evora_derived;
+
+/* Defaults of readparameter (parameter.f90:41-82).  Note g = 1.4 and the
+ * other defaults there are single-precision literals: g is stored as
+ * (double)1.4f = 1.39999997615814..., as the reference does. */
+void evora_params_default(evora_params* p);
+
+/* compparameter (parameter.f90:164-265), hydro subset.  Returns
+ * EVORA_ERR_ARG for non-positive sizes, EVORA_ERR_SOLVER /
+ * EVORA_ERR_LIMITER for unknown options (riemann.f90:38-41,
+ * muscl.f90:164-167 stop at first use; here they are checked up front). */
+int evora_compparameter(const evora_params* p, evora_derived* d);
+
+/* Element counts of the reference arrays for the given grid (main.f90:72-75):
+ *   q(nq, nx, ny, nz), w(nw, nx+4, ny+4, nz+4), evo(nw, nx+2, ny+2, nz+2),
+ *   s(nw, 3, nx+2, ny+2, nz+2).  The ghost frames exist in every axis, also
+ *   for 1D and 2D grids, as in the reference. */
+void evora_array_sizes(const evora_params* p, int64_t* nq_elems, int64_t* nw_elems,
+                       int64_t* nevo_elems, int64_t* ns_elems);
+
+/* Last CUDA error string seen by the library (static storage). */
+const char* evora_last_error(void);
+
+/* Library version string. */
+const char* evora_version(void);
+
+/* -------------------------------------------------------- drop-in layer -- */
+/* Set the module-global hydro parameters used by the routines below (the
+ * analogue of `use global` after compparameter).  Must be called first. */
+int evora_set_params(const evora_params* p);
+
+/* Arithmetic mode of the drop-in layer: 0 = default (contracted FMAs), 1 =
+ * strict (no FMA contraction; matches a gfortran -O3 x86-64 build of the
+ * reference bit for bit where libm is not involved). */
+int evora_set_strict(int32_t strict);
+
+/* primitive(w,q), muscl.f90:26-43.  w interior <- q2w(q) for every cell.
+ * With dualenergy the routine writes back q(5) or q(6) (comp.f90:60-72). */
+int evora_primitive(double* w, double* q);
+
+/* bound(w), boundary.f90:26-113.  Fills the two ghost layers of w: x faces,
+ * then y faces, then z faces, each over the full ghost-inclusive extent. */
+int evora_bound(double* w);
+
+/* hydrostep(w), timestep.f90:26-57.  *dt = min(cfl * v, *dt) with
+ * v = min(1e6, min over interior cells of dx_d / (|u_d| + a)).
+ * Returns EVORA_ERR_DT if the result is <= 0. */
+int evora_hydrostep(const double* w, double* dt);
+
+/* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch:
+ * if tend - t <= dt then dt = tend - t, go = false; then t = t + dt.
+ * dump and k are accepted for signature parity (they only matter in the
+ * supercomoving branch, which is outside the hydro path). */
+int evora_updatetime(int32_t* go, int32_t* dump, int32_t* k, double* t, double* dt);
+
+/* compevo(w,evo,s), muscl.f90:45-113, with comp_slope (115-169).
+ * Fills the slopes s and the half-step predictor evo over the interior plus
+ * one ghost layer, using the step size dt. */
+int evora_compevo(const double* w, double* evo, double* s, double dt);
+
+/* sweep(w,q,evo,s), muscl.f90:171-274.  Updates q in place with the x, y
+ * and z flux differences of each cell, in that order (integration,
+ * muscl.f90:276-290), using one Riemann solve per interface. */
+int evora_sweep(const double* w, double* q, const double* evo, const double* s, double dt);
+
+/* ------------------------------------------------------- resident layer -- */
+typedef struct evora_grid evora_grid;
+
+enum evora_precision { EVORA_FP64 = 0, EVORA_FP32 = 1 };
+
+enum evora_grid_flags {
+  /* Carry the entropy field S = q(6) (as the reference does).  Without this
+   * flag only rho, m, E are advanced: S never feeds back into them when
+   * dualenergy is off, so rho, m, E are unchanged bit for bit. */
+  EVORA_CARRY_ENTROPY = 1,
+  /* Strict arithmetic (no FMA contraction) for FP64 grids. */
+  EVORA_STRICT = 2,
+  /* Run the step with the drop-in layer's per-routine kernels on
+   * device-resident arrays in the reference layouts (FP64 only), instead of
+   * the fused kernel.  Slower; kept as the reference-shaped device path. */
+  EVORA_REFERENCE_KERNELS = 4
+};
+
+/* Creates a grid on the current CUDA device.  Allocates the resident state
+ * (two copies of the conserved fields plus a few scalars). */
+int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags,
+                      evora_grid** out);
+int evora_grid_destroy(evora_grid* g);
+
+/* Work on this CUDA stream (cudaStream_t); NULL = the default stream. */
+int evora_grid_set_stream(evora_grid* g, void* stream);
+
+/* Load / read back the conserved state in the reference layout
+ * q(6, nx, ny, nz) (column-major, field fastest).  Host or device pointer.
+ * set_q also resets t = tstart, k = 0, go = true and the status word. */
+int evora_grid_set_q(evora_grid* g, const double* q);
+int evora_grid_get_q(evora_grid* g, double* q);
+
+/* Advances up to nsteps steps of the reference loop (main.f90:109-155):
+ * primitive, bound, hydrostep, updatetime, compevo, sweep.  Stops early when
+ * updatetime clears go.  Asynchronous: returns after enqueueing, unless a
+ * status check is requested with sync != 0, in which case it waits for the
+ * stream and returns the accumulated error mask. */
+int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync);
+
+/* Time, last step size, go flag and step count (synchronises the stream). */
+int evora_grid_time(evora_grid* g, double* t, double* dt, int32_t* go, int64_t* k);
+
+/* Accumulated device error mask (synchronises the stream). */
+int evora_grid_status(evora_grid* g);
+
+/* Sums of q(1..6) over the interior in FP64 (the totals of evolution,
+ * snapshot.f90:159-193, before the multiplication by the cell volume). */
+int evora_grid_totals(evora_grid* g, double out[6]);
+
+/* Kernel timing (no counterpart in the reference): when on, every step
+ * records CUDA events around its CFL kernel and its update kernel on the
+ * grid's stream.  evora_grid_timing synchronises, returns the summed event
+ * times in ms, the number of timed steps and the number of kernels the grid
+ * launched since timing was switched on, and clears the record. */
+int evora_grid_set_timing(evora_grid* g, int32_t on);
+int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps,
+                      int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EVORA_GPU_H */

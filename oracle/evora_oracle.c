@@ -1,0 +1,774 @@
+/*
+ * evora_oracle.c -- TEST INFRASTRUCTURE ONLY.  Not part of the product.
+ *
+ * A plain-C, FP64 restatement of the hydro update of evora, used by tests/,
+ * by __graft_entry__.smoke() and by the CPU legs of bench.py as the checker
+ * and the CPU baseline.  Nothing in evora_b200/ links or calls it.
+ *
+ * It follows the reference line by line: the same array-of-structures
+ * layouts (field index fastest, ghost frames as allocated in main.f90:72-75),
+ * the same loop order, and the same association of every floating-point
+ * expression (Fortran evaluates a*b*c as (a*b)*c; gfortran -O3 on x86-64
+ * emits no FMA, so this file is compiled with -ffp-contract=off).  Integer
+ * powers x**2 are written x*x as gfortran expands them; real powers call
+ * libm pow.  MIN/MAX are evaluated left to right as "take the next argument
+ * if it is smaller (larger)".
+ *
+ * Pinning: the reference ships no test vectors (its tests only draw plots),
+ * and no Fortran compiler exists here, so the reference cannot be run as is.
+ * oracle/ref_f2c.py translates the reference's own Fortran sources
+ * mechanically into C (oracle/_ref/), and tests/test_oracle_pin.py checks
+ * this restatement against that translation bit for bit.
+ *
+ * The reference stops the program on each error condition; this file
+ * records the first error as an EVORA_ERR_* bit and carries on, so that the
+ * caller can stop.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/evora_gpu.h"
+
+#define NQ 6
+#define NW 5
+#define NF 6
+
+/* ------------------------------------------------------ module global -- */
+/* The hydro subset of module global (global.f90:44-86), filled by
+ * orc_compparameter. */
+static struct {
+  int nx, ny, nz;
+  int solver, limiter, boundtype, secondorder, dualenergy;
+  double g, g1, g1inv, gg1, cfl, de_thresh1;
+  double dx, dy, dz, dxinv, dyinv, dzinv, x0, y0, z0, volume;
+  double tstart, tend;
+  int onedimension, twodimension;
+} G;
+
+static int orc_err = 0;
+
+static void set_err(int code) {
+#pragma omp atomic
+  orc_err |= code;
+}
+
+int orc_error(void) { return orc_err; }
+void orc_clear_error(void) { orc_err = 0; }
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* Fortran MIN/MAX of two reals, left to right. */
+static inline double fmin2(double a, double b) { return (b < a) ? b : a; }
+static inline double fmax2(double a, double b) { return (b > a) ? b : a; }
+
+/* compparameter, parameter.f90:164-265 (hydro subset). */
+int orc_compparameter(const evora_params* p) {
+  if (p->nx < 1 || p->ny < 1 || p->nz < 1) return EVORA_ERR_ARG;
+  if (p->nx == 1) return EVORA_ERR_ARG;                 /* x is always swept */
+  if (p->nz > 1 && p->ny == 1) return EVORA_ERR_ARG;    /* y ghosts never filled */
+  if (p->solver != 1 && p->solver != 2) return EVORA_ERR_SOLVER;
+  if (p->limiter < 1 || p->limiter > 3) return EVORA_ERR_LIMITER;
+  if (p->boundtype < 1 || p->boundtype > 3) return EVORA_ERR_ARG; /* bound fills nothing else */
+  G.nx = p->nx; G.ny = p->ny; G.nz = p->nz;
+  G.solver = p->solver; G.limiter = p->limiter; G.boundtype = p->boundtype;
+  G.secondorder = p->secondorder != 0; G.dualenergy = p->dualenergy != 0;
+  G.g = p->g;
+  if (p->atomic) G.g = (double)(5.0f / 3.0f);           /* parameter.f90:169-171 */
+  G.cfl = p->cfl;
+  G.tstart = p->tstart; G.tend = p->tend;
+  G.onedimension = (p->ny == 1 && p->nz == 1);          /* parameter.f90:173-177 */
+  G.twodimension = (p->nz == 1);                        /* parameter.f90:178-182 */
+  double xmin = p->xmin, xmax = p->xmax, ymin = p->ymin, ymax = p->ymax;
+  double zmin = p->zmin, zmax = p->zmax;
+  G.dx = (xmax - xmin) / p->nx;                         /* parameter.f90:192-194 */
+  G.dy = (ymax - ymin) / p->ny;
+  G.dz = (zmax - zmin) / p->nz;
+  if (G.onedimension) {                                 /* parameter.f90:195-205 */
+    G.dy = G.dx; G.dz = G.dx;
+    ymin = 0.0; ymax = G.dy; zmin = 0.0; zmax = G.dz;
+    G.dy = (ymax - ymin) / p->ny;
+    G.dz = (zmax - zmin) / p->nz;
+  }
+  if (G.twodimension) {                                 /* parameter.f90:206-212 */
+    G.dz = G.dx;
+    zmin = 0.0; zmax = G.dz;
+    G.dz = (zmax - zmin) / p->nz;
+  }
+  G.dxinv = 1.0 / G.dx; G.dyinv = 1.0 / G.dy; G.dzinv = 1.0 / G.dz;
+  G.x0 = xmin + G.dx / 2; G.y0 = ymin + G.dy / 2; G.z0 = zmin + G.dz / 2;
+  G.volume = (xmax - xmin) * (ymax - ymin) * (zmax - zmin);
+  G.g1 = G.g - 1.0;                                     /* parameter.f90:227-231 */
+  G.g1inv = 1.0 / G.g1;
+  G.gg1 = G.g / G.g1;
+  G.de_thresh1 = G.dualenergy ? 1.0 - p->de_thresh : 1.0; /* parameter.f90:244-248 */
+  return 0;
+}
+
+void orc_get_derived(evora_derived* d) {
+  d->g = G.g; d->g1 = G.g1; d->g1inv = G.g1inv; d->gg1 = G.gg1; d->cfl = G.cfl;
+  d->de_thresh1 = G.de_thresh1;
+  d->dx = G.dx; d->dy = G.dy; d->dz = G.dz;
+  d->dxinv = G.dxinv; d->dyinv = G.dyinv; d->dzinv = G.dzinv;
+  d->x0 = G.x0; d->y0 = G.y0; d->z0 = G.z0; d->volume = G.volume;
+  d->onedimension = G.onedimension; d->twodimension = G.twodimension;
+}
+
+/* --------------------------------------------------------- array index -- */
+/* q(nq, 1:nx, 1:ny, 1:nz) */
+static inline size_t iq(int i, int j, int k) {
+  return (size_t)NQ * ((size_t)(i - 1) + (size_t)G.nx * ((size_t)(j - 1) + (size_t)G.ny * (size_t)(k - 1)));
+}
+/* w(nw, -1:nx+2, -1:ny+2, -1:nz+2) */
+static inline size_t iw(int i, int j, int k) {
+  return (size_t)NW * ((size_t)(i + 1) + (size_t)(G.nx + 4) * ((size_t)(j + 1) + (size_t)(G.ny + 4) * (size_t)(k + 1)));
+}
+/* evo(nw, 0:nx+1, 0:ny+1, 0:nz+1) */
+static inline size_t ie(int i, int j, int k) {
+  return (size_t)NW * ((size_t)i + (size_t)(G.nx + 2) * ((size_t)j + (size_t)(G.ny + 2) * (size_t)k));
+}
+/* s(nw, 3, 0:nx+1, 0:ny+1, 0:nz+1); d = 1..3 */
+static inline size_t is_(int d, int i, int j, int k) {
+  return (size_t)NW * ((size_t)(d - 1) + 3 * ((size_t)i + (size_t)(G.nx + 2) * ((size_t)j + (size_t)(G.ny + 2) * (size_t)k)));
+}
+
+void orc_array_sizes(int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
+  *nq = (int64_t)NQ * G.nx * G.ny * G.nz;
+  *nw = (int64_t)NW * (G.nx + 4) * (G.ny + 4) * (G.nz + 4);
+  *ne = (int64_t)NW * (G.nx + 2) * (G.ny + 2) * (G.nz + 2);
+  *ns = (int64_t)NW * 3 * (G.nx + 2) * (G.ny + 2) * (G.nz + 2);
+}
+
+/* ------------------------------------------------------------ comp.f90 -- */
+/* pressure(q,press), comp.f90:45-85 (may write q(5) or q(6)). */
+static double orc_pressure(double* q) {
+  double m2 = (q[1] * q[1]) + (q[2] * q[2]) + (q[3] * q[3]);
+  double kin = 0.5 * m2 / q[0];
+  double ratio = kin / q[4];
+  double press;
+  if (G.dualenergy) {
+    if (ratio > G.de_thresh1) {            /* S - system */
+      press = q[5] * pow(q[0], G.g1);
+      q[4] = kin + press * G.g1inv;
+    } else {                               /* E - system */
+      press = G.g1 * (q[4] - kin);
+      q[5] = press / pow(q[0], G.g1);
+    }
+  } else {
+    press = G.g1 * (q[4] - kin);
+  }
+  if (press <= 0.0) set_err(EVORA_ERR_PRESSURE);
+  return press;
+}
+
+/* q2w(q,w), comp.f90:26-43 (nw = 5: no species loop). */
+static void orc_q2w(double* q, double* w) {
+  double densinv = 1.0 / q[0];
+  w[0] = q[0];
+  w[1] = q[1] * densinv;
+  w[2] = q[2] * densinv;
+  w[3] = q[3] * densinv;
+  w[4] = orc_pressure(q);
+}
+
+/* ----------------------------------------------------------- muscl.f90 -- */
+/* primitive(w,q), muscl.f90:26-43. */
+void orc_primitive(double* w, double* q) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+#pragma omp parallel for schedule(static) if (nz > 1)
+  for (int iz = 1; iz <= nz; ++iz)
+    for (int iy = 1; iy <= ny; ++iy)
+      for (int ix = 1; ix <= nx; ++ix) orc_q2w(&q[iq(ix, iy, iz)], &w[iw(ix, iy, iz)]);
+}
+
+/* bound(w), boundary.f90:26-113.  Copy of a full ghost-inclusive plane;
+ * sign = -1 negates the three velocity components (reflection). */
+static void copy_xplane(double* w, int dst, int src, int reflect) {
+  for (int k = -1; k <= G.nz + 2; ++k)
+    for (int j = -1; j <= G.ny + 2; ++j) {
+      double* d = &w[iw(dst, j, k)];
+      const double* s = &w[iw(src, j, k)];
+      d[0] = s[0];
+      d[1] = reflect ? -s[1] : s[1];
+      d[2] = reflect ? -s[2] : s[2];
+      d[3] = reflect ? -s[3] : s[3];
+      d[4] = s[4];
+    }
+}
+static void copy_yplane(double* w, int dst, int src) {
+  for (int k = -1; k <= G.nz + 2; ++k)
+    for (int i = -1; i <= G.nx + 2; ++i)
+      memcpy(&w[iw(i, dst, k)], &w[iw(i, src, k)], NW * sizeof(double));
+}
+static void copy_zplane(double* w, int dst, int src) {
+  for (int j = -1; j <= G.ny + 2; ++j)
+    for (int i = -1; i <= G.nx + 2; ++i)
+      memcpy(&w[iw(i, j, dst)], &w[iw(i, j, src)], NW * sizeof(double));
+}
+
+void orc_bound(double* w) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz, bt = G.boundtype;
+  /* index bounds of a single rank: lx=1, mx=nx, lx0=2, mx0=nx-1,
+   * lx1=0, lx2=-1, mx1=nx+1, mx2=nx+2 (parallel.f90:26-66) */
+  if (nx != 1) {                                      /* boundary.f90:33-66 */
+    if (bt == 1 || bt == 3) {          /* lower: zero gradient (the reflecting
+                                          branch at 41-48 is unreachable) */
+      copy_xplane(w, -1, 2, 0);
+      copy_xplane(w, 0, 1, 0);
+    } else if (bt == 2) {
+      copy_xplane(w, -1, nx - 1, 0);
+      copy_xplane(w, 0, nx, 0);
+    }
+    if (bt == 1) {
+      copy_xplane(w, nx + 2, nx - 1, 0);
+      copy_xplane(w, nx + 1, nx, 0);
+    } else if (bt == 2) {
+      copy_xplane(w, nx + 2, 2, 0);
+      copy_xplane(w, nx + 1, 1, 0);
+    } else if (bt == 3) {              /* reflecting upper x face */
+      copy_xplane(w, nx + 1, nx, 1);
+      copy_xplane(w, nx + 2, nx - 1, 1);
+    }
+  }
+  if (ny != 1) {                                      /* boundary.f90:69-88 */
+    if (bt == 1 || bt == 3) {
+      copy_yplane(w, -1, 2);
+      copy_yplane(w, 0, 1);
+      copy_yplane(w, ny + 2, ny - 1);
+      copy_yplane(w, ny + 1, ny);
+    } else if (bt == 2) {
+      copy_yplane(w, -1, ny - 1);
+      copy_yplane(w, 0, ny);
+      copy_yplane(w, ny + 2, 2);
+      copy_yplane(w, ny + 1, 1);
+    }
+  }
+  if (nz != 1) {                                      /* boundary.f90:91-111 */
+    if (bt == 1 || bt == 3) {
+      copy_zplane(w, -1, 2);
+      copy_zplane(w, 0, 1);
+      copy_zplane(w, nz + 2, nz - 1);
+      copy_zplane(w, nz + 1, nz);
+    } else if (bt == 2) {              /* mpisize == 1 */
+      copy_zplane(w, -1, nz - 1);
+      copy_zplane(w, 0, nz);
+      copy_zplane(w, nz + 2, 2);
+      copy_zplane(w, nz + 1, 1);
+    }
+  }
+}
+
+/* comp_slope(wl,w,wr,s), muscl.f90:115-169. */
+static void orc_comp_slope(const double* wl, const double* w, const double* wr, double* s) {
+  double dwl[NW], dwr[NW];
+  for (int i = 0; i < NW; ++i) {
+    dwl[i] = w[i] - wl[i];
+    dwr[i] = wr[i] - w[i];
+  }
+  if (G.limiter == 1) {                               /* minmod */
+    for (int i = 0; i < NW; ++i) {
+      int lp = dwl[i] >= 0.0, rp = dwr[i] >= 0.0;
+      if (lp != rp) s[i] = 0.0;
+      else if (rp) s[i] = fmin2(dwl[i], dwr[i]);
+      else s[i] = fmax2(dwl[i], dwr[i]);
+    }
+  } else if (G.limiter == 2) {                        /* moncen */
+    for (int i = 0; i < NW; ++i) {
+      double dwc = (wr[i] - wl[i]) * 0.5;
+      int lp = dwl[i] >= 0.0, rp = dwr[i] >= 0.0;
+      if (lp != rp) s[i] = 0.0;
+      else if (rp) s[i] = fmin2(fmin2(2.0 * dwl[i], dwc), 2.0 * dwr[i]);
+      else s[i] = fmax2(fmax2(2.0 * dwl[i], dwc), 2.0 * dwr[i]);
+    }
+  } else if (G.limiter == 3) {                        /* van Leer */
+    for (int i = 0; i < NW; ++i) {
+      double pro = dwl[i] * dwr[i];
+      if (pro <= 0.0) s[i] = 0.0;
+      else s[i] = 2.0 * pro / (dwr[i] + dwl[i]);
+    }
+  } else {
+    set_err(EVORA_ERR_LIMITER);
+  }
+}
+
+/* compevo(w,evo,s), muscl.f90:45-113. */
+void orc_compevo(const double* w, double* evo, double* s, double dt) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  const double dt2 = -0.5 * dt;
+  const double g = G.g;
+  if (G.onedimension) {                               /* muscl.f90:60-69 */
+    for (int ix = 0; ix <= nx + 1; ++ix) {
+      double* sx = &s[is_(1, ix, 1, 1)];
+      const double* wc = &w[iw(ix, 1, 1)];
+      double a[NW];
+      orc_comp_slope(&w[iw(ix - 1, 1, 1)], wc, &w[iw(ix + 1, 1, 1)], sx);
+      for (int f = 0; f < NW; ++f) a[f] = wc[1] * sx[f];
+      a[4] = a[4] + g * wc[4] * sx[1];
+      a[1] = a[1] + sx[4] / wc[0];
+      double* e = &evo[ie(ix, 1, 1)];
+      for (int f = 0; f < NW; ++f) e[f] = dt2 * a[f] * G.dxinv;
+    }
+  } else if (G.twodimension) {                        /* muscl.f90:70-88 */
+    for (int iy = 0; iy <= ny + 1; ++iy)
+      for (int ix = 0; ix <= nx + 1; ++ix) {
+        double* s1 = &s[is_(1, ix, iy, 1)];
+        double* s2 = &s[is_(2, ix, iy, 1)];
+        const double* wc = &w[iw(ix, iy, 1)];
+        double a1[NW], a2[NW];
+        orc_comp_slope(&w[iw(ix - 1, iy, 1)], wc, &w[iw(ix + 1, iy, 1)], s1);
+        orc_comp_slope(&w[iw(ix, iy - 1, 1)], wc, &w[iw(ix, iy + 1, 1)], s2);
+        for (int f = 0; f < NW; ++f) a1[f] = wc[1] * s1[f];
+        a1[4] = a1[4] + g * wc[4] * s1[1];
+        a1[1] = a1[1] + s1[4] / wc[0];
+        for (int f = 0; f < NW; ++f) a2[f] = wc[2] * s2[f];
+        a2[4] = a2[4] + g * wc[4] * s2[2];
+        a2[2] = a2[2] + s2[4] / wc[0];
+        double* e = &evo[ie(ix, iy, 1)];
+        for (int f = 0; f < NW; ++f) e[f] = dt2 * (a1[f] * G.dxinv + a2[f] * G.dyinv);
+      }
+  } else {                                            /* muscl.f90:89-111 */
+#pragma omp parallel for schedule(static)
+    for (int iz = 0; iz <= nz + 1; ++iz)
+      for (int iy = 0; iy <= ny + 1; ++iy)
+        for (int ix = 0; ix <= nx + 1; ++ix) {
+          const double* wc = &w[iw(ix, iy, iz)];
+          double* sd[3] = {&s[is_(1, ix, iy, iz)], &s[is_(2, ix, iy, iz)], &s[is_(3, ix, iy, iz)]};
+          double a[3][NW];
+          orc_comp_slope(&w[iw(ix - 1, iy, iz)], wc, &w[iw(ix + 1, iy, iz)], sd[0]);
+          orc_comp_slope(&w[iw(ix, iy - 1, iz)], wc, &w[iw(ix, iy + 1, iz)], sd[1]);
+          orc_comp_slope(&w[iw(ix, iy, iz - 1)], wc, &w[iw(ix, iy, iz + 1)], sd[2]);
+          for (int i = 0; i < 3; ++i) {
+            for (int f = 0; f < NW; ++f) a[i][f] = wc[i + 1] * sd[i][f];
+            a[i][4] = a[i][4] + g * wc[4] * sd[i][i + 1];
+            a[i][i + 1] = a[i][i + 1] + sd[i][4] / wc[0];
+          }
+          double* e = &evo[ie(ix, iy, iz)];
+          for (int f = 0; f < NW; ++f)
+            e[f] = dt2 * (a[0][f] * G.dxinv + a[1][f] * G.dyinv + a[2][f] * G.dzinv);
+        }
+  }
+}
+
+/* --------------------------------------------------------- riemann.f90 -- */
+/* flux(w,f,dir), riemann.f90:157-205. */
+static void orc_flux(const double* w, double* f, int dir) {
+  double u2 = w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
+  if (dir == 1) {
+    f[0] = w[0] * w[1];
+    f[1] = w[0] * (w[1] * w[1]) + w[4];
+    f[2] = w[0] * w[1] * w[2];
+    f[3] = w[0] * w[1] * w[3];
+    f[4] = w[1] * (0.5 * w[0] * u2 + G.gg1 * w[4]);
+    f[5] = w[1] * w[4] / pow(w[0], G.g1);
+  } else if (dir == 2) {
+    f[0] = w[0] * w[2];
+    f[1] = w[0] * w[2] * w[1];
+    f[2] = w[0] * (w[2] * w[2]) + w[4];
+    f[3] = w[0] * w[2] * w[3];
+    f[4] = w[2] * (0.5 * w[0] * u2 + G.gg1 * w[4]);
+    f[5] = w[2] * w[4] / pow(w[0], G.g1);
+  } else {
+    f[0] = w[0] * w[3];
+    f[1] = w[0] * w[3] * w[1];
+    f[2] = w[0] * w[3] * w[2];
+    f[3] = w[0] * (w[3] * w[3]) + w[4];
+    f[4] = w[3] * (0.5 * w[0] * u2 + G.gg1 * w[4]);
+    f[5] = w[3] * w[4] / pow(w[0], G.g1);
+  }
+}
+
+/* state(w,q), riemann.f90:207-239. */
+static void orc_state(const double* w, double* q) {
+  q[0] = w[0];
+  q[1] = w[0] * w[1];
+  q[2] = w[0] * w[2];
+  q[3] = w[0] * w[3];
+  double u2 = (w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3]);
+  q[4] = 0.5 * w[0] * u2 + w[4] / G.g1;
+  q[5] = w[4] / pow(w[0], G.g1);
+}
+
+/* statex(w,qx,s,sm,dir), riemann.f90:241-288. */
+static void orc_statex(const double* w, double* qx, double s, double sm, int dir) {
+  const double wd = w[dir];
+  qx[0] = w[0] * (s - wd) / (s - sm);
+  if (dir == 1) {
+    qx[1] = sm * qx[0];
+    qx[2] = w[2] * qx[0];
+    qx[3] = w[3] * qx[0];
+  } else if (dir == 2) {
+    qx[1] = w[1] * qx[0];
+    qx[2] = sm * qx[0];
+    qx[3] = w[3] * qx[0];
+  } else {
+    qx[1] = w[1] * qx[0];
+    qx[2] = w[2] * qx[0];
+    qx[3] = sm * qx[0];
+  }
+  double energy = 0.5 * w[0] * ((w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3])) + w[4] / G.g1;
+  qx[4] = qx[0] * (energy / w[0] + (sm - wd) * (sm + (w[4] / (w[0] * (s - wd)))));
+  qx[5] = qx[0] * w[4] / pow(w[0], G.g);
+}
+
+/* hll(wl,wr,f,dir), riemann.f90:47-92. */
+static void orc_hll(const double* wl, const double* wr, double* f, int dir) {
+  if (wl[4] <= 0 || wr[4] <= 0) set_err(EVORA_ERR_RIEMANN_PRESSURE);
+  double al = sqrt(G.g * wl[4] / wl[0]);
+  double ar = sqrt(G.g * wr[4] / wr[0]);
+  double sl = fmin2(wl[dir] - al, wr[dir] - ar);
+  double sr = fmax2(wl[dir] + al, wr[dir] + ar);
+  if (0 < sl) {
+    orc_flux(wl, f, dir);
+  } else if (0 > sr) {
+    orc_flux(wr, f, dir);
+  } else if (sl <= 0 && 0 <= sr) {
+    double fl[NF], fr[NF], ql[NQ], qr[NQ];
+    orc_flux(wl, fl, dir);
+    orc_flux(wr, fr, dir);
+    orc_state(wl, ql);
+    orc_state(wr, qr);
+    for (int i = 0; i < NF; ++i)
+      f[i] = (sr * fl[i] - sl * fr[i] + sl * sr * (qr[i] - ql[i])) / (sr - sl);
+  } else {
+    set_err(EVORA_ERR_HLL);
+    for (int i = 0; i < NF; ++i) f[i] = 0.0;
+  }
+}
+
+/* hllc(wl,wr,f,dir), riemann.f90:96-153. */
+static void orc_hllc(const double* wl, const double* wr, double* f, int dir) {
+  if (wl[4] <= 0 || wr[4] <= 0) set_err(EVORA_ERR_RIEMANN_PRESSURE);
+  double al = sqrt(G.g * wl[4] / wl[0]);
+  double ar = sqrt(G.g * wr[4] / wr[0]);
+  double sl = fmin2(wl[dir] - al, wr[dir] - ar);
+  double sr = fmax2(wl[dir] + al, wr[dir] + ar);
+  double facl = wl[0] * (sl - wl[dir]);
+  double facr = wr[0] * (sr - wr[dir]);
+  double sm = (wr[4] - wl[4] + facl * wl[dir] - facr * wr[dir]) / (facl - facr);
+  if (0 < sl) {
+    orc_flux(wl, f, dir);
+  } else if (0 > sr) {
+    orc_flux(wr, f, dir);
+  } else if (sl < 0 && 0 < sm) {
+    double fl[NF], ql[NQ], qx[NQ];
+    orc_flux(wl, fl, dir);
+    orc_state(wl, ql);
+    orc_statex(wl, qx, sl, sm, dir);
+    for (int i = 0; i < NF; ++i) f[i] = fl[i] + sl * (qx[i] - ql[i]);
+  } else if (sm <= 0 && 0 < sr) {
+    double fr[NF], qr[NQ], qx[NQ];
+    orc_flux(wr, fr, dir);
+    orc_state(wr, qr);
+    orc_statex(wr, qx, sr, sm, dir);
+    for (int i = 0; i < NF; ++i) f[i] = fr[i] + sr * (qx[i] - qr[i]);
+  } else {
+    set_err(EVORA_ERR_HLLC);
+    for (int i = 0; i < NF; ++i) f[i] = 0.0;
+  }
+}
+
+/* riemannsolver(wl,wr,f,dir), riemann.f90:26-43. */
+static void orc_riemann(const double* wl, const double* wr, double* f, int dir) {
+  if (G.solver == 1) orc_hll(wl, wr, f, dir);
+  else if (G.solver == 2) orc_hllc(wl, wr, f, dir);
+  else set_err(EVORA_ERR_SOLVER);
+}
+
+/* Single interface flux for tests: wl, wr are primitive 5-vectors. */
+void orc_riemann_single(const double* wl, const double* wr, double* f, int dir) {
+  orc_riemann(wl, wr, f, dir);
+}
+
+/* integration(fl,fr,q,delta), muscl.f90:276-290 (nf = 6). */
+static inline void orc_integration(const double* fl, const double* fr, double* q, double delta) {
+  for (int i = 0; i < NF; ++i) q[i] = q[i] + delta * (fl[i] - fr[i]);
+}
+
+/* Left face state of the interface (a|b) along axis d: w + 0.5 s + evo. */
+static inline void face_left(const double* w, const double* s, const double* e, double* out) {
+  for (int f = 0; f < NW; ++f) out[f] = w[f] + 0.5 * s[f] + e[f];
+}
+static inline void face_right(const double* w, const double* s, const double* e, double* out) {
+  for (int f = 0; f < NW; ++f) out[f] = w[f] - 0.5 * s[f] + e[f];
+}
+
+/* One pencil of sweep (muscl.f90:194-215 and the y/z copies): cells 1..n
+ * along axis d, addressed through the index callbacks. */
+void orc_sweep(const double* w, double* q, const double* evo, const double* s, double dt) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz, so = G.secondorder;
+  if (nx != 1) {                                      /* muscl.f90:191-216 */
+    const double delta = dt * G.dxinv;
+#pragma omp parallel for schedule(static) if (nz > 1)
+    for (int iz = 1; iz <= nz; ++iz)
+      for (int iy = 1; iy <= ny; ++iy) {
+        double wl[NW], wr[NW], fl[NF], fr[NF];
+        if (so) {
+          face_left(&w[iw(0, iy, iz)], &s[is_(1, 0, iy, iz)], &evo[ie(0, iy, iz)], wl);
+          face_right(&w[iw(1, iy, iz)], &s[is_(1, 1, iy, iz)], &evo[ie(1, iy, iz)], wr);
+        } else {
+          memcpy(wl, &w[iw(0, iy, iz)], sizeof wl);
+          memcpy(wr, &w[iw(1, iy, iz)], sizeof wr);
+        }
+        orc_riemann(wl, wr, fr, 1);
+        for (int ix = 1; ix <= nx; ++ix) {
+          memcpy(fl, fr, sizeof fl);
+          if (so) {
+            face_left(&w[iw(ix, iy, iz)], &s[is_(1, ix, iy, iz)], &evo[ie(ix, iy, iz)], wl);
+            face_right(&w[iw(ix + 1, iy, iz)], &s[is_(1, ix + 1, iy, iz)], &evo[ie(ix + 1, iy, iz)], wr);
+          } else {
+            memcpy(wl, &w[iw(ix, iy, iz)], sizeof wl);
+            memcpy(wr, &w[iw(ix + 1, iy, iz)], sizeof wr);
+          }
+          orc_riemann(wl, wr, fr, 1);
+          orc_integration(fl, fr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+  if (ny != 1) {                                      /* muscl.f90:219-244 */
+    const double delta = dt * G.dyinv;
+#pragma omp parallel for schedule(static) if (nz > 1)
+    for (int iz = 1; iz <= nz; ++iz)
+      for (int ix = 1; ix <= nx; ++ix) {
+        double wl[NW], wr[NW], fl[NF], fr[NF];
+        if (so) {
+          face_left(&w[iw(ix, 0, iz)], &s[is_(2, ix, 0, iz)], &evo[ie(ix, 0, iz)], wl);
+          face_right(&w[iw(ix, 1, iz)], &s[is_(2, ix, 1, iz)], &evo[ie(ix, 1, iz)], wr);
+        } else {
+          memcpy(wl, &w[iw(ix, 0, iz)], sizeof wl);
+          memcpy(wr, &w[iw(ix, 1, iz)], sizeof wr);
+        }
+        orc_riemann(wl, wr, fr, 2);
+        for (int iy = 1; iy <= ny; ++iy) {
+          memcpy(fl, fr, sizeof fl);
+          if (so) {
+            face_left(&w[iw(ix, iy, iz)], &s[is_(2, ix, iy, iz)], &evo[ie(ix, iy, iz)], wl);
+            face_right(&w[iw(ix, iy + 1, iz)], &s[is_(2, ix, iy + 1, iz)], &evo[ie(ix, iy + 1, iz)], wr);
+          } else {
+            memcpy(wl, &w[iw(ix, iy, iz)], sizeof wl);
+            memcpy(wr, &w[iw(ix, iy + 1, iz)], sizeof wr);
+          }
+          orc_riemann(wl, wr, fr, 2);
+          orc_integration(fl, fr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+  if (nz != 1) {                                      /* muscl.f90:247-272 */
+    const double delta = dt * G.dzinv;
+#pragma omp parallel for schedule(static)
+    for (int iy = 1; iy <= ny; ++iy)
+      for (int ix = 1; ix <= nx; ++ix) {
+        double wl[NW], wr[NW], fl[NF], fr[NF];
+        if (so) {
+          face_left(&w[iw(ix, iy, 0)], &s[is_(3, ix, iy, 0)], &evo[ie(ix, iy, 0)], wl);
+          face_right(&w[iw(ix, iy, 1)], &s[is_(3, ix, iy, 1)], &evo[ie(ix, iy, 1)], wr);
+        } else {
+          memcpy(wl, &w[iw(ix, iy, 0)], sizeof wl);
+          memcpy(wr, &w[iw(ix, iy, 1)], sizeof wr);
+        }
+        orc_riemann(wl, wr, fr, 3);
+        for (int iz = 1; iz <= nz; ++iz) {
+          memcpy(fl, fr, sizeof fl);
+          if (so) {
+            face_left(&w[iw(ix, iy, iz)], &s[is_(3, ix, iy, iz)], &evo[ie(ix, iy, iz)], wl);
+            face_right(&w[iw(ix, iy, iz + 1)], &s[is_(3, ix, iy, iz + 1)], &evo[ie(ix, iy, iz + 1)], wr);
+          } else {
+            memcpy(wl, &w[iw(ix, iy, iz)], sizeof wl);
+            memcpy(wr, &w[iw(ix, iy, iz + 1)], sizeof wr);
+          }
+          orc_riemann(wl, wr, fr, 3);
+          orc_integration(fl, fr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+}
+
+/* --------------------------------------------------------- timestep.f90 -- */
+/* hydrostep(w), timestep.f90:26-57: returns min(cfl*v, dt_in). */
+double orc_hydrostep(const double* w, double dt_in) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  double v = 1e6;
+#pragma omp parallel for schedule(static) reduction(min : v) if (nz > 1)
+  for (int iy = 1; iy <= ny; ++iy)
+    for (int ix = 1; ix <= nx; ++ix)
+      for (int iz = 1; iz <= nz; ++iz) {
+        const double* c = &w[iw(ix, iy, iz)];
+        double a = sqrt(G.g * c[4] / c[0]);
+        double vx = G.dx / (fabs(c[1]) + a);
+        double vy = G.dy / (fabs(c[2]) + a);
+        double vz = G.dz / (fabs(c[3]) + a);
+        double m = vx;
+        m = fmin2(m, vy);
+        m = fmin2(m, vz);
+        m = fmin2(m, v);
+        v = m;
+      }
+  double dt = fmin2(G.cfl * v, dt_in);
+  if (dt <= 0.0) set_err(EVORA_ERR_DT);
+  return dt;
+}
+
+/* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch. */
+void orc_updatetime(int* go, double* t, double* dt) {
+  if (G.tend - *t <= *dt) {
+    *dt = G.tend - *t;
+    *go = 0;
+  }
+  *t = *t + *dt;
+}
+
+/* ------------------------------------------------------------- driver -- */
+/* The hydro subset of the time loop of main.f90:109-203 (no gravity,
+ * chemistry, conduction, expansion, output).  Runs until go is cleared,
+ * max_steps is reached or an error is raised.  Arrays w, evo, s are
+ * scratch of orc_array_sizes() elements, allocated here.  Returns the error
+ * mask; *t and *steps report the end state, *dt_last the last step. */
+int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, int* go_out) {
+  int64_t nq, nw, ne, ns;
+  orc_array_sizes(&nq, &nw, &ne, &ns);
+  double* w = (double*)calloc((size_t)nw, sizeof(double));
+  double* evo = (double*)calloc((size_t)ne, sizeof(double));   /* main.f90:76-77 */
+  double* s = (double*)calloc((size_t)ns, sizeof(double));
+  if (!w || !evo || !s) {
+    free(w); free(evo); free(s);
+    return EVORA_ERR_NOMEM;
+  }
+  int go = 1, k = 0;
+  double dt = 0.0;
+  *t = G.tstart;
+  orc_err = 0;
+  while (go && k < max_steps) {
+    orc_primitive(w, q);
+    orc_bound(w);
+    dt = 1e99;
+    dt = orc_hydrostep(w, dt);
+    orc_updatetime(&go, t, &dt);
+    if (orc_err) break;
+    if (G.secondorder) orc_compevo(w, evo, s, dt);
+    orc_sweep(w, q, evo, s, dt);
+    ++k;
+    if (orc_err) break;
+  }
+  free(w); free(evo); free(s);
+  *steps = k;
+  *dt_last = dt;
+  if (go_out) *go_out = go;
+  return orc_err;
+}
+
+/* ------------------------------------------------------------------ ICs -- */
+/* ic(q) of ic/shocktube.f90:59-100: Riemann problem split at x_diss along
+ * direction dir (1..3); coordinates of comp.f90:150-162. */
+int orc_ic_shocktube(double* q, double dl, double ul, double pl, double dr, double ur,
+                     double pr, double x_diss, int dir) {
+  if (dir < 1 || dir > 3) return EVORA_ERR_ARG;
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double x = G.x0 + (double)(ix - 1) * G.dx;
+        double y = G.y0 + (double)(iy - 1) * G.dy;
+        double z = G.z0 + (double)(iz - 1) * G.dz;
+        double d, u, p;
+        if ((dir == 1 && x < x_diss) || (dir == 2 && y < x_diss) || (dir == 3 && z < x_diss)) {
+          d = dl; u = ul; p = pl;
+        } else {
+          d = dr; u = ur; p = pr;
+        }
+        double* c = &q[iq(ix, iy, iz)];
+        c[0] = d;
+        c[1] = dir == 1 ? d * u : 0.0;
+        c[2] = dir == 2 ? d * u : 0.0;
+        c[3] = dir == 3 ? d * u : 0.0;
+        c[4] = 0.5 * d * (u * u) + p / G.g1;
+        c[5] = p / pow(d, G.g1);
+      }
+  return 0;
+}
+
+/* ic(q) of ic/kevinhelmholtz.f90:40-69 (2D shear layer with a localised
+ * sinusoidal vy perturbation; pi and the literals 0.1, 0.05 are single
+ * precision there, global.f90:98). */
+int orc_ic_kh2d(double* q) {
+  const double pi = (double)3.1415927f;
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double x = G.x0 + (double)(ix - 1) * G.dx;
+        double y = G.y0 + (double)(iy - 1) * G.dy;
+        double r = fabs(y - 0.5);
+        double d, u;
+        if (r <= 0.25) { d = 2.0; u = 0.5; } else { d = 1.0; u = -0.5; }
+        double v = (double)0.1f * sin(4 * pi * x) *
+                   (exp(-((y - 0.25) * (y - 0.25)) / (double)0.05f) +
+                    exp(-((y - 0.75) * (y - 0.75)) / (double)0.05f));
+        double p = 2.5;
+        double* c = &q[iq(ix, iy, iz)];
+        c[0] = d;
+        c[1] = d * u;
+        c[2] = d * v;
+        c[3] = 0;
+        c[4] = .5 * d * ((u * u) + (v * v)) + p / (G.g - 1);
+        c[5] = p / pow(d, G.g - 1);
+      }
+  return 0;
+}
+
+/* SplitMix64 (Steele, Lea, Flood 2014), the seeded generator of the
+ * synthetic 3D Kelvin-Helmholtz workload. */
+static uint64_t splitmix64(uint64_t* x) {
+  uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+/* The 3D Kelvin-Helmholtz workload (no counterpart in the reference's ic/):
+ * slab |y - 0.5| < 0.25 with rho = 2, vx = +0.5, outside rho = 1,
+ * vx = -0.5, uniform p = 2.5, vz = 0 and
+ *   vy = amp * sum_{k=1..4} sin(2 pi k x + phi_k),
+ * phi_k = 2 pi u_k with u_k the top 53 bits of successive SplitMix64 draws
+ * from `seed`.  Conserved fields as in ic/kevinhelmholtz.f90:61-66. */
+int orc_ic_kh3d(double* q, uint64_t seed, double amp) {
+  const double twopi = 6.283185307179586;
+  double phi[4];
+  uint64_t st = seed;
+  for (int k = 0; k < 4; ++k) phi[k] = twopi * ((double)(splitmix64(&st) >> 11) * 0x1.0p-53);
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double x = G.x0 + (double)(ix - 1) * G.dx;
+        double y = G.y0 + (double)(iy - 1) * G.dy;
+        double d, u;
+        if (fabs(y - 0.5) < 0.25) { d = 2.0; u = 0.5; } else { d = 1.0; u = -0.5; }
+        double v = 0.0;
+        for (int k = 0; k < 4; ++k) v += sin(twopi * (double)(k + 1) * x + phi[k]);
+        v = amp * v;
+        double p = 2.5;
+        double* c = &q[iq(ix, iy, iz)];
+        c[0] = d;
+        c[1] = d * u;
+        c[2] = d * v;
+        c[3] = 0.0;
+        c[4] = 0.5 * d * ((u * u) + (v * v)) + p / G.g1;
+        c[5] = p / pow(d, G.g1);
+      }
+  return 0;
+}

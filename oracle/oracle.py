@@ -1,0 +1,223 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/_build/libevora_oracle.so (the plain-C FP64 restatement of the
+evora hydro update, evora_oracle.c), building it with make if it is missing.
+Only tests/, __graft_entry__.smoke() and the CPU legs of bench.py use this
+module, as the checker and the CPU baseline; the product never imports it.
+
+Array shapes follow the reference's column-major layouts read in C order:
+  q   (nz, ny, nx, 6)            q(6, nx, ny, nz)                main.f90:72
+  w   (nz+4, ny+4, nx+4, 5)      w(5, -1:nx+2, -1:ny+2, -1:nz+2) main.f90:73
+  evo (nz+2, ny+2, nx+2, 5)      evo(5, 0:nx+1, ...)             main.f90:74
+  s   (nz+2, ny+2, nx+2, 3, 5)   s(5, 3, 0:nx+1, ...)            main.f90:75
+The oracle keeps one set of module-global parameters (like `use global`), so
+every call works on the grid last passed to `Oracle.__init__`/`configure`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libevora_oracle.so")
+_lock = threading.Lock()
+_lib = None
+
+c_int = ctypes.c_int
+c_double = ctypes.c_double
+c_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class OracleParams(ctypes.Structure):
+    """evora_params of include/evora_gpu.h (the &para subset)."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("solver", ctypes.c_int32), ("limiter", ctypes.c_int32),
+        ("boundtype", ctypes.c_int32), ("secondorder", ctypes.c_int32),
+        ("dualenergy", ctypes.c_int32), ("atomic", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("g", c_double), ("cfl", c_double), ("de_thresh", c_double),
+        ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
+        ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
+        ("tstart", c_double), ("tend", c_double),
+    ]
+
+
+class OracleDerived(ctypes.Structure):
+    _fields_ = [(n, c_double) for n in (
+        "g", "g1", "g1inv", "gg1", "cfl", "de_thresh1", "dx", "dy", "dz",
+        "dxinv", "dyinv", "dzinv", "x0", "y0", "z0", "volume")] + [
+        ("onedimension", ctypes.c_int32), ("twodimension", ctypes.c_int32)]
+
+
+def build():
+    """Compile the oracle library (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            src = os.path.join(_HERE, "evora_oracle.c")
+            if (not os.path.exists(_LIB_PATH)
+                    or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)):
+                build()
+            L = ctypes.CDLL(_LIB_PATH)
+            L.orc_compparameter.argtypes = [ctypes.POINTER(OracleParams)]
+            L.orc_get_derived.argtypes = [ctypes.POINTER(OracleDerived)]
+            L.orc_primitive.argtypes = [_dp, _dp]
+            L.orc_bound.argtypes = [_dp]
+            L.orc_hydrostep.argtypes = [_dp, c_double]
+            L.orc_hydrostep.restype = c_double
+            L.orc_updatetime.argtypes = [ctypes.POINTER(c_int), _dp, _dp]
+            L.orc_compevo.argtypes = [_dp, _dp, _dp, c_double]
+            L.orc_sweep.argtypes = [_dp, _dp, _dp, _dp, c_double]
+            L.orc_riemann_single.argtypes = [_dp, _dp, _dp, c_int]
+            L.orc_run.argtypes = [_dp, c_int, _dp, ctypes.POINTER(c_int), _dp,
+                                  ctypes.POINTER(c_int)]
+            L.orc_ic_shocktube.argtypes = [_dp] + [c_double] * 7 + [c_int]
+            L.orc_ic_kh2d.argtypes = [_dp]
+            L.orc_ic_kh3d.argtypes = [_dp, ctypes.c_uint64, c_double]
+            L.orc_set_threads.argtypes = [c_int]
+            _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def make_params(**kw) -> OracleParams:
+    """Parameters with the readparameter defaults (parameter.f90:41-82),
+    overridden by keyword arguments."""
+    p = OracleParams()
+    p.nx = p.ny = p.nz = 32
+    p.solver, p.limiter, p.boundtype = 2, 1, 2
+    p.secondorder, p.dualenergy, p.atomic = 1, 0, 0
+    p.g = float(np.float32(1.4))
+    p.cfl = 0.5
+    p.de_thresh = 0.0
+    p.xmin = p.ymin = p.zmin = 0.0
+    p.xmax = p.ymax = p.zmax = 1.0
+    p.tstart, p.tend = 0.0, 1.0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Oracle:
+    """The module-global state of the oracle for one grid."""
+
+    def __init__(self, params: OracleParams | None = None, **kw):
+        self.L = lib()
+        self.configure(params if params is not None else make_params(**kw))
+
+    def configure(self, params: OracleParams):
+        self.p = params
+        rc = self.L.orc_compparameter(ctypes.byref(params))
+        if rc:
+            raise ValueError(f"oracle compparameter rejected parameters (status {rc})")
+        self.d = OracleDerived()
+        self.L.orc_get_derived(ctypes.byref(self.d))
+        self.L.orc_clear_error()
+
+    # -- shapes ------------------------------------------------------------
+    @property
+    def shape_q(self):
+        p = self.p
+        return (p.nz, p.ny, p.nx, 6)
+
+    @property
+    def shape_w(self):
+        p = self.p
+        return (p.nz + 4, p.ny + 4, p.nx + 4, 5)
+
+    @property
+    def shape_evo(self):
+        p = self.p
+        return (p.nz + 2, p.ny + 2, p.nx + 2, 5)
+
+    @property
+    def shape_s(self):
+        p = self.p
+        return (p.nz + 2, p.ny + 2, p.nx + 2, 3, 5)
+
+    def zeros_q(self):
+        return np.zeros(self.shape_q)
+
+    # -- error word --------------------------------------------------------
+    def error(self) -> int:
+        return int(self.L.orc_error())
+
+    def clear_error(self):
+        self.L.orc_clear_error()
+
+    def set_threads(self, n: int):
+        self.L.orc_set_threads(int(n))
+
+    def max_threads(self) -> int:
+        return int(self.L.orc_max_threads())
+
+    # -- the reference routines --------------------------------------------
+    def primitive(self, w, q):
+        self.L.orc_primitive(_ptr(w), _ptr(q))
+
+    def bound(self, w):
+        self.L.orc_bound(_ptr(w))
+
+    def hydrostep(self, w, dt_in=1e99) -> float:
+        return float(self.L.orc_hydrostep(_ptr(w), float(dt_in)))
+
+    def updatetime(self, t: float, dt: float):
+        go = c_int(1)
+        tt, dd = c_double(t), c_double(dt)
+        self.L.orc_updatetime(ctypes.byref(go), ctypes.byref(tt), ctypes.byref(dd))
+        return bool(go.value), tt.value, dd.value
+
+    def compevo(self, w, evo, s, dt):
+        self.L.orc_compevo(_ptr(w), _ptr(evo), _ptr(s), float(dt))
+
+    def sweep(self, w, q, evo, s, dt):
+        self.L.orc_sweep(_ptr(w), _ptr(q), _ptr(evo), _ptr(s), float(dt))
+
+    def riemann(self, wl, wr, direction: int):
+        wl = np.ascontiguousarray(wl, dtype=np.float64)
+        wr = np.ascontiguousarray(wr, dtype=np.float64)
+        f = np.zeros(6)
+        self.L.orc_riemann_single(_ptr(wl), _ptr(wr), _ptr(f), int(direction))
+        return f
+
+    def run(self, q, max_steps: int):
+        """The hydro loop of main.f90:109-155 on q (in place).
+        Returns dict(t, steps, dt, go, status)."""
+        t, dt = c_double(0.0), c_double(0.0)
+        steps, go = c_int(0), c_int(0)
+        st = self.L.orc_run(_ptr(q), int(max_steps), ctypes.byref(t), ctypes.byref(steps),
+                            ctypes.byref(dt), ctypes.byref(go))
+        return dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), status=int(st))
+
+    # -- initial conditions -------------------------------------------------
+    def ic_shocktube(self, dl, ul, pl, dr, ur, pr, x_diss, direction=1):
+        q = self.zeros_q()
+        rc = self.L.orc_ic_shocktube(_ptr(q), dl, ul, pl, dr, ur, pr, x_diss, int(direction))
+        if rc:
+            raise ValueError("bad shocktube direction")
+        return q
+
+    def ic_kh2d(self):
+        q = self.zeros_q()
+        self.L.orc_ic_kh2d(_ptr(q))
+        return q
+
+    def ic_kh3d(self, seed=42, amp=0.01):
+        q = self.zeros_q()
+        self.L.orc_ic_kh3d(_ptr(q), int(seed), float(amp))
+        return q

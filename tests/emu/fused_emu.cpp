@@ -1,0 +1,67 @@
+// Host emulation of the fused CUDA kernels (test harness): the tile program
+// of evora_b200/csrc/fused_kernel.cuh compiled with g++, each CTA's threads
+// run as std::threads meeting at a std::barrier.  With -ffp-contract=off
+// the arithmetic is the reference's, so its output must equal the CPU oracle
+// bit for bit; a difference points at the tiling, halo or boundary logic.
+#define EVORA_HOST_EMU 1
+#define EVORA_FNS emu
+#include "../../evora_b200/csrc/fused_kernel.cuh"
+
+#include <memory>
+#include <thread>
+#include <vector>
+
+thread_local std::barrier<>* evora_emu::tl_barrier = nullptr;
+
+using namespace evora;
+using namespace evora::emu;
+
+template <int NF, int DIM, int TX, int TY, int ZC>
+static void run_tiles(const FusedArgs<double>& A) {
+  constexpr int NT = TX * TY;
+  const HydroParams& P = A.P;
+  const int gx = (P.nx + TX - 1) / TX, gy = (P.ny + TY - 1) / TY;
+  const int gz = DIM == 3 ? (P.nz + ZC - 1) / ZC : 1;
+  auto sm = std::make_unique<FusedSmem<double, NF, TX, TY>>();
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) {
+        std::barrier<> bar(NT);
+        std::vector<std::thread> th;
+        th.reserve(NT);
+        for (int t = 0; t < NT; ++t)
+          th.emplace_back([&, t] {
+            evora_emu::tl_barrier = &bar;
+            fused_tile<double, NF, DIM, TX, TY, ZC>(A, *sm, t, bx, by, bz);
+          });
+        for (auto& x : th) x.join();
+      }
+}
+
+extern "C" int emu_fused_update(const HydroParams* P, int nf, const double* qin, double* qout, double dt,
+                                int tile) {
+  GridCtl ctl{};
+  ctl.dt = dt;
+  ctl.go = 1;
+  ctl.active = 1;
+  const int dim = P->onedimension ? 1 : (P->twodimension ? 2 : 3);
+  FusedArgs<double> A{*P, qin, qout, &ctl, (int64_t)P->nx * P->ny * P->nz};
+  if (dim == 1) {
+    for (int i = 0; i < P->nx; ++i) {
+      if (nf == 5) fused_cell1d<double, 5>(A, i);
+      else fused_cell1d<double, 6>(A, i);
+    }
+    return (int)ctl.err;
+  }
+#define RUN(NF, DIM)                                            \
+  do {                                                          \
+    if (tile == 0) run_tiles<NF, DIM, 8, 4, 4>(A);              \
+    else run_tiles<NF, DIM, 32, 4, 32>(A);                      \
+  } while (0)
+  if (nf == 5 && dim == 2) RUN(5, 2);
+  else if (nf == 5) RUN(5, 3);
+  else if (dim == 2) RUN(6, 2);
+  else RUN(6, 3);
+#undef RUN
+  return (int)ctl.err;
+}

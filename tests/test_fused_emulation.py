@@ -1,0 +1,81 @@
+"""The tile program of the fused CUDA kernel (evora_b200/csrc/fused_kernel.cuh),
+compiled for the host with g++ (tests/emu, one std::thread per CUDA thread,
+std::barrier for __syncthreads) and without FMA contraction, must reproduce
+the oracle's step bit for bit: tiling, halos, ring cells, the z march and the
+boundary index maps may not change a single bit of the reference result."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, make_params
+from helpers import oracle_step, random_q
+
+EMU = os.path.join(os.path.dirname(__file__), "emu")
+
+
+class HP(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in
+                "nx ny nz solver limiter boundtype secondorder dualenergy onedimension twodimension".split()] + \
+               [(n, ctypes.c_double) for n in "g g1 g1inv gg1 cfl de_thresh1 dx dy dz dxinv dyinv dzinv".split()]
+
+
+@pytest.fixture(scope="module")
+def emu():
+    subprocess.run(["make", "-s", "-C", EMU], check=True)
+    L = ctypes.CDLL(os.path.join(EMU, "_build", "libfused_emu.so"))
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.emu_fused_update.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int]
+    return L
+
+
+def hp_of(o):
+    h = HP()
+    for k in "nx ny nz solver limiter boundtype secondorder dualenergy".split():
+        setattr(h, k, getattr(o.p, k))
+    h.onedimension, h.twodimension = o.d.onedimension, o.d.twodimension
+    for k in "g g1 g1inv gg1 cfl de_thresh1 dx dy dz dxinv dyinv dzinv".split():
+        setattr(h, k, getattr(o.d, k))
+    return h
+
+
+CASES = [
+    # nx, ny, nz, boundtype, nf, limiter, solver, tile, secondorder
+    (16, 12, 8, 2, 5, 1, 2, 0, 1),
+    (13, 11, 9, 2, 5, 1, 2, 0, 1),
+    (13, 11, 9, 1, 5, 1, 2, 0, 1),
+    (13, 11, 9, 3, 5, 1, 2, 0, 1),
+    (40, 9, 35, 3, 5, 1, 2, 1, 1),
+    (16, 16, 1, 2, 5, 1, 2, 0, 1),
+    (21, 13, 1, 3, 5, 1, 2, 0, 1),
+    (64, 1, 1, 1, 5, 1, 2, 0, 1),
+    (37, 1, 1, 3, 5, 1, 2, 0, 1),
+    (13, 11, 9, 2, 6, 1, 2, 0, 1),
+    (13, 11, 9, 1, 5, 2, 2, 0, 1),
+    (13, 11, 9, 1, 5, 3, 1, 0, 1),
+    (13, 11, 9, 3, 5, 2, 1, 0, 1),
+    (21, 13, 1, 3, 6, 3, 1, 0, 1),
+    (13, 11, 9, 2, 5, 1, 2, 0, 0),
+    (64, 1, 1, 1, 5, 1, 2, 0, 0),
+    (2, 2, 2, 2, 5, 1, 2, 0, 1),      # smallest 3D grid: ghosts wrap twice
+    (2, 3, 1, 1, 6, 2, 2, 0, 1),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-bt{c[3]}-nf{c[4]}-l{c[5]}-s{c[6]}-t{c[7]}-o{c[8]}")
+def test_emulated_fused_step_is_bitwise_oracle(emu, case):
+    nx, ny, nz, bt, nf, lim, sol, tile, so = case
+    o = Oracle(make_params(nx=nx, ny=ny, nz=nz, boundtype=bt, limiter=lim, solver=sol, g=5 / 3, cfl=0.4,
+                           secondorder=so))
+    q = random_q(o, np.random.default_rng(nx * 131 + ny * 7 + nz))
+    q2, dt, _ = oracle_step(o, q)
+    assert o.error() == 0
+    n = nx * ny * nz
+    qin = np.ascontiguousarray(q.reshape(n, 6).T[:nf])
+    qout = np.zeros_like(qin)
+    dp = ctypes.POINTER(ctypes.c_double)
+    err = emu.emu_fused_update(ctypes.byref(hp_of(o)), nf, qin.ctypes.data_as(dp), qout.ctypes.data_as(dp), dt, tile)
+    assert err == 0
+    np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
