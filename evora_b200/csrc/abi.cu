@@ -194,8 +194,9 @@ int begin(DropinState& S) {
   if (S.device != dev || !S.d_err) {
     if (S.d_err) cudaFree(S.d_err);
     S.d_err = nullptr;
-    CU(cudaMalloc(&S.d_err, sizeof(unsigned) + 3 * sizeof(unsigned long long)));
-    S.d_smax = reinterpret_cast<unsigned long long*>(S.d_err + 2);
+    // [0]: error word; [8, 32): the three CFL maxima
+    CU(cudaMalloc(&S.d_err, 8 + 3 * sizeof(unsigned long long)));
+    S.d_smax = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(S.d_err) + 8);
     for (auto& b : S.stage) {
       if (b) cudaFree(b);
       b = nullptr;
