@@ -20,6 +20,8 @@ void set_cuda_error(cudaError_t e, const char* where) {
   std::snprintf(g_last_error, sizeof g_last_error, "%s: %s", where, cudaGetErrorString(e));
 }
 
+void set_error_message(const char* msg) { std::snprintf(g_last_error, sizeof g_last_error, "%s", msg); }
+
 bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, int* status) {
   evora_derived dd;
   int rc = evora_compparameter(p, &dd);
@@ -219,6 +221,14 @@ int finish(DropinState& S) {
 const DropinOps& ops(const DropinState& S) { return S.strict ? evora::strict::kOps : evora::fast::kOps; }
 
 }  // namespace
+
+bool evora::dropin_params(HydroParams* P) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return false;
+  *P = S.P;
+  return true;
+}
 
 extern "C" {
 

@@ -17,4 +17,10 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
 // True for device or managed memory.
 bool is_device_pointer(const void* ptr);
 
+// Records a message for evora_last_error().
+void set_error_message(const char* msg);
+
+// The module-global parameters set by evora_set_params (false if unset).
+bool dropin_params(HydroParams* P);
+
 }  // namespace evora

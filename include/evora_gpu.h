@@ -136,6 +136,22 @@ int evora_bound(double* w);
  * Returns EVORA_ERR_DT if the result is <= 0. */
 int evora_hydrostep(const double* w, double* dt);
 
+/* A variant of evora_hydrostep that allocates nothing (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc: a driver that
+ * allocates all device memory at start-up and none inside its time loop, or
+ * code running while a memory pool owns the device or other work is being
+ * captured.  Same arithmetic and result as evora_hydrostep, bit for bit.
+ * Differences: w must be device memory (no staging copy is made); the
+ * reduction scratch is a fixed file-scope device array (about 1.5 MB, held by
+ * every GPU that loads the library until exit), which limits the grid to
+ * nx*ny*nz <= 16777216 interior cells -- larger grids return EVORA_ERR_ARG
+ * with a message in evora_last_error().  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (concurrent host threads or
+ * streams) race on it.  Synchronous: returns after dt is known. */
+int evora_hydrostep_noalloc(const double* w, double* dt);
+
 /* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch:
  * if tend - t <= dt then dt = tend - t, go = false; then t = t + dt.
  * dump and k are accepted for signature parity (they only matter in the
