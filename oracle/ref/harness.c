@@ -1,0 +1,162 @@
+/*
+ * harness.c -- TEST INFRASTRUCTURE ONLY.  Drives the mechanical C
+ * translation of the reference's Fortran (oracle/_ref/evora_ref.c, made by
+ * oracle/ref/f2c.py from the reference sources) the way main.f90 does:
+ * namelist values -> compparameter -> decomposition, then the hydro subset
+ * of the time loop (main.f90:109-155).  The routines the translation calls
+ * but that are not part of the hydro path (cleanstop, MPI broadcasts, the
+ * comoving time iteration) are provided here; a Fortran `stop` returns to
+ * the caller through longjmp with a nonzero status.
+ */
+#include <setjmp.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/evora_gpu.h"
+#include "../_ref/evora_ref.c"
+
+static jmp_buf g_jmp;
+static int g_armed = 0;
+
+void ref_stop(void) {
+  if (g_armed) longjmp(g_jmp, 1);
+  abort();
+}
+void ref_cleanstop(void) { ref_stop(); }
+void ref_bcastdouble(double* x) { (void)x; }
+void ref_timestepiteration(double* z) { (void)z; ref_stop(); }
+
+/* &ic_para of ic/shocktube.f90:39 */
+static double nml_dl = 1.0, nml_ul = 0.0, nml_pl = 1.0, nml_dr = 0.125, nml_ur = 0.0, nml_pr = 0.1,
+              nml_x_diss = 0.5;
+static int nml_dir = 1;
+void ref_namelist_ic_para(double* dl, double* ul, double* pl, double* dr, double* ur, double* pr,
+                          double* x_diss, int* dir) {
+  *dl = nml_dl; *ul = nml_ul; *pl = nml_pl; *dr = nml_dr; *ur = nml_ur; *pr = nml_pr;
+  *x_diss = nml_x_diss; *dir = nml_dir;
+}
+
+#define GUARD(body)            \
+  do {                         \
+    if (setjmp(g_jmp)) {       \
+      g_armed = 0;             \
+      return 1;                \
+    }                          \
+    g_armed = 1;               \
+    body;                      \
+    g_armed = 0;               \
+  } while (0)
+
+/* readparameter defaults (parameter.f90:41-82) for the namelist variables
+ * that compparameter and decomposition read, then the hydro subset from p;
+ * a single rank (startstop.f90:59-63 with mpisize = 1). */
+int ref_setup_c(const evora_params* p) {
+  G_iconly = 0; G_hydro = 1;
+  G_secondorder = p->secondorder; G_solver = p->solver; G_limiter = p->limiter;
+  G_cfl = p->cfl; G_g = p->g; G_atomic = p->atomic;
+  G_nx = p->nx; G_ny = p->ny; G_nz = p->nz;
+  G_xmin = p->xmin; G_xmax = p->xmax; G_ymin = p->ymin; G_ymax = p->ymax;
+  G_zmin = p->zmin; G_zmax = p->zmax;
+  G_boundtype = p->boundtype;
+  G_gravity = 0;
+  G_tstart = p->tstart; G_tend = p->tend;
+  G_supercomoving = 0; G_c_cosmo = 0.1f; G_omega0 = 1.0f; G_lambda0 = 0.0f; G_hubble0 = 50.0f;
+  G_fb = 1.0f; G_box = 1.0f; G_zstart = 99.0f; G_zend = 0.0f;
+  G_chemistry = 0; G_noncie = 0; G_cooling = 0; G_background = 0;
+  G_conduction = 0;
+  G_dualenergy = p->dualenergy; G_de_thresh = p->de_thresh;
+  G_mpisize = 1; G_mpirank = 0; G_master = 1; G_parallel = 0;
+  G_local_x_start = 0; G_local_nx = p->nz;
+  G_redshift = 0.0;
+  GUARD(ref_compparameter(); ref_decomposition());
+  return 0;
+}
+
+void ref_sizes_c(int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
+  *nq = (int64_t)G_nq * G_nx * G_ny * G_nz;
+  *nw = (int64_t)G_nw * (G_nx + 4) * (G_ny + 4) * (G_nz + 4);
+  *ne = (int64_t)G_nw * (G_nx + 2) * (G_ny + 2) * (G_nz + 2);
+  *ns = (int64_t)G_nw * 3 * (G_nx + 2) * (G_ny + 2) * (G_nz + 2);
+}
+
+void ref_derived_c(double* out) {
+  double v[] = {G_g, G_g1, G_g1inv, G_gg1, G_cfl, G_de_thresh1, G_dx, G_dy, G_dz,
+                G_dxinv, G_dyinv, G_dzinv, G_x0, G_y0, G_z0, G_volume};
+  memcpy(out, v, sizeof v);
+}
+
+int ref_primitive_c(double* w, double* q) { GUARD(ref_primitive(w, q)); return 0; }
+int ref_bound_c(double* w) { GUARD(ref_bound(w)); return 0; }
+int ref_hydrostep_c(double* w, double* dt) {
+  G_dt = *dt;
+  GUARD(ref_hydrostep(w));
+  *dt = G_dt;
+  return 0;
+}
+int ref_updatetime_c(int* go, double* t, double* dt) {
+  int dump = 0, k4 = 1;
+  G_t = *t; G_dt = *dt;
+  GUARD(ref_updatetime(go, &dump, &k4));
+  *t = G_t; *dt = G_dt;
+  return 0;
+}
+int ref_compevo_c(double* w, double* evo, double* s, double dt) {
+  G_dt = dt;
+  GUARD(ref_compevo(w, evo, s));
+  return 0;
+}
+int ref_sweep_c(double* w, double* q, double* evo, double* s, double dt) {
+  G_dt = dt;
+  GUARD(ref_sweep(w, q, evo, s));
+  return 0;
+}
+
+/* main.f90:109-155, hydro subset: no cooling, conduction, gravity,
+ * chemistry, expansion or output. */
+int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* go_out) {
+  int64_t nq, nw, ne, ns;
+  ref_sizes_c(&nq, &nw, &ne, &ns);
+  double* w = calloc((size_t)nw, sizeof(double));
+  double* evo = calloc((size_t)ne, sizeof(double));
+  double* s = calloc((size_t)ns, sizeof(double));
+  int go = 1, dump = 0, k = 0, k4 = 1, rc = 0;
+  G_t = G_tstart;
+  if (setjmp(g_jmp)) {
+    g_armed = 0;
+    rc = 1;
+    goto done;
+  }
+  g_armed = 1;
+  while (go && k < max_steps) {
+    ref_primitive(w, q);
+    ref_bound(w);
+    G_dt = 1e99;
+    if (G_hydro) ref_hydrostep(w);
+    ref_updatetime(&go, &dump, &k4);
+    if (G_secondorder) ref_compevo(w, evo, s);
+    if (G_hydro) ref_sweep(w, q, evo, s);
+    k = k + 1;
+  }
+  g_armed = 0;
+done:
+  *t = G_t;
+  *dt = G_dt;
+  *steps = k;
+  if (go_out) *go_out = go;
+  free(w); free(evo); free(s);
+  return rc;
+}
+
+int ref_ic_shocktube_c(double* q, double dl, double ul, double pl, double dr, double ur, double pr,
+                       double x_diss, int dir) {
+  nml_dl = dl; nml_ul = ul; nml_pl = pl; nml_dr = dr; nml_ur = ur; nml_pr = pr;
+  nml_x_diss = x_diss; nml_dir = dir;
+  GUARD(ref_ic_shocktube(q));
+  return 0;
+}
+int ref_ic_kh_c(double* q) { GUARD(ref_ic_kevinhelmholtz(q)); return 0; }
+int ref_riemann_c(double* wl, double* wr, double* f, int dir) {
+  GUARD(ref_riemannsolver(wl, wr, f, &dir));
+  return 0;
+}

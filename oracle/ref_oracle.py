@@ -1,0 +1,138 @@
+"""ctypes front end of oracle/_ref/libevora_ref.so -- TEST INFRASTRUCTURE ONLY.
+
+libevora_ref.so is the reference's own Fortran hydro path translated
+mechanically to C (oracle/ref/f2c.py) plus a harness that drives it like
+main.f90 (oracle/ref/harness.c).  It pins the hand-written oracle
+(evora_oracle.c) to the reference's sources.  The library is built here from
+the sources under /root/reference (make -C oracle/ref); elsewhere the
+prebuilt copy is used.  Same method names and array shapes as oracle.Oracle.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from .oracle import OracleParams, make_params  # noqa: F401  (re-exported for tests)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libevora_ref.so")
+REF_SOURCES = "/root/reference/source"
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH) or os.path.isdir(REF_SOURCES)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if os.path.isdir(REF_SOURCES):
+            subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref")], check=True)
+        L = ctypes.CDLL(LIB_PATH)
+        L.ref_setup_c.argtypes = [ctypes.POINTER(OracleParams)]
+        L.ref_sizes_c.argtypes = [ctypes.POINTER(ctypes.c_int64)] * 4
+        L.ref_derived_c.argtypes = [_dp]
+        L.ref_primitive_c.argtypes = [_dp, _dp]
+        L.ref_bound_c.argtypes = [_dp]
+        L.ref_hydrostep_c.argtypes = [_dp, _dp]
+        L.ref_updatetime_c.argtypes = [_ip, _dp, _dp]
+        L.ref_compevo_c.argtypes = [_dp, _dp, _dp, ctypes.c_double]
+        L.ref_sweep_c.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_double]
+        L.ref_run_c.argtypes = [_dp, ctypes.c_int, _dp, _ip, _dp, _ip]
+        L.ref_ic_shocktube_c.argtypes = [_dp] + [ctypes.c_double] * 7 + [ctypes.c_int]
+        L.ref_ic_kh_c.argtypes = [_dp]
+        L.ref_riemann_c.argtypes = [_dp, _dp, _dp, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class RefOracle:
+    """The translated reference for one grid (module global state)."""
+
+    def __init__(self, params: OracleParams | None = None, **kw):
+        self.L = lib()
+        self.p = params if params is not None else make_params(**kw)
+        if self.L.ref_setup_c(ctypes.byref(self.p)):
+            raise ValueError("the reference stopped in compparameter/decomposition")
+        d = np.zeros(16)
+        self.L.ref_derived_c(_p(d))
+        self.derived = dict(zip(["g", "g1", "g1inv", "gg1", "cfl", "de_thresh1", "dx", "dy", "dz",
+                                 "dxinv", "dyinv", "dzinv", "x0", "y0", "z0", "volume"], d))
+
+    @property
+    def shape_q(self):
+        return (self.p.nz, self.p.ny, self.p.nx, 6)
+
+    @property
+    def shape_w(self):
+        return (self.p.nz + 4, self.p.ny + 4, self.p.nx + 4, 5)
+
+    @property
+    def shape_evo(self):
+        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, 5)
+
+    @property
+    def shape_s(self):
+        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, 3, 5)
+
+    def zeros_q(self):
+        return np.zeros(self.shape_q)
+
+    def primitive(self, w, q):
+        return self.L.ref_primitive_c(_p(w), _p(q))
+
+    def bound(self, w):
+        return self.L.ref_bound_c(_p(w))
+
+    def hydrostep(self, w, dt_in=1e99):
+        d = ctypes.c_double(dt_in)
+        st = self.L.ref_hydrostep_c(_p(w), ctypes.byref(d))
+        return d.value, st
+
+    def updatetime(self, t, dt):
+        go = ctypes.c_int(1)
+        tt, dd = ctypes.c_double(t), ctypes.c_double(dt)
+        self.L.ref_updatetime_c(ctypes.byref(go), ctypes.byref(tt), ctypes.byref(dd))
+        return bool(go.value), tt.value, dd.value
+
+    def compevo(self, w, evo, s, dt):
+        return self.L.ref_compevo_c(_p(w), _p(evo), _p(s), float(dt))
+
+    def sweep(self, w, q, evo, s, dt):
+        return self.L.ref_sweep_c(_p(w), _p(q), _p(evo), _p(s), float(dt))
+
+    def riemann(self, wl, wr, direction):
+        wl = np.ascontiguousarray(wl, dtype=np.float64)
+        wr = np.ascontiguousarray(wr, dtype=np.float64)
+        f = np.zeros(6)
+        st = self.L.ref_riemann_c(_p(wl), _p(wr), _p(f), int(direction))
+        return f, st
+
+    def run(self, q, max_steps):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        steps, go = ctypes.c_int(), ctypes.c_int()
+        st = self.L.ref_run_c(_p(q), int(max_steps), ctypes.byref(t), ctypes.byref(steps),
+                              ctypes.byref(dt), ctypes.byref(go))
+        return dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), stopped=int(st))
+
+    def ic_shocktube(self, dl, ul, pl, dr, ur, pr, x_diss, direction=1):
+        q = self.zeros_q()
+        if self.L.ref_ic_shocktube_c(_p(q), dl, ul, pl, dr, ur, pr, x_diss, int(direction)):
+            raise ValueError("the reference stopped in ic")
+        return q
+
+    def ic_kh2d(self):
+        q = self.zeros_q()
+        self.L.ref_ic_kh_c(_p(q))
+        return q
