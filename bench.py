@@ -41,6 +41,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NX = NY = NZ = 256
+AUTOTUNE = True
 GAMMA = 5.0 / 3.0
 CFL = 0.5
 METRIC = "cell-updates/s"
@@ -171,6 +172,7 @@ def time_grid(ev, torch, q, precision, steps, warmup, stream):
     g = ev.Grid(kh_params(ev), precision)
     g.set_stream(stream)
     g.set_q(q)
+    g.tuning = g.autotune(reps=3) if AUTOTUNE else (0, [])
     g.step(warmup, sync=True)
     torch.cuda.synchronize()
     g.set_timing(True)
@@ -277,9 +279,11 @@ def main():
     ap.add_argument("--size", type=int, default=256,
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
     args = ap.parse_args()
-    global NX, NY, NZ
+    global NX, NY, NZ, AUTOTUNE
     NX = NY = NZ = args.size
+    AUTOTUNE = not args.no_autotune
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -311,6 +315,7 @@ def main():
                           "unit": METRIC, "note": "profiling run (FP32 only)"}), flush=True)
         return 0
     # accuracy of the FP32 form against FP64 after the same steps
+    tune32, tune64 = g32.tuning, g64.tuning
     r32 = g32.get_q()[..., 0]
     r64 = g64.get_q()[..., 0]
     l1 = float(np.abs(r32 - r64).sum() / np.abs(r64).sum())
@@ -342,6 +347,8 @@ def main():
         "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                  "roofline": roofline(kt64, "f64", "fused_update_kh256_fp64.md")},
         "fp32_over_fp64": value32 / value64,
+        "autotune": {"fp32": {"chosen": tune32[0], "ms_per_tile": tune32[1]},
+                     "fp64": {"chosen": tune64[0], "ms_per_tile": tune64[1]}},
         "l1_density_fp32_vs_fp64": l1,
         "gpu_launches": kt32["launches"],
         "clocks": clocks,

@@ -108,6 +108,8 @@ def _declare(L):
         "evora_grid_time": ([G, _dp, _dp, ctypes.POINTER(c_int32), ctypes.POINTER(c_int64)], c_int32),
         "evora_grid_status": ([G], c_int32),
         "evora_grid_totals": ([G, _dp], c_int32),
+        "evora_grid_autotune": ([G, c_int32, ctypes.POINTER(c_int32), _dp, c_int32], c_int32),
+        "evora_grid_set_tile": ([G, c_int32], c_int32),
         "evora_grid_set_timing": ([G, c_int32], c_int32),
         "evora_grid_timing": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], c_int32),
     }

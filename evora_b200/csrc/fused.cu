@@ -2,6 +2,7 @@
 // (structure-of-arrays) backend.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/evora_gpu.h"
@@ -9,6 +10,36 @@
 #include "fused.h"
 
 namespace evora {
+
+namespace {
+struct Inst {
+  FusedLaunch (*pick)(int, int, int, int*, int*, int*, size_t*, int*);
+  int (*tiles)();
+  void (*cfl)(const FusedPlan&, const void*, GridCtl*, cudaStream_t);
+};
+Inst inst_of(int precision, int strict) {
+  if (precision == EVORA_FP32) return {f32::pick, f32::tiles, f32::cfl};
+  if (strict) return {f64s::pick, f64s::tiles, f64s::cfl};
+  return {f64::pick, f64::tiles, f64::cfl};
+}
+}  // namespace
+
+void fused_set_tile(FusedPlan* pl, int tile) {
+  const Inst in = inst_of(pl->precision, pl->strict);
+  if (tile < 0 || tile >= in.tiles()) tile = 0;
+  pl->tile = tile;
+  pl->launch = in.pick(pl->nf, pl->dim, tile, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads);
+  const HydroParams& P = pl->P;
+  if (pl->dim == 1) {
+    int64_t b = (P.nx + 127) / 128;
+    pl->grid = dim3((unsigned)(b < 1 ? 1 : b), 1, 1);
+  } else {
+    pl->grid = dim3((P.nx + pl->tx - 1) / pl->tx, (P.ny + pl->ty - 1) / pl->ty,
+                    pl->dim == 3 ? (P.nz + pl->zc - 1) / pl->zc : 1);
+  }
+}
+
+int fused_tiles(const FusedPlan& pl) { return inst_of(pl.precision, pl.strict).tiles(); }
 
 int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* pl) {
   *pl = FusedPlan{};
@@ -18,28 +49,14 @@ int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPla
   pl->strict = strict;
   pl->dim = P.onedimension ? 1 : (P.twodimension ? 2 : 3);
   pl->n = (int64_t)P.nx * P.ny * P.nz;
-  FusedLaunch (*pick)(int, int, int*, int*, int*, size_t*, int*);
-  if (precision == EVORA_FP32) {
-    pick = f32::pick;
-    pl->cfl = f32::cfl;
-  } else if (strict) {
-    pick = f64s::pick;
-    pl->cfl = f64s::cfl;
-  } else {
-    pick = f64::pick;
-    pl->cfl = f64::cfl;
-  }
-  pl->launch = pick(nf, pl->dim, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads);
-  if (pl->dim == 1) {
-    int64_t b = (P.nx + 127) / 128;
-    pl->grid = dim3((unsigned)(b < 1 ? 1 : b), 1, 1);
-  } else {
-    pl->grid = dim3((P.nx + pl->tx - 1) / pl->tx, (P.ny + pl->ty - 1) / pl->ty,
-                    pl->dim == 3 ? (P.nz + pl->zc - 1) / pl->zc : 1);
-  }
+  if ((int64_t)P.nx * P.ny * P.nz >= ((int64_t)1 << 31)) return EVORA_ERR_ARG;  // in-field index is 32-bit
+  pl->cfl = inst_of(precision, strict).cfl;
+  int tile = 0;
+  if (const char* e = getenv("EVORA_TILE")) tile = atoi(e);
+  fused_set_tile(pl, tile);
   int64_t nb = (pl->n + 255) / 256;
   pl->nblk_tot = (int)(nb > 148 * 4 ? 148 * 4 : nb);
-  if (cudaMalloc(&pl->partials, sizeof(double) * 6 * pl->nblk_tot) != cudaSuccess) {
+  if (cudaMalloc(&pl->partials, sizeof(double) * 6 * (pl->nblk_tot + 1)) != cudaSuccess) {
     cudaGetLastError();
     return EVORA_ERR_NOMEM;
   }
@@ -142,19 +159,12 @@ void fused_to_aos(const FusedPlan& pl, const void* q, double* aos, cudaStream_t 
 
 static int totals_run(const void* q, bool f32, int64_t n, int nf, int aos, double g1, double* part, int nb,
                       double out[6], cudaStream_t st) {
-  double* dout = part + 6 * (nb - 1) + 6;  // not used: final goes to a small buffer below
-  (void)dout;
-  double* fin = nullptr;
-  if (cudaMalloc(&fin, 6 * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return EVORA_ERR_NOMEM;
-  }
+  double* fin = part + 6 * nb;   // part holds nb + 1 rows of six
   if (f32) k_totals_part<float><<<nb, 256, 0, st>>>((const float*)q, n, nf, aos, g1, part);
   else k_totals_part<double><<<nb, 256, 0, st>>>((const double*)q, n, nf, aos, g1, part);
   k_totals_final<<<1, 32, 0, st>>>(part, nb, fin);
   cudaError_t e = cudaMemcpyAsync(out, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(fin);
   if (e != cudaSuccess) {
     set_cuda_error(e, "totals");
     return EVORA_ERR_CUDA;
@@ -170,7 +180,7 @@ int fused_totals_aos(const double* aos, int64_t n, double out[6], cudaStream_t s
   int64_t nb64 = (n + 255) / 256;
   int nb = (int)(nb64 > 148 * 4 ? 148 * 4 : nb64);
   double* part = nullptr;
-  if (cudaMalloc(&part, sizeof(double) * 6 * nb) != cudaSuccess) {
+  if (cudaMalloc(&part, sizeof(double) * 6 * (nb + 1)) != cudaSuccess) {
     cudaGetLastError();
     return EVORA_ERR_NOMEM;
   }

@@ -20,6 +20,7 @@ struct FusedPlan {
   int strict = 0;
   int dim = 3;         // 1, 2 or 3
   int64_t n = 0;       // cells
+  int tile = 0;        // entry of the precision's tile table
   int tx = 0, ty = 0, zc = 0;
   size_t smem = 0;
   dim3 grid{1, 1, 1};
@@ -32,6 +33,9 @@ struct FusedPlan {
 
 // Chooses tiles and the kernel instantiation; allocates small scratch.
 int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* plan);
+// Number of tile shapes of the plan's precision, and switching between them.
+int fused_tiles(const FusedPlan& plan);
+void fused_set_tile(FusedPlan* plan, int tile);
 void fused_plan_free(FusedPlan* plan);
 
 // hydrostep part 1: per-axis maxima of |u_d| + a into ctl->smax (FP64).
@@ -53,7 +57,8 @@ int fused_totals_aos(const double* aos, int64_t n, double out[6], cudaStream_t s
 // Instantiation launchers (fused_f64.cu, fused_f64_strict.cu, fused_f32.cu).
 #define EVORA_DECLARE_FUSED_NS(ns)                                                           \
   namespace ns {                                                                             \
-  FusedLaunch pick(int nf, int dim, int* tx, int* ty, int* zc, size_t* smem, int* threads);   \
+  FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads); \
+  int tiles();                                                                               \
   void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st);                \
   }
 EVORA_DECLARE_FUSED_NS(f64)

@@ -3,7 +3,5 @@
 // kin > E/2, for the CFL reduction and for the conserved totals.
 #define EVORA_FNS f32
 #define EVORA_T float
-#define EVORA_TX 32
-#define EVORA_TY 8
-#define EVORA_ZC 32
+#define EVORA_PRECISION_F32 1
 #include "fused_inst.cuh"

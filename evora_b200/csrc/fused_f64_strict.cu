@@ -3,7 +3,5 @@
 // on rho, m and E (the entropy field goes through pow).
 #define EVORA_FNS f64s
 #define EVORA_T double
-#define EVORA_TX 32
-#define EVORA_TY 4
-#define EVORA_ZC 32
+#define EVORA_PRECISION_F32 0
 #include "fused_inst.cuh"

@@ -12,41 +12,70 @@ namespace evora {
 namespace EVORA_FNS {
 
 using TT = EVORA_T;
-constexpr int TX = EVORA_TX, TY = EVORA_TY, ZC = EVORA_ZC;
 
-template <int NF, int DIM>
+// Tile table of this precision: (TX, TY, ZC, CTAs per SM).  Entry 0 is the
+// default; evora_grid_autotune times all entries on the grid itself.  The
+// 5-field 3D kernel is instantiated for every entry, the other variants for
+// entry 0 only.
+template <int I> struct Tile;
+#if EVORA_PRECISION_F32
+template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3; };
+template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MINB = 3; };
+template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4; };
+#else
+template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3; };
+template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3; };
+template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3; };
+#endif
+constexpr int kTiles = 4;
+
+template <int NF, int DIM, int I>
 void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
   FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n};
   if constexpr (DIM == 1) {
     k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
   } else {
-    k_fused<TT, NF, DIM, TX, TY, ZC><<<pl.grid, pl.threads, pl.smem, st>>>(A);
+    using C = Tile<I>;
+    k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A);
   }
 }
 
-template <int NF, int DIM>
+template <int NF, int DIM, int I>
 FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads) {
   if constexpr (DIM == 1) {
     *tx = 128; *ty = 1; *zc = 1; *smem = 0; *threads = 128;
   } else {
-    *tx = TX; *ty = TY; *zc = DIM == 3 ? ZC : 1;
-    *smem = sizeof(FusedSmem<TT, NF, TX, TY>);
-    *threads = TX * TY;
-    cudaFuncSetAttribute(k_fused<TT, NF, DIM, TX, TY, ZC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)*smem);
+    using C = Tile<I>;
+    *tx = C::TX; *ty = C::TY; *zc = DIM == 3 ? C::ZC : 1;
+    *smem = sizeof(FusedSmem<TT, NF, C::TX, C::TY>);
+    *threads = C::TX * C::TY;
+    auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   }
-  return &launch<NF, DIM>;
+  return &launch<NF, DIM, I>;
 }
 
-FusedLaunch pick(int nf, int dim, int* tx, int* ty, int* zc, size_t* smem, int* threads) {
-  if (nf == 5) {
-    if (dim == 1) return pick_one<5, 1>(tx, ty, zc, smem, threads);
-    if (dim == 2) return pick_one<5, 2>(tx, ty, zc, smem, threads);
-    return pick_one<5, 3>(tx, ty, zc, smem, threads);
+int tiles() { return kTiles; }
+
+FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads) {
+  if (nf == 5 && dim == 3) {
+    switch (tile) {
+      case 1: return pick_one<5, 3, 1>(tx, ty, zc, smem, threads);
+      case 2: return pick_one<5, 3, 2>(tx, ty, zc, smem, threads);
+      case 3: return pick_one<5, 3, 3>(tx, ty, zc, smem, threads);
+      default: return pick_one<5, 3, 0>(tx, ty, zc, smem, threads);
+    }
   }
-  if (dim == 1) return pick_one<6, 1>(tx, ty, zc, smem, threads);
-  if (dim == 2) return pick_one<6, 2>(tx, ty, zc, smem, threads);
-  return pick_one<6, 3>(tx, ty, zc, smem, threads);
+  if (nf == 5) {
+    if (dim == 1) return pick_one<5, 1, 0>(tx, ty, zc, smem, threads);
+    return pick_one<5, 2, 0>(tx, ty, zc, smem, threads);
+  }
+  if (dim == 1) return pick_one<6, 1, 0>(tx, ty, zc, smem, threads);
+  if (dim == 2) return pick_one<6, 2, 0>(tx, ty, zc, smem, threads);
+  return pick_one<6, 3, 0>(tx, ty, zc, smem, threads);
 }
 
 // hydrostep part 1 on the SoA state: maxima of |u_d| + a in FP64 (the state

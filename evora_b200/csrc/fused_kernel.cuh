@@ -208,22 +208,32 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
   const T dtdx = (T)(dtd * P.dxinv), dtdy = (T)(dtd * P.dyinv), dtdz = (T)(dtd * P.dzinv);
 
   // A: primitives of plane z (global index, may be a ghost plane) into slot.
+  // Tiles whose x/y halo lies inside the grid need no index map in x and y
+  // (block-uniform test); the plane index is mapped once per plane.
+  const bool interior_xy = X0 >= 2 && X0 + TX + 2 <= nx && Y0 >= 2 && Y0 + TY + 2 <= ny;
   auto load_plane = [&](int z, int slot) {
+    bool zflip = false;
+    const int mz = DIM == 3 ? ghost_map(z, nz, P.boundtype, 2, zflip) : 0;
+    const T* plane = A.qin + (size_t)mz * ((size_t)nx * ny);   // cell index within a field < 2^31
     for (int it = tid; it < RX * RY; it += NT) {
       const int lx = it % RX, ly = it / RX;
       int gx = X0 - 2 + lx, gy = Y0 - 2 + ly;
-      // cells past the first two ghosts of a partial tile feed no owned
-      // cell; clamp them onto valid cells so they hold physical data
-      gx = gx > nx + 1 ? nx + 1 : gx;
-      gy = gy > ny + 1 ? ny + 1 : gy;
       bool flip = false;
-      const int mx = ghost_map(gx, nx, P.boundtype, 0, flip);
-      const int my = ghost_map(gy, ny, P.boundtype, 1, flip);
-      const int mz = DIM == 3 ? ghost_map(z, nz, P.boundtype, 2, flip) : 0;
-      const int64_t idx = ((int64_t)mz * ny + my) * nx + mx;
+      int idx;
+      if (interior_xy) {
+        idx = gy * nx + gx;
+      } else {
+        // cells past the first two ghosts of a partial tile feed no owned
+        // cell; clamp them onto valid cells so they hold physical data
+        gx = gx > nx + 1 ? nx + 1 : gx;
+        gy = gy > ny + 1 ? ny + 1 : gy;
+        const int mx = ghost_map(gx, nx, P.boundtype, 0, flip);
+        const int my = ghost_map(gy, ny, P.boundtype, 1, flip);
+        idx = my * nx + mx;
+      }
       T qv[6], wv[5];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
+      for (int f = 0; f < NF; ++f) qv[f] = ld(plane + (size_t)f * n + idx);
       prim(qv, wv, c, P, de, err);
       if (flip) {
         wv[1] = -wv[1];
@@ -478,8 +488,10 @@ __global__ void __launch_bounds__(128) k_fused1d(FusedArgs<T> A) {
     fused_cell1d<T, NF>(A, i);
 }
 
-template <typename T, int NF, int DIM, int TX, int TY, int ZC>
-__global__ void __launch_bounds__(TX* TY) k_fused(FusedArgs<T> A) {
+// MINB: CTAs per SM the register allocation must allow (shared memory is
+// sized for the same count; see the tile table in fused_inst.cuh).
+template <typename T, int NF, int DIM, int TX, int TY, int ZC, int MINB>
+__global__ void __launch_bounds__(TX* TY, MINB) k_fused(FusedArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto& sm = *reinterpret_cast<FusedSmem<T, NF, TX, TY>*>(smem_raw);
   fused_tile<T, NF, DIM, TX, TY, ZC>(A, sm, threadIdx.x, blockIdx.x, blockIdx.y, blockIdx.z);

@@ -329,6 +329,61 @@ int evora_grid_status(evora_grid* g) {
   return (int)c.err;
 }
 
+int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms_per_tile, int32_t max_tiles) {
+  if (!g || reps < 1) return EVORA_ERR_ARG;
+  if (reference_backend(g)) {
+    if (chosen) *chosen = 0;
+    return 0;
+  }
+  const int nt = fused_tiles(g->plan);
+  // Save the control block, compute this step's dt, then time each tile's
+  // update from the current buffer into the other one; the current state is
+  // untouched and the control block is restored afterwards.
+  GridCtl saved;
+  CU(cudaMemcpyAsync(&saved, g->ctl, sizeof saved, cudaMemcpyDeviceToHost, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  k_step_begin<<<1, 1, 0, g->stream>>>(g->ctl);
+  fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, g->stream);
+  k_step_time<<<1, 1, 0, g->stream>>>(g->P, g->ctl);
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  int best = g->plan.tile;
+  double best_ms = 1e300;
+  for (int t = 0; t < nt; ++t) {
+    fused_set_tile(&g->plan, t);
+    fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, g->stream);  // warm-up
+    CU(cudaEventRecord(e0, g->stream));
+    for (int r = 0; r < reps; ++r) fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, g->stream);
+    CU(cudaEventRecord(e1, g->stream));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    const double per = ms / reps;
+    if (ms_per_tile && t < max_tiles) ms_per_tile[t] = per;
+    if (per < best_ms) {
+      best_ms = per;
+      best = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  fused_set_tile(&g->plan, best);
+  CU(cudaMemcpyAsync(g->ctl, &saved, sizeof saved, cudaMemcpyHostToDevice, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  CU(cudaGetLastError());
+  if (chosen) *chosen = best;
+  return 0;
+}
+
+int evora_grid_set_tile(evora_grid* g, int32_t tile) {
+  if (!g) return EVORA_ERR_ARG;
+  if (reference_backend(g)) return tile == 0 ? 0 : EVORA_ERR_ARG;
+  if (tile < 0 || tile >= fused_tiles(g->plan)) return EVORA_ERR_ARG;
+  fused_set_tile(&g->plan, tile);
+  return 0;
+}
+
 int evora_grid_set_timing(evora_grid* g, int32_t on) {
   if (!g) return EVORA_ERR_ARG;
   g->timing = on != 0;

@@ -193,6 +193,17 @@ class Grid:
         check(lib().evora_grid_totals(self._h, out), "grid_totals")
         return np.array(out[:])
 
+    def autotune(self, reps: int = 3):
+        """Times every tile shape of the fused kernel on this grid, keeps the
+        fastest; returns (chosen index, ms per launch for each shape)."""
+        chosen = ctypes.c_int32()
+        ms = (ctypes.c_double * 16)()
+        check(lib().evora_grid_autotune(self._h, int(reps), ctypes.byref(chosen), ms, 16), "grid_autotune")
+        return chosen.value, [v for v in ms[:16] if v > 0]
+
+    def set_tile(self, tile: int):
+        check(lib().evora_grid_set_tile(self._h, int(tile)), "grid_set_tile")
+
     def set_timing(self, on: bool = True):
         check(lib().evora_grid_set_timing(self._h, 1 if on else 0), "grid_set_timing")
 

@@ -218,6 +218,15 @@ int evora_grid_status(evora_grid* g);
  * snapshot.f90:159-193, before the multiplication by the cell volume). */
 int evora_grid_totals(evora_grid* g, double out[6]);
 
+/* Tile autotuner (no counterpart in the reference): times every tile shape
+ * of the fused update kernel (`reps` launches each) on the grid's own state
+ * and keeps the fastest.  The state and the time of the grid are unchanged.
+ * ms_per_tile (optional, max_tiles entries) receives the timings. */
+int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms_per_tile,
+                        int32_t max_tiles);
+/* Selects a tile shape by index (0 = the default). */
+int evora_grid_set_tile(evora_grid* g, int32_t tile);
+
 /* Kernel timing (no counterpart in the reference): when on, every step
  * records CUDA events around its CFL kernel and its update kernel on the
  * grid's stream.  evora_grid_timing synchronises, returns the summed event

@@ -158,3 +158,27 @@ def test_error_stops_the_grid(cuda_device):
         assert e.value.status & 1
         assert g.time()["k"] == 0
         np.testing.assert_array_equal(g.get_q()[..., :5], q[..., :5])
+
+
+def test_autotune_keeps_state_and_time(cuda_device):
+    kw = dict(nx=64, ny=48, nz=40, g=5 / 3, cfl=0.5, boundtype=2, tend=100.0)
+    p = ev.default_params(**kw)
+    q = ev.ic.kh3d(p)
+    for prec in (ev.FP64, ev.FP32):
+        with ev.Grid(p, prec) as g:
+            g.set_q(q)
+            g.step(2)
+            before, t0 = g.get_q(), g.time()
+            chosen, ms = g.autotune(reps=2)
+            assert 0 <= chosen < len(ms) and all(m > 0 for m in ms)
+            np.testing.assert_array_equal(g.get_q(), before)
+            assert g.time() == t0
+            g.step(3)
+            after = g.get_q()
+        # every tile shape gives the same answer bit for bit
+        for tile in range(len(ms)):
+            with ev.Grid(p, prec) as g:
+                g.set_tile(tile)
+                g.set_q(q)
+                g.step(5)
+                np.testing.assert_array_equal(g.get_q(), after)
