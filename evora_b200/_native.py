@@ -141,6 +141,9 @@ def _declare_batch(L):
         "evora_batch_info": ([G, c_int32, _dp, _dp, ctypes.POINTER(c_int32),
                               ctypes.POINTER(c_int64), ctypes.POINTER(c_int32)], c_int32),
         "evora_batch_steps_done": ([G, ctypes.POINTER(c_int64)], c_int32),
+        "evora_batch_set_tend": ([G, c_int32, c_double], c_int32),
+        "evora_batch_configure": ([G, c_int32, c_int32], c_int32),
+        "evora_batch_autotune": ([G, c_int32, ctypes.POINTER(c_int32), ctypes.POINTER(c_int32)], c_int32),
         "evora_hydrostep_noalloc": ([c_void_p, _dp], c_int32),
     }
     for name, (args, res) in sig.items():

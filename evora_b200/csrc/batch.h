@@ -1,0 +1,73 @@
+// batch.h -- structures shared by the batched-tube kernel and its host code.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "hydro_math.cuh"
+
+namespace evora {
+
+enum TubeStatus { TUBE_RUNNING = 0, TUBE_DONE = 1, TUBE_ERROR = 2, TUBE_IDLE = 3 };
+
+// One tube's bookkeeping (device array, one entry per tube).
+struct TubeState {
+  long long offset;   // first cell of the tube in the packed state
+  int n;              // cells
+  int status;         // TubeStatus
+  double t, dt, tend;
+  long long k;        // steps done
+  unsigned err;       // EVORA_ERR_* mask
+  int pad;
+};
+
+template <typename T>
+struct BatchArgs {
+  HydroParams P;          // shared options (nx and dx are per tube)
+  double xmin, xmax;
+  T* q;                   // NF planes of ntot cells (tubes packed)
+  long long ntot;
+  TubeState* tubes;
+  const int* order;       // queue order (tube indices, largest work first)
+  int ntubes;
+  int* head;              // queue head (reset to 0 before each launch)
+  int budget;             // max steps per tube in this launch
+  int cap;                // tubes with n <= cap live in shared memory
+  T* gscratch;            // per-CTA scratch for longer tubes: (NF + 5) * (nmax + 4) each
+  int nmax;
+  unsigned long long* cell_updates;  // running total
+};
+
+struct BatchPlan;
+typedef void (*BatchLaunch)(const BatchPlan& pl, void* q, cudaStream_t st);
+
+struct BatchPlan {
+  HydroParams P{};
+  double xmin = 0.0, xmax = 1.0;
+  int nf = 5;
+  long long ntot = 0;
+  TubeState* tubes = nullptr;
+  const int* order = nullptr;
+  int ntubes = 0;
+  int* head = nullptr;
+  int budget = 1;
+  int cap = 0;
+  void* gscratch = nullptr;
+  int nmax = 0;
+  unsigned long long* cell_updates = nullptr;
+  int threads = 256;   // NT
+  int ctas = 1;        // persistent grid
+  size_t smem = 0;
+};
+
+#define EVORA_DECLARE_BATCH_NS(ns)                                                          \
+  namespace ns {                                                                            \
+  /* configures launch for nf fields and `threads` per CTA; sets plan->smem from cap */     \
+  BatchLaunch batch_pick(int nf, int threads, BatchPlan* plan);                             \
+  int batch_max_ctas_per_sm(int nf, int threads, size_t smem);                              \
+  }
+EVORA_DECLARE_BATCH_NS(f64)
+EVORA_DECLARE_BATCH_NS(f64s)
+EVORA_DECLARE_BATCH_NS(f32)
+#undef EVORA_DECLARE_BATCH_NS
+
+}  // namespace evora

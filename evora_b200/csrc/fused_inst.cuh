@@ -5,6 +5,7 @@
 // EVORA_TX, EVORA_TY, EVORA_ZC.
 #pragma once
 
+#include "batch_kernel.cuh"
 #include "fused.h"
 #include "fused_kernel.cuh"
 
@@ -129,6 +130,67 @@ void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st) {
   if (blocks > 148 * 8) blocks = 148 * 8;
   if (pl.nf == 5) k_cfl_soa<5><<<(int)blocks, 256, 0, st>>>(pl.P, (const TT*)q, pl.n, ctl);
   else k_cfl_soa<6><<<(int)blocks, 256, 0, st>>>(pl.P, (const TT*)q, pl.n, ctl);
+}
+
+// ---- batched tubes
+template <int NF, int NT>
+void batch_launch(const BatchPlan& pl, void* q, cudaStream_t st) {
+  BatchArgs<TT> A;
+  A.P = pl.P;
+  A.xmin = pl.xmin;
+  A.xmax = pl.xmax;
+  A.q = (TT*)q;
+  A.ntot = pl.ntot;
+  A.tubes = pl.tubes;
+  A.order = pl.order;
+  A.ntubes = pl.ntubes;
+  A.head = pl.head;
+  A.budget = pl.budget;
+  A.cap = pl.cap;
+  A.gscratch = (TT*)pl.gscratch;
+  A.nmax = pl.nmax;
+  A.cell_updates = pl.cell_updates;
+  k_tubes<TT, NF, NT><<<pl.ctas, NT, pl.smem, st>>>(A);
+}
+
+template <int NF, int NT>
+BatchLaunch batch_pick_one(BatchPlan* pl) {
+  pl->threads = NT;
+  pl->smem = ((size_t)NF * pl->cap + 5 * ((size_t)pl->cap + 4)) * sizeof(TT);
+  auto k = k_tubes<TT, NF, NT>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem);
+  cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  return &batch_launch<NF, NT>;
+}
+
+BatchLaunch batch_pick(int nf, int threads, BatchPlan* pl) {
+  if (nf == 5) {
+    if (threads == 128) return batch_pick_one<5, 128>(pl);
+    if (threads == 512) return batch_pick_one<5, 512>(pl);
+    return batch_pick_one<5, 256>(pl);
+  }
+  if (threads == 128) return batch_pick_one<6, 128>(pl);
+  if (threads == 512) return batch_pick_one<6, 512>(pl);
+  return batch_pick_one<6, 256>(pl);
+}
+
+template <int NF, int NT>
+int max_ctas_one(size_t smem) {
+  int nb = 0;
+  cudaFuncSetAttribute(k_tubes<TT, NF, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tubes<TT, NF, NT>, NT, smem);
+  return nb;
+}
+
+int batch_max_ctas_per_sm(int nf, int threads, size_t smem) {
+  if (nf == 5) {
+    if (threads == 128) return max_ctas_one<5, 128>(smem);
+    if (threads == 512) return max_ctas_one<5, 512>(smem);
+    return max_ctas_one<5, 256>(smem);
+  }
+  if (threads == 128) return max_ctas_one<6, 128>(smem);
+  if (threads == 512) return max_ctas_one<6, 512>(smem);
+  return max_ctas_one<6, 256>(smem);
 }
 
 }  // namespace EVORA_FNS

@@ -227,4 +227,78 @@ class Grid:
 
 
 __all__ = ["EvoraError", "EvoraParams", "EvoraDerived", "default_params", "derived", "shapes",
-           "DropIn", "Grid", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS"]
+           "DropIn", "Grid", "Batch", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS"]
+
+
+# --------------------------------------------------------- batched tubes --
+class Batch:
+    """Independent 1D tubes advanced together (evora_batch_*): each tube is a
+    run of the reference loop on its own grid of n[i] cells, with its own
+    time and end time."""
+
+    def __init__(self, params: EvoraParams, lengths, precision: int = FP32, flags: int = 0):
+        self.params = params
+        self.n = [int(x) for x in lengths]
+        self.offsets = np.concatenate([[0], np.cumsum(self.n)]).astype(np.int64)
+        arr = (ctypes.c_int32 * len(self.n))(*self.n)
+        h = ctypes.c_void_p()
+        check(lib().evora_batch_create(ctypes.byref(params), len(self.n), arr, precision, flags,
+                                       ctypes.byref(h)), "batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().evora_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_q(self, q, tube: int = -1):
+        """q: (n[tube], 6) for one tube, or (sum n, 6) for all (tube = -1)."""
+        cells = sum(self.n) if tube < 0 else self.n[tube]
+        check(lib().evora_batch_set_q(self._h, tube, _ptr(q, (cells, 6), False)), "batch_set_q")
+
+    def get_q(self, tube: int = -1, out=None):
+        cells = sum(self.n) if tube < 0 else self.n[tube]
+        if out is None:
+            out = np.empty((cells, 6))
+        check(lib().evora_batch_get_q(self._h, tube, _ptr(out, (cells, 6))), "batch_get_q")
+        return out
+
+    def set_tend(self, tube: int, tend: float):
+        check(lib().evora_batch_set_tend(self._h, tube, float(tend)), "batch_set_tend")
+
+    def run(self, max_steps: int = 0, sync: bool = True):
+        """Advances every running tube; returns the OR of tube errors (sync)."""
+        return int(lib().evora_batch_run(self._h, int(max_steps), 1 if sync else 0))
+
+    def info(self, tube: int):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        go, st = ctypes.c_int32(), ctypes.c_int32()
+        k = ctypes.c_int64()
+        err = lib().evora_batch_info(self._h, tube, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(go),
+                                     ctypes.byref(k), ctypes.byref(st))
+        return dict(t=t.value, dt=dt.value, go=bool(go.value), k=k.value, status=st.value, err=int(err))
+
+    def cell_updates(self) -> int:
+        v = ctypes.c_int64()
+        check(lib().evora_batch_steps_done(self._h, ctypes.byref(v)), "batch_steps_done")
+        return v.value
+
+    def configure(self, threads: int = 256, ctas_per_sm: int = 2):
+        check(lib().evora_batch_configure(self._h, threads, ctas_per_sm), "batch_configure")
+
+    def autotune(self, steps: int = 20):
+        th, ct = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().evora_batch_autotune(self._h, int(steps), ctypes.byref(th), ctypes.byref(ct)), "batch_autotune")
+        return th.value, ct.value

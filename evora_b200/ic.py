@@ -104,3 +104,34 @@ def kh3d(p: EvoraParams, seed=42, amp=0.01):
     q[..., 4] = 0.5 * rho * ((u * u) + (v * v)) + 2.5 / d.g1
     q[..., 5] = 2.5 / rho ** d.g1
     return q
+
+
+def random_tubes(ntubes, seed=7, nmin=128, nmax=4096, gamma=5.0 / 3.0):
+    """The batched Riemann-problem workload: tube lengths uniform in
+    [nmin, nmax]; left/right rho log-uniform in [0.1, 10], p log-uniform in
+    [0.01, 10], v uniform in [-1, 1]; interface uniform in [0.3, 0.7].
+    Returns (lengths, q) with q of shape (sum lengths, 6) in the reference
+    layout, tubes concatenated, built like ic/shocktube.f90:59-100."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(nmin, nmax + 1, ntubes)
+    rho = np.exp(rng.uniform(np.log(0.1), np.log(10.0), (ntubes, 2)))
+    pre = np.exp(rng.uniform(np.log(0.01), np.log(10.0), (ntubes, 2)))
+    vel = rng.uniform(-1.0, 1.0, (ntubes, 2))
+    xd = rng.uniform(0.3, 0.7, ntubes)
+    g1 = gamma - 1.0
+    parts = []
+    for i in range(ntubes):
+        n = int(lengths[i])
+        dx = 1.0 / n
+        x = dx / 2 + np.arange(n) * dx
+        left = x < xd[i]
+        d = np.where(left, rho[i, 0], rho[i, 1])
+        u = np.where(left, vel[i, 0], vel[i, 1])
+        p = np.where(left, pre[i, 0], pre[i, 1])
+        q = np.zeros((n, 6))
+        q[:, 0] = d
+        q[:, 1] = d * u
+        q[:, 4] = 0.5 * d * (u * u) + p / g1
+        q[:, 5] = p / d ** g1
+        parts.append(q)
+    return [int(x) for x in lengths], np.ascontiguousarray(np.concatenate(parts))

@@ -236,6 +236,45 @@ int evora_grid_set_timing(evora_grid* g, int32_t on);
 int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps,
                       int64_t* launches);
 
+/* ------------------------------------------------------- batched tubes -- */
+/* No counterpart in the reference (a one-run CLI): many independent 1D
+ * tubes (ny = nz = 1), each a run of the reference loop main.f90:109-155 on
+ * its own grid, with its own length n[i], time, step size and end time, all
+ * sharing the options of *p (solver, limiter, boundtype, secondorder, g,
+ * cfl, xmin/xmax, tstart, tend).  One persistent kernel launch advances every
+ * unfinished tube; each CTA stages a whole tube in shared memory and runs its
+ * steps there.  Tubes are independent: a tube's result does not depend on the
+ * others (bit for bit), and a tube that raises an error stops alone. */
+typedef struct evora_batch evora_batch;
+
+int evora_batch_create(const evora_params* p, int32_t ntubes, const int32_t* n, int32_t precision,
+                       int32_t flags, evora_batch** out);
+int evora_batch_destroy(evora_batch* b);
+/* A capturable (non-default) stream; the batch owns one until this is set. */
+int evora_batch_set_stream(evora_batch* b, void* stream);
+/* q in the reference layout q(6, n[tube]); tube = -1: all tubes concatenated.
+ * Host or device pointer.  (Re)starts the tube(s): t = tstart, k = 0. */
+int evora_batch_set_q(evora_batch* b, int32_t tube, const double* q);
+int evora_batch_get_q(evora_batch* b, int32_t tube, double* q);
+/* Per-tube end time (default p->tend); takes effect at the next set_q/run. */
+int evora_batch_set_tend(evora_batch* b, int32_t tube, double tend);
+/* Advances every running tube by up to max_steps steps (<= 0: until each
+ * reaches its end time), in one launch replayed from a CUDA graph cached per
+ * step budget.  With sync, waits and returns the OR of the tubes' errors. */
+int evora_batch_run(evora_batch* b, int32_t max_steps, int32_t sync);
+/* Tube state; returns the tube's error mask.  status: 0 running, 1 done,
+ * 2 stopped by an error, 3 idle (no state loaded). */
+int evora_batch_info(evora_batch* b, int32_t tube, double* t, double* dt, int32_t* go, int64_t* k,
+                     int32_t* status);
+/* Total cell-updates done by the batch so far. */
+int evora_batch_steps_done(evora_batch* b, int64_t* cell_updates);
+/* Threads per CTA (128, 256, 512) and CTAs per SM the shared-memory staging
+ * is sized for (tubes longer than that capacity run from global memory). */
+int evora_batch_configure(evora_batch* b, int32_t threads, int32_t ctas_per_sm);
+/* Autotuner: times every (threads, CTAs per SM) candidate for `steps` steps
+ * on the batch's own state (restored after each trial) and keeps the fastest. */
+int evora_batch_autotune(evora_batch* b, int32_t steps, int32_t* threads, int32_t* ctas_per_sm);
+
 #ifdef __cplusplus
 }
 #endif
