@@ -275,6 +275,11 @@ class Batch:
         check(lib().evora_batch_get_q(self._h, tube, _ptr(out, (cells, 6))), "batch_get_q")
         return out
 
+    def set_stream(self, stream):
+        """stream: a (non-default) torch.cuda.Stream or raw cudaStream_t."""
+        raw = getattr(stream, "cuda_stream", stream)
+        check(lib().evora_batch_set_stream(self._h, ctypes.c_void_p(int(raw))), "batch_set_stream")
+
     def set_tend(self, tube: int, tend: float):
         check(lib().evora_batch_set_tend(self._h, tube, float(tend)), "batch_set_tend")
 
