@@ -29,7 +29,7 @@ PER_FILE = {
     "fused_f32.cu": ["--use_fast_math"],
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
-           "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu"]
+           "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu"]
 
 
 def _deps():

@@ -162,6 +162,32 @@ int grid_of(long long n) {
   return (int)std::max(1LL, std::min(g, 148LL * 8));
 }
 
+}  // namespace
+
+void evora::tube_from_aos(const double* aos, void* q, bool f32, long long ntot, long long off, long long n, int nf,
+                          cudaStream_t st) {
+  if (f32) k_tube_from_aos<float><<<grid_of(n), 256, 0, st>>>(aos, (float*)q, ntot, off, n, nf);
+  else k_tube_from_aos<double><<<grid_of(n), 256, 0, st>>>(aos, (double*)q, ntot, off, n, nf);
+}
+
+void evora::tube_to_aos(const void* q, double* aos, bool f32, long long ntot, long long off, long long n, int nf,
+                        double g1, cudaStream_t st) {
+  if (f32) k_tube_to_aos<float><<<grid_of(n), 256, 0, st>>>((const float*)q, aos, ntot, off, n, nf, g1);
+  else k_tube_to_aos<double><<<grid_of(n), 256, 0, st>>>((const double*)q, aos, ntot, off, n, nf, g1);
+}
+
+evora::BatchLaunch evora::batch_pick_for(int precision, int strict, int nf, int threads, BatchPlan* pl) {
+  if (precision == EVORA_FP32) return f32::batch_pick(nf, threads, pl);
+  return strict ? f64s::batch_pick(nf, threads, pl) : f64::batch_pick(nf, threads, pl);
+}
+
+int evora::batch_ctas_per_sm(int precision, int strict, int nf, int threads, size_t smem) {
+  if (precision == EVORA_FP32) return f32::batch_max_ctas_per_sm(nf, threads, smem);
+  return strict ? f64s::batch_max_ctas_per_sm(nf, threads, smem) : f64::batch_max_ctas_per_sm(nf, threads, smem);
+}
+
+namespace {
+
 // Range of tubes [t0, t1) and its cells for tube index `tube` (-1 = all).
 bool tube_range(const evora_batch* b, int tube, int* t0, int* t1, long long* off, long long* cells) {
   if (tube < -1 || tube >= b->ntubes) return false;

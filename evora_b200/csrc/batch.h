@@ -70,4 +70,13 @@ EVORA_DECLARE_BATCH_NS(f64s)
 EVORA_DECLARE_BATCH_NS(f32)
 #undef EVORA_DECLARE_BATCH_NS
 
+// Reference layout q(6, n) (FP64) <-> packed SoA tube storage.
+void tube_from_aos(const double* aos, void* q, bool f32, long long ntot, long long off, long long n, int nf,
+                   cudaStream_t st);
+void tube_to_aos(const void* q, double* aos, bool f32, long long ntot, long long off, long long n, int nf,
+                 double g1, cudaStream_t st);
+// Instantiation dispatch by precision.
+BatchLaunch batch_pick_for(int precision, int strict, int nf, int threads, BatchPlan* pl);
+int batch_ctas_per_sm(int precision, int strict, int nf, int threads, size_t smem);
+
 }  // namespace evora

@@ -1,0 +1,494 @@
+// server.cu -- a request loop for hydro solves with continuous batching
+// (no counterpart in the reference, which runs one simulation per process).
+//
+// A request is an initial state q(6, nx, ny, nz) in the reference layout, a
+// grid size and an end time.  The loop (evora_server_tick) admits pending
+// requests in arrival order while their device footprint fits the HBM
+// budget, keeps every admitted state resident, and on each tick advances all
+// active work by up to `steps_per_tick` steps:
+//   * 1D requests become tubes of one shared pool (a packed arena plus a tube
+//     table) advanced together by one persistent launch of the batched-tube
+//     kernel (batch_kernel.cuh), each tube with its own dt and t;
+//   * 2D and 3D requests become resident grids (grid.cu) stepped on their own
+//     streams, so small grids run concurrently with the tube launch.
+// Requests that arrive while others run are admitted at the next tick, as
+// memory and tube slots free up.  Finished requests are read back and their
+// time to solution (submit -> read back) is recorded.  A request's arithmetic
+// does not depend on what else is in flight.
+//
+// Single-threaded: one host thread drives a server.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "../../include/evora_gpu.h"
+#include "batch.h"
+#include "common.h"
+
+using namespace evora;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
+
+struct Request {
+  int64_t id = 0;
+  int nx = 0, ny = 0, nz = 0;
+  double tend = 0.0;
+  std::vector<double> q0;        // initial state (host copy), freed at admission
+  double t_submit = 0.0, t_done = 0.0;
+  int state = REQ_PENDING;
+  bool tube = false;
+  int slot = -1;                 // tube slot
+  long long off = 0;             // arena offset (tubes)
+  evora_grid* grid = nullptr;    // 2D/3D
+  int stream = 0;
+  size_t bytes = 0;              // device footprint (grids)
+  int64_t steps = 0;
+  unsigned err = 0;
+  std::vector<double> result;
+  long long cells() const { return (long long)nx * ny * nz; }
+};
+
+#define CU(call)                 \
+  do {                           \
+    cudaError_t e_ = (call);     \
+    if (e_ != cudaSuccess) {     \
+      set_cuda_error(e_, #call); \
+      return EVORA_ERR_CUDA;     \
+    }                            \
+  } while (0)
+
+}  // namespace
+
+struct evora_server {
+  evora_params base{};
+  HydroParams P{};
+  int precision = EVORA_FP32;
+  int flags = 0;
+  int nf = 5;
+  size_t budget = 0, used = 0;
+  int steps_per_tick = 64;
+  Clock::time_point t0;
+  int64_t next_id = 1;
+  std::deque<int64_t> pending;
+  std::map<int64_t, Request> reqs;
+  // tube pool
+  int max_slots = 0;
+  int max_tube = 0;
+  long long arena = 0;
+  void* q = nullptr;
+  TubeState* tubes = nullptr;
+  int* order = nullptr;
+  int* head = nullptr;
+  unsigned long long* cu = nullptr;
+  void* gscratch = nullptr;
+  double* stage = nullptr;       // AoS staging of one tube
+  std::vector<int64_t> slot_req; // slot -> request id (0 = free)
+  std::vector<std::pair<long long, long long>> free_seg;  // (offset, length), sorted
+  BatchPlan plan{};
+  BatchLaunch launch = nullptr;
+  bool order_dirty = true;
+  int active_tubes = 0;
+  cudaStream_t tstream = nullptr;
+  std::vector<cudaStream_t> gstreams;
+  int next_stream = 0;
+  std::vector<double> latencies;
+  long long grid_cell_updates = 0;
+  double first_submit = -1.0, last_done = 0.0;
+  size_t fixed = 0;              // arena and staging
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+  size_t esize() const { return precision == EVORA_FP32 ? 4 : 8; }
+};
+
+namespace {
+
+bool alloc_segment(evora_server* s, long long n, long long* off) {
+  for (size_t i = 0; i < s->free_seg.size(); ++i) {
+    auto& seg = s->free_seg[i];
+    if (seg.second >= n) {
+      *off = seg.first;
+      seg.first += n;
+      seg.second -= n;
+      if (seg.second == 0) s->free_seg.erase(s->free_seg.begin() + (long)i);
+      return true;
+    }
+  }
+  return false;
+}
+
+void free_segment(evora_server* s, long long off, long long n) {
+  auto& fs = s->free_seg;
+  auto it = std::lower_bound(fs.begin(), fs.end(), std::make_pair(off, 0LL));
+  it = fs.insert(it, {off, n});
+  // merge with neighbours
+  size_t i = (size_t)(it - fs.begin());
+  if (i + 1 < fs.size() && fs[i].first + fs[i].second == fs[i + 1].first) {
+    fs[i].second += fs[i + 1].second;
+    fs.erase(fs.begin() + (long)i + 1);
+  }
+  if (i > 0 && fs[i - 1].first + fs[i - 1].second == fs[i].first) {
+    fs[i - 1].second += fs[i].second;
+    fs.erase(fs.begin() + (long)i);
+  }
+}
+
+size_t grid_bytes(const evora_server* s, long long cells) {
+  // two SoA copies + the reference-layout staging used by set_q / get_q
+  return (size_t)cells * (2 * (size_t)s->nf * s->esize() + EVORA_NQ * sizeof(double)) + (1 << 16);
+}
+
+int admit(evora_server* s, Request& r) {
+  if (r.tube) {
+    int slot = -1;
+    for (int i = 0; i < s->max_slots; ++i)
+      if (s->slot_req[i] == 0) {
+        slot = i;
+        break;
+      }
+    long long off = 0;
+    if (slot < 0 || !alloc_segment(s, r.nx, &off)) return 1;   // not now
+    r.slot = slot;
+    r.off = off;
+    s->slot_req[slot] = r.id;
+    CU(cudaMemcpyAsync(s->stage, r.q0.data(), sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->tstream));
+    tube_from_aos(s->stage, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->tstream);
+    TubeState ts{};
+    ts.offset = off;
+    ts.n = r.nx;
+    ts.status = TUBE_RUNNING;
+    ts.t = s->base.tstart;
+    ts.tend = r.tend;
+    CU(cudaMemcpyAsync(s->tubes + slot, &ts, sizeof ts, cudaMemcpyHostToDevice, s->tstream));
+    CU(cudaStreamSynchronize(s->tstream));
+    s->active_tubes++;
+    s->order_dirty = true;
+  } else {
+    const size_t bytes = grid_bytes(s, r.cells());
+    if (s->used + bytes > s->budget) return 1;
+    evora_params p = s->base;
+    p.nx = r.nx;
+    p.ny = r.ny;
+    p.nz = r.nz;
+    p.tend = r.tend;
+    evora_grid* g = nullptr;
+    int rc = evora_grid_create(&p, s->precision, s->flags & ~EVORA_REFERENCE_KERNELS, &g);
+    if (rc) return rc == EVORA_ERR_NOMEM ? 1 : rc;
+    r.stream = s->next_stream;
+    s->next_stream = (s->next_stream + 1) % (int)s->gstreams.size();
+    evora_grid_set_stream(g, s->gstreams[r.stream]);
+    rc = evora_grid_set_q(g, r.q0.data());
+    if (rc) {
+      evora_grid_destroy(g);
+      return rc == EVORA_ERR_NOMEM ? 1 : rc;
+    }
+    r.grid = g;
+    r.bytes = bytes;
+    s->used += bytes;
+  }
+  r.state = REQ_RUNNING;
+  std::vector<double>().swap(r.q0);
+  return 0;
+}
+
+void finish(evora_server* s, Request& r, unsigned err) {
+  r.err = err;
+  r.state = err ? REQ_FAILED : REQ_DONE;
+  r.t_done = s->now();
+  s->last_done = r.t_done;
+  s->latencies.push_back(r.t_done - r.t_submit);
+}
+
+int upload_order(evora_server* s) {
+  std::vector<int> ord;
+  std::vector<double> work;
+  for (int i = 0; i < s->max_slots; ++i)
+    if (s->slot_req[i]) {
+      const Request& r = s->reqs[s->slot_req[i]];
+      if (r.state != REQ_RUNNING) continue;
+      ord.push_back(i);
+    }
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    return s->reqs[s->slot_req[a]].nx > s->reqs[s->slot_req[b]].nx;
+  });
+  if (!ord.empty())
+    CU(cudaMemcpyAsync(s->order, ord.data(), sizeof(int) * ord.size(), cudaMemcpyHostToDevice, s->tstream));
+  s->plan.ntubes = (int)ord.size();
+  s->order_dirty = false;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int evora_server_create(const evora_params* base, int32_t precision, int32_t flags, double hbm_budget_bytes,
+                        int32_t steps_per_tick, int32_t max_tube_cells, int32_t max_tubes, evora_server** out) {
+  if (!base || !out || hbm_budget_bytes <= 0 || steps_per_tick < 1 || max_tube_cells < 2 || max_tubes < 1)
+    return EVORA_ERR_ARG;
+  if (precision != EVORA_FP32 && precision != EVORA_FP64) return EVORA_ERR_ARG;
+  *out = nullptr;
+  evora_server* s = new (std::nothrow) evora_server();
+  if (!s) return EVORA_ERR_NOMEM;
+  s->base = *base;
+  s->precision = precision;
+  s->flags = flags;
+  s->nf = (flags & EVORA_CARRY_ENTROPY) || base->dualenergy ? 6 : 5;
+  s->budget = (size_t)hbm_budget_bytes;
+  s->steps_per_tick = steps_per_tick;
+  s->t0 = Clock::now();
+  s->max_slots = max_tubes;
+  s->max_tube = max_tube_cells;
+  evora_params pp = *base;
+  pp.nx = max_tube_cells;
+  pp.ny = pp.nz = 1;
+  int rc = 0;
+  if (!params_to_hydro(&pp, &s->P, nullptr, &rc)) {
+    delete s;
+    return rc;
+  }
+  // the tube arena takes a quarter of the budget, at least one tube per slot of average size
+  s->arena = std::max<long long>((long long)max_tube_cells,
+                                 (long long)(s->budget / 4 / ((size_t)s->nf * s->esize())));
+  const size_t arena_bytes = (size_t)s->arena * s->nf * s->esize();
+  s->slot_req.assign(max_tubes, 0);
+  s->free_seg = {{0, s->arena}};
+  if (cudaStreamCreateWithFlags(&s->tstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  for (int i = 0; i < 8; ++i) {
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+    s->gstreams.push_back(st);
+  }
+  if (cudaMalloc(&s->q, arena_bytes) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->tubes, sizeof(TubeState) * max_tubes) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->order, sizeof(int) * max_tubes) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->head, sizeof(int)) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->cu, sizeof(unsigned long long)) != cudaSuccess) goto fail;
+  if (cudaMemset(s->cu, 0, sizeof(unsigned long long)) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->stage, sizeof(double) * EVORA_NQ * max_tube_cells) != cudaSuccess) goto fail;
+  {
+    std::vector<TubeState> ts(max_tubes);
+    for (auto& t : ts) {
+      t = TubeState{};
+      t.status = TUBE_IDLE;
+    }
+    if (cudaMemcpy(s->tubes, ts.data(), sizeof(TubeState) * max_tubes, cudaMemcpyHostToDevice) != cudaSuccess)
+      goto fail;
+  }
+  {
+    BatchPlan& pl = s->plan;
+    pl.P = s->P;
+    pl.xmin = base->xmin;
+    pl.xmax = base->xmax;
+    pl.nf = s->nf;
+    pl.ntot = s->arena;
+    pl.tubes = s->tubes;
+    pl.order = s->order;
+    pl.ntubes = 0;
+    pl.head = s->head;
+    pl.budget = steps_per_tick;
+    pl.nmax = max_tube_cells;
+    pl.cell_updates = s->cu;
+    const size_t per_cell = (size_t)(s->nf + 5) * s->esize();
+    pl.cap = std::min(max_tube_cells, (int)((227 * 1024 / 2 - 2048) / per_cell) - 4);
+    s->launch = batch_pick_for(precision, (flags & EVORA_STRICT) != 0, s->nf, 256, &pl);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = batch_ctas_per_sm(precision, (flags & EVORA_STRICT) != 0, s->nf, 256, pl.smem);
+    pl.ctas = std::max(1, sms * std::max(1, per_sm));
+    if (max_tube_cells > pl.cap) {
+      size_t need = (size_t)pl.ctas * (size_t)(s->nf + 5) * (size_t)(max_tube_cells + 4) * s->esize();
+      if (cudaMalloc(&s->gscratch, need) != cudaSuccess) goto fail;
+    }
+    pl.gscratch = s->gscratch;
+  }
+  s->used = arena_bytes + sizeof(double) * EVORA_NQ * max_tube_cells;
+  s->fixed = s->used;
+  if (s->used > s->budget) {
+    evora_server_destroy(s);
+    return EVORA_ERR_ARG;
+  }
+  *out = s;
+  return 0;
+fail:
+  cudaGetLastError();
+  evora_server_destroy(s);
+  return EVORA_ERR_NOMEM;
+}
+
+int evora_server_destroy(evora_server* s) {
+  if (!s) return EVORA_ERR_ARG;
+  cudaDeviceSynchronize();
+  for (auto& kv : s->reqs)
+    if (kv.second.grid) evora_grid_destroy(kv.second.grid);
+  cudaFree(s->q);
+  cudaFree(s->tubes);
+  cudaFree(s->order);
+  cudaFree(s->head);
+  cudaFree(s->cu);
+  cudaFree(s->gscratch);
+  cudaFree(s->stage);
+  if (s->tstream) cudaStreamDestroy(s->tstream);
+  for (auto st : s->gstreams) cudaStreamDestroy(st);
+  delete s;
+  return 0;
+}
+
+int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, const double* q0,
+                        int64_t* id) {
+  if (!s || !q0 || !id || nx < 2 || ny < 1 || nz < 1 || (nz > 1 && ny == 1)) return EVORA_ERR_ARG;
+  const bool tube = (ny == 1 && nz == 1);
+  if (tube && nx > s->max_tube) return EVORA_ERR_ARG;
+  Request r;
+  r.id = s->next_id++;
+  r.nx = nx;
+  r.ny = ny;
+  r.nz = nz;
+  r.tend = tend;
+  r.tube = tube;
+  r.q0.assign(q0, q0 + (size_t)EVORA_NQ * nx * ny * nz);
+  r.t_submit = s->now();
+  if (s->first_submit < 0) s->first_submit = r.t_submit;
+  if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) return EVORA_ERR_ARG;  // could never fit
+  *id = r.id;
+  s->pending.push_back(r.id);
+  s->reqs.emplace(r.id, std::move(r));
+  return 0;
+}
+
+int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
+  if (!s) return EVORA_ERR_ARG;
+  // 1. admission, in arrival order, while memory and slots allow
+  while (!s->pending.empty()) {
+    Request& r = s->reqs[s->pending.front()];
+    int rc = admit(s, r);
+    if (rc == 1) {
+      bool idle = s->active_tubes == 0;
+      for (auto& kv : s->reqs) idle = idle && !(kv.second.state == REQ_RUNNING);
+      if (!idle) break;           // head of the queue waits for room
+      rc = EVORA_ERR_NOMEM;       // nothing running and still no room: it never fits
+    }
+    s->pending.pop_front();
+    if (rc) finish(s, r, (unsigned)rc);
+  }
+  // 2. one round of steps for everything active, tubes and grids concurrently
+  if (s->order_dirty) {
+    int rc = upload_order(s);
+    if (rc) return rc;
+  }
+  if (s->plan.ntubes > 0) {
+    CU(cudaMemsetAsync(s->head, 0, sizeof(int), s->tstream));
+    s->launch(s->plan, s->q, s->tstream);
+    CU(cudaGetLastError());
+  }
+  std::vector<Request*> grids;
+  for (auto& kv : s->reqs)
+    if (kv.second.state == REQ_RUNNING && kv.second.grid) {
+      grids.push_back(&kv.second);
+      int rc = evora_grid_step(kv.second.grid, s->steps_per_tick, 0);
+      if (rc) return rc;
+    }
+  CU(cudaStreamSynchronize(s->tstream));
+  for (auto st : s->gstreams) CU(cudaStreamSynchronize(st));
+  // 3. retire finished work
+  if (s->plan.ntubes > 0) {
+    std::vector<TubeState> ts(s->max_slots);
+    CU(cudaMemcpy(ts.data(), s->tubes, sizeof(TubeState) * s->max_slots, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < s->max_slots; ++i) {
+      if (!s->slot_req[i]) continue;
+      Request& r = s->reqs[s->slot_req[i]];
+      if (r.state != REQ_RUNNING || ts[i].status == TUBE_RUNNING) continue;
+      r.steps = ts[i].k;
+      r.result.resize((size_t)EVORA_NQ * r.nx);
+      tube_to_aos(s->q, s->stage, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->tstream);
+      CU(cudaMemcpyAsync(r.result.data(), s->stage, sizeof(double) * r.result.size(), cudaMemcpyDeviceToHost,
+                         s->tstream));
+      CU(cudaStreamSynchronize(s->tstream));
+      TubeState idle{};
+      idle.status = TUBE_IDLE;
+      CU(cudaMemcpy(s->tubes + i, &idle, sizeof idle, cudaMemcpyHostToDevice));
+      free_segment(s, r.off, r.nx);
+      s->slot_req[i] = 0;
+      s->active_tubes--;
+      s->order_dirty = true;
+      finish(s, r, ts[i].err);
+    }
+  }
+  for (Request* r : grids) {
+    double t, dt;
+    int32_t go;
+    int64_t k;
+    int rc = evora_grid_time(r->grid, &t, &dt, &go, &k);
+    if (rc) return rc;
+    const int st = evora_grid_status(r->grid);
+    if (go && !st) continue;
+    r->steps = k;
+    r->result.resize((size_t)EVORA_NQ * r->cells());
+    rc = evora_grid_get_q(r->grid, r->result.data());
+    s->grid_cell_updates += (long long)k * r->cells();
+    evora_grid_destroy(r->grid);
+    r->grid = nullptr;
+    s->used -= r->bytes;
+    finish(s, *r, (unsigned)(st | rc));
+  }
+  int act = 0;
+  for (auto& kv : s->reqs) act += kv.second.state == REQ_RUNNING;
+  if (n_active) *n_active = act;
+  if (n_pending) *n_pending = (int32_t)s->pending.size();
+  return 0;
+}
+
+int evora_server_result(evora_server* s, int64_t id, double* q_out, double* latency_s, int64_t* steps,
+                        int32_t* state) {
+  if (!s) return EVORA_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) {
+    if (state) *state = -1;
+    return EVORA_ERR_ARG;
+  }
+  Request& r = it->second;
+  if (state) *state = r.state;
+  if (r.state != REQ_DONE && r.state != REQ_FAILED) return 0;
+  if (latency_s) *latency_s = r.t_done - r.t_submit;
+  if (steps) *steps = r.steps;
+  if (q_out && !r.result.empty()) std::memcpy(q_out, r.result.data(), sizeof(double) * r.result.size());
+  const int err = (int)r.err;
+  if (q_out) s->reqs.erase(it);   // delivered
+  return err;
+}
+
+int evora_server_stats(evora_server* s, double* p50_s, double* p99_s, int64_t* completed, int64_t* cell_updates,
+                       double* span_s) {
+  if (!s) return EVORA_ERR_ARG;
+  std::vector<double> l = s->latencies;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double f) {
+    if (l.empty()) return 0.0;
+    size_t i = (size_t)std::min<double>((double)l.size() - 1, std::ceil(f * l.size()) - 1);
+    return l[i];
+  };
+  if (p50_s) *p50_s = pct(0.50);
+  if (p99_s) *p99_s = pct(0.99);
+  if (completed) *completed = (int64_t)l.size();
+  if (cell_updates) {
+    unsigned long long v = 0;
+    CU(cudaMemcpy(&v, s->cu, sizeof v, cudaMemcpyDeviceToHost));
+    *cell_updates = (int64_t)v + s->grid_cell_updates;
+  }
+  if (span_s) *span_s = s->first_submit < 0 ? 0.0 : s->last_done - s->first_submit;
+  return 0;
+}
+
+}  // extern "C"

@@ -303,6 +303,9 @@ class Batch:
     def configure(self, threads: int = 256, ctas_per_sm: int = 2):
         check(lib().evora_batch_configure(self._h, threads, ctas_per_sm), "batch_configure")
 
+    def autotune_batch(self, steps: int = 20):
+        return self.autotune(steps)
+
     def autotune(self, steps: int = 20):
         th, ct = ctypes.c_int32(), ctypes.c_int32()
         check(lib().evora_batch_autotune(self._h, int(steps), ctypes.byref(th), ctypes.byref(ct)), "batch_autotune")

@@ -275,6 +275,40 @@ int evora_batch_configure(evora_batch* b, int32_t threads, int32_t ctas_per_sm);
  * on the batch's own state (restored after each trial) and keeps the fastest. */
 int evora_batch_autotune(evora_batch* b, int32_t steps, int32_t* threads, int32_t* ctas_per_sm);
 
+/* ------------------------------------------------------------- serving -- */
+/* No counterpart in the reference (one simulation per process): a request
+ * loop with continuous batching.  A request is an initial state q(6, nx, ny,
+ * nz) (reference layout, host memory, copied at submit), a grid size and an
+ * end time; the other options come from *base.  evora_server_tick admits
+ * pending requests in arrival order while their device footprint fits the
+ * HBM budget (1D requests also need a free tube slot and arena room), then
+ * advances everything admitted by up to steps_per_tick steps: 1D requests
+ * together in one persistent batched-tube launch, 2D/3D requests as resident
+ * grids on their own streams, concurrently; finished requests are read back
+ * and their time to solution (submit to read-back) recorded.  A request's
+ * result does not depend on what else is in flight.  One host thread drives
+ * a server. */
+typedef struct evora_server evora_server;
+
+int evora_server_create(const evora_params* base, int32_t precision, int32_t flags, double hbm_budget_bytes,
+                        int32_t steps_per_tick, int32_t max_tube_cells, int32_t max_tubes,
+                        evora_server** out);
+int evora_server_destroy(evora_server* s);
+/* Queues a request; *id identifies it.  EVORA_ERR_ARG if it can never fit. */
+int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, const double* q0,
+                        int64_t* id);
+/* One scheduling round (admit, step, retire); reports active/pending counts. */
+int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending);
+/* state: 0 pending, 1 running, 2 done, 3 failed, -1 unknown id.  When done or
+ * failed and q_out is given, copies the final state (reference layout),
+ * latency and step count, and forgets the request.  Returns its error mask. */
+int evora_server_result(evora_server* s, int64_t id, double* q_out, double* latency_s, int64_t* steps,
+                        int32_t* state);
+/* p50 / p99 time to solution of completed requests, their count, the total
+ * cell-updates and the time from the first submit to the last completion. */
+int evora_server_stats(evora_server* s, double* p50_s, double* p99_s, int64_t* completed,
+                       int64_t* cell_updates, double* span_s);
+
 #ifdef __cplusplus
 }
 #endif
