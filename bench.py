@@ -339,6 +339,106 @@ def run_tubes(args):
     return 0
 
 
+def run_serving(args):
+    """Serving mix: Poisson arrivals (rate --rate per second, --nrequests
+    requests, seed 11) of solve requests -- 60% 1D tubes of 128-8192 cells
+    (random Riemann states as in the batched workload, to t=0.05), 30% 2D
+    Kelvin-Helmholtz 64^2-1024^2 (ic/kevinhelmholtz.f90 IC, to t=0.02), 10% 3D
+    Kelvin-Helmholtz 32^3-128^3 (seeded IC, to t=0.02) -- FP32, admitted under
+    a 150 GB HBM budget with the state kept resident.  Reports the p50/p99
+    time to solution (submit to read-back) and the aggregate cell-updates/s;
+    a few small requests are rerun alone in FP64 as spot checks of the FP32
+    results."""
+    import torch
+    import evora_b200 as ev
+    from evora_b200.serving import Server
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(args.nrequests):
+        u = rng.random()
+        if u < 0.6:
+            n = int(rng.integers(128, 8193))
+            _, q = ev.ic.random_tubes(1, seed=int(rng.integers(1 << 30)), nmin=n, nmax=n)
+            reqs.append(("1d", q.reshape(1, 1, n, 6), 0.05))
+        elif u < 0.9:
+            n = int(rng.integers(64, 1025))
+            reqs.append(("2d", ev.ic.kh2d(ev.default_params(nx=n, ny=n, nz=1, g=5.0 / 3.0)), 0.02))
+        else:
+            n = int(rng.integers(32, 129))
+            reqs.append(("3d", ev.ic.kh3d(ev.default_params(nx=n, ny=n, nz=n, g=5.0 / 3.0),
+                                          seed=int(rng.integers(1 << 30))), 0.02))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, len(reqs)))
+    # one server; tubes are outflow (boundtype 1), KH boxes periodic (2)
+    lat = {"1d": [], "2d": [], "3d": []}
+    server = Server(ev.default_params(g=5.0 / 3.0, cfl=0.5, boundtype=1, tend=1.0), ev.FP32, 0,
+                    hbm_budget_bytes=150e9, steps_per_tick=args.tick_steps, max_tube_cells=8192, max_tubes=4096)
+    servers = {0: server}
+    t0 = time.perf_counter()
+    nxt = 0
+    ids = {}
+    done = 0
+    ticks, tick_s = 0, 0.0
+    while done < len(reqs):
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and arrivals[nxt] <= now:
+            kind, q, tend = reqs[nxt]
+            rid = server.submit(q, tend, boundtype=1 if kind == "1d" else 2)
+            ids[rid] = nxt
+            nxt += 1
+        tk = time.perf_counter()
+        a, p = server.tick()
+        tick_s += time.perf_counter() - tk
+        ticks += 1
+        for rid in server.completed():
+            r = server.result(rid)
+            i = ids.pop(rid)
+            lat[reqs[i][0]].append(r[1])
+            reqs[i] = reqs[i] + (r[0], r[3])
+            done += 1
+        if a == 0 and p == 0 and nxt < len(reqs):
+            time.sleep(max(0.0, min(0.01, arrivals[nxt] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    phases = server.profile()
+    st = [s.stats() for s in servers.values()]
+    cu = sum(s["cell_updates"] for s in st)
+    allat = sorted(lat["1d"] + lat["2d"] + lat["3d"])
+    pct = lambda a, f: float(np.percentile(a, f)) if a else None  # noqa: E731
+    # FP64 spot checks of small FP32 results (alone, same server options)
+    checks = []
+    for i, r in enumerate(reqs):
+        if len(checks) >= 4:
+            break
+        kind, q, tend, q32, err = r
+        if err or q.size > 6 * 300_000:
+            continue
+        bt = 1 if kind == "1d" else 2
+        with Server(ev.default_params(g=5.0 / 3.0, cfl=0.5, boundtype=1, tend=1.0), ev.FP64,
+                    0, hbm_budget_bytes=10e9, steps_per_tick=256, max_tube_cells=8192, max_tubes=4) as s64:
+            rid = s64.submit(q, tend, boundtype=bt)
+            while s64.tick() != (0, 0):
+                pass
+            q64 = s64.result(rid)[0]
+        checks.append({"kind": kind, "cells": int(q.size // 6),
+                       "l1_density_f32_vs_f64": float(np.abs(q32[..., 0] - q64[..., 0]).sum()
+                                                      / np.abs(q64[..., 0]).sum())})
+    for s in servers.values():
+        s.close()
+    line = {"metric": METRIC, "value": cu / wall, "unit": METRIC, "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+            "ms_per_step": 1e3 * wall / len(reqs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "serving mix: 60% 1D tubes 128-8192, 30% 2D KH 64^2-1024^2, 10% 3D KH "
+                                   "32^3-128^3, Poisson arrivals", "rate_per_s": args.rate,
+                       "requests": len(reqs), "tick_steps": args.tick_steps, "hbm_budget_gb": 150},
+            "latency_s": {"p50": pct(allat, 50), "p99": pct(allat, 99),
+                          "by_kind": {k: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99)} for k, v in lat.items()}},
+            "wall_s": wall, "cell_updates": cu, "rounds": ticks, "mean_round_ms": 1e3 * tick_s / max(1, ticks),
+            "round_phases_s": phases,
+            "spot_checks_fp64": checks}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -351,9 +451,12 @@ def main():
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
-    ap.add_argument("--workload", default="kh3d", choices=["kh3d", "tubes"],
-                    help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes")
+    ap.add_argument("--workload", default="kh3d", choices=["kh3d", "tubes", "serving"],
+                    help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes; serving: request mix")
     ap.add_argument("--ntubes", type=int, default=4096)
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
+    ap.add_argument("--nrequests", type=int, default=400)
+    ap.add_argument("--tick-steps", type=int, default=32)
     args = ap.parse_args()
     global NX, NY, NZ, AUTOTUNE
     NX = NY = NZ = args.size
@@ -362,6 +465,8 @@ def main():
         args.warmup = 3
     if args.workload == "tubes":
         return run_tubes(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if args.impl == "reference":
         return run_reference(args)
 

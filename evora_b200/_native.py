@@ -148,12 +148,14 @@ def _declare_batch(L):
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),
         "evora_server_destroy": ([G], c_int32),
-        "evora_server_submit": ([G, c_int32, c_int32, c_int32, c_double, c_void_p, ctypes.POINTER(c_int64)],
-                                c_int32),
+        "evora_server_submit": ([G, c_int32, c_int32, c_int32, c_double, c_int32, c_void_p,
+                                 ctypes.POINTER(c_int64)], c_int32),
         "evora_server_tick": ([G, ctypes.POINTER(c_int32), ctypes.POINTER(c_int32)], c_int32),
         "evora_server_result": ([G, c_int64, c_void_p, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int32)],
                                 c_int32),
         "evora_server_stats": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64), _dp], c_int32),
+        "evora_server_completed": ([G, ctypes.POINTER(c_int64), c_int32, ctypes.POINTER(c_int32)], c_int32),
+        "evora_server_profile": ([G, _dp], c_int32),
     }
     for name, (args, res) in sig.items():
         if hasattr(L, name):

@@ -17,7 +17,7 @@ struct TubeState {
   double t, dt, tend;
   long long k;        // steps done
   unsigned err;       // EVORA_ERR_* mask
-  int pad;
+  int bt;             // boundary type of this tube (0: the batch's)
 };
 
 template <typename T>
@@ -31,6 +31,7 @@ struct BatchArgs {
   int ntubes;
   int* head;              // queue head (reset to 0 before each launch)
   int budget;             // max steps per tube in this launch
+  long long quantum;      // if > 0: a tube of n cells runs at most max(1, quantum / n) steps
   int cap;                // tubes with n <= cap live in shared memory
   T* gscratch;            // per-CTA scratch for longer tubes: (NF + 5) * (nmax + 4) each
   int nmax;
@@ -50,6 +51,7 @@ struct BatchPlan {
   int ntubes = 0;
   int* head = nullptr;
   int budget = 1;
+  long long quantum = 0;
   int cap = 0;
   void* gscratch = nullptr;
   int nmax = 0;

@@ -38,6 +38,7 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
   const HydroParams& PP = A.P;
   // compparameter for this tube (parameter.f90:192-205, 1D branch)
   HydroParams P = PP;
+  if (ts->bt) P.boundtype = ts->bt;
   P.nx = n;
   P.ny = 1;
   P.nz = 1;
@@ -62,8 +63,13 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
   unsigned err = 0;
   int steps = 0, go = 1;
   if (tid == 0) *s_err = 0u;
+  int budget = A.budget;
+  if (A.quantum > 0) {
+    const long long b = A.quantum / n;
+    budget = (int)(b < 1 ? 1 : (b < budget ? b : budget));
+  }
   __syncthreads();
-  while (steps < A.budget) {
+  while (steps < budget) {
     // ---- phase 1: primitives (+ ghosts) and the CFL maxima
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
     for (int i = tid; i < wst; i += NT) {

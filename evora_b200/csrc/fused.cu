@@ -41,7 +41,7 @@ void fused_set_tile(FusedPlan* pl, int tile) {
 
 int fused_tiles(const FusedPlan& pl) { return inst_of(pl.precision, pl.strict).tiles(); }
 
-int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* pl) {
+int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* pl, cudaStream_t astream) {
   *pl = FusedPlan{};
   pl->P = P;
   pl->precision = precision;
@@ -56,7 +56,11 @@ int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPla
   fused_set_tile(pl, tile);
   int64_t nb = (pl->n + 255) / 256;
   pl->nblk_tot = (int)(nb > 148 * 4 ? 148 * 4 : nb);
-  if (cudaMalloc(&pl->partials, sizeof(double) * 6 * (pl->nblk_tot + 1)) != cudaSuccess) {
+  pl->alloc_stream = astream;
+  const size_t pbytes = sizeof(double) * 6 * (pl->nblk_tot + 1);
+  const cudaError_t ae = astream ? cudaMallocAsync((void**)&pl->partials, pbytes, astream)
+                                 : cudaMalloc(&pl->partials, pbytes);
+  if (ae != cudaSuccess) {
     cudaGetLastError();
     return EVORA_ERR_NOMEM;
   }
@@ -64,7 +68,10 @@ int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPla
 }
 
 void fused_plan_free(FusedPlan* pl) {
-  if (pl->partials) cudaFree(pl->partials);
+  if (pl->partials) {
+    if (pl->alloc_stream) cudaFreeAsync(pl->partials, pl->alloc_stream);
+    else cudaFree(pl->partials);
+  }
   pl->partials = nullptr;
 }
 

@@ -28,11 +28,14 @@ struct FusedPlan {
   FusedLaunch launch = nullptr;
   void (*cfl)(const FusedPlan&, const void* q, GridCtl* ctl, cudaStream_t st) = nullptr;
   double* partials = nullptr;  // device scratch of the totals reduction
+  cudaStream_t alloc_stream = nullptr;  // non-null: partials came from cudaMallocAsync on it
   int nblk_tot = 0;
 };
 
 // Chooses tiles and the kernel instantiation; allocates small scratch.
-int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* plan);
+// alloc_stream non-null: scratch is allocated stream-ordered on it.
+int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPlan* plan,
+               cudaStream_t alloc_stream = nullptr);
 // Number of tile shapes of the plan's precision, and switching between them.
 int fused_tiles(const FusedPlan& plan);
 void fused_set_tile(FusedPlan* plan, int tile);

@@ -146,6 +146,7 @@ void batch_launch(const BatchPlan& pl, void* q, cudaStream_t st) {
   A.ntubes = pl.ntubes;
   A.head = pl.head;
   A.budget = pl.budget;
+  A.quantum = pl.quantum;
   A.cap = pl.cap;
   A.gscratch = (TT*)pl.gscratch;
   A.nmax = pl.nmax;

@@ -13,6 +13,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <vector>
 
@@ -48,6 +49,9 @@ struct evora_grid {
   std::vector<cudaEvent_t> events;  // 4 per timed step
   size_t ev_used = 0;
   int64_t launches = 0;
+  // multi-step CUDA graphs, key = 2 * steps + starting buffer
+  std::map<long long, cudaGraphExec_t> graphs;
+  bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
 };
 
 namespace {
@@ -97,6 +101,11 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
 
 __global__ void k_step_end(GridCtl* ctl) {
   if (ctl->active && ctl->err == 0) ctl->k += 1;
+}
+
+void drop_graphs(evora_grid* g) {
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();
 }
 
 cudaEvent_t next_event(evora_grid* g) {
@@ -154,26 +163,55 @@ int enqueue_fused_step(evora_grid* g) {
   return 0;
 }
 
+// Device memory of a grid: cudaMalloc, or stream-ordered on the grid's
+// stream for grids made by evora_grid_create_async.
+cudaError_t dalloc(evora_grid* g, void** p, size_t bytes) {
+  return g->async_alloc ? cudaMallocAsync(p, bytes, g->stream) : cudaMalloc(p, bytes);
+}
+void dfree(evora_grid* g, void* p) {
+  if (!p) return;
+  if (g->async_alloc) cudaFreeAsync(p, g->stream);
+  else cudaFree(p);
+}
+
 void free_grid(evora_grid* g) {
   if (!g) return;
+  drop_graphs(g);
   for (cudaEvent_t e : g->events) cudaEventDestroy(e);
   fused_plan_free(&g->plan);
-  cudaFree(g->ctl);
-  cudaFree(g->q_aos);
-  cudaFree(g->w);
-  cudaFree(g->evo);
-  cudaFree(g->s);
-  cudaFree(g->qbuf[0]);
-  cudaFree(g->qbuf[1]);
-  cudaFree(g->aos_stage);
+  dfree(g, g->ctl);
+  dfree(g, g->q_aos);
+  dfree(g, g->w);
+  dfree(g, g->evo);
+  dfree(g, g->s);
+  dfree(g, g->qbuf[0]);
+  dfree(g, g->qbuf[1]);
+  dfree(g, g->aos_stage);
   delete g;
 }
+
+int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStream_t astream, evora_grid** out);
+int graph_steps(evora_grid* g, int nsteps);
 
 }  // namespace
 
 extern "C" {
 
 int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags, evora_grid** out) {
+  return create_grid(p, precision, flags, nullptr, out);
+}
+
+int evora_grid_create_async(const evora_params* p, int32_t precision, int32_t flags, void* stream,
+                            evora_grid** out) {
+  if (!stream) return EVORA_ERR_ARG;
+  return create_grid(p, precision, flags, (cudaStream_t)stream, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStream_t astream, evora_grid** out) {
   if (!p || !out) return EVORA_ERR_ARG;
   *out = nullptr;
   if (precision != EVORA_FP64 && precision != EVORA_FP32) return EVORA_ERR_ARG;
@@ -197,22 +235,24 @@ int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags, e
     return EVORA_ERR_ARG;  // the dual-energy switch is evaluated in FP64 only
   }
   cudaGetDevice(&g->device);
-  if (cudaMalloc(&g->ctl, sizeof(GridCtl)) != cudaSuccess) goto nomem;
+  g->stream = astream;
+  g->async_alloc = astream != nullptr;
+  if (dalloc(g, (void**)&g->ctl, sizeof(GridCtl)) != cudaSuccess) goto nomem;
   if (reference_backend(g)) {
     int64_t nq, nw, ne, ns;
     evora_array_sizes(p, &nq, &nw, &ne, &ns);
-    if (cudaMalloc(&g->q_aos, nq * 8) != cudaSuccess) goto nomem;
-    if (cudaMalloc(&g->w, nw * 8) != cudaSuccess) goto nomem;
-    if (cudaMalloc(&g->evo, ne * 8) != cudaSuccess) goto nomem;
-    if (cudaMalloc(&g->s, ns * 8) != cudaSuccess) goto nomem;
-    if (cudaMemset(g->w, 0, nw * 8) != cudaSuccess) goto nomem;
-    if (cudaMemset(g->evo, 0, ne * 8) != cudaSuccess) goto nomem;  // main.f90:76-77
-    if (cudaMemset(g->s, 0, ns * 8) != cudaSuccess) goto nomem;
+    if (dalloc(g, (void**)&g->q_aos, nq * 8) != cudaSuccess) goto nomem;
+    if (dalloc(g, (void**)&g->w, nw * 8) != cudaSuccess) goto nomem;
+    if (dalloc(g, (void**)&g->evo, ne * 8) != cudaSuccess) goto nomem;
+    if (dalloc(g, (void**)&g->s, ns * 8) != cudaSuccess) goto nomem;
+    if (cudaMemsetAsync(g->w, 0, nw * 8, g->stream) != cudaSuccess) goto nomem;
+    if (cudaMemsetAsync(g->evo, 0, ne * 8, g->stream) != cudaSuccess) goto nomem;  // main.f90:76-77
+    if (cudaMemsetAsync(g->s, 0, ns * 8, g->stream) != cudaSuccess) goto nomem;
   } else {
     size_t bytes = (size_t)g->nf * ncells(g) * elem_size(g);
-    if (cudaMalloc(&g->qbuf[0], bytes) != cudaSuccess) goto nomem;
-    if (cudaMalloc(&g->qbuf[1], bytes) != cudaSuccess) goto nomem;
-    rc = fused_plan(g->P, g->precision, g->nf, (flags & EVORA_STRICT) != 0, &g->plan);
+    if (dalloc(g, &g->qbuf[0], bytes) != cudaSuccess) goto nomem;
+    if (dalloc(g, &g->qbuf[1], bytes) != cudaSuccess) goto nomem;
+    rc = fused_plan(g->P, g->precision, g->nf, (flags & EVORA_STRICT) != 0, &g->plan, astream);
     if (rc) {
       free_grid(g);
       return rc;
@@ -223,7 +263,8 @@ int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags, e
     c.t = p->tstart;
     c.tend = p->tend;
     c.go = 1;
-    if (cudaMemcpy(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess) goto nomem;
+    if (cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream) != cudaSuccess) goto nomem;
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) goto nomem;
   }
   *out = g;
   return 0;
@@ -233,8 +274,16 @@ nomem:
   return EVORA_ERR_NOMEM;
 }
 
+}  // namespace
+
+extern "C" {
+
 int evora_grid_destroy(evora_grid* g) {
   if (!g) return EVORA_ERR_ARG;
+  if (g->async_alloc) {
+    free_grid(g);   // stream-ordered frees: no device-wide synchronisation
+    return 0;
+  }
   if (g->stream) cudaStreamSynchronize(g->stream);
   else cudaDeviceSynchronize();
   free_grid(g);
@@ -243,6 +292,8 @@ int evora_grid_destroy(evora_grid* g) {
 
 int evora_grid_set_stream(evora_grid* g, void* stream) {
   if (!g) return EVORA_ERR_ARG;
+  if (g->async_alloc && (cudaStream_t)stream != g->stream) return EVORA_ERR_ARG;  // memory is ordered on it
+  drop_graphs(g);
   g->stream = (cudaStream_t)stream;
   return 0;
 }
@@ -258,7 +309,7 @@ int evora_grid_set_q(evora_grid* g, const double* q) {
   } else {
     const double* src = q;
     if (!dev) {
-      if (!g->aos_stage) CU(cudaMalloc(&g->aos_stage, nq * 8));
+      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
       CU(cudaMemcpyAsync(g->aos_stage, q, nq * 8, cudaMemcpyHostToDevice, g->stream));
       src = g->aos_stage;
     }
@@ -285,7 +336,7 @@ int evora_grid_get_q(evora_grid* g, double* q) {
   } else {
     double* dst = q;
     if (!dev) {
-      if (!g->aos_stage) CU(cudaMalloc(&g->aos_stage, nq * 8));
+      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
       dst = g->aos_stage;
     }
     fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream);
@@ -297,6 +348,14 @@ int evora_grid_get_q(evora_grid* g, double* q) {
 
 int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync) {
   if (!g || nsteps < 0) return EVORA_ERR_ARG;
+  // Several steps on a capturable stream replay graphs of at most 32 steps
+  // (instantiating a graph costs with its node count; replays are cheap).
+  while (g->stream != nullptr && nsteps >= 2 && !g->timing) {
+    const int chunk = nsteps < 32 ? nsteps : 32;
+    int rc = graph_steps(g, chunk);
+    if (rc) return rc;
+    nsteps -= chunk;
+  }
   for (int i = 0; i < nsteps; ++i) {
     int rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
     if (rc) return rc;
@@ -304,6 +363,53 @@ int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync) {
   if (sync) return evora_grid_status(g);
   return 0;
 }
+
+}  // extern "C"
+
+namespace {
+
+int graph_steps(evora_grid* g, int nsteps) {
+  {
+    // Steps replayed from a CUDA graph (cached per step count and starting
+    // buffer); the step kernels read dt and the active flag from the device
+    // control block, so a graph is valid for any time of the run.
+    const int start = g->cur;
+    const long long key = 2LL * nsteps + start;
+    auto it = g->graphs.find(key);
+    if (it == g->graphs.end()) {
+      cudaGraph_t graph;
+      CU(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = 0;
+      const int64_t launches0 = g->launches;
+      for (int i = 0; i < nsteps && !rc; ++i)
+        rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
+      cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+      g->cur = start;
+      g->launches = launches0;
+      if (rc) return rc;
+      if (e != cudaSuccess) {
+        set_cuda_error(e, "cudaStreamEndCapture");
+        return EVORA_ERR_CUDA;
+      }
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        set_cuda_error(e, "cudaGraphInstantiate");
+        return EVORA_ERR_CUDA;
+      }
+      it = g->graphs.emplace(key, ex).first;
+    }
+    CU(cudaGraphLaunch(it->second, g->stream));
+    if (!reference_backend(g)) g->cur = start ^ (nsteps & 1);
+    g->launches += (int64_t)nsteps * (reference_backend(g) ? 10 : 5);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
 
 int evora_grid_time(evora_grid* g, double* t, double* dt, int32_t* go, int64_t* k) {
   if (!g) return EVORA_ERR_ARG;
@@ -336,6 +442,7 @@ int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms
     return 0;
   }
   const int nt = fused_tiles(g->plan);
+  drop_graphs(g);
   // Save the control block, compute this step's dt, then time each tile's
   // update from the current buffer into the other one; the current state is
   // untouched and the control block is restored afterwards.
@@ -380,6 +487,7 @@ int evora_grid_set_tile(evora_grid* g, int32_t tile) {
   if (!g) return EVORA_ERR_ARG;
   if (reference_backend(g)) return tile == 0 ? 0 : EVORA_ERR_ARG;
   if (tile < 0 || tile >= fused_tiles(g->plan)) return EVORA_ERR_ARG;
+  drop_graphs(g);
   fused_set_tile(&g->plan, tile);
   return 0;
 }

@@ -39,12 +39,15 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
+// REQ_FINISHING: done on the device, result not yet read back (reported as
+// running).
+enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3, REQ_FINISHING = 4 };
 
 struct Request {
   int64_t id = 0;
   int nx = 0, ny = 0, nz = 0;
   double tend = 0.0;
+  int bt = 0;                    // boundary type (0: the server's)
   std::vector<double> q0;        // initial state (host copy), freed at admission
   double t_submit = 0.0, t_done = 0.0;
   int state = REQ_PENDING;
@@ -52,9 +55,10 @@ struct Request {
   int slot = -1;                 // tube slot
   long long off = 0;             // arena offset (tubes)
   evora_grid* grid = nullptr;    // 2D/3D
-  int stream = 0;
+  int stream = 0;                // index into the server's grid streams
   size_t bytes = 0;              // device footprint (grids)
   int64_t steps = 0;
+  int round_steps = 1;           // steps per round (grids)
   unsigned err = 0;
   std::vector<double> result;
   long long cells() const { return (long long)nx * ny * nz; }
@@ -78,7 +82,8 @@ struct evora_server {
   int flags = 0;
   int nf = 5;
   size_t budget = 0, used = 0;
-  int steps_per_tick = 64;
+  int steps_per_tick = 64;       // base step count of a round
+  int max_round_steps = 512;     // cap on a grid's / the tube launch's steps per round
   Clock::time_point t0;
   int64_t next_id = 1;
   std::deque<int64_t> pending;
@@ -93,7 +98,12 @@ struct evora_server {
   int* head = nullptr;
   unsigned long long* cu = nullptr;
   void* gscratch = nullptr;
-  double* stage = nullptr;       // AoS staging of one tube
+  double* stage = nullptr;       // AoS staging of one tube (admission)
+  double* stage2 = nullptr;      // AoS staging of one tube (read-back)
+  cudaStream_t rstream = nullptr;  // read-back of finished tubes
+  std::vector<int> free_streams;   // indices of idle grid streams
+  std::vector<Request*> to_free;   // grids read back, destroyed after the round
+  std::deque<int64_t> completed;   // ids finished since the last evora_server_completed
   std::vector<int64_t> slot_req; // slot -> request id (0 = free)
   std::vector<std::pair<long long, long long>> free_seg;  // (offset, length), sorted
   BatchPlan plan{};
@@ -107,6 +117,9 @@ struct evora_server {
   long long grid_cell_updates = 0;
   double first_submit = -1.0, last_done = 0.0;
   size_t fixed = 0;              // arena and staging
+  // host time per round phase: launch, read-back, admission, wait, free, detect
+  double phase_s[6] = {0, 0, 0, 0, 0, 0};
+  long long rounds = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
   size_t esize() const { return precision == EVORA_FP32 ? 4 : 8; }
@@ -162,16 +175,19 @@ int admit(evora_server* s, Request& r) {
     r.slot = slot;
     r.off = off;
     s->slot_req[slot] = r.id;
-    CU(cudaMemcpyAsync(s->stage, r.q0.data(), sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->tstream));
-    tube_from_aos(s->stage, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->tstream);
+    // on the read-back stream: the running tube launch never touches a free
+    // slot or a free arena segment, so the upload overlaps it
+    CU(cudaMemcpyAsync(s->stage, r.q0.data(), sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->rstream));
+    tube_from_aos(s->stage, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->rstream);
     TubeState ts{};
     ts.offset = off;
     ts.n = r.nx;
     ts.status = TUBE_RUNNING;
     ts.t = s->base.tstart;
     ts.tend = r.tend;
-    CU(cudaMemcpyAsync(s->tubes + slot, &ts, sizeof ts, cudaMemcpyHostToDevice, s->tstream));
-    CU(cudaStreamSynchronize(s->tstream));
+    ts.bt = r.bt;
+    CU(cudaMemcpyAsync(s->tubes + slot, &ts, sizeof ts, cudaMemcpyHostToDevice, s->rstream));
+    CU(cudaStreamSynchronize(s->rstream));
     s->active_tubes++;
     s->order_dirty = true;
   } else {
@@ -182,19 +198,37 @@ int admit(evora_server* s, Request& r) {
     p.ny = r.ny;
     p.nz = r.nz;
     p.tend = r.tend;
+    if (r.bt) p.boundtype = r.bt;
     evora_grid* g = nullptr;
-    int rc = evora_grid_create(&p, s->precision, s->flags & ~EVORA_REFERENCE_KERNELS, &g);
+    // a stream per running grid (recycled), so that waiting for or reading
+    // back one grid never waits for another; the grid's memory is
+    // stream-ordered on it, so retiring a grid never synchronises the device
+    if (s->free_streams.empty()) {
+      cudaStream_t st;
+      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+      }
+      s->gstreams.push_back(st);
+      s->free_streams.push_back((int)s->gstreams.size() - 1);
+    }
+    const int si = s->free_streams.back();
+    int rc = evora_grid_create_async(&p, s->precision, s->flags & ~EVORA_REFERENCE_KERNELS, s->gstreams[si], &g);
     if (rc) return rc == EVORA_ERR_NOMEM ? 1 : rc;
-    r.stream = s->next_stream;
-    s->next_stream = (s->next_stream + 1) % (int)s->gstreams.size();
-    evora_grid_set_stream(g, s->gstreams[r.stream]);
+    s->free_streams.pop_back();
+    r.stream = si;
     rc = evora_grid_set_q(g, r.q0.data());
     if (rc) {
       evora_grid_destroy(g);
+      s->free_streams.push_back(si);
       return rc == EVORA_ERR_NOMEM ? 1 : rc;
     }
     r.grid = g;
     r.bytes = bytes;
+    // time quantum: a round gives each grid about the same device time, so
+    // its step count falls with its size (2^20 cell-updates per base step)
+    const double quantum = (double)s->steps_per_tick * (double)(1 << 20);
+    r.round_steps = (int)std::max(1.0, std::min((double)s->max_round_steps, quantum / (double)r.cells()));
     s->used += bytes;
   }
   r.state = REQ_RUNNING;
@@ -208,6 +242,7 @@ void finish(evora_server* s, Request& r, unsigned err) {
   r.t_done = s->now();
   s->last_done = r.t_done;
   s->latencies.push_back(r.t_done - r.t_submit);
+  s->completed.push_back(r.id);
 }
 
 int upload_order(evora_server* s) {
@@ -265,11 +300,20 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
   s->slot_req.assign(max_tubes, 0);
   s->free_seg = {{0, s->arena}};
   if (cudaStreamCreateWithFlags(&s->tstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
-  for (int i = 0; i < 8; ++i) {
-    cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) goto fail;
-    s->gstreams.push_back(st);
+  {
+    // keep memory freed by retired grids in the device's default pool for
+    // the next admissions instead of returning it to the driver
+    int dev = 0;
+    cudaMemPool_t pool;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = (uint64_t)s->budget;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
   }
+  if (cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->stage2, sizeof(double) * EVORA_NQ * max_tube_cells) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->q, arena_bytes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->tubes, sizeof(TubeState) * max_tubes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->order, sizeof(int) * max_tubes) != cudaSuccess) goto fail;
@@ -297,16 +341,22 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
     pl.order = s->order;
     pl.ntubes = 0;
     pl.head = s->head;
-    pl.budget = steps_per_tick;
+    // a round gives each tube about steps_per_tick * 2^14 cell-steps (at
+    // most 8 * steps_per_tick steps), so long and short tubes take similar
+    // device time per round
+    s->max_round_steps = 8 * steps_per_tick;
+    pl.budget = 8 * steps_per_tick;
+    pl.quantum = (long long)steps_per_tick << 14;
     pl.nmax = max_tube_cells;
     pl.cell_updates = s->cu;
     const size_t per_cell = (size_t)(s->nf + 5) * s->esize();
-    pl.cap = std::min(max_tube_cells, (int)((227 * 1024 / 2 - 2048) / per_cell) - 4);
-    s->launch = batch_pick_for(precision, (flags & EVORA_STRICT) != 0, s->nf, 256, &pl);
+    // one CTA of 512 threads per SM, the largest shared-memory staging
+    pl.cap = std::min(max_tube_cells, (int)((227 * 1024 - 4096) / per_cell) - 4);
+    s->launch = batch_pick_for(precision, (flags & EVORA_STRICT) != 0, s->nf, 512, &pl);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = batch_ctas_per_sm(precision, (flags & EVORA_STRICT) != 0, s->nf, 256, pl.smem);
+    int per_sm = batch_ctas_per_sm(precision, (flags & EVORA_STRICT) != 0, s->nf, 512, pl.smem);
     pl.ctas = std::max(1, sms * std::max(1, per_sm));
     if (max_tube_cells > pl.cap) {
       size_t need = (size_t)pl.ctas * (size_t)(s->nf + 5) * (size_t)(max_tube_cells + 4) * s->esize();
@@ -340,15 +390,18 @@ int evora_server_destroy(evora_server* s) {
   cudaFree(s->cu);
   cudaFree(s->gscratch);
   cudaFree(s->stage);
+  cudaFree(s->stage2);
+  if (s->rstream) cudaStreamDestroy(s->rstream);
   if (s->tstream) cudaStreamDestroy(s->tstream);
   for (auto st : s->gstreams) cudaStreamDestroy(st);
   delete s;
   return 0;
 }
 
-int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, const double* q0,
-                        int64_t* id) {
+int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int32_t boundtype,
+                        const double* q0, int64_t* id) {
   if (!s || !q0 || !id || nx < 2 || ny < 1 || nz < 1 || (nz > 1 && ny == 1)) return EVORA_ERR_ARG;
+  if (boundtype < 0 || boundtype > 3) return EVORA_ERR_ARG;
   const bool tube = (ny == 1 && nz == 1);
   if (tube && nx > s->max_tube) return EVORA_ERR_ARG;
   Request r;
@@ -357,6 +410,7 @@ int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, dou
   r.ny = ny;
   r.nz = nz;
   r.tend = tend;
+  r.bt = boundtype;
   r.tube = tube;
   r.q0.assign(q0, q0 + (size_t)EVORA_NQ * nx * ny * nz);
   r.t_submit = s->now();
@@ -370,20 +424,15 @@ int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, dou
 
 int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   if (!s) return EVORA_ERR_ARG;
-  // 1. admission, in arrival order, while memory and slots allow
-  while (!s->pending.empty()) {
-    Request& r = s->reqs[s->pending.front()];
-    int rc = admit(s, r);
-    if (rc == 1) {
-      bool idle = s->active_tubes == 0;
-      for (auto& kv : s->reqs) idle = idle && !(kv.second.state == REQ_RUNNING);
-      if (!idle) break;           // head of the queue waits for room
-      rc = EVORA_ERR_NOMEM;       // nothing running and still no room: it never fits
-    }
-    s->pending.pop_front();
-    if (rc) finish(s, r, (unsigned)rc);
-  }
-  // 2. one round of steps for everything active, tubes and grids concurrently
+  double tp = s->now();
+  auto mark = [&](int phase) {
+    const double t = s->now();
+    s->phase_s[phase] += t - tp;
+    tp = t;
+  };
+  // 1. (admission happens below, while the round runs; new work starts next round)
+  // 2. launch one round of steps for everything running: the tube launch and
+  //    each grid's graph on its own stream, concurrently
   if (s->order_dirty) {
     int rc = upload_order(s);
     if (rc) return rc;
@@ -397,12 +446,61 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   for (auto& kv : s->reqs)
     if (kv.second.state == REQ_RUNNING && kv.second.grid) {
       grids.push_back(&kv.second);
-      int rc = evora_grid_step(kv.second.grid, s->steps_per_tick, 0);
+      int rc = evora_grid_step(kv.second.grid, kv.second.round_steps, 0);
       if (rc) return rc;
     }
+  mark(0);
+  // 3. while the GPU works: read back what finished in the previous round
+  for (auto& kv : s->reqs) {
+    Request& r = kv.second;
+    if (r.state != REQ_FINISHING) continue;
+    r.result.resize((size_t)EVORA_NQ * r.cells());
+    int rc = 0;
+    if (r.tube) {
+      tube_to_aos(s->q, s->stage2, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->rstream);
+      CU(cudaMemcpyAsync(r.result.data(), s->stage2, sizeof(double) * r.result.size(), cudaMemcpyDeviceToHost,
+                         s->rstream));
+      CU(cudaStreamSynchronize(s->rstream));
+      free_segment(s, r.off, r.nx);
+      s->slot_req[r.slot] = 0;
+    } else {
+      rc = evora_grid_get_q(r.grid, r.result.data());
+      s->grid_cell_updates += (long long)r.steps * r.cells();
+      s->to_free.push_back(&r);
+    }
+    finish(s, r, r.err | (unsigned)rc);
+  }
+  mark(1);
+  // 3b. admission, in arrival order, while memory and slots allow (host
+  //     copies overlap the round); admitted work starts with the next round
+  while (!s->pending.empty()) {
+    Request& r = s->reqs[s->pending.front()];
+    int rc = admit(s, r);
+    if (rc == 1) {
+      bool idle = s->active_tubes == 0 && s->to_free.empty() && grids.empty();
+      for (auto& kv : s->reqs)
+        idle = idle && kv.second.state != REQ_RUNNING && kv.second.state != REQ_FINISHING;
+      if (!idle) break;           // head of the queue waits for room
+      rc = EVORA_ERR_NOMEM;       // nothing running and still no room: it never fits
+    }
+    s->pending.pop_front();
+    if (rc) finish(s, r, (unsigned)rc);
+  }
+  mark(2);
+  // 4. wait for the round
   CU(cudaStreamSynchronize(s->tstream));
-  for (auto st : s->gstreams) CU(cudaStreamSynchronize(st));
-  // 3. retire finished work
+  for (Request* r : grids) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+  mark(3);
+  // 5. grids read back above can go now (their streams are idle)
+  for (Request* r : s->to_free) {
+    evora_grid_destroy(r->grid);
+    r->grid = nullptr;
+    s->used -= r->bytes;
+    s->free_streams.push_back(r->stream);
+  }
+  s->to_free.clear();
+  mark(4);
+  // 6. detect finished work; it is read back during the next round
   if (s->plan.ntubes > 0) {
     std::vector<TubeState> ts(s->max_slots);
     CU(cudaMemcpy(ts.data(), s->tubes, sizeof(TubeState) * s->max_slots, cudaMemcpyDeviceToHost));
@@ -411,19 +509,10 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       Request& r = s->reqs[s->slot_req[i]];
       if (r.state != REQ_RUNNING || ts[i].status == TUBE_RUNNING) continue;
       r.steps = ts[i].k;
-      r.result.resize((size_t)EVORA_NQ * r.nx);
-      tube_to_aos(s->q, s->stage, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->tstream);
-      CU(cudaMemcpyAsync(r.result.data(), s->stage, sizeof(double) * r.result.size(), cudaMemcpyDeviceToHost,
-                         s->tstream));
-      CU(cudaStreamSynchronize(s->tstream));
-      TubeState idle{};
-      idle.status = TUBE_IDLE;
-      CU(cudaMemcpy(s->tubes + i, &idle, sizeof idle, cudaMemcpyHostToDevice));
-      free_segment(s, r.off, r.nx);
-      s->slot_req[i] = 0;
+      r.err = ts[i].err;
+      r.state = REQ_FINISHING;
       s->active_tubes--;
       s->order_dirty = true;
-      finish(s, r, ts[i].err);
     }
   }
   for (Request* r : grids) {
@@ -435,16 +524,13 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     const int st = evora_grid_status(r->grid);
     if (go && !st) continue;
     r->steps = k;
-    r->result.resize((size_t)EVORA_NQ * r->cells());
-    rc = evora_grid_get_q(r->grid, r->result.data());
-    s->grid_cell_updates += (long long)k * r->cells();
-    evora_grid_destroy(r->grid);
-    r->grid = nullptr;
-    s->used -= r->bytes;
-    finish(s, *r, (unsigned)(st | rc));
+    r->err = (unsigned)st;
+    r->state = REQ_FINISHING;
   }
+  mark(5);
+  s->rounds++;
   int act = 0;
-  for (auto& kv : s->reqs) act += kv.second.state == REQ_RUNNING;
+  for (auto& kv : s->reqs) act += kv.second.state == REQ_RUNNING || kv.second.state == REQ_FINISHING;
   if (n_active) *n_active = act;
   if (n_pending) *n_pending = (int32_t)s->pending.size();
   return 0;
@@ -459,7 +545,7 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
     return EVORA_ERR_ARG;
   }
   Request& r = it->second;
-  if (state) *state = r.state;
+  if (state) *state = r.state == REQ_FINISHING ? REQ_RUNNING : r.state;
   if (r.state != REQ_DONE && r.state != REQ_FAILED) return 0;
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (steps) *steps = r.steps;
@@ -467,6 +553,24 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
   const int err = (int)r.err;
   if (q_out) s->reqs.erase(it);   // delivered
   return err;
+}
+
+int evora_server_profile(evora_server* s, double out[7]) {
+  if (!s || !out) return EVORA_ERR_ARG;
+  for (int i = 0; i < 6; ++i) out[i] = s->phase_s[i];
+  out[6] = (double)s->rounds;
+  return 0;
+}
+
+int evora_server_completed(evora_server* s, int64_t* ids, int32_t max_ids, int32_t* n) {
+  if (!s || !n || (max_ids > 0 && !ids)) return EVORA_ERR_ARG;
+  int32_t k = 0;
+  while (k < max_ids && !s->completed.empty()) {
+    ids[k++] = s->completed.front();
+    s->completed.pop_front();
+  }
+  *n = k;
+  return 0;
 }
 
 int evora_server_stats(evora_server* s, double* p50_s, double* p99_s, int64_t* completed, int64_t* cell_updates,

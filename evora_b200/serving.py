@@ -45,16 +45,17 @@ class Server:
     def __exit__(self, *exc):
         self.close()
 
-    def submit(self, q0: np.ndarray, tend: float) -> int:
-        """q0: (nz, ny, nx, 6) float64 (a 1D tube may be given as (n, 6))."""
+    def submit(self, q0: np.ndarray, tend: float, boundtype: int = 0) -> int:
+        """q0: (nz, ny, nx, 6) float64 (a 1D tube may be given as (n, 6));
+        boundtype 1..3 overrides the server's for this request."""
         q0 = np.ascontiguousarray(q0, dtype=np.float64)
         if q0.ndim == 2:
             nz, ny, nx = 1, 1, q0.shape[0]
         else:
             nz, ny, nx = q0.shape[:3]
         rid = ctypes.c_int64()
-        check(lib().evora_server_submit(self._h, nx, ny, nz, float(tend), ctypes.c_void_p(q0.ctypes.data),
-                                        ctypes.byref(rid)), "server_submit")
+        check(lib().evora_server_submit(self._h, nx, ny, nz, float(tend), int(boundtype),
+                                        ctypes.c_void_p(q0.ctypes.data), ctypes.byref(rid)), "server_submit")
         self.shapes[rid.value] = q0.shape
         return rid.value
 
@@ -87,3 +88,19 @@ class Server:
                                        ctypes.byref(cu), ctypes.byref(span)), "server_stats")
         return dict(p50_s=p50.value, p99_s=p99.value, completed=done.value, cell_updates=cu.value,
                     span_s=span.value)
+
+    def completed(self, max_ids: int = 4096):
+        """Ids finished since the last call (oldest first)."""
+        buf = (ctypes.c_int64 * max_ids)()
+        n = ctypes.c_int32()
+        check(lib().evora_server_completed(self._h, buf, max_ids, ctypes.byref(n)), "server_completed")
+        return list(buf[:n.value])
+
+    def profile(self):
+        """Host seconds per round phase and the number of rounds."""
+        out = (ctypes.c_double * 7)()
+        check(lib().evora_server_profile(self._h, out), "server_profile")
+        names = ["launch", "readback", "admission", "wait", "free", "detect"]
+        d = {n: out[i] for i, n in enumerate(names)}
+        d["rounds"] = int(out[6])
+        return d

@@ -192,6 +192,15 @@ int evora_grid_create(const evora_params* p, int32_t precision, int32_t flags,
                       evora_grid** out);
 int evora_grid_destroy(evora_grid* g);
 
+/* As evora_grid_create, but all device memory of the grid is allocated
+ * stream-ordered on `stream` (cudaMallocAsync from the device's default
+ * pool) and freed the same way by evora_grid_destroy, so creating and
+ * destroying grids never synchronises the device; the grid works on that
+ * stream for its whole life.  For callers that create and retire many grids
+ * while others run (a request loop). */
+int evora_grid_create_async(const evora_params* p, int32_t precision, int32_t flags, void* stream,
+                            evora_grid** out);
+
 /* Work on this CUDA stream (cudaStream_t); NULL = the default stream. */
 int evora_grid_set_stream(evora_grid* g, void* stream);
 
@@ -282,7 +291,9 @@ int evora_batch_autotune(evora_batch* b, int32_t steps, int32_t* threads, int32_
  * end time; the other options come from *base.  evora_server_tick admits
  * pending requests in arrival order while their device footprint fits the
  * HBM budget (1D requests also need a free tube slot and arena room), then
- * advances everything admitted by up to steps_per_tick steps: 1D requests
+ * advances everything admitted by one round -- a time quantum: a grid of c
+ * cells gets min(8 * steps_per_tick, steps_per_tick * 2^20 / c) steps, the
+ * tube launch up to 8 * steps_per_tick steps per tube: 1D requests
  * together in one persistent batched-tube launch, 2D/3D requests as resident
  * grids on their own streams, concurrently; finished requests are read back
  * and their time to solution (submit to read-back) recorded.  A request's
@@ -294,9 +305,10 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
                         int32_t steps_per_tick, int32_t max_tube_cells, int32_t max_tubes,
                         evora_server** out);
 int evora_server_destroy(evora_server* s);
-/* Queues a request; *id identifies it.  EVORA_ERR_ARG if it can never fit. */
-int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, const double* q0,
-                        int64_t* id);
+/* Queues a request; *id identifies it.  boundtype 1..3 overrides the
+ * server's for this request (0 keeps it).  EVORA_ERR_ARG if it can never fit. */
+int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int32_t boundtype,
+                        const double* q0, int64_t* id);
 /* One scheduling round (admit, step, retire); reports active/pending counts. */
 int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending);
 /* state: 0 pending, 1 running, 2 done, 3 failed, -1 unknown id.  When done or
@@ -304,6 +316,13 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending);
  * latency and step count, and forgets the request.  Returns its error mask. */
 int evora_server_result(evora_server* s, int64_t id, double* q_out, double* latency_s, int64_t* steps,
                         int32_t* state);
+/* Host seconds spent per round phase so far: out[0] launch, [1] read-back,
+ * [2] admission, [3] waiting for the device, [4] freeing, [5] completion
+ * checks; out[6] the number of rounds. */
+int evora_server_profile(evora_server* s, double out[7]);
+/* Ids of requests finished (done or failed) since the last call, oldest
+ * first, at most max_ids of them; *n receives the count. */
+int evora_server_completed(evora_server* s, int64_t* ids, int32_t max_ids, int32_t* n);
 /* p50 / p99 time to solution of completed requests, their count, the total
  * cell-updates and the time from the first submit to the last completion. */
 int evora_server_stats(evora_server* s, double* p50_s, double* p99_s, int64_t* completed,
