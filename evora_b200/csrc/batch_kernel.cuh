@@ -78,7 +78,7 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
       T qv[6], wv[5];
 #pragma unroll
       for (int f = 0; f < NF; ++f) qv[f] = qs[f * n + g];
-      prim(qv, wv, c, P, de, err);
+      prim_k(qv, wv, c, P, de, err);
       if (flip) {
         wv[1] = -wv[1];
         wv[2] = -wv[2];
@@ -152,8 +152,8 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
         if (P.secondorder) {
           T s[5], a[5];
 #pragma unroll
-          for (int f = 0; f < 5; ++f) s[f] = slope1(w[f * wst + wi - 1], wc[f], w[f * wst + wi + 1], P.limiter);
-          predictor_term(wc, s, 1, c.g, a);
+          for (int f = 0; f < 5; ++f) s[f] = slope_k(w[f * wst + wi - 1], wc[f], w[f * wst + wi + 1], P.limiter);
+          pred_k(wc, s, 1, c.g, kFast ? rcp_fast(wc[0]) : (T)0, a);
 #pragma unroll
           for (int f = 0; f < 5; ++f) {
             const T e = dt2 * a[f] * dxi;                  // muscl.f90:68
@@ -166,7 +166,7 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
         }
         if (cc > i0 - 1) {
           T fr[NF];
-          riemann<T, NF>(fp_prev, fm, fr, 1, P.solver, c, err);   // interface cc-1/2
+          riemann_k<T, NF, 1>(fp_prev, fm, fr, P.solver, c, err);   // interface cc-1/2
           if (cc - 1 >= i0) {
             T qv[6], wd[5];
 #pragma unroll

@@ -3,5 +3,6 @@
 // on rho, m and E (the entropy field goes through pow).
 #define EVORA_FNS f64s
 #define EVORA_T double
+#define EVORA_FAST 0
 #define EVORA_PRECISION_F32 0
 #include "fused_inst.cuh"

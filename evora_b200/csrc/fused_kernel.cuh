@@ -115,6 +115,44 @@ __device__ __forceinline__ void prim(T* q, T* w, const Gas<T>& c, const HydroPar
   }
 }
 
+// Arithmetic form of this translation unit: EVORA_FAST = 1 selects the fast
+// forms of hydro_math.cuh (FP32, default FP64), 0 the literal reference
+// forms (strict FP64, and the host emulation).
+#ifndef EVORA_FAST
+#define EVORA_FAST 0
+#endif
+constexpr bool kFast = EVORA_FAST != 0;
+
+template <typename T>
+__device__ __forceinline__ T slope_k(T wl, T w, T wr, int limiter) {
+  if constexpr (kFast) return slope_fast(wl, w, wr, limiter);
+  else return slope1(wl, w, wr, limiter);
+}
+
+template <typename T>
+__device__ __forceinline__ void pred_k(const T* w, const T* s, int d, T g, T rinv, T* a) {
+  if constexpr (kFast) predictor_term_fast(w, s, d, g, rinv, a);
+  else predictor_term(w, s, d, g, a);
+}
+
+template <typename T, int NF, int DIR>
+__device__ __forceinline__ void riemann_k(const T* wl, const T* wr, T* f, int solver, const Gas<T>& c,
+                                          unsigned& err) {
+  if constexpr (kFast) riemann_fast<T, NF, DIR>(wl, wr, f, solver, c, err);
+  else riemann<T, NF>(wl, wr, f, DIR, solver, c, err);
+}
+
+template <typename T>
+__device__ __forceinline__ void prim_k(T* q, T* w, const Gas<T>& c, const HydroParams& P, bool de, unsigned& err) {
+  if constexpr (kFast && sizeof(T) == 8) {
+    if (!de) {
+      q2w_fast(q, w, c, err);
+      return;
+    }
+  }
+  prim(q, w, c, P, de, err);
+}
+
 // Shared-memory layout of one CTA (all arrays field-major).
 template <typename T, int NF, int TX, int TY>
 struct FusedSmem {
@@ -136,9 +174,9 @@ __device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn,
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
     wv[f] = sm.w[sc][f][cy][cx];
-    sx[f] = slope1(sm.w[sc][f][cy][cx - 1], wv[f], sm.w[sc][f][cy][cx + 1], P.limiter);
-    sy[f] = slope1(sm.w[sc][f][cy - 1][cx], wv[f], sm.w[sc][f][cy + 1][cx], P.limiter);
-    if (DIM == 3) sz[f] = slope1(sm.w[sp][f][cy][cx], wv[f], sm.w[sn][f][cy][cx], P.limiter);
+    sx[f] = slope_k(sm.w[sc][f][cy][cx - 1], wv[f], sm.w[sc][f][cy][cx + 1], P.limiter);
+    sy[f] = slope_k(sm.w[sc][f][cy - 1][cx], wv[f], sm.w[sc][f][cy + 1][cx], P.limiter);
+    if (DIM == 3) sz[f] = slope_k(sm.w[sp][f][cy][cx], wv[f], sm.w[sn][f][cy][cx], P.limiter);
   }
   if (!P.secondorder) {
     // first-order Godunov: the face states are the cell averages (sweep,
@@ -151,9 +189,10 @@ __device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn,
   }
   T a1[5], a2[5], a3[5], evo[5];
   const T g = (T)P.g;
-  predictor_term(wv, sx, 1, g, a1);
-  predictor_term(wv, sy, 2, g, a2);
-  if (DIM == 3) predictor_term(wv, sz, 3, g, a3);
+  const T rinv = kFast ? rcp_fast(wv[0]) : (T)0;
+  pred_k(wv, sx, 1, g, rinv, a1);
+  pred_k(wv, sy, 2, g, rinv, a2);
+  if (DIM == 3) pred_k(wv, sz, 3, g, rinv, a3);
   const T dxi = (T)P.dxinv, dyi = (T)P.dyinv, dzi = (T)P.dzinv;
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
@@ -234,7 +273,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
       T qv[6], wv[5];
 #pragma unroll
       for (int f = 0; f < NF; ++f) qv[f] = ld(plane + (size_t)f * n + idx);
-      prim(qv, wv, c, P, de, err);
+      prim_k(qv, wv, c, P, de, err);
       if (flip) {
         wv[1] = -wv[1];
         wv[2] = -wv[2];
@@ -338,7 +377,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
             wl[f] = sm.xf[1][f][j][i];
             wr[f] = sm.xf[0][f][j][i + 1];
           }
-          riemann<T, NF>(wl, wr, fv, 1, P.solver, c, err);
+          riemann_k<T, NF, 1>(wl, wr, fv, P.solver, c, err);
 #pragma unroll
           for (int f = 0; f < NF; ++f) sm.fx[f][j][i] = fv[f];
         } else {
@@ -349,7 +388,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
             wl[f] = sm.yf[1][f][j][i];
             wr[f] = sm.yf[0][f][j + 1][i];
           }
-          riemann<T, NF>(wl, wr, fv, 2, P.solver, c, err);
+          riemann_k<T, NF, 2>(wl, wr, fv, P.solver, c, err);
 #pragma unroll
           for (int f = 0; f < NF; ++f) sm.fy[f][j][i] = fv[f];
         }
@@ -358,7 +397,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
     T fz[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) fz[f] = (T)0;
-    if (DIM == 3 && owned && cz > zfirst) riemann<T, NF>(wzp_prev, wzm_cur, fz, 3, P.solver, c, err);
+    if (DIM == 3 && owned && cz > zfirst) riemann_k<T, NF, 3>(wzp_prev, wzm_cur, fz, P.solver, c, err);
     EV_SYNC();
     // ---- D
     if (owned) {
@@ -434,7 +473,7 @@ __device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
     T qv[6];
 #pragma unroll
     for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + m);
-    prim(qv, w[o], c, P, de, err);
+    prim_k(qv, w[o], c, P, de, err);
     if (flip) {
       w[o][1] = -w[o][1];
       w[o][2] = -w[o][2];
@@ -447,8 +486,8 @@ __device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
     if (P.secondorder) {
       T s[5], a[5];
 #pragma unroll
-      for (int f = 0; f < 5; ++f) s[f] = slope1(w[k][f], w[k + 1][f], w[k + 2][f], P.limiter);
-      predictor_term(w[k + 1], s, 1, (T)P.g, a);
+      for (int f = 0; f < 5; ++f) s[f] = slope_k(w[k][f], w[k + 1][f], w[k + 2][f], P.limiter);
+      pred_k(w[k + 1], s, 1, (T)P.g, kFast ? rcp_fast(w[k + 1][0]) : (T)0, a);
 #pragma unroll
       for (int f = 0; f < 5; ++f) {
         const T e = dt2 * a[f] * dxi;
@@ -461,8 +500,8 @@ __device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
     }
   }
   T flo[NF], fhi[NF];
-  riemann<T, NF>(fp[0], fm[1], flo, 1, P.solver, c, err);
-  riemann<T, NF>(fp[1], fm[2], fhi, 1, P.solver, c, err);
+  riemann_k<T, NF, 1>(fp[0], fm[1], flo, P.solver, c, err);
+  riemann_k<T, NF, 1>(fp[1], fm[2], fhi, P.solver, c, err);
   T qv[6], wd[5];
 #pragma unroll
   for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + i);

@@ -262,6 +262,136 @@ __device__ __forceinline__ void riemann(const T* wl, const T* wr, T* f, int dir,
   else hllc<T, NF>(wl, wr, f, dir, c, err);
 }
 
+// ------------------------------------------------------------------------
+// Fast forms (FP32, and FP64 outside the strict mode).  Same formulas as the
+// reference routines above, with the divisions shared through reciprocals
+// and the energy flux written as u_d (E + p) from one E; results agree with
+// the literal forms to a few ulp per operation (the strict FP64 mode keeps
+// the literal forms).
+
+// Reciprocal.  FP32: the fast-math division of its translation unit.  FP64:
+// Newton-Raphson on a single-precision seed (two iterations: the relative
+// error e of the seed becomes e^2 then e^4, ~2^-92 from 2^-23, i.e. the
+// result is within an ulp).  Valid for |x| in about [1e-37, 1e37], the range
+// of the single-precision seed.
+__device__ __forceinline__ float rcp_fast(float x) { return 1.0f / x; }
+__device__ __forceinline__ double rcp_fast(double x) {
+#if defined(__CUDA_ARCH__)
+  double r = (double)__frcp_rn((float)x);
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+#else
+  return 1.0 / x;
+#endif
+}
+
+// minmod without branches: 0 unless both differences have the same sign,
+// else the one of smaller magnitude.
+template <typename T>
+__device__ __forceinline__ T minmod_fast(T dwl, T dwr) {
+  const T m = fmin(fabs(dwl), fabs(dwr));
+  return dwl * dwr > (T)0 ? copysign(m, dwl) : (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ T slope_fast(T wl, T w, T wr, int limiter) {
+  if (limiter == 1) return minmod_fast(w - wl, wr - w);
+  return slope1(wl, w, wr, limiter);
+}
+
+// q2w with one reciprocal (comp.f90:26-43, 56-71 without dual energy).
+template <typename T>
+__device__ __forceinline__ void q2w_fast(const T* q, T* w, const Gas<T>& c, unsigned& err) {
+  const T densinv = rcp_fast(q[0]);
+  w[0] = q[0];
+  w[1] = q[1] * densinv;
+  w[2] = q[2] * densinv;
+  w[3] = q[3] * densinv;
+  const T m2 = (q[1] * q[1]) + (q[2] * q[2]) + (q[3] * q[3]);
+  const T p = c.g1 * (q[4] - (T)0.5 * m2 * densinv);
+  if (p <= (T)0) err |= EVORA_ERR_PRESSURE;
+  w[4] = p;
+}
+
+// predictor term with the 1/rho of the cell given (muscl.f90:100-104).
+template <typename T>
+__device__ __forceinline__ void predictor_term_fast(const T* w, const T* s, int d, T g, T rinv, T* a) {
+#pragma unroll
+  for (int f = 0; f < 5; ++f) a[f] = w[d] * s[f];
+  a[4] = a[4] + g * w[4] * s[d];
+  a[d] = a[d] + s[4] * rinv;
+}
+
+// HLLC (riemann.f90:96-153) in the fast form.  DIR = 1..3.
+template <typename T, int NF, int DIR>
+__device__ __forceinline__ void hllc_fast(const T* wl, const T* wr, T* f, const Gas<T>& c, unsigned& err) {
+  if (wl[4] <= (T)0 || wr[4] <= (T)0) err |= EVORA_ERR_RIEMANN_PRESSURE;
+  const T ril = rcp_fast(wl[0]), rir = rcp_fast(wr[0]);
+  const T al = dsqrt(c.g * wl[4] * ril);
+  const T ar = dsqrt(c.g * wr[4] * rir);
+  const T ul = wl[DIR], ur = wr[DIR];
+  const T sl = fmin2(ul - al, ur - ar);
+  const T sr = fmax2(ul + al, ur + ar);
+  const T facl = wl[0] * (sl - ul);
+  const T facr = wr[0] * (sr - ur);
+  const T sm = (wr[4] - wl[4] + facl * ul - facr * ur) * rcp_fast(facl - facr);
+  // the side whose state (or star state) gives the flux
+  const bool left = (T)0 < sl || (!((T)0 > sr) && sl < (T)0 && (T)0 < sm);
+  const bool star = !((T)0 < sl) && !((T)0 > sr);
+  if (star && !(sl < (T)0 && (T)0 < sm) && !(sm <= (T)0 && (T)0 < sr)) err |= EVORA_ERR_HLLC;
+  const T* w = left ? wl : wr;
+  const T ri = left ? ril : rir;
+  const T sk = left ? sl : sr;
+  const T fk = left ? facl : facr;
+  const T ud = w[DIR];
+  const T u2 = w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
+  const T e = (T)0.5 * w[0] * u2 + w[4] * c.g1inv;   // total energy
+  const T mu = w[0] * ud;                            // mass flux
+  T fl[6], ql[6];
+  ql[0] = w[0];
+  ql[1] = w[0] * w[1];
+  ql[2] = w[0] * w[2];
+  ql[3] = w[0] * w[3];
+  ql[4] = e;
+  fl[0] = mu;
+  fl[1] = mu * w[1];
+  fl[2] = mu * w[2];
+  fl[3] = mu * w[3];
+  fl[DIR] += w[4];
+  fl[4] = ud * (e + w[4]);
+  if (NF == 6) {
+    const T pg = dpow(w[0], c.g1);
+    fl[5] = ud * w[4] / pg;
+    ql[5] = w[4] / pg;
+  }
+  if (!star) {
+#pragma unroll
+    for (int i = 0; i < NF; ++i) f[i] = fl[i];
+    return;
+  }
+  // star state (statex, riemann.f90:241-288)
+  const T chi = fk * rcp_fast(sk - sm);           // rho (s - u_d) / (s - sm)
+  T qx[6];
+  qx[0] = chi;
+  qx[1] = chi * w[1];
+  qx[2] = chi * w[2];
+  qx[3] = chi * w[3];
+  qx[DIR] = chi * sm;
+  qx[4] = chi * (e * ri + (sm - ud) * (sm + w[4] * rcp_fast(fk)));
+  if (NF == 6) qx[5] = chi * w[4] / dpow(w[0], c.g);
+#pragma unroll
+  for (int i = 0; i < NF; ++i) f[i] = fl[i] + sk * (qx[i] - ql[i]);
+}
+
+template <typename T, int NF, int DIR>
+__device__ __forceinline__ void riemann_fast(const T* wl, const T* wr, T* f, int solver, const Gas<T>& c,
+                                             unsigned& err) {
+  if (solver == 2) hllc_fast<T, NF, DIR>(wl, wr, f, c, err);
+  else hll<T, NF>(wl, wr, f, DIR, c, err);
+}
+
 // Interface states of sweep (muscl.f90:199-200, 208-209): the state a cell
 // shows on its upper face, w + 0.5 s + evo, and on its lower face,
 // w - 0.5 s + evo.
