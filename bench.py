@@ -277,9 +277,14 @@ def run_tubes(args):
     data are discarded."""
     import torch
     import evora_b200 as ev
-    torch.cuda.set_device(0)
-    lengths, q = ev.ic.random_tubes(args.ntubes, seed=7, nmin=128, nmax=4096)
-    cells = sum(lengths)
+    from evora_b200 import sharding
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    lengths_all, q_all = ev.ic.random_tubes(args.ntubes, seed=7, nmin=128, nmax=4096)
+    # N > 1: whole tubes per rank, balanced by estimated work; no exchange
+    shards = sharding.shard_by_work(sharding.tube_work(lengths_all, q_all), world)
+    lengths, q = sharding.pack(lengths_all, q_all, shards[rank])
+    cells = sum(lengths_all)
     res = {}
     for solver in (2, 1):
         p = ev.default_params(nx=max(lengths), ny=1, nz=1, g=5.0 / 3.0, cfl=0.8, boundtype=1,
@@ -302,11 +307,11 @@ def run_tubes(args):
                 b.run(sync=False)
                 s1.record(stream)
                 torch.cuda.synchronize()
-                ms = s0.elapsed_time(s1)
-                work = b.cell_updates() - cu0
+                ms = sharding.max_over_ranks(s0.elapsed_time(s1), dev)
+                work = sharding.sum_over_ranks(b.cell_updates() - cu0, dev)
                 infos = [b.info(i) for i in range(len(lengths))]
                 qq = b.get_q()
-            failed = sum(1 for i in infos if i["status"] == 2)
+            failed = int(sharding.sum_over_ranks(sum(1 for i in infos if i["status"] == 2), dev))
             steps = [i["k"] for i in infos]
             out[name] = {"value": work / (ms * 1e-3), "ms": ms, "cell_updates": work, "failed_tubes": failed,
                          "steps_min": min(steps), "steps_max": max(steps), "autotune": tune, "q": qq,
@@ -320,11 +325,17 @@ def run_tubes(args):
         for v in out.values():
             v.pop("q")
             v.pop("ok")
-        res["hllc" if solver == 2 else "hll"] = dict(out, l1_density_f32_vs_f64_median=float(np.median(l1)),
-                                                     l1_density_f32_vs_f64_max=float(np.max(l1)))
+        res["hllc" if solver == 2 else "hll"] = dict(
+            out, l1_density_f32_vs_f64_median=float(np.median(l1)) if l1 else None,
+            l1_density_f32_vs_f64_max=sharding.max_over_ranks(float(np.max(l1)) if l1 else 0.0, dev))
     peak, peak_kind = measured_peaks()
     v = res["hllc"]["f32"]
-    line = {"metric": METRIC, "value": v["value"], "unit": METRIC, "n_gpus": 1, "steps": 1, "warmup": 1,
+    if rank != 0:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+        return 0
+    line = {"metric": METRIC, "value": v["value"], "unit": METRIC, "n_gpus": world, "steps": 1, "warmup": 1,
             "ms_per_step": v["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.ntubes} batched 1D Riemann tubes, 128-4096 cells, to t=0.1, "
@@ -335,7 +346,14 @@ def run_tubes(args):
                          "peak_kind": peak_kind,
                          "note": "each tube crosses HBM once per launch; the kernel is compute bound"},
             "tubes": res}
+    if world > 1:
+        line["scaling"] = "strong"
+        line["config"]["parallelism"] = f"tubes sharded by estimated work over {world} ranks, no exchange"
     print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
