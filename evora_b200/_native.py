@@ -62,6 +62,7 @@ class EvoraError(RuntimeError):
         256: "CUDA error",
         512: "device allocation failed",
         1024: "timeout",
+        2048: "file i/o",
     }
 
     def __init__(self, status: int, where: str = ""):
@@ -124,7 +125,43 @@ def _declare(L):
         fn.argtypes = args
         fn.restype = res
     _declare_batch(L)
+    _declare_io(L)
     return L
+
+
+class EvoraUnits(ctypes.Structure):
+    """evora_units: the unit scales of a unit file (units.f90:92-109)."""
+
+    NAMES = ("t", "cosmo", "redshift", "length0", "time0", "density0", "velocity0", "temp0",
+             "press0", "number0", "chem0", "photo0", "cool0", "heat0", "jeans0", "jeansfloor0",
+             "kappa0", "meanfreepath0")
+    _fields_ = [(n, c_double) for n in NAMES]
+
+
+def _declare_io(L):
+    """File-format entry points of include/evora_io.h."""
+    P = ctypes.POINTER(EvoraParams)
+    U = ctypes.POINTER(EvoraUnits)
+    G = c_void_p
+    s = ctypes.c_char_p
+    i32p = ctypes.POINTER(c_int32)
+    sig = {
+        "evora_write_dump": ([s, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_int32], c_int32),
+        "evora_read_dump_header": ([s, i32p], c_int32),
+        "evora_read_dump": ([s, i32p, c_void_p, c_int64], c_int32),
+        "evora_units_noncomoving": ([c_double, c_double, c_double, U], None),
+        "evora_write_units": ([s, U], c_int32),
+        "evora_read_units": ([s, U], c_int32),
+        "evora_snapshot": ([P, c_void_p, U, c_int32, c_int32, s], c_int32),
+        "evora_grid_snapshot": ([G, U, c_int32, c_int32, s], c_int32),
+        "evora_grid_get_plane": ([G, c_int32, c_int32, c_void_p], c_int32),
+        "evora_grid_set_plane": ([G, c_int32, c_int32, c_void_p], c_int32),
+        "evora_cuts_and_slices": ([P, c_double, U, s, s, s], c_int32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
 
 
 def _declare_batch(L):

@@ -2,6 +2,7 @@
 
 Every translation unit is compiled for sm_100a only.  Per-file flags:
   dropin_strict.cu, fused_f64_strict.cu   --fmad=false (bit-exact FP64 mode)
+  fused.cu                                --fmad=false (conversions, snapshot fields)
   fused_f32.cu                            --use_fast_math (FP32 form)
 Run as `python -m evora_b200.build` (add -v for the ptxas register report).
 """
@@ -26,10 +27,12 @@ BASE = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed
 PER_FILE = {
     "dropin_strict.cu": ["--fmad=false"],
     "fused_f64_strict.cu": ["--fmad=false"],
+    "fused.cu": ["--fmad=false"],
     "fused_f32.cu": ["--use_fast_math"],
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
-           "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu"]
+           "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu",
+           "io.cu"]
 
 
 def _deps():
@@ -61,6 +64,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     sources = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     os.makedirs(OBJDIR, exist_ok=True)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest(_deps()):
+        build_drivers()
         return LIB
     with cf.ThreadPoolExecutor(max_workers=min(8, len(sources))) as ex:
         results = list(ex.map(lambda s: _compile(s, verbose), sources))
@@ -74,7 +78,29 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_drivers()
     return LIB
+
+
+DRIVERS = {"evora_run": "evora_run.cpp", "evora_post": "evora_post.cpp"}
+
+
+def build_drivers() -> None:
+    """The command-line drivers (csrc/driver/), linked against the library
+    with an $ORIGIN run path so that they find it beside themselves."""
+    ddir = os.path.join(CSRC, "driver")
+    for exe, src in DRIVERS.items():
+        out = os.path.join(LIBDIR, exe)
+        deps = [os.path.join(ddir, f) for f in os.listdir(ddir)] + [LIB] + _deps()
+        if os.path.exists(out) and os.path.getmtime(out) >= _newest(deps):
+            continue
+        cmd = [NVCC, "-O2", "-std=c++17", "-Xcompiler", "-Wall", "-I", INCLUDE, "-I", CSRC,
+               os.path.join(ddir, src), "-o", out + ".tmp", "-L", LIBDIR, "-levora_b200",
+               "-Xlinker", "-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed for {src}:\n{r.stdout}\n{r.stderr}")
+        os.replace(out + ".tmp", out)
 
 
 if __name__ == "__main__":

@@ -23,4 +23,12 @@ void set_error_message(const char* msg);
 // The module-global parameters set by evora_set_params (false if unset).
 bool dropin_params(HydroParams* P);
 
+// The parameters a grid was created with.
+const evora_params* grid_params(const evora_grid* g);
+
+// Per cell FP32 density and temperature of the grid's state into host
+// arrays of nx*ny*nz values (snapshot.f90:317-341); returns 0, an error
+// status of pressure(), or EVORA_ERR_CUDA.
+int grid_bov(evora_grid* g, double temp0, float* dens, float* temp);
+
 }  // namespace evora

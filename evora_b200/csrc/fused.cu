@@ -150,7 +150,108 @@ int grid_of(int64_t n) {
   return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
 }
 
+// One cell of the state (SoA with nf fields, or the reference's AoS) as the
+// six FP64 values of q(1:6, cell); S derived as in k_to_aos when not carried.
+template <typename T>
+__device__ __forceinline__ void cell_load(const T* q, int64_t n, int nf, int aos, double g1, int64_t i,
+                                          double v[6]) {
+  if (aos) {
+    for (int f = 0; f < 6; ++f) v[f] = (double)q[6 * i + f];
+    return;
+  }
+  for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+  if (nf == 5) {
+    double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
+    double kin = 0.5 * m2 / v[0];
+    double p = g1 * (v[4] - kin);
+    v[5] = p / pow(v[0], g1);
+  }
+}
+
+template <typename T>
+__global__ void k_get_plane(const T* __restrict__ q, int64_t n, int nf, int aos, double g1, PlaneMap m,
+                            double* __restrict__ out) {
+  const int64_t np = (int64_t)m.na * m.nb;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < np; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = m.base + (j % m.na) * m.sa + (j / m.na) * m.sb;
+    double v[6];
+    cell_load(q, n, nf, aos, g1, i, v);
+    for (int f = 0; f < 6; ++f) out[6 * j + f] = v[f];
+  }
+}
+
+template <typename T>
+__global__ void k_set_plane(T* __restrict__ q, int64_t n, int nf, int aos, PlaneMap m,
+                            const double* __restrict__ in) {
+  const int64_t np = (int64_t)m.na * m.nb;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < np; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = m.base + (j % m.na) * m.sa + (j / m.na) * m.sb;
+    if (aos) {
+      for (int f = 0; f < 6; ++f) q[6 * i + f] = (T)in[6 * j + f];
+    } else {
+      for (int f = 0; f < nf; ++f) q[f * n + i] = (T)in[6 * j + f];
+    }
+  }
+}
+
+// snapshot.f90:317-341 per cell: real(q(1)) and real(temp), temp from
+// pressure() (comp.f90:45-85, its dual-energy resynchronisation written
+// back to the state) and press2temp (comp.f90:87-102, no chemistry).  This
+// translation unit is compiled without FMA contraction, so press and temp
+// are the reference's FP64 values of the cell.
+template <typename T>
+__global__ void k_bov(T* __restrict__ q, int64_t n, int nf, int aos, HydroParams P, double temp0,
+                      float* __restrict__ dens, float* __restrict__ temp, unsigned* err) {
+  const Gas<double> c = Gas<double>::make(P);
+  const bool de = P.dualenergy != 0;
+  unsigned e = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v[6];
+    cell_load(q, n, nf, aos, P.g1, i, v);
+    const double press = pressure(v, c, de, e);
+    if (de) {
+      if (aos) {
+        q[6 * i + 4] = (T)v[4];
+        q[6 * i + 5] = (T)v[5];
+      } else {
+        q[4 * n + i] = (T)v[4];
+        if (nf == 6) q[5 * n + i] = (T)v[5];
+      }
+    }
+    dens[i] = (float)v[0];
+    temp[i] = (float)(press / v[0] * temp0);
+  }
+  if (e) atomicOr(err, e);
+}
+
 }  // namespace
+
+PlaneMap plane_map(const HydroParams& P, int axis, int index0) {
+  const int64_t nx = P.nx, nxy = (int64_t)P.nx * P.ny;
+  if (axis == 1) return {index0, nx, nxy, P.ny, P.nz};
+  if (axis == 2) return {(int64_t)index0 * nx, 1, nxy, P.nx, P.nz};
+  return {(int64_t)index0 * nxy, 1, nx, P.nx, P.ny};
+}
+
+void state_get_plane(const void* q, bool f32, int64_t n, int nf, int aos, double g1, const PlaneMap& m,
+                     double* out, cudaStream_t st) {
+  const int64_t np = (int64_t)m.na * m.nb;
+  if (f32) k_get_plane<float><<<grid_of(np), 256, 0, st>>>((const float*)q, n, nf, aos, g1, m, out);
+  else k_get_plane<double><<<grid_of(np), 256, 0, st>>>((const double*)q, n, nf, aos, g1, m, out);
+}
+
+void state_set_plane(void* q, bool f32, int64_t n, int nf, int aos, const PlaneMap& m, const double* in,
+                     cudaStream_t st) {
+  const int64_t np = (int64_t)m.na * m.nb;
+  if (f32) k_set_plane<float><<<grid_of(np), 256, 0, st>>>((float*)q, n, nf, aos, m, in);
+  else k_set_plane<double><<<grid_of(np), 256, 0, st>>>((double*)q, n, nf, aos, m, in);
+}
+
+void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams& P, double temp0, float* dens,
+               float* temp, unsigned* err, cudaStream_t st) {
+  if (f32) k_bov<float><<<grid_of(n), 256, 0, st>>>((float*)q, n, nf, aos, P, temp0, dens, temp, err);
+  else k_bov<double><<<grid_of(n), 256, 0, st>>>((double*)q, n, nf, aos, P, temp0, dens, temp, err);
+}
 
 void fused_from_aos(const FusedPlan& pl, const double* aos, void* q, cudaStream_t st) {
   if (pl.precision == EVORA_FP32) k_from_aos<float><<<grid_of(pl.n), 256, 0, st>>>(aos, (float*)q, pl.n, pl.nf);

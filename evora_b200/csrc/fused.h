@@ -57,6 +57,25 @@ void fused_to_aos(const FusedPlan& plan, const void* q, double* aos, cudaStream_
 int fused_totals(const FusedPlan& plan, const void* q, double out[6], cudaStream_t st);
 int fused_totals_aos(const double* aos, int64_t n, double out[6], cudaStream_t st);
 
+// A plane of cells: cell (a, b), a < na fastest, is linear cell
+// base + a * sa + b * sb.
+struct PlaneMap {
+  int64_t base, sa, sb;
+  int na, nb;
+};
+// axis 1: x plane ix = index0 + 1, 2: y plane, 3: z plane (index0 0-based).
+PlaneMap plane_map(const HydroParams& P, int axis, int index0);
+// Plane copies between a state (SoA with nf fields, FP32 or FP64, or the
+// reference AoS layout when aos != 0) and q(6, plane) in FP64.
+void state_get_plane(const void* q, bool f32, int64_t n, int nf, int aos, double g1, const PlaneMap& m,
+                     double* out, cudaStream_t st);
+void state_set_plane(void* q, bool f32, int64_t n, int nf, int aos, const PlaneMap& m, const double* in,
+                     cudaStream_t st);
+// Per cell FP32 density and temperature of the brick-of-values snapshot;
+// pressure() errors are OR-ed into *err (device).
+void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams& P, double temp0, float* dens,
+               float* temp, unsigned* err, cudaStream_t st);
+
 // Instantiation launchers (fused_f64.cu, fused_f64_strict.cu, fused_f32.cu).
 #define EVORA_DECLARE_FUSED_NS(ns)                                                           \
   namespace ns {                                                                             \

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/evora_gpu.h"
+#include "../../include/evora_io.h"
 #include "common.h"
 #include "dropin_api.h"
 #include "fused.h"
@@ -521,6 +522,62 @@ int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t*
   return 0;
 }
 
+static int plane_args(evora_grid* g, int32_t axis, int32_t index, PlaneMap* m) {
+  if (!g || axis < 1 || axis > 3) return EVORA_ERR_ARG;
+  const int extent = axis == 1 ? g->P.nx : (axis == 2 ? g->P.ny : g->P.nz);
+  if (index < 1 || index > extent) return EVORA_ERR_ARG;
+  *m = plane_map(g->P, axis, index - 1);
+  return 0;
+}
+
+// Plane copies through a device staging buffer when the caller's memory is
+// on the host (stream-ordered allocation on the grid's stream).
+int evora_grid_get_plane(evora_grid* g, int32_t axis, int32_t index, double* out) {
+  PlaneMap m;
+  int rc = plane_args(g, axis, index, &m);
+  if (rc || !out) return rc ? rc : EVORA_ERR_ARG;
+  const size_t bytes = sizeof(double) * 6 * (size_t)m.na * m.nb;
+  const bool dev = is_device_pointer(out);
+  double* dst = out;
+  if (!dev) CU(cudaMallocAsync((void**)&dst, bytes, g->stream));
+  const bool ref = reference_backend(g);
+  state_get_plane(ref ? (const void*)g->q_aos : g->qbuf[g->cur], !ref && g->precision == EVORA_FP32, ncells(g),
+                  g->nf, ref ? 1 : 0, g->P.g1, m, dst, g->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && !dev) e = cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, g->stream);
+  if (!dev) cudaFreeAsync(dst, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "evora_grid_get_plane");
+    return EVORA_ERR_CUDA;
+  }
+  return 0;
+}
+
+int evora_grid_set_plane(evora_grid* g, int32_t axis, int32_t index, const double* in) {
+  PlaneMap m;
+  int rc = plane_args(g, axis, index, &m);
+  if (rc || !in) return rc ? rc : EVORA_ERR_ARG;
+  const size_t bytes = sizeof(double) * 6 * (size_t)m.na * m.nb;
+  const bool dev = is_device_pointer(in);
+  double* src = const_cast<double*>(in);
+  if (!dev) CU(cudaMallocAsync((void**)&src, bytes, g->stream));
+  cudaError_t e = dev ? cudaSuccess : cudaMemcpyAsync(src, in, bytes, cudaMemcpyHostToDevice, g->stream);
+  const bool ref = reference_backend(g);
+  if (e == cudaSuccess) {
+    state_set_plane(ref ? (void*)g->q_aos : g->qbuf[g->cur], !ref && g->precision == EVORA_FP32, ncells(g), g->nf,
+                    ref ? 1 : 0, m, src, g->stream);
+    e = cudaGetLastError();
+  }
+  if (!dev) cudaFreeAsync(src, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "evora_grid_set_plane");
+    return EVORA_ERR_CUDA;
+  }
+  return 0;
+}
+
 int evora_grid_totals(evora_grid* g, double out[6]) {
   if (!g || !out) return EVORA_ERR_ARG;
   if (reference_backend(g)) {
@@ -530,3 +587,35 @@ int evora_grid_totals(evora_grid* g, double out[6]) {
 }
 
 }  // extern "C"
+
+namespace evora {
+
+const evora_params* grid_params(const evora_grid* g) { return &g->params; }
+
+int grid_bov(evora_grid* g, double temp0, float* dens, float* temp) {
+  const int64_t n = ncells(g);
+  float* d = nullptr;
+  unsigned* err = nullptr;
+  CU(cudaMallocAsync((void**)&d, sizeof(float) * 2 * n + 16, g->stream));
+  err = reinterpret_cast<unsigned*>(d + 2 * n);
+  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), g->stream);
+  const bool ref = reference_backend(g);
+  if (e == cudaSuccess) {
+    state_bov(ref ? (void*)g->q_aos : g->qbuf[g->cur], !ref && g->precision == EVORA_FP32, n, g->nf, ref ? 1 : 0,
+              g->P, temp0, d, d + n, err, g->stream);
+    e = cudaGetLastError();
+  }
+  unsigned herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dens, d, sizeof(float) * n, cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(temp, d + n, sizeof(float) * n, cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, g->stream);
+  cudaFreeAsync(d, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "snapshot fields");
+    return EVORA_ERR_CUDA;
+  }
+  return (int)herr;
+}
+
+}  // namespace evora

@@ -54,7 +54,8 @@ enum evora_status {
   EVORA_ERR_ARG = 128,            /* invalid argument, size or call order */
   EVORA_ERR_CUDA = 256,           /* CUDA runtime error (see evora_last_error) */
   EVORA_ERR_NOMEM = 512,          /* device allocation failed */
-  EVORA_ERR_TIMEOUT = 1024        /* a bounded host or device wait gave up */
+  EVORA_ERR_TIMEOUT = 1024,       /* a bounded host or device wait gave up */
+  EVORA_ERR_IO = 2048             /* a file could not be opened, written or read */
 };
 
 /* Number of conserved / primitive / flux fields of the plain build
