@@ -51,6 +51,7 @@ int fused_plan(const HydroParams& P, int precision, int nf, int strict, FusedPla
   pl->n = (int64_t)P.nx * P.ny * P.nz;
   if ((int64_t)P.nx * P.ny * P.nz >= ((int64_t)1 << 31)) return EVORA_ERR_ARG;  // in-field index is 32-bit
   pl->cfl = inst_of(precision, strict).cfl;
+  pl->cfl_fused = pl->dim >= 2 ? 1 : 0;
   int tile = 0;
   if (const char* e = getenv("EVORA_TILE")) tile = atoi(e);
   fused_set_tile(pl, tile);

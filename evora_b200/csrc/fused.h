@@ -30,6 +30,10 @@ struct FusedPlan {
   double* partials = nullptr;  // device scratch of the totals reduction
   cudaStream_t alloc_stream = nullptr;  // non-null: partials came from cudaMallocAsync on it
   int nblk_tot = 0;
+  // 1: the update also reduces the next step's CFL maxima of the state it
+  // writes into ctl->snext (2D and 3D kernels), so that step needs no CFL
+  // kernel
+  int cfl_fused = 0;
 };
 
 // Chooses tiles and the kernel instantiation; allocates small scratch.

@@ -34,7 +34,7 @@ constexpr int kTiles = 4;
 
 template <int NF, int DIM, int I>
 void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
-  FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n};
+  FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n, pl.cfl_fused};
   if constexpr (DIM == 1) {
     k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
   } else {
@@ -79,21 +79,19 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
   return pick_one<6, 3, 0>(tx, ty, zc, smem, threads);
 }
 
-// hydrostep part 1 on the SoA state: maxima of |u_d| + a in FP64 (the state
-// is widened to FP64 first; q2w as in primitive, comp.f90:26-85).
+// hydrostep part 1 on the SoA state: maxima of |u_d| + a (per cell in the
+// working precision, cfl_speeds; maxima and dt in FP64).
 template <int NF>
 __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const Gas<double> c = Gas<double>::make(P);
   double m0 = 0.0, m1 = 0.0, m2 = 0.0;
   unsigned err = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double qv[6], w[5];
+    TT qv[6], s[3];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) qv[f] = (double)__ldg(q + f * n + i);
-    q2w(qv, w, c, P.dualenergy != 0, err);
-    double a = sqrt(P.g * w[4] / w[0]);
-    double s0 = fabs(w[1]) + a, s1 = fabs(w[2]) + a, s2 = fabs(w[3]) + a;
+    for (int f = 0; f < NF; ++f) qv[f] = __ldg(q + f * n + i);
+    cfl_speeds<TT, NF>(qv, P, P.dualenergy != 0, err, s);
+    const double s0 = s[0], s1 = s[1], s2 = s[2];
     if (s0 > m0) m0 = s0;
     if (s1 > m1) m1 = s1;
     if (s2 > m2) m2 = s2;

@@ -63,6 +63,7 @@ struct FusedArgs {
   T* qout;
   GridCtl* ctl;     // dt, active flag, error mask
   int64_t n;        // cells per field
+  int cfl_next = 0; // 1: reduce the next step's CFL maxima into ctl->snext
 };
 
 // Boundary index map of one axis (0-based), boundary.f90:26-113: g in
@@ -162,7 +163,35 @@ struct FusedSmem {
   T yf[2][5][TY + 2][TX];     // y face states of the tile + y ring
   T fx[NF][TY][TX + 1];       // x fluxes, interface i-1/2 at column i
   T fy[NF][TY + 1][TX];       // y fluxes, interface j-1/2 at row j
+  // maxima of |u_d| + a of the written cells: per thread for FP32 state
+  // (whose register budget is tight), per warp otherwise
+  T cfl[3][sizeof(T) == 4 ? TX * TY : 32];
 };
+
+// hydrostep per cell (timestep.f90:40-43): the signal speeds |u_d| + a of
+// a conserved state, in the working precision.  FP64: q2w and a = sqrt(g p
+// / rho).  FP32 form: its primitives (FP64 pressure recovery where kin >
+// E/2) and a in FP32; the maxima over cells and dt are formed in FP64 from
+// these exactly representable values.  The CFL kernel and the fused
+// update's reduction for the next step both call this, so either gives the
+// same dt.
+template <typename T, int NF>
+__device__ __forceinline__ void cfl_speeds(const T* qs, const HydroParams& P, bool de, unsigned& err, T s[3]) {
+  T q[6], w[5];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) q[f] = qs[f];
+  T a;
+  if constexpr (sizeof(T) == 8) {
+    q2w(q, w, Gas<double>::make(P), de, err);
+    a = sqrt(P.g * w[4] / w[0]);
+  } else {
+    prim(q, w, Gas<float>::make(P), P, de, err);
+    a = sqrtf((float)P.g * w[4] / w[0]);
+  }
+  s[0] = fabs(w[1]) + a;
+  s[1] = fabs(w[2]) + a;
+  s[2] = fabs(w[3]) + a;
+}
 
 // Slopes, predictor and face states of one cell of plane c.  (cx, cy) are
 // coordinates in the halo ring arrays.  DIM = 2 or 3 selects the 2D
@@ -245,6 +274,31 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
   const double dtd = A.ctl->dt;
   const T dt2 = (T)(-0.5 * dtd);
   const T dtdx = (T)(dtd * P.dxinv), dtdy = (T)(dtd * P.dyinv), dtdz = (T)(dtd * P.dzinv);
+
+  // The next step's hydrostep maxima (timestep.f90:26-57) over the cells
+  // this tile writes, computed from the written values with the CFL kernel's
+  // own per-cell function (cfl_speeds), so the grid can skip that kernel's
+  // pass over HBM.  With FP32 state the running maxima live in shared memory
+  // (one slot per thread) rather than in registers held across the plane
+  // loop.
+  constexpr bool kSlots = sizeof(T) == 4;
+  unsigned cerr = 0;
+  T cm0 = (T)0, cm1 = (T)0, cm2 = (T)0;
+  if constexpr (kSlots)
+    if (A.cfl_next) sm.cfl[0][tid] = sm.cfl[1][tid] = sm.cfl[2][tid] = (T)0;
+  auto track = [&](const T* qo) {
+    T s[3];
+    cfl_speeds<T, NF>(qo, P, de, cerr, s);
+    if constexpr (kSlots) {
+      if (s[0] > sm.cfl[0][tid]) sm.cfl[0][tid] = s[0];
+      if (s[1] > sm.cfl[1][tid]) sm.cfl[1][tid] = s[1];
+      if (s[2] > sm.cfl[2][tid]) sm.cfl[2][tid] = s[2];
+    } else {
+      if (s[0] > cm0) cm0 = s[0];
+      if (s[1] > cm1) cm1 = s[1];
+      if (s[2] > cm2) cm2 = s[2];
+    }
+  };
 
   // A: primitives of plane z (global index, may be a ghost plane) into slot.
   // Tiles whose x/y halo lies inside the grid need no index map in x and y
@@ -404,8 +458,13 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
       if (DIM == 3 && cz - 1 >= Z0 && cz - 1 < Z0 + ze) {
         // plane cz-1 gets its z term and is written out
         const int64_t idx = ((int64_t)(cz - 1) * ny + (Y0 + oj)) * nx + (X0 + oi);
+        T qo[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) A.qout[f * n + idx] = qacc[f] + dtdz * (fz_prev[f] - fz[f]);
+        for (int f = 0; f < NF; ++f) {
+          qo[f] = qacc[f] + dtdz * (fz_prev[f] - fz[f]);
+          A.qout[f * n + idx] = qo[f];
+        }
+        if (A.cfl_next) track(qo);
       }
       if (inner) {
         const int64_t idx = ((int64_t)cz * ny + (Y0 + oj)) * nx + (X0 + oi);
@@ -426,6 +485,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
         } else {
 #pragma unroll
           for (int f = 0; f < NF; ++f) A.qout[f * n + idx] = qv[f];
+          if (A.cfl_next) track(qv);
         }
       }
       if (DIM == 3) {
@@ -441,6 +501,49 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
     reinterpret_cast<std::atomic<unsigned>*>(&A.ctl->err)->fetch_or(err);
 #else
     atomicOr(&A.ctl->err, err);
+#endif
+  }
+  if (A.cfl_next) {
+    if constexpr (kSlots) {
+      cm0 = sm.cfl[0][tid];
+      cm1 = sm.cfl[1][tid];
+      cm2 = sm.cfl[2][tid];
+    }
+#if defined(EVORA_HOST_EMU)
+    const double cm[3] = {cm0, cm1, cm2};
+    for (int d = 0; d < 3; ++d) {
+      std::atomic_ref<unsigned long long> r(A.ctl->snext[d]);
+      unsigned long long cur = r.load(), v = ordered_bits(cm[d]);
+      while (v > cur && !r.compare_exchange_weak(cur, v)) {
+      }
+    }
+    if (cerr) std::atomic_ref<unsigned>(A.ctl->errnext).fetch_or(cerr);
+#else
+    for (int o = 16; o > 0; o >>= 1) {
+      cm0 = fmax2(cm0, __shfl_xor_sync(0xffffffffu, cm0, o));
+      cm1 = fmax2(cm1, __shfl_xor_sync(0xffffffffu, cm1, o));
+      cm2 = fmax2(cm2, __shfl_xor_sync(0xffffffffu, cm2, o));
+    }
+    EV_SYNC();   // every thread has read its own slots
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) {
+      sm.cfl[0][wid] = cm0;
+      sm.cfl[1][wid] = cm1;
+      sm.cfl[2][wid] = cm2;
+    }
+    EV_SYNC();
+    if (tid == 0) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      for (int k = 0; k < NT / 32; ++k) {
+        a0 = fmax2(a0, (double)sm.cfl[0][k]);
+        a1 = fmax2(a1, (double)sm.cfl[1][k]);
+        a2 = fmax2(a2, (double)sm.cfl[2][k]);
+      }
+      atomicMax(&A.ctl->snext[0], ordered_bits(a0));
+      atomicMax(&A.ctl->snext[1], ordered_bits(a1));
+      atomicMax(&A.ctl->snext[2], ordered_bits(a2));
+    }
+    if (cerr) atomicOr(&A.ctl->errnext, cerr);
 #endif
   }
 }

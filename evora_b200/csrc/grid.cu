@@ -22,6 +22,7 @@
 #include "common.h"
 #include "dropin_api.h"
 #include "fused.h"
+#include "gravity.h"
 
 using namespace evora;
 
@@ -50,8 +51,15 @@ struct evora_grid {
   std::vector<cudaEvent_t> events;  // 4 per timed step
   size_t ev_used = 0;
   int64_t launches = 0;
-  // multi-step CUDA graphs, key = 2 * steps + starting buffer
+  // multi-step CUDA graphs, key = 4 * steps + 2 * (CFL maxima fresh) +
+  // starting buffer
   std::map<long long, cudaGraphExec_t> graphs;
+  // the previous update reduced the CFL maxima of the current state into
+  // ctl->snext; any other change of the state clears this
+  bool cfl_fresh = false;
+  // self-gravity after each hydro step (params.gravity)
+  bool gravity = false;
+  GravPlan grav{};
   bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
 };
 
@@ -72,9 +80,19 @@ int64_t ncells(const evora_grid* g) { return (int64_t)g->P.nx * g->P.ny * g->P.n
 
 size_t elem_size(const evora_grid* g) { return g->precision == EVORA_FP32 ? 4 : 8; }
 
-__global__ void k_step_begin(GridCtl* ctl) {
+// use_next: the CFL maxima of this step's state were reduced by the previous
+// step's update (with the errors that computation raised); otherwise a CFL
+// kernel fills smax.
+__global__ void k_step_begin(GridCtl* ctl, int use_next) {
+  if (use_next) {
+    ctl->err |= ctl->errnext;
+    for (int i = 0; i < 3; ++i) ctl->smax[i] = ctl->snext[i];
+  } else {
+    ctl->smax[0] = ctl->smax[1] = ctl->smax[2] = 0ull;
+  }
+  ctl->errnext = 0u;
+  ctl->snext[0] = ctl->snext[1] = ctl->snext[2] = 0ull;
   ctl->active = (ctl->go != 0 && ctl->err == 0) ? 1 : 0;
-  ctl->smax[0] = ctl->smax[1] = ctl->smax[2] = 0ull;
 }
 
 // hydrostep part 2 + updatetime (timestep.f90:26-57, 147-171).
@@ -129,7 +147,7 @@ int enqueue_reference_step(evora_grid* g) {
   cudaStream_t st = g->stream;
   const int nb = (g->P.nx != 1) + (g->P.ny != 1) + (g->P.nz != 1);
   g->launches += 7 + nb;
-  k_step_begin<<<1, 1, 0, st>>>(g->ctl);
+  k_step_begin<<<1, 1, 0, st>>>(g->ctl, 0);
   mark(g);
   o.primitive(g->P, g->w, g->q_aos, &g->ctl->err, g->ctl, st);
   o.bound(g->P, g->w, g->ctl, st);
@@ -139,6 +157,11 @@ int enqueue_reference_step(evora_grid* g) {
   mark(g);
   if (g->P.secondorder) o.compevo(g->P, g->w, g->evo, g->s, 0.0, g->ctl, st);
   o.sweep(g->P, g->w, g->q_aos, g->evo, g->s, 0.0, &g->ctl->err, g->ctl, st);
+  if (g->gravity) {
+    int rc = grav_potential(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl);
+    if (!rc) rc = grav_integrate(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl, 0.0);
+    if (rc) return rc;
+  }
   mark(g);
   k_step_end<<<1, 1, 0, st>>>(g->ctl);
   CU(cudaGetLastError());
@@ -147,20 +170,29 @@ int enqueue_reference_step(evora_grid* g) {
 
 int enqueue_fused_step(evora_grid* g) {
   cudaStream_t st = g->stream;
-  g->launches += 5;
-  k_step_begin<<<1, 1, 0, st>>>(g->ctl);
+  const bool use_next = g->cfl_fresh;
+  g->launches += use_next ? 4 : 5;
+  k_step_begin<<<1, 1, 0, st>>>(g->ctl, use_next ? 1 : 0);
   mark(g);
-  fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
+  if (!use_next) fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
   mark(g);
   k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
   mark(g);
   fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
+  if (g->gravity) {
+    // gravpotential + gravintegration on the updated state (main.f90:158-165)
+    int rc = grav_potential(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl);
+    if (!rc) rc = grav_integrate(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 0.0);
+    if (rc) return rc;
+    g->launches += 5;   // own kernels; cuFFT adds its own
+  }
   mark(g);
   k_step_end<<<1, 1, 0, st>>>(g->ctl);
   CU(cudaGetLastError());
   // The swap is unconditional on the host; an inactive step copies q through
   // unchanged (fused_update does that when the step is inactive).
   g->cur ^= 1;
+  g->cfl_fresh = g->plan.cfl_fused != 0;
   return 0;
 }
 
@@ -180,6 +212,7 @@ void free_grid(evora_grid* g) {
   drop_graphs(g);
   for (cudaEvent_t e : g->events) cudaEventDestroy(e);
   fused_plan_free(&g->plan);
+  grav_plan_free(&g->grav);
   dfree(g, g->ctl);
   dfree(g, g->q_aos);
   dfree(g, g->w);
@@ -259,6 +292,17 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
       return rc;
     }
   }
+  if (p->gravity) {
+    // the potential changes the state after the update: the next step's
+    // CFL maxima come from the CFL kernel, not from the update
+    g->gravity = true;
+    g->plan.cfl_fused = 0;
+    rc = grav_plan(g->P, &g->grav, g->stream);
+    if (rc) {
+      free_grid(g);
+      return rc;
+    }
+  }
   {
     GridCtl c{};
     c.t = p->tstart;
@@ -296,6 +340,7 @@ int evora_grid_set_stream(evora_grid* g, void* stream) {
   if (g->async_alloc && (cudaStream_t)stream != g->stream) return EVORA_ERR_ARG;  // memory is ordered on it
   drop_graphs(g);
   g->stream = (cudaStream_t)stream;
+  if (g->gravity) grav_set_stream(&g->grav, g->stream);
   return 0;
 }
 
@@ -317,6 +362,7 @@ int evora_grid_set_q(evora_grid* g, const double* q) {
     g->cur = 0;
     fused_from_aos(g->plan, src, g->qbuf[0], g->stream);
   }
+  g->cfl_fresh = false;
   GridCtl c{};
   c.t = g->params.tstart;
   c.tend = g->params.tend;
@@ -375,7 +421,8 @@ int graph_steps(evora_grid* g, int nsteps) {
     // buffer); the step kernels read dt and the active flag from the device
     // control block, so a graph is valid for any time of the run.
     const int start = g->cur;
-    const long long key = 2LL * nsteps + start;
+    const bool fresh = g->cfl_fresh;
+    const long long key = 4LL * nsteps + (fresh ? 2 : 0) + start;
     auto it = g->graphs.find(key);
     if (it == g->graphs.end()) {
       cudaGraph_t graph;
@@ -386,6 +433,7 @@ int graph_steps(evora_grid* g, int nsteps) {
         rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
       cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
       g->cur = start;
+      g->cfl_fresh = fresh;
       g->launches = launches0;
       if (rc) return rc;
       if (e != cudaSuccess) {
@@ -402,8 +450,14 @@ int graph_steps(evora_grid* g, int nsteps) {
       it = g->graphs.emplace(key, ex).first;
     }
     CU(cudaGraphLaunch(it->second, g->stream));
-    if (!reference_backend(g)) g->cur = start ^ (nsteps & 1);
-    g->launches += (int64_t)nsteps * (reference_backend(g) ? 10 : 5);
+    if (reference_backend(g)) {
+      g->launches += (int64_t)nsteps * 10;
+    } else {
+      g->cur = start ^ (nsteps & 1);
+      const bool fused = g->plan.cfl_fused != 0;
+      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0)) + (fused && !fresh ? 1 : 0);
+      g->cfl_fresh = fused;
+    }
   }
   return 0;
 }
@@ -450,7 +504,7 @@ int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms
   GridCtl saved;
   CU(cudaMemcpyAsync(&saved, g->ctl, sizeof saved, cudaMemcpyDeviceToHost, g->stream));
   CU(cudaStreamSynchronize(g->stream));
-  k_step_begin<<<1, 1, 0, g->stream>>>(g->ctl);
+  k_step_begin<<<1, 1, 0, g->stream>>>(g->ctl, 0);
   fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, g->stream);
   k_step_time<<<1, 1, 0, g->stream>>>(g->P, g->ctl);
   cudaEvent_t e0, e1;
@@ -564,6 +618,7 @@ int evora_grid_set_plane(evora_grid* g, int32_t axis, int32_t index, const doubl
   if (!dev) CU(cudaMallocAsync((void**)&src, bytes, g->stream));
   cudaError_t e = dev ? cudaSuccess : cudaMemcpyAsync(src, in, bytes, cudaMemcpyHostToDevice, g->stream);
   const bool ref = reference_backend(g);
+  g->cfl_fresh = false;   // the state changed under the reduced CFL maxima
   if (e == cudaSuccess) {
     state_set_plane(ref ? (void*)g->q_aos : g->qbuf[g->cur], !ref && g->precision == EVORA_FP32, ncells(g), g->nf,
                     ref ? 1 : 0, m, src, g->stream);
@@ -600,6 +655,7 @@ int grid_bov(evora_grid* g, double temp0, float* dens, float* temp) {
   err = reinterpret_cast<unsigned*>(d + 2 * n);
   cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned), g->stream);
   const bool ref = reference_backend(g);
+  g->cfl_fresh = false;   // pressure() may resynchronise E or S in place
   if (e == cudaSuccess) {
     state_bov(ref ? (void*)g->q_aos : g->qbuf[g->cur], !ref && g->precision == EVORA_FP32, n, g->nf, ref ? 1 : 0,
               g->P, temp0, d, d + n, err, g->stream);

@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #if !defined(__CUDACC__)
 // Host compilation of the device arithmetic (used by the CPU emulation of the
@@ -35,8 +36,9 @@ struct GridCtl {
   int active;    // the current step runs
   long long k;   // steps completed
   unsigned err;  // accumulated EVORA_ERR_* mask
-  unsigned pad;
-  unsigned long long smax[3];  // CFL maxima of |u_d| + a (ordered bits)
+  unsigned errnext;  // errors of the CFL maxima in snext (raised when used)
+  unsigned long long smax[3];   // CFL maxima of |u_d| + a (ordered bits)
+  unsigned long long snext[3];  // the same, over the state the update wrote
 };
 
 __device__ __forceinline__ bool ctl_skip(const GridCtl* ctl) {
@@ -400,11 +402,17 @@ __device__ __forceinline__ T face_plus(T w, T s, T e) { return w + (T)0.5 * s + 
 template <typename T>
 __device__ __forceinline__ T face_minus(T w, T s, T e) { return w - (T)0.5 * s + e; }
 
-#if defined(__CUDACC__)
 // Positive doubles order like their bit patterns as unsigned integers; the
 // CFL reduction keeps maxima of signal speeds that way (atomicMax on u64).
+#if defined(__CUDACC__)
 __device__ __forceinline__ unsigned long long ordered_bits(double v) {
   return (unsigned long long)__double_as_longlong(v);
+}
+#else
+inline unsigned long long ordered_bits(double v) {
+  unsigned long long u;
+  std::memcpy(&u, &v, sizeof u);
+  return u;
 }
 #endif
 

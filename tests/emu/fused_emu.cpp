@@ -7,6 +7,7 @@
 #define EVORA_FNS emu
 #include "../../evora_b200/csrc/fused_kernel.cuh"
 
+#include <cstring>
 #include <memory>
 #include <thread>
 #include <vector>
@@ -38,14 +39,24 @@ static void run_tiles(const FusedArgs<double>& A) {
       }
 }
 
-extern "C" int emu_fused_update(const HydroParams* P, int nf, const double* qin, double* qout, double dt,
-                                int tile) {
+// smax_next (may be null): the next step's CFL maxima that the update
+// reduces over the state it writes (2D and 3D tiles), as doubles.
+extern "C" int emu_fused_update_cfl(const HydroParams* P, int nf, const double* qin, double* qout, double dt,
+                                    int tile, double* smax_next) {
   GridCtl ctl{};
   ctl.dt = dt;
   ctl.go = 1;
   ctl.active = 1;
   const int dim = P->onedimension ? 1 : (P->twodimension ? 2 : 3);
-  FusedArgs<double> A{*P, qin, qout, &ctl, (int64_t)P->nx * P->ny * P->nz};
+  FusedArgs<double> A{*P, qin, qout, &ctl, (int64_t)P->nx * P->ny * P->nz, smax_next != nullptr ? 1 : 0};
+  struct Out {
+    GridCtl& c;
+    double* s;
+    ~Out() {
+      if (s)
+        for (int d = 0; d < 3; ++d) std::memcpy(&s[d], &c.snext[d], sizeof(double));
+    }
+  } out{ctl, smax_next};
   if (dim == 1) {
     for (int i = 0; i < P->nx; ++i) {
       if (nf == 5) fused_cell1d<double, 5>(A, i);
@@ -64,4 +75,9 @@ extern "C" int emu_fused_update(const HydroParams* P, int nf, const double* qin,
   else RUN(6, 3);
 #undef RUN
   return (int)ctl.err;
+}
+
+extern "C" int emu_fused_update(const HydroParams* P, int nf, const double* qin, double* qout, double dt,
+                                int tile) {
+  return emu_fused_update_cfl(P, nf, qin, qout, dt, tile, nullptr);
 }

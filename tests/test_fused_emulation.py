@@ -28,6 +28,7 @@ def emu():
     L = ctypes.CDLL(os.path.join(EMU, "_build", "libfused_emu.so"))
     dp = ctypes.POINTER(ctypes.c_double)
     L.emu_fused_update.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int]
+    L.emu_fused_update_cfl.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, dp]
     return L
 
 
@@ -79,3 +80,40 @@ def test_emulated_fused_step_is_bitwise_oracle(emu, case):
     err = emu.emu_fused_update(ctypes.byref(hp_of(o)), nf, qin.ctypes.data_as(dp), qout.ctypes.data_as(dp), dt, tile)
     assert err == 0
     np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
+
+
+def cfl_dt(o, s):
+    """hydrostep part 2 (timestep.f90:26-57) from per-axis maxima."""
+    vx, vy, vz = o.d.dx / s[0], o.d.dy / s[1], o.d.dz / s[2]
+    m = vx
+    if vy < m:
+        m = vy
+    if vz < m:
+        m = vz
+    v = 1e6
+    if m < v:
+        v = m
+    return o.d.cfl * v
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c[1] > 1],
+                         ids=lambda c: "x".join(map(str, c[:3])) + f"-bt{c[3]}-nf{c[4]}-t{c[7]}")
+def test_emulated_update_reduces_next_cfl_maxima(emu, case):
+    # the maxima the update reduces over the state it writes give the next
+    # step's dt exactly as hydrostep over that state does
+    nx, ny, nz, bt, nf, lim, sol, tile, so = case
+    o = Oracle(make_params(nx=nx, ny=ny, nz=nz, boundtype=bt, limiter=lim, solver=sol, g=5 / 3, cfl=0.4,
+                           secondorder=so))
+    q = random_q(o, np.random.default_rng(nx * 131 + ny * 7 + nz))
+    q2, dt, _ = oracle_step(o, q)
+    _, dt_next, _ = oracle_step(o, q2)
+    n = nx * ny * nz
+    qin = np.ascontiguousarray(q.reshape(n, 6).T[:nf])
+    qout = np.zeros_like(qin)
+    smax = np.zeros(3)
+    dp = ctypes.POINTER(ctypes.c_double)
+    err = emu.emu_fused_update_cfl(ctypes.byref(hp_of(o)), nf, qin.ctypes.data_as(dp), qout.ctypes.data_as(dp),
+                                   dt, tile, smax.ctypes.data_as(dp))
+    assert err == 0
+    np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
+    assert cfl_dt(o, smax) == dt_next
