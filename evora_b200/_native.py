@@ -27,7 +27,7 @@ class EvoraParams(ctypes.Structure):
         ("nx", c_int32), ("ny", c_int32), ("nz", c_int32),
         ("solver", c_int32), ("limiter", c_int32), ("boundtype", c_int32),
         ("secondorder", c_int32), ("dualenergy", c_int32), ("atomic", c_int32),
-        ("reserved", c_int32),
+        ("gravity", c_int32),
         ("g", c_double), ("cfl", c_double), ("de_thresh", c_double),
         ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
@@ -35,7 +35,7 @@ class EvoraParams(ctypes.Structure):
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class EvoraDerived(ctypes.Structure):
@@ -182,6 +182,8 @@ def _declare_batch(L):
         "evora_batch_configure": ([G, c_int32, c_int32], c_int32),
         "evora_batch_autotune": ([G, c_int32, ctypes.POINTER(c_int32), ctypes.POINTER(c_int32)], c_int32),
         "evora_hydrostep_noalloc": ([c_void_p, _dp], c_int32),
+        "evora_gravpotential": ([c_void_p, c_void_p], c_int32),
+        "evora_gravintegration": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),
         "evora_server_destroy": ([G], c_int32),

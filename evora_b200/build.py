@@ -2,7 +2,7 @@
 
 Every translation unit is compiled for sm_100a only.  Per-file flags:
   dropin_strict.cu, fused_f64_strict.cu   --fmad=false (bit-exact FP64 mode)
-  fused.cu                                --fmad=false (conversions, snapshot fields)
+  fused.cu, gravity.cu                    --fmad=false (conversions, snapshot fields, gravity)
   fused_f32.cu                            --use_fast_math (FP32 form)
 Run as `python -m evora_b200.build` (add -v for the ptxas register report).
 """
@@ -28,11 +28,12 @@ PER_FILE = {
     "dropin_strict.cu": ["--fmad=false"],
     "fused_f64_strict.cu": ["--fmad=false"],
     "fused.cu": ["--fmad=false"],
+    "gravity.cu": ["--fmad=false"],
     "fused_f32.cu": ["--use_fast_math"],
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
            "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu",
-           "io.cu"]
+           "io.cu", "gravity.cu"]
 
 
 def _deps():
@@ -73,7 +74,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             sys.stderr.write(f"== {src}\n{log}")
     objs = [o for o, _ in results]
     tmp = LIB + ".tmp"
-    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcufft"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

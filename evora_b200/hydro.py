@@ -126,6 +126,25 @@ class DropIn:
                                 _ptr(evo, self.shape["evo"], False), _ptr(s, self.shape["s"], False),
                                 float(dt)), "sweep")
 
+    def _phi_ptr(self, phi):
+        if not isinstance(phi, np.ndarray) or phi.dtype != np.complex128 or not phi.flags["C_CONTIGUOUS"]:
+            raise TypeError("phi must be a C-contiguous complex128 array")
+        if phi.shape != tuple(self.shape["q"][:3]):
+            raise ValueError(f"phi shape {phi.shape} != {tuple(self.shape['q'][:3])}")
+        return ctypes.c_void_p(phi.ctypes.data)
+
+    def gravpotential(self, q, phi):
+        """gravpotential(q,phi), gravitation.f90:26-53 (non-comoving): phi is
+        complex(8) phi(nx,ny,nz), C shape (nz, ny, nx) complex128; its
+        imaginary part is written as 0."""
+        check(lib().evora_gravpotential(_ptr(q, self.shape["q"], False), self._phi_ptr(phi)), "gravpotential")
+
+    def gravintegration(self, q, phi, dt: float):
+        """gravintegration(q,phi,...), gravitation.f90:170-243 (one process,
+        so no boundary buffers): the gravitational source terms over dt."""
+        check(lib().evora_gravintegration(_ptr(q, self.shape["q"]), self._phi_ptr(phi), float(dt)),
+              "gravintegration")
+
 
 # ---------------------------------------------------------- resident grid --
 class Grid:

@@ -75,7 +75,8 @@ typedef struct evora_params {
   int32_t secondorder;  /* Fortran logical: MUSCL-Hancock predictor on       */
   int32_t dualenergy;   /* Fortran logical: dual-energy pressure recovery    */
   int32_t atomic;       /* Fortran logical: forces g = 5.0/3.0 (single prec) */
-  int32_t reserved;
+  int32_t gravity;      /* Fortran logical: self-gravity after each hydro
+                           step (gravitation.f90, non-comoving branch)      */
   double g, cfl, de_thresh;
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double tstart, tend;
