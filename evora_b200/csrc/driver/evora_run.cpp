@@ -9,9 +9,10 @@
 // Input: namelist group para (parameter.f90:26-105) and, for the shocktube,
 // ic_para (ic/shocktube.f90:39-47).  The reference compiles one ic/<name>.f90
 // into the binary (object/Makefile:57-58); here --ic chooses at run time.
-// Runs with gravity, comoving coordinates, chemistry, conduction or the
-// temperature / Jeans floors are refused: those physics are not on the hydro
-// path this library implements.
+// Self-gravity (gravity = .true.) runs on the device after each hydro step
+// as in main.f90:158-165 (non-comoving).  Runs with comoving coordinates,
+// chemistry, conduction or the temperature / Jeans floors are refused: those
+// physics are not on the path this library implements.
 //
 // Output, under the working directory, as the reference writes it:
 //   data/parameter           writeparameter (parameter.f90:267-337)

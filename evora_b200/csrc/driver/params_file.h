@@ -243,6 +243,7 @@ inline evora_params hydro_params(const RunParams& r) {
   p.limiter = (int)r["limiter"];
   p.boundtype = (int)r["boundtype"];
   p.secondorder = r.flag("secondorder");
+  p.gravity = r.flag("gravity");
   p.dualenergy = r.flag("dualenergy");
   p.atomic = r.flag("atomic");
   p.g = r["g"];
@@ -262,7 +263,7 @@ inline evora_params hydro_params(const RunParams& r) {
 // The parts of a run outside the hydro path that these drivers do not have.
 inline std::string unsupported(const RunParams& r) {
   std::string s;
-  for (const char* k : {"gravity", "supercomoving", "chemistry", "conduction", "tempfloor", "jeansfloor"})
+  for (const char* k : {"supercomoving", "chemistry", "conduction", "tempfloor", "jeansfloor"})
     if (r.flag(k)) s += (s.empty() ? "" : ", ") + std::string(k);
   if (!r.flag("hydro")) s += (s.empty() ? "" : ", ") + std::string("hydro = .false.");
   return s;
