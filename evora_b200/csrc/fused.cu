@@ -2,6 +2,7 @@
 // (structure-of-arrays) backend.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -13,7 +14,7 @@ namespace evora {
 
 namespace {
 struct Inst {
-  FusedLaunch (*pick)(int, int, int, int*, int*, int*, size_t*, int*);
+  FusedLaunch (*pick)(int, int, int, int*, int*, int*, size_t*, int*, int*);
   int (*tiles)();
   void (*cfl)(const FusedPlan&, const void*, GridCtl*, cudaStream_t);
 };
@@ -24,12 +25,44 @@ Inst inst_of(int precision, int strict) {
 }
 }  // namespace
 
+// Planes per CTA of the 3D march.  The grid has tiles_xy x chunks CTAs, run
+// in waves of SMs x CTAs-per-SM; the last wave is partly empty, and every
+// chunk reloads two planes of halo.  The choice maximises
+// (waves / ceil(waves)) x zc / (zc + 2) over chunk counts with zc >= 16
+// (EVORA_ZC overrides).
+int choose_zc(const HydroParams& P, int tx, int ty, int minb, int zc_default) {
+  if (const char* e = getenv("EVORA_ZC")) {
+    const int z = atoi(e);
+    if (z > 0) return z;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaGetLastError();
+  const long long tiles_xy = (long long)((P.nx + tx - 1) / tx) * ((P.ny + ty - 1) / ty);
+  const double slots = (double)sms * (minb > 0 ? minb : 1);
+  double best = -1.0;
+  int best_zc = zc_default;
+  for (int chunks = 1; chunks <= P.nz; ++chunks) {
+    const int zc = (P.nz + chunks - 1) / chunks;
+    if (zc < 16 && chunks > 1) break;
+    if ((P.nz + zc - 1) / zc != chunks) continue;   // the same split as a smaller count
+    const double waves = (double)(tiles_xy * chunks) / slots;
+    const double score = waves / std::ceil(waves) * (double)zc / (zc + 2);
+    if (score > best + 1e-9) {
+      best = score;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
+}
+
 void fused_set_tile(FusedPlan* pl, int tile) {
   const Inst in = inst_of(pl->precision, pl->strict);
   if (tile < 0 || tile >= in.tiles()) tile = 0;
   pl->tile = tile;
-  pl->launch = in.pick(pl->nf, pl->dim, tile, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads);
+  pl->launch = in.pick(pl->nf, pl->dim, tile, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads, &pl->minb);
   const HydroParams& P = pl->P;
+  if (pl->dim == 3) pl->zc = choose_zc(P, pl->tx, pl->ty, pl->minb, pl->zc);
   if (pl->dim == 1) {
     int64_t b = (P.nx + 127) / 128;
     pl->grid = dim3((unsigned)(b < 1 ? 1 : b), 1, 1);

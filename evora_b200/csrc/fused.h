@@ -22,6 +22,7 @@ struct FusedPlan {
   int64_t n = 0;       // cells
   int tile = 0;        // entry of the precision's tile table
   int tx = 0, ty = 0, zc = 0;
+  int minb = 1;        // CTAs per SM the tile is built for
   size_t smem = 0;
   dim3 grid{1, 1, 1};
   int threads = 0;
@@ -83,7 +84,7 @@ void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams&
 // Instantiation launchers (fused_f64.cu, fused_f64_strict.cu, fused_f32.cu).
 #define EVORA_DECLARE_FUSED_NS(ns)                                                           \
   namespace ns {                                                                             \
-  FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads); \
+  FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb); \
   int tiles();                                                                               \
   void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st);                \
   }

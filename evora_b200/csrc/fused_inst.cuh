@@ -34,7 +34,7 @@ constexpr int kTiles = 4;
 
 template <int NF, int DIM, int I>
 void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
-  FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n, pl.cfl_fused};
+  FusedArgs<TT> A{pl.P, (const TT*)qin, (TT*)qout, ctl, pl.n, pl.cfl_fused, pl.zc};
   if constexpr (DIM == 1) {
     k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
   } else {
@@ -44,12 +44,12 @@ void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cuda
 }
 
 template <int NF, int DIM, int I>
-FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads) {
+FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb) {
   if constexpr (DIM == 1) {
-    *tx = 128; *ty = 1; *zc = 1; *smem = 0; *threads = 128;
+    *tx = 128; *ty = 1; *zc = 1; *smem = 0; *threads = 128; *minb = 1;
   } else {
     using C = Tile<I>;
-    *tx = C::TX; *ty = C::TY; *zc = DIM == 3 ? C::ZC : 1;
+    *tx = C::TX; *ty = C::TY; *zc = DIM == 3 ? C::ZC : 1; *minb = C::MINB;
     *smem = sizeof(FusedSmem<TT, NF, C::TX, C::TY>);
     *threads = C::TX * C::TY;
     auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>;
@@ -61,22 +61,22 @@ FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads) {
 
 int tiles() { return kTiles; }
 
-FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads) {
+FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb) {
   if (nf == 5 && dim == 3) {
     switch (tile) {
-      case 1: return pick_one<5, 3, 1>(tx, ty, zc, smem, threads);
-      case 2: return pick_one<5, 3, 2>(tx, ty, zc, smem, threads);
-      case 3: return pick_one<5, 3, 3>(tx, ty, zc, smem, threads);
-      default: return pick_one<5, 3, 0>(tx, ty, zc, smem, threads);
+      case 1: return pick_one<5, 3, 1>(tx, ty, zc, smem, threads, minb);
+      case 2: return pick_one<5, 3, 2>(tx, ty, zc, smem, threads, minb);
+      case 3: return pick_one<5, 3, 3>(tx, ty, zc, smem, threads, minb);
+      default: return pick_one<5, 3, 0>(tx, ty, zc, smem, threads, minb);
     }
   }
   if (nf == 5) {
-    if (dim == 1) return pick_one<5, 1, 0>(tx, ty, zc, smem, threads);
-    return pick_one<5, 2, 0>(tx, ty, zc, smem, threads);
+    if (dim == 1) return pick_one<5, 1, 0>(tx, ty, zc, smem, threads, minb);
+    return pick_one<5, 2, 0>(tx, ty, zc, smem, threads, minb);
   }
-  if (dim == 1) return pick_one<6, 1, 0>(tx, ty, zc, smem, threads);
-  if (dim == 2) return pick_one<6, 2, 0>(tx, ty, zc, smem, threads);
-  return pick_one<6, 3, 0>(tx, ty, zc, smem, threads);
+  if (dim == 1) return pick_one<6, 1, 0>(tx, ty, zc, smem, threads, minb);
+  if (dim == 2) return pick_one<6, 2, 0>(tx, ty, zc, smem, threads, minb);
+  return pick_one<6, 3, 0>(tx, ty, zc, smem, threads, minb);
 }
 
 // hydrostep part 1 on the SoA state: maxima of |u_d| + a (per cell in the

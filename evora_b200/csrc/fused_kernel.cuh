@@ -64,6 +64,7 @@ struct FusedArgs {
   GridCtl* ctl;     // dt, active flag, error mask
   int64_t n;        // cells per field
   int cfl_next = 0; // 1: reduce the next step's CFL maxima into ctl->snext
+  int zc = 0;       // planes per CTA (0: the instantiation's ZC)
 };
 
 // Boundary index map of one axis (0-based), boundary.f90:26-113: g in
@@ -249,10 +250,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
   constexpr int RX = TX + 4, RY = TY + 4;
   const HydroParams& P = A.P;
   const int nx = P.nx, ny = P.ny, nz = DIM == 3 ? P.nz : 1;
-  const int X0 = bx * TX, Y0 = by * TY, Z0 = DIM == 3 ? bz * ZC : 0;
+  const int zc = A.zc > 0 ? A.zc : ZC;
+  const int X0 = bx * TX, Y0 = by * TY, Z0 = DIM == 3 ? bz * zc : 0;
   const int xe = nx - X0 < TX ? nx - X0 : TX;
   const int ye = ny - Y0 < TY ? ny - Y0 : TY;
-  const int ze = DIM == 3 ? (nz - Z0 < ZC ? nz - Z0 : ZC) : 1;
+  const int ze = DIM == 3 ? (nz - Z0 < zc ? nz - Z0 : zc) : 1;
   const int oi = tid % TX, oj = tid / TX;
   const bool owned = oi < xe && oj < ye;
   const int64_t n = A.n;
