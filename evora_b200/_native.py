@@ -32,6 +32,7 @@ class EvoraParams(ctypes.Structure):
         ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
         ("tstart", c_double), ("tend", c_double),
+        ("conduction", c_int32), ("simplekappa", c_int32), ("c_cond", c_double),
     ]
 
     def as_dict(self):
@@ -184,6 +185,8 @@ def _declare_batch(L):
         "evora_hydrostep_noalloc": ([c_void_p, _dp], c_int32),
         "evora_gravpotential": ([c_void_p, c_void_p], c_int32),
         "evora_gravintegration": ([c_void_p, c_void_p, c_double], c_int32),
+        "evora_thermalstep": ([c_void_p, c_void_p, _dp], c_int32),
+        "evora_thermalconduction": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),
         "evora_server_destroy": ([G], c_int32),

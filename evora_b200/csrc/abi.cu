@@ -9,6 +9,7 @@
 #include <mutex>
 
 #include "../../include/evora_gpu.h"
+#include "../../include/evora_io.h"
 #include "common.h"
 #include "dropin_api.h"
 
@@ -36,6 +37,13 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->de_thresh1 = dd.de_thresh1;
   P->dx = dd.dx; P->dy = dd.dy; P->dz = dd.dz;
   P->dxinv = dd.dxinv; P->dyinv = dd.dyinv; P->dzinv = dd.dzinv;
+  P->conduction = p->conduction != 0;
+  P->simplekappa = p->simplekappa != 0;
+  P->c_cond = p->c_cond;
+  evora_units u;   // compunits (units.f90:26-73), non-comoving
+  evora_units_noncomoving(p->tstart, dd.g, 1.0, &u);
+  P->kappa0 = u.kappa0;
+  P->temp0 = u.temp0;
   return true;
 }
 
@@ -76,6 +84,9 @@ void evora_params_default(evora_params* p) {
   p->tstart = 0.0; p->tend = 1.0;
   p->dualenergy = 0;
   p->de_thresh = 0.0;
+  p->conduction = 0;
+  p->simplekappa = 0;
+  p->c_cond = (double)0.1f;
 }
 
 int evora_compparameter(const evora_params* p, evora_derived* d) {
@@ -85,6 +96,10 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
   if (p->solver != 1 && p->solver != 2) return EVORA_ERR_SOLVER;
   if (p->limiter < 1 || p->limiter > 3) return EVORA_ERR_LIMITER;
   if (p->boundtype < 1 || p->boundtype > 3) return EVORA_ERR_ARG;
+  // thermalflux's Spitzer branch (conduction.f90:140-144) reads the electron
+  // density that w2n leaves unset without chemistry, and a gradient before
+  // it is assigned: only the simplekappa branch is defined in this build
+  if (p->conduction && !p->simplekappa) return EVORA_ERR_ARG;
   // parameter.f90:164-265
   double g = p->atomic ? (double)(5.0f / 3.0f) : p->g;
   d->g = g;

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "batch_kernel.cuh"
+#include "conduction.h"
 #include "fused.h"
 #include "fused_kernel.cuh"
 
@@ -84,7 +85,7 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
 template <int NF>
 __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, vmin = 1e99;
   unsigned err = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     TT qv[6], s[3];
@@ -95,6 +96,19 @@ __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, Gr
     if (s0 > m0) m0 = s0;
     if (s1 > m1) m1 = s1;
     if (s2 > m2) m2 = s2;
+    if (P.conduction) {
+      // thermalstep (timestep.f90:84-93): min over cells of rho / kappa
+      double qd[6], w[5];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) qd[f] = (double)qv[f];
+      q2w(qd, w, Gas<double>::make(P), P.dualenergy != 0, err);
+      const double v = thermal_v(P, w[0], w[4]);
+      if (v < vmin) vmin = v;
+    }
+  }
+  if (P.conduction) {
+    for (int off = 16; off > 0; off >>= 1) vmin = fmin2(vmin, __shfl_xor_sync(0xffffffffu, vmin, off));
+    if ((threadIdx.x & 31) == 0) atomicMin(&ctl->vcond, ordered_bits(vmin));
   }
   for (int off = 16; off > 0; off >>= 1) {
     m0 = fmax2(m0, __shfl_xor_sync(0xffffffffu, m0, off));

@@ -23,6 +23,7 @@
 #include "dropin_api.h"
 #include "fused.h"
 #include "gravity.h"
+#include "conduction.h"
 
 using namespace evora;
 
@@ -60,6 +61,9 @@ struct evora_grid {
   // self-gravity after each hydro step (params.gravity)
   bool gravity = false;
   GravPlan grav{};
+  // thermal conduction after each step (params.conduction)
+  bool conduction = false;
+  CondPlan cond{};
   bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
 };
 
@@ -92,6 +96,7 @@ __global__ void k_step_begin(GridCtl* ctl, int use_next) {
   }
   ctl->errnext = 0u;
   ctl->snext[0] = ctl->snext[1] = ctl->snext[2] = 0ull;
+  ctl->vcond = ordered_bits(1e99);   // thermalstep's initial v (timestep.f90:82)
   ctl->active = (ctl->go != 0 && ctl->err == 0) ? 1 : 0;
 }
 
@@ -105,6 +110,7 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   for (int i = 0; i < 3; ++i) sm[i] = __longlong_as_double((long long)ctl->smax[i]);
   unsigned e = 0;
   double dt = cfl_dt(P, sm[0], sm[1], sm[2], 1e99, e);
+  if (!e && P.conduction) dt = thermal_dt(P, __longlong_as_double((long long)ctl->vcond), dt, e);
   if (e) {
     ctl->err |= e;
     ctl->active = 0;
@@ -186,6 +192,12 @@ int enqueue_fused_step(evora_grid* g) {
     if (rc) return rc;
     g->launches += 5;   // own kernels; cuFFT adds its own
   }
+  if (g->conduction) {
+    // primitive + bound + thermalconduction on the updated state (main.f90:169-175)
+    int rc = cond_step(g->cond, g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, g->ctl, 0.0, st);
+    if (rc) return rc;
+    g->launches += 2;
+  }
   mark(g);
   k_step_end<<<1, 1, 0, st>>>(g->ctl);
   CU(cudaGetLastError());
@@ -213,6 +225,7 @@ void free_grid(evora_grid* g) {
   for (cudaEvent_t e : g->events) cudaEventDestroy(e);
   fused_plan_free(&g->plan);
   grav_plan_free(&g->grav);
+  cond_plan_free(&g->cond);
   dfree(g, g->ctl);
   dfree(g, g->q_aos);
   dfree(g, g->w);
@@ -287,6 +300,19 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
     if (dalloc(g, &g->qbuf[0], bytes) != cudaSuccess) goto nomem;
     if (dalloc(g, &g->qbuf[1], bytes) != cudaSuccess) goto nomem;
     rc = fused_plan(g->P, g->precision, g->nf, (flags & EVORA_STRICT) != 0, &g->plan, astream);
+    if (rc) {
+      free_grid(g);
+      return rc;
+    }
+  }
+  if (p->conduction) {
+    if (reference_backend(g)) {
+      free_grid(g);
+      return EVORA_ERR_ARG;   // conduction runs on the resident SoA state
+    }
+    g->conduction = true;
+    g->plan.cfl_fused = 0;     // the state changes after the update
+    rc = cond_plan(ncells(g), &g->cond);
     if (rc) {
       free_grid(g);
       return rc;
@@ -455,7 +481,8 @@ int graph_steps(evora_grid* g, int nsteps) {
     } else {
       g->cur = start ^ (nsteps & 1);
       const bool fused = g->plan.cfl_fused != 0;
-      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0)) + (fused && !fresh ? 1 : 0);
+      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0) + (g->conduction ? 2 : 0)) +
+                     (fused && !fresh ? 1 : 0);
       g->cfl_fresh = fused;
     }
   }

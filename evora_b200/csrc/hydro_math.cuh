@@ -39,6 +39,7 @@ struct GridCtl {
   unsigned errnext;  // errors of the CFL maxima in snext (raised when used)
   unsigned long long smax[3];   // CFL maxima of |u_d| + a (ordered bits)
   unsigned long long snext[3];  // the same, over the state the update wrote
+  unsigned long long vcond;     // thermalstep: min over cells of rho / kappa (ordered bits)
 };
 
 __device__ __forceinline__ bool ctl_skip(const GridCtl* ctl) {
@@ -52,6 +53,9 @@ struct HydroParams {
   int onedimension, twodimension;
   double g, g1, g1inv, gg1, cfl, de_thresh1;
   double dx, dy, dz, dxinv, dyinv, dzinv;
+  // thermal conduction (conduction.f90, thermalstep timestep.f90:72-104)
+  int conduction, simplekappa;
+  double c_cond, kappa0, temp0;
 };
 
 template <typename T>

@@ -139,6 +139,19 @@ class DropIn:
         imaginary part is written as 0."""
         check(lib().evora_gravpotential(_ptr(q, self.shape["q"], False), self._phi_ptr(phi)), "gravpotential")
 
+    def thermalstep(self, q, w, dt: float = 1e99) -> float:
+        """thermalstep(q,w), timestep.f90:72-104: min(dt, conduction limit);
+        q is resynchronised in place with dual energy, as in the reference."""
+        d = ctypes.c_double(dt)
+        check(lib().evora_thermalstep(_ptr(q, self.shape["q"]), _ptr(w, self.shape["w"], False),
+                                      ctypes.byref(d)), "thermalstep")
+        return d.value
+
+    def thermalconduction(self, q, w, dt: float):
+        """thermalconduction(q,w), conduction.f90:26-122 (simplekappa)."""
+        check(lib().evora_thermalconduction(_ptr(q, self.shape["q"]), _ptr(w, self.shape["w"], False),
+                                            float(dt)), "thermalconduction")
+
     def gravintegration(self, q, phi, dt: float):
         """gravintegration(q,phi,...), gravitation.f90:170-243 (one process,
         so no boundary buffers): the gravitational source terms over dt."""

@@ -80,6 +80,13 @@ typedef struct evora_params {
   double g, cfl, de_thresh;
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double tstart, tend;
+  int32_t conduction;   /* Fortran logical: explicit thermal conduction after
+                           each step (conduction.f90) and its time-step
+                           limit (thermalstep, timestep.f90:72-104)         */
+  int32_t simplekappa;  /* Fortran logical: conductivity 1/(g-1); the other
+                           branch reads unset variables in the reference's
+                           plain build and is refused (EVORA_ERR_ARG)       */
+  double c_cond;        /* conduction time-step factor                      */
 } evora_params;
 
 /* The derived constants of compparameter (parameter.f90:164-265) that the
@@ -153,6 +160,29 @@ int evora_hydrostep(const double* w, double* dt);
  * the array: calls that overlap on the GPU (concurrent host threads or
  * streams) race on it.  Synchronous: returns after dt is known. */
 int evora_hydrostep_noalloc(const double* w, double* dt);
+
+/* thermalstep(q,w), timestep.f90:72-104 (conduction on, simplekappa):
+ * dt = min(c_cond dx^2 min(rho / (kappa0 T^2.5)) / temp0, dt) with T from
+ * pressure(q) (which resynchronises q in place with dual energy, as the
+ * reference's call does) and rho from w.  EVORA_ERR_DT if dt <= 0,
+ * EVORA_ERR_ARG unless conduction and simplekappa are set. */
+int evora_thermalstep(double* q, const double* w, double* dt);
+
+/* thermalconduction(q,w), conduction.f90:26-122 (simplekappa): the x, y
+ * and z conduction sweeps over dt from the primitives w (ghosts filled by
+ * bound), updating E and S of q in place. */
+int evora_thermalconduction(double* q, const double* w, double dt);
+
+/* gravpotential(q,phi), gravitation.f90:26-53, non-comoving branch: the
+ * potential of the density of q (FFT Poisson solve with the reference's
+ * discrete Green's function).  phi is the reference's complex(8)
+ * phi(nx,ny,nz) (interleaved re, im); the imaginary part is written as 0. */
+int evora_gravpotential(const double* q, double* phi);
+
+/* gravintegration(q,phi,...), gravitation.f90:170-243, for one process:
+ * the gravitational source terms of m and E over dt from the real part of
+ * phi (periodic centred differences). */
+int evora_gravintegration(double* q, const double* phi, double dt);
 
 /* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch:
  * if tend - t <= dt then dt = tend - t, go = false; then t = t + dt.

@@ -49,6 +49,8 @@ static struct {
   double dx, dy, dz, dxinv, dyinv, dzinv, x0, y0, z0, volume;
   double tstart, tend;
   int onedimension, twodimension;
+  int conduction, simplekappa;
+  double c_cond, kappa0, temp0;
 } G;
 
 static int orc_err = 0;
@@ -96,6 +98,21 @@ int orc_compparameter(const evora_params* p) {
   if (p->atomic) G.g = (double)(5.0f / 3.0f);           /* parameter.f90:169-171 */
   G.cfl = p->cfl;
   G.tstart = p->tstart; G.tend = p->tend;
+  /* thermal conduction: only the simplekappa branch of thermalflux is
+   * defined without chemistry (conduction.f90:140-144 reads the electron
+   * density w2n leaves unset, and a gradient before it is assigned) */
+  if (p->conduction && !p->simplekappa) return EVORA_ERR_ARG;
+  G.conduction = p->conduction != 0;
+  G.simplekappa = p->simplekappa != 0;
+  G.c_cond = p->c_cond;
+  {
+    /* compunits, units.f90:26-73, without comoving coordinates:
+     * cosmo = h = d0 = t0 = l0 = 1, m0 = kb */
+    const double kb = 1.3806200e-16, cosmo = 1.0, t0 = 1.0, d0 = 1.0, l0 = 1.0, m0 = kb;
+    G.temp0 = pow(l0, 2.0) / pow(cosmo, 2.0) / pow(t0, 2.0) * m0 / kb;
+    const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
+    G.kappa0 = pow(cosmo, 5.0) * pow(t0, 3.0) / d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
+  }
   G.onedimension = (p->ny == 1 && p->nz == 1);          /* parameter.f90:173-177 */
   G.twodimension = (p->nz == 1);                        /* parameter.f90:178-182 */
   double xmin = p->xmin, xmax = p->xmax, ymin = p->ymin, ymax = p->ymax;
@@ -626,6 +643,90 @@ double orc_hydrostep(const double* w, double dt_in) {
   return dt;
 }
 
+/* thermalstep(q,w), timestep.f90:72-104: returns min(conduction limit,
+ * dt_in).  pressure(q) resynchronises q in place with dual energy, as the
+ * reference's call does. */
+double orc_thermalstep(double* q, const double* w, double dt_in) {
+  double v = 1e99;
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double* c = &q[iq(ix, iy, iz)];
+        double press = orc_pressure(c);
+        double temp = press / c[0] * G.temp0;            /* press2temp, comp.f90:87-102 */
+        double kappa = G.kappa0 * pow(temp, 2.5);
+        v = fmin2(w[iw(ix, iy, iz)] / kappa, v);
+      }
+  v = G.c_cond * pow(G.dx, 2.0) * v / G.temp0;
+  double dt = fmin2(v, dt_in);
+  if (dt <= 0.0) set_err(EVORA_ERR_DT);
+  return dt;
+}
+
+/* thermalflux, conduction.f90:126-148 (simplekappa) */
+static double orc_thermalflux(double templ, double tempr, double deltainv) {
+  double kappa_eff = 1.0 / G.g1;
+  double dtempdx = (tempr - templ) * deltainv;
+  return -(kappa_eff * dtempdx);
+}
+
+/* thermalintegration, conduction.f90:150-164 */
+static void orc_thermalintegration(double jl, double jr, double* q, double delta) {
+  double de = delta * (jl - jr);
+  q[4] = q[4] + de;
+  q[5] = q[5] + G.g1 * de / pow(q[0], G.g1);
+}
+
+static double orc_temp(const double* w) { return w[4] / w[0] * G.temp0; }
+
+/* thermalconduction(q,w), conduction.f90:26-122: sweeps in x, y, z from
+ * the same w (ghosts from bound), the interface flux carried along each
+ * pencil. */
+void orc_thermalconduction(double* q, const double* w, double dt) {
+  if (G.nx != 1) {
+    double delta = dt * G.dxinv;
+    for (int iz = 1; iz <= G.nz; ++iz)
+      for (int iy = 1; iy <= G.ny; ++iy) {
+        double tempr = orc_temp(&w[iw(1, iy, iz)]);
+        double jr = orc_thermalflux(orc_temp(&w[iw(0, iy, iz)]), tempr, G.dxinv);
+        for (int ix = 1; ix <= G.nx; ++ix) {
+          double jl = jr, templ = tempr;
+          tempr = orc_temp(&w[iw(ix + 1, iy, iz)]);
+          jr = orc_thermalflux(templ, tempr, G.dxinv);
+          orc_thermalintegration(jl, jr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+  if (G.ny != 1) {
+    double delta = dt * G.dyinv;
+    for (int iz = 1; iz <= G.nz; ++iz)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double tempr = orc_temp(&w[iw(ix, 1, iz)]);
+        double jr = orc_thermalflux(orc_temp(&w[iw(ix, 0, iz)]), tempr, G.dyinv);
+        for (int iy = 1; iy <= G.ny; ++iy) {
+          double jl = jr, templ = tempr;
+          tempr = orc_temp(&w[iw(ix, iy + 1, iz)]);
+          jr = orc_thermalflux(templ, tempr, G.dyinv);
+          orc_thermalintegration(jl, jr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+  if (G.nz != 1) {
+    double delta = dt * G.dzinv;
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double tempr = orc_temp(&w[iw(ix, iy, 1)]);
+        double jr = orc_thermalflux(orc_temp(&w[iw(ix, iy, 0)]), tempr, G.dzinv);
+        for (int iz = 1; iz <= G.nz; ++iz) {
+          double jl = jr, templ = tempr;
+          tempr = orc_temp(&w[iw(ix, iy, iz + 1)]);
+          jr = orc_thermalflux(templ, tempr, G.dzinv);
+          orc_thermalintegration(jl, jr, &q[iq(ix, iy, iz)], delta);
+        }
+      }
+  }
+}
+
 /* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch. */
 void orc_updatetime(int* go, double* t, double* dt) {
   if (G.tend - *t <= *dt) {
@@ -637,7 +738,7 @@ void orc_updatetime(int* go, double* t, double* dt) {
 
 /* ------------------------------------------------------------- driver -- */
 /* The hydro subset of the time loop of main.f90:109-203 (no gravity,
- * chemistry, conduction, expansion, output).  Runs until go is cleared,
+ * chemistry, expansion, output; thermal conduction when enabled).  Runs until go is cleared,
  * max_steps is reached or an error is raised.  Arrays w, evo, s are
  * scratch of orc_array_sizes() elements, allocated here.  Returns the error
  * mask; *t and *steps report the end state, *dt_last the last step. */
@@ -660,10 +761,16 @@ int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, in
     orc_bound(w);
     dt = 1e99;
     dt = orc_hydrostep(w, dt);
+    if (G.conduction) dt = orc_thermalstep(q, w, dt);      /* main.f90:121 */
     orc_updatetime(&go, t, &dt);
     if (orc_err) break;
     if (G.secondorder) orc_compevo(w, evo, s, dt);
     orc_sweep(w, q, evo, s, dt);
+    if (G.conduction) {                                     /* main.f90:169-175 */
+      orc_primitive(w, q);
+      orc_bound(w);
+      orc_thermalconduction(q, w, dt);
+    }
     ++k;
     if (orc_err) break;
   }

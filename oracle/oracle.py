@@ -46,6 +46,7 @@ class OracleParams(ctypes.Structure):
         ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
         ("tstart", c_double), ("tend", c_double),
+        ("conduction", ctypes.c_int32), ("simplekappa", ctypes.c_int32), ("c_cond", c_double),
     ]
 
 
@@ -86,6 +87,9 @@ def lib():
             L.orc_ic_kh2d.argtypes = [_dp]
             L.orc_ic_kh3d.argtypes = [_dp, ctypes.c_uint64, c_double]
             L.orc_set_threads.argtypes = [c_int]
+            L.orc_thermalstep.argtypes = [_dp, _dp, c_double]
+            L.orc_thermalstep.restype = c_double
+            L.orc_thermalconduction.argtypes = [_dp, _dp, c_double]
             _lib = L
     return _lib
 
@@ -108,6 +112,7 @@ def make_params(**kw) -> OracleParams:
     p.xmin = p.ymin = p.zmin = 0.0
     p.xmax = p.ymax = p.zmax = 1.0
     p.tstart, p.tend = 0.0, 1.0
+    p.conduction, p.simplekappa, p.c_cond = 0, 0, float(np.float32(0.1))
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -187,6 +192,15 @@ class Oracle:
 
     def sweep(self, w, q, evo, s, dt):
         self.L.orc_sweep(_ptr(w), _ptr(q), _ptr(evo), _ptr(s), float(dt))
+
+    def thermalstep(self, q, w, dt_in=1e99) -> float:
+        """thermalstep(q,w), timestep.f90:72-104 (q resynchronised in place
+        with dual energy, as the reference's pressure() call does)."""
+        return float(self.L.orc_thermalstep(_ptr(q), _ptr(w), float(dt_in)))
+
+    def thermalconduction(self, q, w, dt):
+        """thermalconduction(q,w), conduction.f90:26-122."""
+        self.L.orc_thermalconduction(_ptr(q), _ptr(w), float(dt))
 
     def riemann(self, wl, wr, direction: int):
         wl = np.ascontiguousarray(wl, dtype=np.float64)

@@ -4,8 +4,9 @@
 TEST INFRASTRUCTURE ONLY.  No Fortran compiler exists on this image, so the
 reference cannot be built as is.  This script reads the reference's own
 sources (module global, compparameter, decomposition, q2w, pressure,
-coordinates, muscl.f90, riemann.f90, boundary.f90, hydrostep, updatetime and
-the shocktube / Kelvin-Helmholtz ICs) and translates the Fortran 90 subset
+coordinates, w2n, press2temp, muscl.f90, riemann.f90, boundary.f90,
+hydrostep, updatetime, thermalstep, conduction.f90, compunits and the
+shocktube / Kelvin-Helmholtz ICs) and translates the Fortran 90 subset
 they use into C, statement by statement, keeping Fortran semantics:
 
   * default-real literals (0.5, 1e6, 3.1415927) are C floats, d-exponent
@@ -37,11 +38,13 @@ UNITS = [
     ("source/global.f90", None, {}),
     ("source/parameter.f90", ["compparameter"], {}),
     ("source/parallel.f90", ["decomposition"], {}),
-    ("source/comp.f90", ["q2w", "pressure", "coordinates"], {}),
+    ("source/comp.f90", ["q2w", "pressure", "coordinates", "w2n", "press2temp"], {}),
     ("source/muscl.f90", None, {}),
     ("source/riemann.f90", None, {}),
     ("source/boundary.f90", None, {}),
-    ("source/timestep.f90", ["hydrostep", "updatetime"], {}),
+    ("source/timestep.f90", ["hydrostep", "updatetime", "thermalstep"], {}),
+    ("source/conduction.f90", None, {}),
+    ("source/units.f90", ["compunits"], {}),
     ("ic/shocktube.f90", None, {"ic": "ic_shocktube"}),
     ("ic/kevinhelmholtz.f90", None, {"ic": "ic_kevinhelmholtz"}),
 ]
@@ -589,6 +592,12 @@ class Translator:
                 return self.promote([self.etype(a, local) for a in node.args])
             if fn == "dble":
                 return "double"
+            if fn == "sum":
+                a = node.args[0]
+                sa = self.sym(a.name, local) if isinstance(a, (Name, Ref)) else None
+                if not sa or not sa.is_array:
+                    raise F2CError("sum of a non-array")
+                return sa.ftype
             raise F2CError(f"unknown function {fn}")
         if isinstance(node, Un):
             return "logical" if node.op == ".not." else self.etype(node.a, local)
@@ -659,6 +668,17 @@ class Translator:
                 lm = loopmap[:len(ranges)] if ranges else None
                 return f"{self.base(s)}[{self.index_expr(s, node.args, lm, local)}]"
             fn = node.name
+            if fn == "sum":
+                # SUM of a whole one-dimensional array, accumulated in
+                # element order (no reassociation without -ffast-math)
+                a = node.args[0]
+                sa = self.sym(a.name, local)
+                if not isinstance(a, Name) or len(sa.dims) != 1:
+                    raise F2CError("sum of an array section")
+                lo, hi = sa.dims[0]
+                t = CTYPE[sa.ftype]
+                ext = f"(({self.c(hi, local)}) - ({self.c(lo, local)}) + 1)"
+                return f"({{ {t} acc_ = 0; for (long i_ = 0; i_ < {ext}; ++i_) acc_ += {self.base(sa)}[i_]; acc_; }})"
             args = [self.c(a, local, loopmap) for a in node.args]
             if fn == "sqrt":
                 return f"sqrt({args[0]})" if self.etype(node, local) == "double" else f"sqrtf({args[0]})"

@@ -64,12 +64,12 @@ int ref_setup_c(const evora_params* p) {
   G_supercomoving = 0; G_c_cosmo = 0.1f; G_omega0 = 1.0f; G_lambda0 = 0.0f; G_hubble0 = 50.0f;
   G_fb = 1.0f; G_box = 1.0f; G_zstart = 99.0f; G_zend = 0.0f;
   G_chemistry = 0; G_noncie = 0; G_cooling = 0; G_background = 0;
-  G_conduction = 0;
+  G_conduction = p->conduction; G_simplekappa = p->simplekappa; G_c_cond = p->c_cond;
   G_dualenergy = p->dualenergy; G_de_thresh = p->de_thresh;
   G_mpisize = 1; G_mpirank = 0; G_master = 1; G_parallel = 0;
   G_local_x_start = 0; G_local_nx = p->nz;
   G_redshift = 0.0;
-  GUARD(ref_compparameter(); ref_decomposition());
+  GUARD(ref_compparameter(); ref_decomposition(); ref_compunits());
   return 0;
 }
 
@@ -112,8 +112,20 @@ int ref_sweep_c(double* w, double* q, double* evo, double* s, double dt) {
   return 0;
 }
 
-/* main.f90:109-155, hydro subset: no cooling, conduction, gravity,
- * chemistry, expansion or output. */
+int ref_thermalstep_c(double* q, double* w, double* dt) {
+  G_dt = *dt;
+  GUARD(ref_thermalstep(q, w));
+  *dt = G_dt;
+  return 0;
+}
+int ref_thermalconduction_c(double* q, double* w, double dt) {
+  G_dt = dt;
+  GUARD(ref_thermalconduction(q, w));
+  return 0;
+}
+
+/* main.f90:109-203 without cooling, gravity, chemistry, expansion or
+ * output: hydro and, when enabled, thermal conduction (121, 169-175). */
 int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* go_out) {
   int64_t nq, nw, ne, ns;
   ref_sizes_c(&nq, &nw, &ne, &ns);
@@ -133,9 +145,15 @@ int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* 
     ref_bound(w);
     G_dt = 1e99;
     if (G_hydro) ref_hydrostep(w);
+    if (G_conduction) ref_thermalstep(q, w);
     ref_updatetime(&go, &dump, &k4);
     if (G_secondorder) ref_compevo(w, evo, s);
     if (G_hydro) ref_sweep(w, q, evo, s);
+    if (G_conduction) {
+      ref_primitive(w, q);
+      ref_bound(w);
+      ref_thermalconduction(q, w);
+    }
     k = k + 1;
   }
   g_armed = 0;

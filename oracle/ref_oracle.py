@@ -48,6 +48,8 @@ def lib():
         L.ref_ic_shocktube_c.argtypes = [_dp] + [ctypes.c_double] * 7 + [ctypes.c_int]
         L.ref_ic_kh_c.argtypes = [_dp]
         L.ref_riemann_c.argtypes = [_dp, _dp, _dp, ctypes.c_int]
+        L.ref_thermalstep_c.argtypes = [_dp, _dp, _dp]
+        L.ref_thermalconduction_c.argtypes = [_dp, _dp, ctypes.c_double]
         _lib = L
     return _lib
 
@@ -111,6 +113,16 @@ class RefOracle:
 
     def sweep(self, w, q, evo, s, dt):
         return self.L.ref_sweep_c(_p(w), _p(q), _p(evo), _p(s), float(dt))
+
+    def thermalstep(self, q, w, dt_in=1e99):
+        """thermalstep(q,w) (timestep.f90:72-104): min(dt_in, conduction limit)."""
+        d = ctypes.c_double(dt_in)
+        st = self.L.ref_thermalstep_c(_p(q), _p(w), ctypes.byref(d))
+        return d.value, st
+
+    def thermalconduction(self, q, w, dt):
+        """thermalconduction(q,w) (conduction.f90:26-122) over dt."""
+        return self.L.ref_thermalconduction_c(_p(q), _p(w), float(dt))
 
     def riemann(self, wl, wr, direction):
         wl = np.ascontiguousarray(wl, dtype=np.float64)

@@ -3,7 +3,7 @@ hydro path (its Fortran sources translated mechanically to C by
 oracle/ref/f2c.py and driven like main.f90 by oracle/ref/harness.c).
 
 Run from the repository root where /root/reference exists:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [classic] [conduction]
 Each fixture holds the inputs (parameters, initial q) and the reference's
 outputs (q after the steps, t, dt, steps).  The reference itself has no test
 vectors (its bin/test only draws plots)."""
@@ -22,7 +22,8 @@ from helpers import random_q  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIELDS = ["nx", "ny", "nz", "solver", "limiter", "boundtype", "secondorder", "dualenergy", "atomic",
-          "g", "cfl", "de_thresh", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "tstart", "tend"]
+          "g", "cfl", "de_thresh", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "tstart", "tend",
+          "conduction", "simplekappa", "c_cond"]
 
 
 class _O:
@@ -46,7 +47,26 @@ def save(name, kw, q0, steps):
     print(name, res)
 
 
-def main():
+def main(only=None):
+    if only:
+        # a subset by name (the other fixtures stay as committed)
+        for name in only:
+            CASES[name]()
+        return
+    for make in CASES.values():
+        make()
+
+
+def _conduction():
+    # thermal conduction (simplekappa) after every hydro step, 3D, a box
+    # large enough for the explicit conduction to be stable
+    kw = dict(nx=14, ny=12, nz=10, g=5 / 3, cfl=0.4, boundtype=1, limiter=1, tend=100.0,
+              xmax=56.0, ymax=48.0, zmax=40.0, conduction=1, simplekappa=1)
+    r = RefOracle(make_params(**kw))
+    save("cond3d_14x12x10_simplekappa", kw, random_q(_O(r), np.random.default_rng(11), pres=(0.5, 3.0)), 8)
+
+
+def _classic():
     kw = dict(nx=1024, ny=1, nz=1, g=1.4, cfl=0.8, boundtype=1, tend=0.2)
     r = RefOracle(make_params(**kw))
     save("sod1024_hllc_minmod", kw, r.ic_shocktube(1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 0.5, 1), 100000)
@@ -69,5 +89,7 @@ def main():
     save("kh3d_16x12x10", kw, ic.kh3d(default_params(**kw)), 10)
 
 
+CASES = {"classic": _classic, "conduction": _conduction}
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -19,7 +19,9 @@ EMU = os.path.join(os.path.dirname(__file__), "emu")
 class HP(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in
                 "nx ny nz solver limiter boundtype secondorder dualenergy onedimension twodimension".split()] + \
-               [(n, ctypes.c_double) for n in "g g1 g1inv gg1 cfl de_thresh1 dx dy dz dxinv dyinv dzinv".split()]
+               [(n, ctypes.c_double) for n in "g g1 g1inv gg1 cfl de_thresh1 dx dy dz dxinv dyinv dzinv".split()] + \
+               [("conduction", ctypes.c_int), ("simplekappa", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in "c_cond kappa0 temp0".split()]
 
 
 @pytest.fixture(scope="module")

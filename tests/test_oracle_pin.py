@@ -22,13 +22,15 @@ pytestmark = pytest.mark.skipif(not ref_oracle.available(), reason="translated r
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 FIELDS = ["nx", "ny", "nz", "solver", "limiter", "boundtype", "secondorder", "dualenergy", "atomic",
-          "g", "cfl", "de_thresh", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "tstart", "tend"]
+          "g", "cfl", "de_thresh", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "tstart", "tend",
+          "conduction", "simplekappa", "c_cond"]
+INT_FIELDS = set(FIELDS[:9]) | {"conduction", "simplekappa"}
 
 
 def params_of(arr):
     kw = {}
     for f, v in zip(FIELDS, arr):
-        kw[f] = int(v) if f in FIELDS[:9] else float(v)
+        kw[f] = int(v) if f in INT_FIELDS else float(v)
     return kw
 
 
