@@ -49,9 +49,10 @@ BYTES_PER_CELL = {"f32": 40, "f64": 80}   # 5 fields read + written once
 WORKLOAD = "3D Kelvin-Helmholtz 256^3 periodic, gamma=5/3, HLLC, minmod, CFL 0.5"
 
 
-def kh_params(ev, nz=None, gravity=0):
+def kh_params(ev, nz=None, gravity=0, conduction=0, box=1.0):
     return ev.default_params(nx=NX, ny=NY, nz=nz or NZ, g=GAMMA, cfl=CFL, boundtype=2, solver=2,
-                             limiter=1, tend=1.0e6, gravity=gravity)
+                             limiter=1, tend=1.0e6, gravity=gravity, conduction=conduction,
+                             simplekappa=conduction, xmax=box, ymax=box, zmax=box)
 
 
 def measured_peaks():
@@ -167,9 +168,9 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
-def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0):
+def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0, conduction=0, box=1.0):
     """Device-timed resident steps; returns (ms_total, kernel timing, grid)."""
-    g = ev.Grid(kh_params(ev, gravity=gravity), precision)
+    g = ev.Grid(kh_params(ev, gravity=gravity, conduction=conduction, box=box), precision)
     g.set_stream(stream)
     g.set_q(q)
     g.tuning = g.autotune(reps=3) if AUTOTUNE else (0, [])
@@ -371,49 +372,59 @@ def run_tubes(args):
 # spectrum), Green's factor (read + write it), Z2D (read it, write phi),
 # integration (read rho, m, E and phi, write m and E).
 GRAV_BYTES = {"f32": 4 + 12 + 16 + 16 + 16 + (20 + 8 + 16), "f64": 8 + 16 + 16 + 16 + 16 + (40 + 8 + 32)}
+# conduction substep: primitives and T (read 5 fields, write T FP64), update
+# (read T, rho, E, write E)
+COND_BYTES = {"f32": (20 + 8) + (8 + 4 + 4 + 4), "f64": (40 + 8) + (8 + 8 + 8 + 8)}
+# KH box edge for the conduction workload: kappa_eff = 1/(g-1) is explicit,
+# and a 640-unit box keeps its diffusion number near 0.1 at the hydro step
+COND_BOX = 640.0
 
 
-def run_gravity(args):
-    """The KH workload with self-gravity (gravitation.f90, non-comoving)
-    after every hydro step: FFT Poisson solve (cuFFT D2Z/Z2D, FP64) and the
-    force update.  Reports cell-updates/s of whole steps with gravity and
-    the gravity substep's time (grid with gravity minus grid without) against
-    its algorithmic bytes."""
+def run_physics(args, kind):
+    """The KH workload with one more physics substep after every hydro step:
+    gravity (gravitation.f90, non-comoving: FFT Poisson solve with cuFFT
+    D2Z/Z2D in FP64 and the force update) or thermal conduction
+    (conduction.f90 simplekappa, with thermalstep in the CFL kernel).
+    Reports cell-updates/s of whole steps and the substep's time (grid with
+    it minus grid without, same box) against its algorithmic bytes."""
     import torch
     import evora_b200 as ev
     world, rank, local = dist_setup(args.gpus)
     stream = torch.cuda.Stream()
-    p = kh_params(ev)
-    q = ev.ic.kh3d(p, seed=42, amp=0.01)
+    q = ev.ic.kh3d(kh_params(ev), seed=42, amp=0.01)
     n = NX * NY * NZ
     peak, peak_kind = measured_peaks()
+    nbytes = GRAV_BYTES if kind == "gravity" else COND_BYTES
+    box = 1.0 if kind == "gravity" else COND_BOX
+    extra = {"gravity": 1} if kind == "gravity" else {"conduction": 1}
     out = {}
     barrier(world)
     with ClockSampler(local) as clk:
         clk.wait_first_sample()
         for prec, name in ((ev.FP32, "f32"), (ev.FP64, "f64")):
-            ms_h, kt_h, g = time_grid(ev, torch, q, prec, args.steps, args.warmup, stream)
+            ms_h, kt_h, g = time_grid(ev, torch, q, prec, args.steps, args.warmup, stream, box=box)
             g.close()
-            ms_g, kt_g, g = time_grid(ev, torch, q, prec, args.steps, args.warmup, stream, gravity=1)
+            ms_x, kt_x, g = time_grid(ev, torch, q, prec, args.steps, args.warmup, stream, box=box, **extra)
             g.close()
-            ms_h, ms_g = max_over_ranks(world, ms_h), max_over_ranks(world, ms_g)
-            grav_ms = (ms_g - ms_h) / args.steps
-            achieved = n * GRAV_BYTES[name] / (grav_ms * 1e-3) / 1e9 if grav_ms > 0 else None
-            out[name] = {"value": world * n * args.steps / (ms_g * 1e-3), "ms_per_step": ms_g / args.steps,
-                         "hydro_ms_per_step": ms_h / args.steps, "gravity_ms_per_step": grav_ms,
-                         "gravity_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            ms_h, ms_x = max_over_ranks(world, ms_h), max_over_ranks(world, ms_x)
+            sub_ms = (ms_x - ms_h) / args.steps
+            achieved = n * nbytes[name] / (sub_ms * 1e-3) / 1e9 if sub_ms > 0 else None
+            out[name] = {"value": world * n * args.steps / (ms_x * 1e-3), "ms_per_step": ms_x / args.steps,
+                         "hydro_ms_per_step": ms_h / args.steps, f"{kind}_ms_per_step": sub_ms,
+                         f"{kind}_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                               "frac": achieved / peak if achieved else None,
-                                              "algorithmic_bytes_per_cell": GRAV_BYTES[name],
+                                              "algorithmic_bytes_per_cell": nbytes[name],
                                               "peak_kind": peak_kind},
-                         "gpu_launches": kt_g["launches"]}
+                         "gpu_launches": kt_x["launches"]}
     if rank == 0:
         v = out["f32"]
+        what = ("self-gravity after every step (FFT Poisson solve, FP64)" if kind == "gravity" else
+                f"thermal conduction after every step (simplekappa, box {COND_BOX:g})")
         line = {"metric": METRIC, "value": v["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": v["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD + ", self-gravity after every step (FFT Poisson solve, FP64)",
-                           "cells": n, "l2": "inputs larger than L2"},
-                "roofline": v["gravity_roofline"], "gravity": out, "gpu_launches": v["gpu_launches"],
+                "config": {"workload": WORKLOAD + ", " + what, "cells": n, "l2": "inputs larger than L2"},
+                "roofline": v[f"{kind}_roofline"], kind: out, "gpu_launches": v["gpu_launches"],
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -535,9 +546,9 @@ def main():
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
-    ap.add_argument("--workload", default="kh3d", choices=["kh3d", "tubes", "serving", "gravity"],
+    ap.add_argument("--workload", default="kh3d", choices=["kh3d", "tubes", "serving", "gravity", "conduction"],
                     help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes; serving: request "
-                         "mix; gravity: the KH benchmark with self-gravity")
+                         "mix; gravity / conduction: the KH benchmark with that substep after every step")
     ap.add_argument("--ntubes", type=int, default=4096)
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--nrequests", type=int, default=400)
@@ -552,8 +563,8 @@ def main():
         return run_tubes(args)
     if args.workload == "serving":
         return run_serving(args)
-    if args.workload == "gravity":
-        return run_gravity(args)
+    if args.workload in ("gravity", "conduction"):
+        return run_physics(args, args.workload)
     if args.impl == "reference":
         return run_reference(args)
 

@@ -73,25 +73,27 @@ __device__ __forceinline__ double thermal_flux(double tl, double tr, double delt
 template <typename T>
 __global__ void k_cond_update(T* __restrict__ q, int64_t n, int nf, HydroParams P, const double* __restrict__ temp,
                               const GridCtl* ctl, double dt_host) {
+  // 3D launch: x by threads, one (y, z) row per block row
   if (ctl_skip(ctl)) return;
   const double dt = ctl ? ctl->dt : dt_host;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int64_t nxy = (int64_t)nx * ny;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % nx);
-    const int64_t r = i / nx;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y, iz = blockIdx.z;
+  if (ix < nx) {
+    const int64_t i = ((int64_t)iz * ny + iy) * nx + ix;
     const double tc = temp[i];
     double e = (double)q[4 * n + i];
-    double s = nf == 6 ? (double)q[5 * n + i] : 0.0;
-    const double rho = (double)q[i];
+    const bool carry_s = nf == 6;
+    double s = carry_s ? (double)q[5 * n + i] : 0.0;
+    // rho^(g-1) of the cell, the same in every axis's thermalintegration
+    const double rg = carry_s ? pow((double)q[i], P.g1) : 1.0;
     auto integrate = [&](double tl, double tr, double deltainv) {
       const double jl = thermal_flux(tl, tc, deltainv, P.g1);
       const double jr = thermal_flux(tc, tr, deltainv, P.g1);
       const double delta = dt * deltainv;
       const double d = delta * (jl - jr);          // thermalintegration (150-164)
       e = e + d;
-      s = s + P.g1 * d / pow(rho, P.g1);
+      if (carry_s) s = s + P.g1 * d / rg;
     };
     if (nx != 1) {
       const int64_t base = i - ix;
@@ -274,12 +276,13 @@ int prepare(DropinCond& D, HydroParams* P, const double* q, const double* w, dou
 int cond_step(CondPlan& c, const HydroParams& P, void* q, bool f32, int nf, GridCtl* ctl, double dt_host,
               cudaStream_t st) {
   unsigned* err = &ctl->err;
+  const dim3 rows((P.nx + 127) / 128, P.ny, P.nz);
   if (f32) {
     k_cond_prim<float><<<grid_of(c.n), kThreads, 0, st>>>((float*)q, c.n, nf, P, c.temp, ctl, err);
-    k_cond_update<float><<<grid_of(c.n), kThreads, 0, st>>>((float*)q, c.n, nf, P, c.temp, ctl, dt_host);
+    k_cond_update<float><<<rows, 128, 0, st>>>((float*)q, c.n, nf, P, c.temp, ctl, dt_host);
   } else {
     k_cond_prim<double><<<grid_of(c.n), kThreads, 0, st>>>((double*)q, c.n, nf, P, c.temp, ctl, err);
-    k_cond_update<double><<<grid_of(c.n), kThreads, 0, st>>>((double*)q, c.n, nf, P, c.temp, ctl, dt_host);
+    k_cond_update<double><<<rows, 128, 0, st>>>((double*)q, c.n, nf, P, c.temp, ctl, dt_host);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -30,6 +30,14 @@ __host__ __device__ inline double thermal_v(const HydroParams& P, double rho, do
   return rho / kappa;
 }
 
+// The same with T^2.5 = T^2 sqrt(T) (within a few ulp of pow; the fast
+// arithmetic forms use it, the strict form keeps pow).
+__host__ __device__ inline double thermal_v_fast(const HydroParams& P, double rho, double press) {
+  const double temp = press / rho * P.temp0;
+  const double kappa = P.kappa0 * (temp * temp * sqrt(temp));
+  return rho / kappa;
+}
+
 // thermalstep part 2: dt = min(c_cond dx^2 vmin / temp0, dt); EVORA_ERR_DT if <= 0.
 __host__ __device__ inline double thermal_dt(const HydroParams& P, double vmin, double dt, unsigned& err) {
   const double v = P.c_cond * (P.dx * P.dx) * vmin / P.temp0;

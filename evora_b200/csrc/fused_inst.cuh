@@ -102,7 +102,7 @@ __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, Gr
 #pragma unroll
       for (int f = 0; f < NF; ++f) qd[f] = (double)qv[f];
       q2w(qd, w, Gas<double>::make(P), P.dualenergy != 0, err);
-      const double v = thermal_v(P, w[0], w[4]);
+      const double v = kFast ? thermal_v_fast(P, w[0], w[4]) : thermal_v(P, w[0], w[4]);
       if (v < vmin) vmin = v;
     }
   }

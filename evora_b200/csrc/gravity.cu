@@ -31,6 +31,7 @@ namespace evora {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kRow = 128;   // threads along x of the row-mapped (3D) launches
 
 int grid_of(int64_t n) {
   int64_t b = (n + kThreads - 1) / kThreads;
@@ -60,13 +61,19 @@ __global__ void k_rho_partial(const T* __restrict__ q, int64_t n, int aos, doubl
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
+// one block of kThreads: strided partial sums, then a fixed tree
 __global__ void k_rho_mean(double* part, int nb, int64_t n, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += part[b];
-    part[nb] = s / (double)n;
+  __shared__ double red[kThreads];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += kThreads) s += part[b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = kThreads / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
   }
+  if (threadIdx.x == 0) part[nb] = red[0] / (double)n;
 }
 
 template <typename T>
@@ -83,19 +90,17 @@ __global__ void k_source(const T* __restrict__ q, int64_t n, int aos, const doub
 __global__ void k_green(cufftDoubleComplex* __restrict__ spec, int nxh, int ny, int nz, const double* __restrict__ sx,
                         const double* __restrict__ sy, const double* __restrict__ sz, double h2, int64_t n3,
                         const GridCtl* ctl) {
+  // 3D launch: x by threads, one (y, z) row per block row
   if (ctl_skip(ctl)) return;
-  const int64_t nh = (int64_t)nxh * ny * nz;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y, iz = blockIdx.z;
+  if (ix >= nxh) return;
   const double dn3 = (double)n3;
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nh; j += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(j % nxh);
-    const int64_t r = j / nxh;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
-    const double green = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : -h2 / (sx[ix] + sy[iy] + sz[iz]);
-    cufftDoubleComplex v = spec[j];
-    v.x = v.x / dn3 * green;
-    v.y = v.y / dn3 * green;
-    spec[j] = v;
-  }
+  const int64_t j = ((int64_t)iz * ny + iy) * nxh + ix;
+  const double green = (ix == 0 && iy == 0 && iz == 0) ? 0.0 : -h2 / (sx[ix] + sy[iy] + sz[iz]);
+  cufftDoubleComplex v = spec[j];
+  v.x = v.x / dn3 * green;
+  v.y = v.y / dn3 * green;
+  spec[j] = v;
 }
 
 // gravintegration + grav_force (gravitation.f90:170-243): periodic centred
@@ -107,13 +112,13 @@ __global__ void k_integrate(T* __restrict__ q, int64_t n, int nf, int aos, const
                             double dt_host) {
   // (the entropy field, when carried, is not touched: gravintegration
   // updates E and m only)
+  // 3D launch: x by threads, one (y, z) row per block row
   if (ctl_skip(ctl)) return;
   const double dt = ctl ? ctl->dt : dt_host;
   const int64_t nxy = (int64_t)nx * ny;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(i % nx);
-    const int64_t r = i / nx;
-    const int iy = (int)(r % ny), iz = (int)(r / ny);
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y, iz = blockIdx.z;
+  if (ix < nx) {
+    const int64_t i = ((int64_t)iz * ny + iy) * nx + ix;
     double f1 = 0.0, f2 = 0.0, f3 = 0.0;
     if (nx != 1) {
       const int xp = ix + 1 == nx ? 0 : ix + 1, xm = ix == 0 ? nx - 1 : ix - 1;
@@ -240,8 +245,9 @@ int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const 
     return EVORA_ERR_CUDA;
   }
   const int nxh = g.nx / 2 + 1;
-  k_green<<<grid_of(g.nh), kThreads, 0, st>>>(g.spec, nxh, g.ny, g.nz, g.green, g.green + nxh,
-                                              g.green + nxh + g.ny, g.h2, g.n, ctl);
+  const dim3 gh((nxh + kRow - 1) / kRow, g.ny, g.nz);
+  k_green<<<gh, kRow, 0, st>>>(g.spec, nxh, g.ny, g.nz, g.green, g.green + nxh, g.green + nxh + g.ny, g.h2, g.n,
+                               ctl);
   if (cufftExecZ2D(g.inv, g.spec, g.phi) != CUFFT_SUCCESS) {
     set_error_message("cufftExecZ2D failed");
     return EVORA_ERR_CUDA;
@@ -256,12 +262,13 @@ int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const 
 
 int grav_integrate(GravPlan& g, void* q, bool f32, int nf, int aos, const GridCtl* ctl, double dt_host) {
   cudaStream_t st = g.stream;
+  const dim3 rows((g.nx + kRow - 1) / kRow, g.ny, g.nz);
   if (f32) {
-    k_integrate<float><<<grid_of(g.n), kThreads, 0, st>>>((float*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv,
-                                                          g.dy2inv, g.dz2inv, ctl, dt_host);
+    k_integrate<float><<<rows, kRow, 0, st>>>((float*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv,
+                                              g.dz2inv, ctl, dt_host);
   } else {
-    k_integrate<double><<<grid_of(g.n), kThreads, 0, st>>>((double*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz,
-                                                           g.dx2inv, g.dy2inv, g.dz2inv, ctl, dt_host);
+    k_integrate<double><<<rows, kRow, 0, st>>>((double*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv,
+                                               g.dz2inv, ctl, dt_host);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
