@@ -9,10 +9,11 @@
 // Input: namelist group para (parameter.f90:26-105) and, for the shocktube,
 // ic_para (ic/shocktube.f90:39-47).  The reference compiles one ic/<name>.f90
 // into the binary (object/Makefile:57-58); here --ic chooses at run time.
-// Self-gravity (gravity = .true.) runs on the device after each hydro step
-// as in main.f90:158-165 (non-comoving).  Runs with comoving coordinates,
-// chemistry, conduction or the temperature / Jeans floors are refused: those
-// physics are not on the path this library implements.
+// Self-gravity (gravity = .true., non-comoving) and thermal conduction
+// (conduction = .true. with simplekappa = .true.) run on the device after
+// each hydro step as in main.f90:121, 158-175.  Runs with comoving
+// coordinates, chemistry or the temperature / Jeans floors are refused:
+// those physics are not on the path this library implements.
 //
 // Output, under the working directory, as the reference writes it:
 //   data/parameter           writeparameter (parameter.f90:267-337)

@@ -244,6 +244,9 @@ inline evora_params hydro_params(const RunParams& r) {
   p.boundtype = (int)r["boundtype"];
   p.secondorder = r.flag("secondorder");
   p.gravity = r.flag("gravity");
+  p.conduction = r.flag("conduction");
+  p.simplekappa = r.flag("simplekappa");
+  p.c_cond = r["c_cond"];
   p.dualenergy = r.flag("dualenergy");
   p.atomic = r.flag("atomic");
   p.g = r["g"];
@@ -263,7 +266,7 @@ inline evora_params hydro_params(const RunParams& r) {
 // The parts of a run outside the hydro path that these drivers do not have.
 inline std::string unsupported(const RunParams& r) {
   std::string s;
-  for (const char* k : {"supercomoving", "chemistry", "conduction", "tempfloor", "jeansfloor"})
+  for (const char* k : {"supercomoving", "chemistry", "tempfloor", "jeansfloor"})
     if (r.flag(k)) s += (s.empty() ? "" : ", ") + std::string(k);
   if (!r.flag("hydro")) s += (s.empty() ? "" : ", ") + std::string("hydro = .false.");
   return s;
