@@ -243,7 +243,9 @@ __device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn,
 }
 
 // The tile program of one CTA.  tid in [0, TX*TY); (bx, by, bz) its tile.
-template <typename T, int NF, int DIM, int TX, int TY, int ZC>
+// PIPE: the 3D march as a two-barrier software pipeline (faster for FP32
+// state; FP64 tiles, with fewer warps per SM, run the three-barrier march).
+template <typename T, int NF, int DIM, int TX, int TY, int ZC, bool PIPE = (sizeof(T) == 4)>
 __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, NF, TX, TY>& sm,
                                            int tid, int bx, int by, int bz) {
   constexpr int NT = TX * TY;
@@ -352,13 +354,180 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
   const int zfirst = DIM == 3 ? Z0 - 1 : 0;
   const int zlast = DIM == 3 ? Z0 + ze : 0;
   auto slot_of = [&](int z) { return (z - (Z0 - 2)) % 3; };
-  if (DIM == 3) {
+
+  if constexpr (DIM == 3 && PIPE) {
+    // Software-pipelined march, two barriers per plane.  Iteration c (an
+    // inner plane) runs
+    //   I1: A(c+2) and the x/y Riemann solves of plane c      | barrier
+    //   I2: D(c), B(c+1) and the z flux through c+1/2         | barrier
+    // with B(c) and the z flux through c-1/2 done before it.  A(c+2) refills
+    // the ring slot of plane c-1, last read by B(c) before the previous
+    // barrier; B(c+1) rewrites face states the solves of plane c consumed
+    // before the last one; C(c+1) rewrites fluxes D(c) read before it.
+    T wzp_c[5];      // upper z face of the current plane
+    T fz_cur[NF];    // z flux through c-1/2 (then c+1/2)
+    auto faces = [&](int cz, bool in, T* wzm, T* wzp) {
+      const int sp = slot_of(cz - 1), sc = slot_of(cz), sn = slot_of(cz + 1);
+      if (owned) {
+        T wv[5], face[3][2][5];
+        cell_faces<T, DIM, TX, TY>(sm, sp, sc, sn, oi + 2, oj + 2, P, dt2, wv, face);
+        if (in) {
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            sm.xf[0][f][oj][oi + 1] = face[0][0][f];
+            sm.xf[1][f][oj][oi + 1] = face[0][1][f];
+            sm.yf[0][f][oj + 1][oi] = face[1][0][f];
+            sm.yf[1][f][oj + 1][oi] = face[1][1][f];
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+          wzm[f] = face[2][0][f];
+          wzp[f] = face[2][1][f];
+        }
+      }
+      if (in) {
+        // ring cells: x ring at x = -1 and x = xe (rows 0..ye-1),
+        // y ring at y = -1 and y = ye (columns 0..xe-1)
+        const int nring = 2 * ye + 2 * xe;
+        for (int r = tid; r < nring; r += NT) {
+          int li, lj;
+          bool xring;
+          if (r < 2 * ye) {
+            xring = true;
+            lj = r >> 1;
+            li = (r & 1) ? xe : -1;
+          } else {
+            xring = false;
+            const int rr = r - 2 * ye;
+            li = rr >> 1;
+            lj = (rr & 1) ? ye : -1;
+          }
+          T wv[5], face[3][2][5];
+          cell_faces<T, DIM, TX, TY>(sm, sp, sc, sn, li + 2, lj + 2, P, dt2, wv, face);
+          if (xring) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+              sm.xf[0][f][lj][li + 1] = face[0][0][f];
+              sm.xf[1][f][lj][li + 1] = face[0][1][f];
+            }
+          } else {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+              sm.yf[0][f][lj + 1][li] = face[1][0][f];
+              sm.yf[1][f][lj + 1][li] = face[1][1][f];
+            }
+          }
+        }
+      }
+    };
+    auto solves_xy = [&]() {
+      // counted from the last thread: the threads that load one halo cell
+      // fewer in A take the extra solves of the same interval
+      const int nxi = (xe + 1) * ye, nyi = xe * (ye + 1);
+      for (int it = NT - 1 - tid; it < nxi + nyi; it += NT) {
+        T wl[5], wr[5], fv[NF];
+        if (it < nxi) {
+          const int i = it % (xe + 1), j = it / (xe + 1);
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            wl[f] = sm.xf[1][f][j][i];
+            wr[f] = sm.xf[0][f][j][i + 1];
+          }
+          riemann_k<T, NF, 1>(wl, wr, fv, P.solver, c, err);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) sm.fx[f][j][i] = fv[f];
+        } else {
+          const int r = it - nxi;
+          const int i = r % xe, j = r / xe;
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            wl[f] = sm.yf[1][f][j][i];
+            wr[f] = sm.yf[0][f][j + 1][i];
+          }
+          riemann_k<T, NF, 2>(wl, wr, fv, P.solver, c, err);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) sm.fy[f][j][i] = fv[f];
+        }
+      }
+    };
+    auto zflux = [&](const T* lo_plane_upper, const T* hi_plane_lower, T* fz) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) fz[f] = (T)0;
+      if (owned) riemann_k<T, NF, 3>(lo_plane_upper, hi_plane_lower, fz, P.solver, c, err);
+    };
+    // plane z (held in qacc after its x and y terms) gets its z term
+    auto write_plane = [&](int z, const T* fz_lo, const T* fz_hi) {
+      if (!owned) return;
+      const int64_t idx = ((int64_t)z * ny + (Y0 + oj)) * nx + (X0 + oi);
+      T qo[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        qo[f] = qacc[f] + dtdz * (fz_lo[f] - fz_hi[f]);
+        A.qout[f * n + idx] = qo[f];
+      }
+      if (A.cfl_next) track(qo);
+    };
+    // plane z: q + the x and y flux differences, into qacc
+    auto update_xy = [&](int z) {
+      if (!owned) return;
+      const int64_t idx = ((int64_t)z * ny + (Y0 + oj)) * nx + (X0 + oi);
+      T qv[6], wdummy[5];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
+      if (de) {
+        unsigned e2 = 0;
+        prim(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
+      }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdx * (sm.fx[f][oj][oi] - sm.fx[f][oj][oi + 1]);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) qacc[f] = qv[f] + dtdy * (sm.fy[f][oj][oi] - sm.fy[f][oj + 1][oi]);
+    };
+
+    // prologue: planes Z0-2 .. Z0+1, B of the plane below the tile and of
+    // the first plane, the z flux through Z0 - 1/2
+    T wzm_n[5], wzp_n[5];
     load_plane(Z0 - 2, slot_of(Z0 - 2));
     load_plane(Z0 - 1, slot_of(Z0 - 1));
-  }
-
+    load_plane(Z0, slot_of(Z0));
+    EV_SYNC();
+    faces(Z0 - 1, false, wzm_n, wzp_c);
+    EV_SYNC();
+    load_plane(Z0 + 1, slot_of(Z0 + 1));
+    EV_SYNC();
+    faces(Z0, true, wzm_n, wzp_n);
+    zflux(wzp_c, wzm_n, fz_cur);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) wzp_c[f] = wzp_n[f];
+    EV_SYNC();
+    for (int cz = Z0; cz < Z0 + ze; ++cz) {
+      // ---- I1
+      load_plane(cz + 2, slot_of(cz + 2));
+      solves_xy();
+      EV_SYNC();
+      // ---- I2
+      if (cz > Z0) write_plane(cz - 1, fz_prev, fz_cur);
+      update_xy(cz);
+      faces(cz + 1, cz + 1 < Z0 + ze, wzm_n, wzp_n);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) fz_prev[f] = fz_cur[f];
+      zflux(wzp_c, wzm_n, fz_cur);
+#pragma unroll
+      for (int f = 0; f < 5; ++f) wzp_c[f] = wzp_n[f];
+      EV_SYNC();
+    }
+    write_plane(Z0 + ze - 1, fz_prev, fz_cur);
+    (void)zfirst;
+    (void)zlast;
+  } else
   for (int cz = zfirst; cz <= zlast; ++cz) {
     const bool inner = cz >= Z0 && cz < Z0 + ze;  // plane cz is updated by this tile
+    if (DIM == 3 && cz == zfirst) {
+      // the two planes below the march
+      load_plane(Z0 - 2, slot_of(Z0 - 2));
+      load_plane(Z0 - 1, slot_of(Z0 - 1));
+    }
     // ---- A
     if (DIM == 3) load_plane(cz + 1, slot_of(cz + 1));
     else load_plane(0, 1);

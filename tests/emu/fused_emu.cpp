@@ -17,6 +17,11 @@ thread_local std::barrier<>* evora_emu::tl_barrier = nullptr;
 using namespace evora;
 using namespace evora::emu;
 
+// 1: the two-barrier pipelined 3D march (the FP32 kernels' schedule),
+// 0: the three-barrier march (the FP64 kernels' schedule)
+static int g_pipe = 0;
+extern "C" void emu_set_pipeline(int on) { g_pipe = on; }
+
 template <int NF, int DIM, int TX, int TY, int ZC>
 static void run_tiles(const FusedArgs<double>& A) {
   constexpr int NT = TX * TY;
@@ -33,7 +38,8 @@ static void run_tiles(const FusedArgs<double>& A) {
         for (int t = 0; t < NT; ++t)
           th.emplace_back([&, t] {
             evora_emu::tl_barrier = &bar;
-            fused_tile<double, NF, DIM, TX, TY, ZC>(A, *sm, t, bx, by, bz);
+            if (g_pipe) fused_tile<double, NF, DIM, TX, TY, ZC, true>(A, *sm, t, bx, by, bz);
+            else fused_tile<double, NF, DIM, TX, TY, ZC, false>(A, *sm, t, bx, by, bz);
           });
         for (auto& x : th) x.join();
       }

@@ -24,13 +24,15 @@ class HP(ctypes.Structure):
                [(n, ctypes.c_double) for n in "c_cond kappa0 temp0".split()]
 
 
-@pytest.fixture(scope="module")
-def emu():
+@pytest.fixture(scope="module", params=[0, 1], ids=["march", "pipelined"])
+def emu(request):
     subprocess.run(["make", "-s", "-C", EMU], check=True)
     L = ctypes.CDLL(os.path.join(EMU, "_build", "libfused_emu.so"))
     dp = ctypes.POINTER(ctypes.c_double)
     L.emu_fused_update.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int]
     L.emu_fused_update_cfl.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, dp]
+    L.emu_set_pipeline.argtypes = [ctypes.c_int]
+    L.emu_set_pipeline(request.param)   # the FP64 (0) and FP32 (1) schedules of the 3D march
     return L
 
 
