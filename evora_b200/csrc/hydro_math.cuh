@@ -343,10 +343,15 @@ __device__ __forceinline__ void hllc_fast(const T* wl, const T* wr, T* f, const 
   const T facl = wl[0] * (sl - ul);
   const T facr = wr[0] * (sr - ur);
   const T sm = (wr[4] - wl[4] + facl * ul - facr * ur) * rcp_fast(facl - facr);
-  // the side whose state (or star state) gives the flux
-  const bool left = (T)0 < sl || (!((T)0 > sr) && sl < (T)0 && (T)0 < sm);
-  const bool star = !((T)0 < sl) && !((T)0 > sr);
-  if (star && !(sl < (T)0 && (T)0 < sm) && !(sm <= (T)0 && (T)0 < sr)) err |= EVORA_ERR_HLLC;
+  // the side whose state (or star state) gives the flux.  The reference's
+  // branches (riemann.f90:130-150) leave sl == 0 with sm > 0 and sr == 0 with
+  // sm <= 0 to its error stop; there the star flux equals the plain left
+  // (right) flux, which the fast form takes.  Only NaN speeds remain an error.
+  const bool pure_left = (T)0 <= sl;
+  const bool pure_right = !pure_left && (T)0 >= sr;
+  const bool star = !pure_left && !pure_right;
+  const bool left = pure_left || (star && (T)0 < sm);
+  if (!(sl == sl && sr == sr && sm == sm)) err |= EVORA_ERR_HLLC;
   const T* w = left ? wl : wr;
   const T ri = left ? ril : rir;
   const T sk = left ? sl : sr;
