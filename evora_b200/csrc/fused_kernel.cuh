@@ -124,6 +124,11 @@ __device__ __forceinline__ void prim(T* q, T* w, const Gas<T>& c, const HydroPar
 #define EVORA_FAST 0
 #endif
 constexpr bool kFast = EVORA_FAST != 0;
+#if defined(EVORA_HOST_EMU)
+constexpr bool kHostEmu = true;    // the host emulation runs both march schedules in FP64
+#else
+constexpr bool kHostEmu = false;
+#endif
 
 template <typename T>
 __device__ __forceinline__ T slope_k(T wl, T w, T wr, int limiter) {
@@ -167,7 +172,32 @@ struct FusedSmem {
   // maxima of |u_d| + a of the written cells: per thread for FP32 state
   // (whose register budget is tight), per warp otherwise
   T cfl[3][sizeof(T) == 4 ? TX * TY : 32];
+  // FP32 pipelined march: the owned cells' conserved state of the plane
+  // being updated, copied asynchronously one interval ahead of its use
+  T dq[NF][(sizeof(T) == 4 || kHostEmu) ? TX * TY : 1];
 };
+
+// Asynchronous 4-byte global -> shared copy (cp.async), its commit and wait.
+template <typename T>
+__device__ __forceinline__ void copy_async(T* dst, const T* src) {
+#if defined(__CUDACC__) && !defined(EVORA_HOST_EMU)
+  static_assert(sizeof(T) == 4, "4-byte copies");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+#else
+  *dst = *src;
+#endif
+}
+__device__ __forceinline__ void copy_async_commit() {
+#if defined(__CUDACC__) && !defined(EVORA_HOST_EMU)
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void copy_async_wait() {
+#if defined(__CUDACC__) && !defined(EVORA_HOST_EMU)
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
 
 // hydrostep per cell (timestep.f90:40-43): the signal speeds |u_d| + a of
 // a conserved state, in the working precision.  FP64: q2w and a = sqrt(g p
@@ -468,13 +498,23 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
       }
       if (A.cfl_next) track(qo);
     };
+    // the owned cell's conserved state of plane z into sm.dq, asynchronously
+    // (waited for by the same thread in update_xy, one interval later)
+    auto prefetch_own = [&](int z) {
+      if (!owned) return;
+      const int64_t idx = ((int64_t)z * ny + (Y0 + oj)) * nx + (X0 + oi);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) copy_async(&sm.dq[f][tid], A.qin + f * n + idx);
+      copy_async_commit();
+    };
     // plane z: q + the x and y flux differences, into qacc
     auto update_xy = [&](int z) {
       if (!owned) return;
-      const int64_t idx = ((int64_t)z * ny + (Y0 + oj)) * nx + (X0 + oi);
+      (void)z;
+      copy_async_wait();
       T qv[6], wdummy[5];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
+      for (int f = 0; f < NF; ++f) qv[f] = sm.dq[f][tid];
       if (de) {
         unsigned e2 = 0;
         prim(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
@@ -503,6 +543,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
     EV_SYNC();
     for (int cz = Z0; cz < Z0 + ze; ++cz) {
       // ---- I1
+      prefetch_own(cz);
       load_plane(cz + 2, slot_of(cz + 2));
       solves_xy();
       EV_SYNC();
