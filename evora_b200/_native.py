@@ -33,6 +33,8 @@ class EvoraParams(ctypes.Structure):
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
         ("tstart", c_double), ("tend", c_double),
         ("conduction", c_int32), ("simplekappa", c_int32), ("c_cond", c_double),
+        ("tempfloor", c_int32), ("jeansfloor", c_int32), ("temp_fl", c_double), ("c_jeans", c_double),
+        ("fb", c_double),
     ]
 
     def as_dict(self):
@@ -186,6 +188,7 @@ def _declare_batch(L):
         "evora_gravpotential": ([c_void_p, c_void_p], c_int32),
         "evora_gravintegration": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_thermalstep": ([c_void_p, c_void_p, _dp], c_int32),
+        "evora_chem": ([c_void_p], c_int32),
         "evora_thermalconduction": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),

@@ -2,7 +2,8 @@
 
 Every translation unit is compiled for sm_100a only.  Per-file flags:
   dropin_strict.cu, fused_f64_strict.cu   --fmad=false (bit-exact FP64 mode)
-  fused.cu, gravity.cu, conduction.cu     --fmad=false (conversions, snapshots, gravity, conduction)
+  fused.cu, gravity.cu, conduction.cu,    --fmad=false (conversions, snapshots, gravity, conduction,
+  chem.cu                                 floors)
   fused_f32.cu                            --use_fast_math (FP32 form)
 Run as `python -m evora_b200.build` (add -v for the ptxas register report).
 """
@@ -30,11 +31,12 @@ PER_FILE = {
     "fused.cu": ["--fmad=false"],
     "gravity.cu": ["--fmad=false"],
     "conduction.cu": ["--fmad=false"],
+    "chem.cu": ["--fmad=false"],
     "fused_f32.cu": ["--use_fast_math"],
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
            "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu",
-           "io.cu", "gravity.cu", "conduction.cu"]
+           "io.cu", "gravity.cu", "conduction.cu", "chem.cu"]
 
 
 def _deps():

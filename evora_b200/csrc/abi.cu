@@ -41,9 +41,22 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->simplekappa = p->simplekappa != 0;
   P->c_cond = p->c_cond;
   evora_units u;   // compunits (units.f90:26-73), non-comoving
-  evora_units_noncomoving(p->tstart, dd.g, 1.0, &u);
+  evora_units_noncomoving(p->tstart, dd.g, p->fb, &u);
   P->kappa0 = u.kappa0;
   P->temp0 = u.temp0;
+  // pressure floors of chem (chemistry.f90:100-119): temp2press with
+  // temp0inv = 1 / temp0, and jeansfloor0 = (dx / jeans0 / c_jeans)^2 when
+  // the Jeans floor is on (units.f90:66-71)
+  P->tempfloor = p->tempfloor != 0;
+  P->jeansfloor = p->jeansfloor != 0;
+  P->temp_fl = p->temp_fl;
+  P->temp0inv = 1.0 / u.temp0;
+  if (p->jeansfloor) {
+    const double r = dd.dx / u.jeans0 / p->c_jeans;
+    P->jeansfloor0 = r * r;
+  } else {
+    P->jeansfloor0 = 0.0;
+  }
   return true;
 }
 
@@ -87,6 +100,11 @@ void evora_params_default(evora_params* p) {
   p->conduction = 0;
   p->simplekappa = 0;
   p->c_cond = (double)0.1f;
+  p->tempfloor = 0;
+  p->jeansfloor = 0;
+  p->temp_fl = 0.0;
+  p->c_jeans = 0.0;
+  p->fb = 1.0;
 }
 
 int evora_compparameter(const evora_params* p, evora_derived* d) {

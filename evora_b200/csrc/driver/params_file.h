@@ -247,6 +247,11 @@ inline evora_params hydro_params(const RunParams& r) {
   p.conduction = r.flag("conduction");
   p.simplekappa = r.flag("simplekappa");
   p.c_cond = r["c_cond"];
+  p.tempfloor = r.flag("tempfloor");
+  p.jeansfloor = r.flag("jeansfloor");
+  p.temp_fl = r["temp_fl"];
+  p.c_jeans = r["c_jeans"];
+  p.fb = r["fb"];
   p.dualenergy = r.flag("dualenergy");
   p.atomic = r.flag("atomic");
   p.g = r["g"];
@@ -266,7 +271,7 @@ inline evora_params hydro_params(const RunParams& r) {
 // The parts of a run outside the hydro path that these drivers do not have.
 inline std::string unsupported(const RunParams& r) {
   std::string s;
-  for (const char* k : {"supercomoving", "chemistry", "tempfloor", "jeansfloor"})
+  for (const char* k : {"supercomoving", "chemistry"})
     if (r.flag(k)) s += (s.empty() ? "" : ", ") + std::string(k);
   if (!r.flag("hydro")) s += (s.empty() ? "" : ", ") + std::string("hydro = .false.");
   return s;

@@ -24,6 +24,7 @@
 #include "fused.h"
 #include "gravity.h"
 #include "conduction.h"
+#include "chem.h"
 
 using namespace evora;
 
@@ -64,6 +65,8 @@ struct evora_grid {
   // thermal conduction after each step (params.conduction)
   bool conduction = false;
   CondPlan cond{};
+  // pressure floors after each step (params.tempfloor / jeansfloor)
+  bool floors = false;
   bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
 };
 
@@ -192,6 +195,12 @@ int enqueue_fused_step(evora_grid* g) {
     if (rc) return rc;
     g->launches += 5;   // own kernels; cuFFT adds its own
   }
+  if (g->floors) {
+    // chem(q) of the plain build: pressure floors (main.f90:167)
+    int rc = chem_floors(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->ctl, st);
+    if (rc) return rc;
+    g->launches += 1;
+  }
   if (g->conduction) {
     // primitive + bound + thermalconduction on the updated state (main.f90:169-175)
     int rc = cond_step(g->cond, g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, g->ctl, 0.0, st);
@@ -304,6 +313,14 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
       free_grid(g);
       return rc;
     }
+  }
+  if (p->tempfloor || p->jeansfloor) {
+    if (reference_backend(g)) {
+      free_grid(g);
+      return EVORA_ERR_ARG;   // the floors run on the resident SoA state
+    }
+    g->floors = true;
+    g->plan.cfl_fused = 0;     // the state changes after the update
   }
   if (p->conduction) {
     if (reference_backend(g)) {
@@ -481,7 +498,8 @@ int graph_steps(evora_grid* g, int nsteps) {
     } else {
       g->cur = start ^ (nsteps & 1);
       const bool fused = g->plan.cfl_fused != 0;
-      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0) + (g->conduction ? 2 : 0)) +
+      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0) + (g->conduction ? 2 : 0) +
+                                       (g->floors ? 1 : 0)) +
                      (fused && !fresh ? 1 : 0);
       g->cfl_fresh = fused;
     }

@@ -56,6 +56,9 @@ struct HydroParams {
   // thermal conduction (conduction.f90, thermalstep timestep.f90:72-104)
   int conduction, simplekappa;
   double c_cond, kappa0, temp0;
+  // pressure floors (chem, chemistry.f90:92-121, plain build)
+  int tempfloor, jeansfloor;
+  double temp_fl, temp0inv, jeansfloor0;
 };
 
 template <typename T>

@@ -139,6 +139,11 @@ class DropIn:
         imaginary part is written as 0."""
         check(lib().evora_gravpotential(_ptr(q, self.shape["q"], False), self._phi_ptr(phi)), "gravpotential")
 
+    def chem(self, q):
+        """chem(q), chemistry.f90:72-121, plain build: pressure() and the
+        temperature / Jeans pressure floors."""
+        check(lib().evora_chem(_ptr(q, self.shape["q"])), "chem")
+
     def thermalstep(self, q, w, dt: float = 1e99) -> float:
         """thermalstep(q,w), timestep.f90:72-104: min(dt, conduction limit);
         q is resynchronised in place with dual energy, as in the reference."""

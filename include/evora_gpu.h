@@ -87,6 +87,12 @@ typedef struct evora_params {
                            branch reads unset variables in the reference's
                            plain build and is refused (EVORA_ERR_ARG)       */
   double c_cond;        /* conduction time-step factor                      */
+  int32_t tempfloor;    /* Fortran logical: pressure floor at temp_fl after
+                           each step (chem, chemistry.f90:92-121)           */
+  int32_t jeansfloor;   /* Fortran logical: pressure floor jeansfloor0 rho^2 */
+  double temp_fl;       /* temperature of the floor                         */
+  double c_jeans;       /* Jeans floor factor (units.f90:66-71)             */
+  double fb;            /* baryon fraction (units: jeans0 = sqrt(pi g fb))  */
 } evora_params;
 
 /* The derived constants of compparameter (parameter.f90:164-265) that the
@@ -172,6 +178,13 @@ int evora_thermalstep(double* q, const double* w, double* dt);
  * and z conduction sweeps over dt from the primitives w (ghosts filled by
  * bound), updating E and S of q in place. */
 int evora_thermalconduction(double* q, const double* w, double dt);
+
+/* chem(q), chemistry.f90:72-121, in the plain build (no species):
+ * pressure() with its dual-energy write-back, then the temperature floor
+ * (tempfloor: press = max(press, temp_fl rho / temp0)) and the Jeans floor
+ * (jeansfloor: press = max(press, jeansfloor0 rho^2)) with E and S
+ * corrected by the pressure change. */
+int evora_chem(double* q);
 
 /* gravpotential(q,phi), gravitation.f90:26-53, non-comoving branch: the
  * potential of the density of q (FFT Poisson solve with the reference's

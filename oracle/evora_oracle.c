@@ -51,6 +51,8 @@ static struct {
   int onedimension, twodimension;
   int conduction, simplekappa;
   double c_cond, kappa0, temp0;
+  int tempfloor, jeansfloor;
+  double temp_fl, temp0inv, jeansfloor0;
 } G;
 
 static int orc_err = 0;
@@ -112,7 +114,11 @@ int orc_compparameter(const evora_params* p) {
     G.temp0 = pow(l0, 2.0) / pow(cosmo, 2.0) / pow(t0, 2.0) * m0 / kb;
     const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
     G.kappa0 = pow(cosmo, 5.0) * pow(t0, 3.0) / d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
+    G.temp0inv = 1.0 / G.temp0;
   }
+  G.tempfloor = p->tempfloor != 0;
+  G.jeansfloor = p->jeansfloor != 0;
+  G.temp_fl = p->temp_fl;
   G.onedimension = (p->ny == 1 && p->nz == 1);          /* parameter.f90:173-177 */
   G.twodimension = (p->nz == 1);                        /* parameter.f90:178-182 */
   double xmin = p->xmin, xmax = p->xmax, ymin = p->ymin, ymax = p->ymax;
@@ -138,6 +144,13 @@ int orc_compparameter(const evora_params* p) {
   G.g1inv = 1.0 / G.g1;
   G.gg1 = G.g / G.g1;
   G.de_thresh1 = G.dualenergy ? 1.0 - p->de_thresh : 1.0; /* parameter.f90:244-248 */
+  {
+    /* compunits after compparameter (main.f90:52-62): jeans0 = sqrt(pi g fb)
+     * with module global's single-precision pi and the gas constant g, and
+     * the Jeans floor (dx / jeans0 / c_jeans)^2 (units.f90:66-71) */
+    const double jeans0 = sqrt((double)3.1415927f * G.g * p->fb);
+    G.jeansfloor0 = p->jeansfloor ? (G.dx / jeans0 / p->c_jeans) * (G.dx / jeans0 / p->c_jeans) : 0.0;
+  }
   return 0;
 }
 
@@ -727,6 +740,30 @@ void orc_thermalconduction(double* q, const double* w, double dt) {
   }
 }
 
+/* chem(q), chemistry.f90:72-121, plain build (no species): pressure()
+ * with its dual-energy write-back, the temperature and Jeans pressure
+ * floors, E and S corrected by the pressure change. */
+void orc_chem(double* q) {
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double* c = &q[iq(ix, iy, iz)];
+        double press = orc_pressure(c);
+        double oldpress = press;
+        if (G.tempfloor) {
+          double pfloor = G.temp_fl * c[0] * G.temp0inv;   /* temp2press, comp.f90:104-119 */
+          press = fmax2(press, pfloor);
+        }
+        if (G.jeansfloor) {
+          double pfloor = G.jeansfloor0 * c[0] * c[0];
+          press = fmax2(press, pfloor);
+        }
+        double dpress = press - oldpress;
+        c[4] = c[4] + dpress * G.g1inv;
+        c[5] = c[5] + dpress / pow(c[0], G.g1);
+      }
+}
+
 /* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch. */
 void orc_updatetime(int* go, double* t, double* dt) {
   if (G.tend - *t <= *dt) {
@@ -766,6 +803,7 @@ int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, in
     if (orc_err) break;
     if (G.secondorder) orc_compevo(w, evo, s, dt);
     orc_sweep(w, q, evo, s, dt);
+    if (G.tempfloor || G.jeansfloor) orc_chem(q);           /* main.f90:167 */
     if (G.conduction) {                                     /* main.f90:169-175 */
       orc_primitive(w, q);
       orc_bound(w);

@@ -47,6 +47,8 @@ class OracleParams(ctypes.Structure):
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
         ("tstart", c_double), ("tend", c_double),
         ("conduction", ctypes.c_int32), ("simplekappa", ctypes.c_int32), ("c_cond", c_double),
+        ("tempfloor", ctypes.c_int32), ("jeansfloor", ctypes.c_int32), ("temp_fl", c_double), ("c_jeans", c_double),
+        ("fb", c_double),
     ]
 
 
@@ -90,6 +92,7 @@ def lib():
             L.orc_thermalstep.argtypes = [_dp, _dp, c_double]
             L.orc_thermalstep.restype = c_double
             L.orc_thermalconduction.argtypes = [_dp, _dp, c_double]
+            L.orc_chem.argtypes = [_dp]
             _lib = L
     return _lib
 
@@ -113,6 +116,7 @@ def make_params(**kw) -> OracleParams:
     p.xmax = p.ymax = p.zmax = 1.0
     p.tstart, p.tend = 0.0, 1.0
     p.conduction, p.simplekappa, p.c_cond = 0, 0, float(np.float32(0.1))
+    p.tempfloor, p.jeansfloor, p.temp_fl, p.c_jeans, p.fb = 0, 0, 0.0, 0.0, 1.0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -197,6 +201,10 @@ class Oracle:
         """thermalstep(q,w), timestep.f90:72-104 (q resynchronised in place
         with dual energy, as the reference's pressure() call does)."""
         return float(self.L.orc_thermalstep(_ptr(q), _ptr(w), float(dt_in)))
+
+    def chem(self, q):
+        """chem(q), chemistry.f90:72-121, plain build: the pressure floors."""
+        self.L.orc_chem(_ptr(q))
 
     def thermalconduction(self, q, w, dt):
         """thermalconduction(q,w), conduction.f90:26-122."""

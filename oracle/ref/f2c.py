@@ -5,8 +5,8 @@ TEST INFRASTRUCTURE ONLY.  No Fortran compiler exists on this image, so the
 reference cannot be built as is.  This script reads the reference's own
 sources (module global, compparameter, decomposition, q2w, pressure,
 coordinates, w2n, press2temp, muscl.f90, riemann.f90, boundary.f90,
-hydrostep, updatetime, thermalstep, conduction.f90, compunits and the
-shocktube / Kelvin-Helmholtz ICs) and translates the Fortran 90 subset
+hydrostep, updatetime, thermalstep, conduction.f90, compunits, temp2press,
+chem and the shocktube / Kelvin-Helmholtz ICs) and translates the Fortran 90 subset
 they use into C, statement by statement, keeping Fortran semantics:
 
   * default-real literals (0.5, 1e6, 3.1415927) are C floats, d-exponent
@@ -38,20 +38,21 @@ UNITS = [
     ("source/global.f90", None, {}),
     ("source/parameter.f90", ["compparameter"], {}),
     ("source/parallel.f90", ["decomposition"], {}),
-    ("source/comp.f90", ["q2w", "pressure", "coordinates", "w2n", "press2temp"], {}),
+    ("source/comp.f90", ["q2w", "pressure", "coordinates", "w2n", "press2temp", "temp2press"], {}),
     ("source/muscl.f90", None, {}),
     ("source/riemann.f90", None, {}),
     ("source/boundary.f90", None, {}),
     ("source/timestep.f90", ["hydrostep", "updatetime", "thermalstep"], {}),
     ("source/conduction.f90", None, {}),
     ("source/units.f90", ["compunits"], {}),
+    ("source/chemistry.f90", ["chem"], {}),
     ("ic/shocktube.f90", None, {"ic": "ic_shocktube"}),
     ("ic/kevinhelmholtz.f90", None, {"ic": "ic_kevinhelmholtz"}),
 ]
 
 # Routines called by the translated code but not translated: the harness
 # provides them (error stop, MPI broadcast no-ops, comoving-time iteration).
-EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "timestepiteration"}
+EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "timestepiteration", "cie", "ncie"}
 
 
 class F2CError(Exception):

@@ -26,6 +26,9 @@ void ref_stop(void) {
 void ref_cleanstop(void) { ref_stop(); }
 void ref_bcastdouble(double* x) { (void)x; }
 void ref_timestepiteration(double* z) { (void)z; ref_stop(); }
+/* the species solvers of chem (not reached without chemistry) */
+void ref_cie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
+void ref_ncie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
 
 /* &ic_para of ic/shocktube.f90:39 */
 static double nml_dl = 1.0, nml_ul = 0.0, nml_pl = 1.0, nml_dr = 0.125, nml_ur = 0.0, nml_pr = 0.1,
@@ -65,6 +68,8 @@ int ref_setup_c(const evora_params* p) {
   G_fb = 1.0f; G_box = 1.0f; G_zstart = 99.0f; G_zend = 0.0f;
   G_chemistry = 0; G_noncie = 0; G_cooling = 0; G_background = 0;
   G_conduction = p->conduction; G_simplekappa = p->simplekappa; G_c_cond = p->c_cond;
+  G_tempfloor = p->tempfloor; G_temp_fl = p->temp_fl; G_jeansfloor = p->jeansfloor; G_c_jeans = p->c_jeans;
+  G_fb = p->fb;
   G_dualenergy = p->dualenergy; G_de_thresh = p->de_thresh;
   G_mpisize = 1; G_mpirank = 0; G_master = 1; G_parallel = 0;
   G_local_x_start = 0; G_local_nx = p->nz;
@@ -112,6 +117,7 @@ int ref_sweep_c(double* w, double* q, double* evo, double* s, double dt) {
   return 0;
 }
 
+int ref_chem_c(double* q) { GUARD(ref_chem(q)); return 0; }
 int ref_thermalstep_c(double* q, double* w, double* dt) {
   G_dt = *dt;
   GUARD(ref_thermalstep(q, w));
@@ -149,6 +155,7 @@ int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* 
     ref_updatetime(&go, &dump, &k4);
     if (G_secondorder) ref_compevo(w, evo, s);
     if (G_hydro) ref_sweep(w, q, evo, s);
+    if (G_chemistry || G_tempfloor || G_jeansfloor) ref_chem(q);
     if (G_conduction) {
       ref_primitive(w, q);
       ref_bound(w);

@@ -49,6 +49,7 @@ def lib():
         L.ref_ic_kh_c.argtypes = [_dp]
         L.ref_riemann_c.argtypes = [_dp, _dp, _dp, ctypes.c_int]
         L.ref_thermalstep_c.argtypes = [_dp, _dp, _dp]
+        L.ref_chem_c.argtypes = [_dp]
         L.ref_thermalconduction_c.argtypes = [_dp, _dp, ctypes.c_double]
         _lib = L
     return _lib
@@ -119,6 +120,10 @@ class RefOracle:
         d = ctypes.c_double(dt_in)
         st = self.L.ref_thermalstep_c(_p(q), _p(w), ctypes.byref(d))
         return d.value, st
+
+    def chem(self, q):
+        """chem(q) (chemistry.f90:72-121), plain build: the pressure floors."""
+        return self.L.ref_chem_c(_p(q))
 
     def thermalconduction(self, q, w, dt):
         """thermalconduction(q,w) (conduction.f90:26-122) over dt."""

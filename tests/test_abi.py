@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(ev.EvoraParams) == 10 * 4 + 11 * 8 + 2 * 4 + 8
+    assert ctypes.sizeof(ev.EvoraParams) == 10 * 4 + 11 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8
     assert ctypes.sizeof(ev.EvoraDerived) == 16 * 8 + 2 * 4
 
 

@@ -21,7 +21,9 @@ class HP(ctypes.Structure):
                 "nx ny nz solver limiter boundtype secondorder dualenergy onedimension twodimension".split()] + \
                [(n, ctypes.c_double) for n in "g g1 g1inv gg1 cfl de_thresh1 dx dy dz dxinv dyinv dzinv".split()] + \
                [("conduction", ctypes.c_int), ("simplekappa", ctypes.c_int)] + \
-               [(n, ctypes.c_double) for n in "c_cond kappa0 temp0".split()]
+               [(n, ctypes.c_double) for n in "c_cond kappa0 temp0".split()] + \
+               [("tempfloor", ctypes.c_int), ("jeansfloor", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in "temp_fl temp0inv jeansfloor0".split()]
 
 
 @pytest.fixture(scope="module", params=[0, 1], ids=["march", "pipelined"])
