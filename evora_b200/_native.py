@@ -18,6 +18,7 @@ c_int64 = ctypes.c_int64
 c_double = ctypes.c_double
 c_void_p = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
+NDUMP = 100   # EVORA_NDUMP (global.f90:137)
 
 
 class EvoraParams(ctypes.Structure):
@@ -35,7 +36,19 @@ class EvoraParams(ctypes.Structure):
         ("conduction", c_int32), ("simplekappa", c_int32), ("c_cond", c_double),
         ("tempfloor", c_int32), ("jeansfloor", c_int32), ("temp_fl", c_double), ("c_jeans", c_double),
         ("fb", c_double),
+        ("supercomoving", c_int32), ("c_cosmo", c_double), ("omega0", c_double), ("lambda0", c_double),
+        ("hubble0", c_double), ("box", c_double), ("zstart", c_double), ("zend", c_double),
+        ("dump_redshift", c_double * NDUMP),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EvoraTime(ctypes.Structure):
+    """evora_time: the time scalars of module global (global.f90:86)."""
+
+    _fields_ = [(n, c_double) for n in ("t", "dt", "cosmo", "oldcosmo", "cosmodot", "expand", "redshift")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -66,6 +79,7 @@ class EvoraError(RuntimeError):
         512: "device allocation failed",
         1024: "timeout",
         2048: "file i/o",
+        4096: "timestepiteration does not converge (timestep.f90:220-223)",
     }
 
     def __init__(self, status: int, where: str = ""):
@@ -87,6 +101,7 @@ _lib = None
 def _declare(L):
     P = ctypes.POINTER(EvoraParams)
     D = ctypes.POINTER(EvoraDerived)
+    T = ctypes.POINTER(EvoraTime)
     G = c_void_p
     sig = {
         "evora_version": ([], ctypes.c_char_p),
@@ -116,6 +131,13 @@ def _declare(L):
         "evora_grid_set_tile": ([G, c_int32], c_int32),
         "evora_grid_set_timing": ([G, c_int32], c_int32),
         "evora_grid_timing": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], c_int32),
+        "evora_grid_cosmo": ([G, T, ctypes.POINTER(c_int32)], c_int32),
+        "evora_cosmostart": ([T], c_int32),
+        "evora_cosmostep": ([T], c_int32),
+        "evora_compcosmo": ([T], c_int32),
+        "evora_updatetime_cosmo": ([ctypes.POINTER(c_int32)] * 3 + [T], c_int32),
+        "evora_settime": ([T], c_int32),
+        "evora_expansion": ([c_void_p], c_int32),
     }
     optional = set()
     for name, (args, res) in sig.items():
@@ -153,6 +175,7 @@ def _declare_io(L):
         "evora_read_dump_header": ([s, i32p], c_int32),
         "evora_read_dump": ([s, i32p, c_void_p, c_int64], c_int32),
         "evora_units_noncomoving": ([c_double, c_double, c_double, U], None),
+        "evora_compunits": ([P, ctypes.POINTER(EvoraTime), U], c_int32),
         "evora_write_units": ([s, U], c_int32),
         "evora_read_units": ([s, U], c_int32),
         "evora_snapshot": ([P, c_void_p, U, c_int32, c_int32, s], c_int32),

@@ -3,7 +3,7 @@
 Every translation unit is compiled for sm_100a only.  Per-file flags:
   dropin_strict.cu, fused_f64_strict.cu   --fmad=false (bit-exact FP64 mode)
   fused.cu, gravity.cu, conduction.cu,    --fmad=false (conversions, snapshots, gravity, conduction,
-  chem.cu                                 floors)
+  chem.cu, expansion.cu, grid.cu          floors, expansion terms, the comoving time scalars)
   fused_f32.cu                            --use_fast_math (FP32 form)
 Run as `python -m evora_b200.build` (add -v for the ptxas register report).
 """
@@ -32,11 +32,13 @@ PER_FILE = {
     "gravity.cu": ["--fmad=false"],
     "conduction.cu": ["--fmad=false"],
     "chem.cu": ["--fmad=false"],
+    "expansion.cu": ["--fmad=false"],
+    "grid.cu": ["--fmad=false"],
     "fused_f32.cu": ["--use_fast_math"],
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
            "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu",
-           "io.cu", "gravity.cu", "conduction.cu", "chem.cu"]
+           "io.cu", "gravity.cu", "conduction.cu", "chem.cu", "expansion.cu"]
 
 
 def _deps():

@@ -11,6 +11,7 @@
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
 #include "common.h"
+#include "cosmology.cuh"
 #include "dropin_api.h"
 
 namespace evora {
@@ -40,8 +41,33 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->conduction = p->conduction != 0;
   P->simplekappa = p->simplekappa != 0;
   P->c_cond = p->c_cond;
-  evora_units u;   // compunits (units.f90:26-73), non-comoving
-  evora_units_noncomoving(p->tstart, dd.g, p->fb, &u);
+  // comoving coordinates (parameter.f90:227-243)
+  P->supercomoving = p->supercomoving != 0;
+  P->expansion = p->supercomoving && !p->atomic;
+  P->omega0 = p->omega0;
+  P->lambda0 = p->lambda0;
+  P->c_cosmo = p->c_cosmo;
+  P->zstart = p->zstart;
+  P->zend = p->zend;
+  P->g35 = 3.0 * dd.g - 5.0;
+  P->gravc = 1.5 * p->omega0;
+  P->fb = p->fb;
+  {
+    double b[5];
+    unit_bases(p, b);
+    const double t0 = b[2], l0 = b[3];
+    P->u_l02 = l0 * l0;
+    P->u_t02 = t0 * t0;
+    P->u_m0 = b[4];
+    P->u_t03 = std::pow(t0, 3.0);
+    P->u_d0 = b[1];
+    P->u_l04 = std::pow(l0, 4.0);
+    P->u_kcoef = kappa_coef();
+  }
+  // compunits (units.f90:26-73) at the start of the run (a = 1/(1+zstart)
+  // with supercomoving, main.f90:58-62)
+  evora_units u;
+  evora_compunits(p, nullptr, &u);
   P->kappa0 = u.kappa0;
   P->temp0 = u.temp0;
   // pressure floors of chem (chemistry.f90:100-119): temp2press with
@@ -51,13 +77,17 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->jeansfloor = p->jeansfloor != 0;
   P->temp_fl = p->temp_fl;
   P->temp0inv = 1.0 / u.temp0;
-  if (p->jeansfloor) {
-    const double r = dd.dx / u.jeans0 / p->c_jeans;
-    P->jeansfloor0 = r * r;
-  } else {
-    P->jeansfloor0 = 0.0;
-  }
+  P->jeansfloor0 = u.jeansfloor0;
   return true;
+}
+
+void start_time(const evora_params* p, const HydroParams& P, CosmoTime* s) {
+  // compparameter: t = tstart, cosmo = 1 (parameter.f90:232-234); then
+  // cosmostart with supercomoving (main.f90:58)
+  std::memset(s, 0, sizeof *s);
+  s->t = p->tstart;
+  s->cosmo = 1.0;
+  if (p->supercomoving) cosmostart(P, *s);
 }
 
 bool is_device_pointer(const void* ptr) {
@@ -105,6 +135,16 @@ void evora_params_default(evora_params* p) {
   p->temp_fl = 0.0;
   p->c_jeans = 0.0;
   p->fb = 1.0;
+  // parameter.f90:60-65, 82
+  p->supercomoving = 0;
+  p->c_cosmo = (double)0.1f;
+  p->omega0 = 1.0;
+  p->lambda0 = 0.0;
+  p->hubble0 = 50.0;
+  p->box = 1.0;
+  p->zstart = 99.0;
+  p->zend = 0.0;
+  for (int i = 0; i < EVORA_NDUMP; ++i) p->dump_redshift[i] = -1.0;
 }
 
 int evora_compparameter(const evora_params* p, evora_derived* d) {
@@ -168,6 +208,7 @@ struct DropinState {
   bool have_params = false;
   evora_params params{};
   HydroParams P{};
+  CosmoTime time{};   // module global's time scalars (evora_settime)
   int strict = 0;
   int device = -1;
   unsigned* d_err = nullptr;
@@ -263,6 +304,14 @@ bool evora::dropin_params(HydroParams* P) {
   return true;
 }
 
+bool evora::dropin_time(CosmoTime* s) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return false;
+  *s = S.time;
+  return true;
+}
+
 extern "C" {
 
 int evora_set_params(const evora_params* p) {
@@ -274,6 +323,7 @@ int evora_set_params(const evora_params* p) {
   if (!params_to_hydro(p, &P, nullptr, &rc)) return rc;
   S.params = *p;
   S.P = P;
+  start_time(p, P, &S.time);
   S.have_params = true;
   return 0;
 }
@@ -351,6 +401,78 @@ int evora_updatetime(int32_t* go, int32_t* dump, int32_t* k, double* t, double* 
   int g = *go;
   update_time(S.params.tend, *t, *dt, g);
   *go = g;
+  return 0;
+}
+
+static_assert(sizeof(evora_time) == sizeof(CosmoTime), "evora_time and CosmoTime share one layout");
+
+int evora_cosmostart(evora_time* s) {
+  if (!s) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  CosmoTime c;
+  start_time(&S.params, S.P, &c);
+  std::memcpy(s, &c, sizeof c);
+  return 0;
+}
+
+int evora_cosmostep(evora_time* s) {
+  if (!s) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  CosmoTime c;
+  std::memcpy(&c, s, sizeof c);
+  unsigned e = 0;
+  cosmostep(S.P, c, e);
+  std::memcpy(s, &c, sizeof c);
+  return (int)e;
+}
+
+int evora_compcosmo(evora_time* s) {
+  if (!s) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  CosmoTime c;
+  std::memcpy(&c, s, sizeof c);
+  compcosmo(S.P, c);
+  std::memcpy(s, &c, sizeof c);
+  return 0;
+}
+
+int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s) {
+  if (!go || !dump || !k || !s) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  CosmoTime c;
+  std::memcpy(&c, s, sizeof c);
+  int g = *go, d = *dump;
+  unsigned e = 0;
+  updatetime(S.P, S.params.tend, S.params.dump_redshift, c, g, d, *k, e);
+  std::memcpy(s, &c, sizeof c);
+  *go = g;
+  *dump = d;
+  return (int)e;
+}
+
+int evora_settime(const evora_time* s) {
+  if (!s) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  std::memcpy(&S.time, s, sizeof S.time);
+  if (S.P.supercomoving) {
+    // compunits after compcosmo (main.f90:132-133), with the host's libm
+    // power for a^5 (the reference's own)
+    evora_units u;
+    evora_compunits(&S.params, s, &u);
+    S.P.temp0 = u.temp0;
+    S.P.temp0inv = 1.0 / u.temp0;
+    S.P.kappa0 = u.kappa0;
+  }
   return 0;
 }
 

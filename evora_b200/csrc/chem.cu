@@ -28,12 +28,13 @@ int grid_of(int64_t n) {
   return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
 }
 
-// One cell: v holds q(1:6) in FP64 (in place).
-__device__ __forceinline__ void floor_cell(double* v, const HydroParams& P, const Gas<double>& c, unsigned& err) {
+// One cell: v holds q(1:6) in FP64 (in place); temp0inv of the step's units.
+__device__ __forceinline__ void floor_cell(double* v, const HydroParams& P, double temp0inv, const Gas<double>& c,
+                                           unsigned& err) {
   double press = pressure(v, c, P.dualenergy != 0, err);
   const double oldpress = press;
   if (P.tempfloor) {
-    const double pfloor = P.temp_fl * v[0] * P.temp0inv;   // temp2press, comp.f90:104-119
+    const double pfloor = P.temp_fl * v[0] * temp0inv;     // temp2press, comp.f90:104-119
     if (pfloor > press) press = pfloor;                     // max(press, pfloor)
   }
   if (P.jeansfloor) {
@@ -49,12 +50,13 @@ template <typename T>
 __global__ void k_floors(T* __restrict__ q, int64_t n, int nf, HydroParams P, const GridCtl* ctl, unsigned* err) {
   if (ctl_skip(ctl)) return;
   const Gas<double> c = Gas<double>::make(P);
+  const double temp0inv = units_of(P, ctl).temp0inv;
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6];
     for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
     if (nf == 5) v[5] = 0.0;   // not carried: the S terms are dropped
-    floor_cell(v, P, c, e);
+    floor_cell(v, P, temp0inv, c, e);
     q[4 * n + i] = (T)v[4];
     if (nf == 6) q[5 * n + i] = (T)v[5];
   }
@@ -65,7 +67,7 @@ __global__ void k_floors_aos(double* __restrict__ q, int64_t n, HydroParams P, u
   const Gas<double> c = Gas<double>::make(P);
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    floor_cell(q + (int64_t)EVORA_NQ * i, P, c, e);
+    floor_cell(q + (int64_t)EVORA_NQ * i, P, P.temp0inv, c, e);
   if (e) atomicOr(err, e);
 }
 

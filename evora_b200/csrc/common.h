@@ -20,8 +20,19 @@ bool is_device_pointer(const void* ptr);
 // Records a message for evora_last_error().
 void set_error_message(const char* msg);
 
-// The module-global parameters set by evora_set_params (false if unset).
+// The module-global parameters set by evora_set_params (false if unset),
+// with the units of the time state evora_settime last set.
 bool dropin_params(HydroParams* P);
+
+struct CosmoTime;
+
+// The time scalars of the drop-in layer (evora_set_params: the start of the
+// run; then evora_settime).  False if no parameters are set.
+bool dropin_time(CosmoTime* s);
+
+// t = tstart and cosmo = 1 (compparameter), then cosmostart with
+// supercomoving (main.f90:52-58).
+void start_time(const evora_params* p, const HydroParams& P, CosmoTime* s);
 
 // The parameters a grid was created with.
 const evora_params* grid_params(const evora_grid* g);

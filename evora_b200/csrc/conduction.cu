@@ -49,6 +49,7 @@ __global__ void k_cond_prim(T* __restrict__ q, int64_t n, int nf, HydroParams P,
   if (ctl_skip(ctl)) return;
   const Gas<double> c = Gas<double>::make(P);
   const bool de = P.dualenergy != 0;
+  const double temp0 = units_of(P, ctl).temp0;
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6], w[5];
@@ -58,7 +59,7 @@ __global__ void k_cond_prim(T* __restrict__ q, int64_t n, int nf, HydroParams P,
       q[4 * n + i] = (T)v[4];
       if (nf == 6) q[5 * n + i] = (T)v[5];
     }
-    temp[i] = w[4] / w[0] * P.temp0;
+    temp[i] = w[4] / w[0] * temp0;
   }
   if (e) atomicOr(err, e);
 }
@@ -323,7 +324,7 @@ int evora_thermalstep(double* q, const double* w, double* dt) {
   if (err) return (int)err;
   double vmin;
   std::memcpy(&vmin, &out[0], sizeof vmin);
-  *dt = thermal_dt(P, vmin, *dt, err);
+  *dt = thermal_dt(P, units_of(P, nullptr), vmin, *dt, err);
   return (int)err;
 }
 

@@ -23,24 +23,25 @@ int cond_step(CondPlan& c, const HydroParams& P, void* q, bool f32, int nf, Grid
               cudaStream_t st);
 
 // thermalstep per cell: rho / kappa with kappa = kappa0 T^2.5, T from
-// pressure() (no write-back) over rho times temp0.
-__host__ __device__ inline double thermal_v(const HydroParams& P, double rho, double press) {
-  const double temp = press / rho * P.temp0;
-  const double kappa = P.kappa0 * pow(temp, 2.5);
+// pressure() (no write-back) over rho times temp0 (U: the step's units).
+__host__ __device__ inline double thermal_v(const Units& U, double rho, double press) {
+  const double temp = press / rho * U.temp0;
+  const double kappa = U.kappa0 * pow(temp, 2.5);
   return rho / kappa;
 }
 
 // The same with T^2.5 = T^2 sqrt(T) (within a few ulp of pow; the fast
 // arithmetic forms use it, the strict form keeps pow).
-__host__ __device__ inline double thermal_v_fast(const HydroParams& P, double rho, double press) {
-  const double temp = press / rho * P.temp0;
-  const double kappa = P.kappa0 * (temp * temp * sqrt(temp));
+__host__ __device__ inline double thermal_v_fast(const Units& U, double rho, double press) {
+  const double temp = press / rho * U.temp0;
+  const double kappa = U.kappa0 * (temp * temp * sqrt(temp));
   return rho / kappa;
 }
 
 // thermalstep part 2: dt = min(c_cond dx^2 vmin / temp0, dt); EVORA_ERR_DT if <= 0.
-__host__ __device__ inline double thermal_dt(const HydroParams& P, double vmin, double dt, unsigned& err) {
-  const double v = P.c_cond * (P.dx * P.dx) * vmin / P.temp0;
+__host__ __device__ inline double thermal_dt(const HydroParams& P, const Units& U, double vmin, double dt,
+                                             unsigned& err) {
+  const double v = P.c_cond * (P.dx * P.dx) * vmin / U.temp0;
   const double d = (dt < v) ? dt : v;
   if (d <= 0.0) err |= EVORA_ERR_DT;
   return d;

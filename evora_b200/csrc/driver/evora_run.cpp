@@ -9,11 +9,15 @@
 // Input: namelist group para (parameter.f90:26-105) and, for the shocktube,
 // ic_para (ic/shocktube.f90:39-47).  The reference compiles one ic/<name>.f90
 // into the binary (object/Makefile:57-58); here --ic chooses at run time.
-// Self-gravity (gravity = .true., non-comoving) and thermal conduction
-// (conduction = .true. with simplekappa = .true.) run on the device after
-// each hydro step as in main.f90:121, 158-175.  Runs with comoving
-// coordinates, chemistry or the temperature / Jeans floors are refused:
-// those physics are not on the path this library implements.
+// Self-gravity (gravity = .true.), the temperature / Jeans pressure floors,
+// thermal conduction (conduction = .true. with simplekappa = .true.) and,
+// with comoving coordinates (supercomoving = .true.), the expansion factor's
+// integration, the comoving units and the expansion terms run on the device
+// with each hydro step as in main.f90:119-185.  Runs with chemistry are
+// refused: the species network is not on the path this library implements.
+// With supercomoving, data/<k4>.000 and data/<k4>.units are written when a
+// step lands on dump_redshift(k4) (main.f90:197-202), and the cadence
+// variable is tsnap = a * nsnap.
 //
 // Output, under the working directory, as the reference writes it:
 //   data/parameter           writeparameter (parameter.f90:267-337)
@@ -206,8 +210,10 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "unknown IC %s\n", icname.c_str());
     return 2;
   }
-  evora_units u;
-  evora_units_noncomoving(p.tstart, d.g, fb, &u);
+  (void)fb;
+  evora_units u;   // compunits at the start (main.f90:58-62)
+  if ((rc = evora_compunits(&p, nullptr, &u))) return fail("compunits", rc);
+  const bool comoving = p.supercomoving != 0;
   auto dump = [&](const char* name) {
     const std::string base = std::string("data/") + name;
     int r = evora_write_dump((base + ".000").c_str(), q.data(), EVORA_NQ, p.nx, p.ny, p.nz, 1, p.nz);
@@ -239,9 +245,15 @@ int main(int argc, char** argv) {
     return append("data/evo", s) ? 0 : EVORA_ERR_IO;
   };
   auto screen = [&]() {      // snapshot.f90:132-155
-    const double tpro = tsnap / nsnap * 100;
-    const std::string s = ft::I(k1, 4) + ft::I(k, 6) + ft::E(t, 12, 4) + ft::E(dt, 12, 4) + std::string(11, ' ') +
-                          ft::F(tpro, 12, 1) + "%\n";
+    std::string s;
+    if (comoving) {
+      s = ft::I(k1, 4) + ft::I(k, 6) + ft::E(t, 12, 4) + ft::E(dt, 12, 4) + ft::F(u.cosmo, 12, 4) +
+          ft::F(u.redshift, 12, 2) + "\n";
+    } else {
+      const double tpro = tsnap / nsnap * 100;
+      s = ft::I(k1, 4) + ft::I(k, 6) + ft::E(t, 12, 4) + ft::E(dt, 12, 4) + std::string(11, ' ') +
+          ft::F(tpro, 12, 1) + "%\n";
+    }
     std::fputs(s.c_str(), stdout);
     std::fflush(stdout);
     append("data/log", s);
@@ -271,10 +283,24 @@ int main(int argc, char** argv) {
       return 1;
     }
     if ((rc = evora_grid_time(g, &t, &dt, &go, &k))) return fail("grid_time", rc);
-    tsnap = (t - p.tstart) / (p.tend - p.tstart) * nsnap;
+    int32_t dumpk = 0;
+    if (comoving) {
+      // compunits after compcosmo (main.f90:132-133); tsnap = cosmo * nsnap
+      evora_time s;
+      if ((rc = evora_grid_cosmo(g, &s, &dumpk))) return fail("grid_cosmo", rc);
+      if ((rc = evora_compunits(&p, &s, &u))) return fail("compunits", rc);
+      tsnap = s.cosmo * nsnap;
+    } else {
+      u.t = t;
+      tsnap = (t - p.tstart) / (p.tend - p.tstart) * nsnap;
+    }
     if (tsnap >= (double)k1) screen();
     if (tsnap >= (double)k2 && (rc = evolution())) return fail("evolution", rc);
     if ((cut || slice || bov) && tsnap >= (double)k3 && (rc = snapshot())) return fail("snapshot", rc);
+    if (dumpk) {   // main.f90:197-202: writedump(q, k4 as I0.3)
+      if ((rc = evora_grid_get_q(g, q.data()))) return fail("grid_get_q", rc);
+      if ((rc = dump(ft::I0(dumpk, 3).c_str()))) return fail("writedump", rc);
+    }
   }
   if ((rc = evora_grid_get_q(g, q.data()))) return fail("grid_get_q", rc);
   u.t = t;

@@ -151,9 +151,10 @@ inline std::string label(const char* name) {
 }
 
 // The run's parameter values (all of namelist para), keyed by lower-case
-// name.
+// name, and the array dump_redshift (global.f90:137-138).
 struct RunParams {
   std::map<std::string, double> v;
+  std::vector<double> dump_redshift = std::vector<double>(EVORA_NDUMP, -1.0);   // parameter.f90:82
   double operator[](const char* k) const { return v.at(k); }
   bool flag(const char* k) const { return v.at(k) != 0.0; }
 };
@@ -164,14 +165,51 @@ inline RunParams defaults() {
   return r;
 }
 
+// A namelist value list: items separated by commas or blanks, each a value
+// or r*value (r repetitions).  False on an item that is not a number.
+inline bool value_list(const std::string& text, std::vector<double>* out) {
+  std::string t = text;
+  for (auto& c : t)
+    if (c == ',') c = ' ';
+  std::istringstream in(t);
+  std::string item;
+  while (in >> item) {
+    long rep = 1;
+    const size_t star = item.find('*');
+    if (star != std::string::npos) {
+      char* end = nullptr;
+      rep = std::strtol(item.c_str(), &end, 10);
+      if (end != item.c_str() + star || rep < 1) return false;
+      item = item.substr(star + 1);
+    }
+    std::string s = item;
+    for (auto& c : s)
+      if (c == 'd' || c == 'D') c = 'e';
+    char* end = nullptr;
+    const double x = std::strtod(s.c_str(), &end);
+    if (end == s.c_str() || *end != '\0') return false;
+    for (long i = 0; i < rep; ++i) out->push_back(x);
+  }
+  return true;
+}
+
 // readparameter (parameter.f90:26-105): defaults, then the namelist values.
-// Unknown keys are reported in *unknown; dump_redshift is accepted and
-// ignored (it only matters for comoving runs).
+// Unknown keys are reported in *unknown; dump_redshift takes a value list
+// (at most EVORA_NDUMP values, filled from the first element on).
 inline void apply_namelist(const std::map<std::string, std::string>& kv, RunParams* r, std::string* unknown) {
   for (const auto& [k, val] : kv) {
+    if (k == "dump_redshift") {
+      std::vector<double> z;
+      if (!value_list(val, &z) || z.size() > (size_t)EVORA_NDUMP) {
+        if (unknown) *unknown += (unknown->empty() ? "" : ", ") + std::string("dump_redshift (bad value list)");
+        continue;
+      }
+      for (size_t i = 0; i < z.size(); ++i) r->dump_redshift[i] = z[i];
+      continue;
+    }
     auto it = r->v.find(k);
     if (it == r->v.end()) {
-      if (k != "dump_redshift" && unknown) *unknown += (unknown->empty() ? "" : ", ") + k;
+      if (unknown) *unknown += (unknown->empty() ? "" : ", ") + k;
       continue;
     }
     char type = 'E';
@@ -265,13 +303,22 @@ inline evora_params hydro_params(const RunParams& r) {
   p.zmax = r["zmax"];
   p.tstart = r["tstart"];
   p.tend = r["tend"];
+  p.supercomoving = r.flag("supercomoving");
+  p.c_cosmo = r["c_cosmo"];
+  p.omega0 = r["omega0"];
+  p.lambda0 = r["lambda0"];
+  p.hubble0 = r["hubble0"];
+  p.box = r["box"];
+  p.zstart = r["zstart"];
+  p.zend = r["zend"];
+  for (int i = 0; i < EVORA_NDUMP; ++i) p.dump_redshift[i] = r.dump_redshift[i];
   return p;
 }
 
 // The parts of a run outside the hydro path that these drivers do not have.
 inline std::string unsupported(const RunParams& r) {
   std::string s;
-  for (const char* k : {"supercomoving", "chemistry"})
+  for (const char* k : {"chemistry"})
     if (r.flag(k)) s += (s.empty() ? "" : ", ") + std::string(k);
   if (!r.flag("hydro")) s += (s.empty() ? "" : ", ") + std::string("hydro = .false.");
   return s;

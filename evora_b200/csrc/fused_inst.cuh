@@ -87,6 +87,7 @@ __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, Gr
   if (ctl_skip(ctl)) return;
   double m0 = 0.0, m1 = 0.0, m2 = 0.0, vmin = 1e99;
   unsigned err = 0;
+  const Units U = units_of(P, ctl);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     TT qv[6], s[3];
 #pragma unroll
@@ -102,7 +103,7 @@ __global__ void k_cfl_soa(HydroParams P, const TT* __restrict__ q, int64_t n, Gr
 #pragma unroll
       for (int f = 0; f < NF; ++f) qd[f] = (double)qv[f];
       q2w(qd, w, Gas<double>::make(P), P.dualenergy != 0, err);
-      const double v = kFast ? thermal_v_fast(P, w[0], w[4]) : thermal_v(P, w[0], w[4]);
+      const double v = kFast ? thermal_v_fast(U, w[0], w[4]) : thermal_v(U, w[0], w[4]);
       if (v < vmin) vmin = v;
     }
   }

@@ -1,7 +1,8 @@
-// gravity.cu -- self-gravity on the device, the non-comoving branch of the
-// reference's gravitation.f90:
+// gravity.cu -- self-gravity on the device, the reference's
+// gravitation.f90:
 //
-//   gravpotential  source grav (rho - <rho>), forward FFT, multigreen (the
+//   gravpotential  source grav (rho - <rho>), or a grav (rho / fb - 1) with
+//                  comoving coordinates, forward FFT, multigreen (the
 //                  discrete Green's function -h2 / sum_d sin^2(k_d pi / n_d)
 //                  over n3), backward FFT                (26-53, 55-84)
 //   gravintegration  centred potential differences (grav_force, periodic)
@@ -25,6 +26,7 @@
 
 #include "../../include/evora_gpu.h"
 #include "common.h"
+#include "cosmology.cuh"
 #include "gravity.h"
 
 namespace evora {
@@ -83,6 +85,18 @@ __global__ void k_source(const T* __restrict__ q, int64_t n, int aos, const doub
   const double m = *mean;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     phi[i] = grav * (rho_of(q, n, aos, i) - m);
+}
+
+// The comoving source cosmo * grav * (rho / fb - 1) with grav = 1.5 omega0
+// (gravitation.f90:36-37); cosmo from the grid's control block, or
+// cosmo_host without one.
+template <typename T>
+__global__ void k_source_comoving(const T* __restrict__ q, int64_t n, int aos, double grav, double fb,
+                                  double cosmo_host, double* __restrict__ phi, const GridCtl* ctl) {
+  if (ctl_skip(ctl)) return;
+  const double cg = (ctl ? ctl->cosmo : cosmo_host) * grav;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    phi[i] = cg * (rho_of(q, n, aos, i) / fb - 1.0);
 }
 
 // multigreen (gravitation.f90:55-84) on the half spectrum (x index 0..nx/2):
@@ -156,7 +170,11 @@ int grav_plan(const HydroParams& P, GravPlan* g, cudaStream_t st) {
   g->n = (int64_t)P.nx * P.ny * P.nz;
   const int nxh = P.nx / 2 + 1;
   g->nh = (int64_t)nxh * P.ny * P.nz;
-  g->grav = 8.38553911e-7;            // fourpig (global.f90:101), parameter.f90:240
+  // grav (parameter.f90:236-241): 1.5 omega0 with supercomoving, else
+  // fourpig (global.f90:101)
+  g->comoving = P.supercomoving != 0;
+  g->grav = g->comoving ? P.gravc : 8.38553911e-7;
+  g->fb = P.fb;
   g->dx2inv = 0.5 / P.dx;             // parameter.f90:219
   g->dy2inv = 0.5 / P.dy;
   g->dz2inv = 0.5 / P.dz;
@@ -225,20 +243,30 @@ void grav_plan_free(GravPlan* g) {
   *g = GravPlan{};
 }
 
-int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const GridCtl* ctl) {
+int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const GridCtl* ctl, double cosmo_host) {
   (void)nf;
   cudaStream_t st = g.stream;
-  if (f32) {
-    k_rho_partial<float><<<g.nred, kThreads, 0, st>>>((const float*)q, g.n, aos, g.red, ctl);
+  if (g.comoving) {
+    if (f32)
+      k_source_comoving<float><<<grid_of(g.n), kThreads, 0, st>>>((const float*)q, g.n, aos, g.grav, g.fb, cosmo_host,
+                                                                   g.phi, ctl);
+    else
+      k_source_comoving<double><<<grid_of(g.n), kThreads, 0, st>>>((const double*)q, g.n, aos, g.grav, g.fb,
+                                                                    cosmo_host, g.phi, ctl);
   } else {
-    k_rho_partial<double><<<g.nred, kThreads, 0, st>>>((const double*)q, g.n, aos, g.red, ctl);
-  }
-  k_rho_mean<<<1, 32, 0, st>>>(g.red, g.nred, g.n, ctl);
-  if (f32) {
-    k_source<float><<<grid_of(g.n), kThreads, 0, st>>>((const float*)q, g.n, aos, g.red + g.nred, g.grav, g.phi, ctl);
-  } else {
-    k_source<double><<<grid_of(g.n), kThreads, 0, st>>>((const double*)q, g.n, aos, g.red + g.nred, g.grav, g.phi,
-                                                        ctl);
+    if (f32) {
+      k_rho_partial<float><<<g.nred, kThreads, 0, st>>>((const float*)q, g.n, aos, g.red, ctl);
+    } else {
+      k_rho_partial<double><<<g.nred, kThreads, 0, st>>>((const double*)q, g.n, aos, g.red, ctl);
+    }
+    k_rho_mean<<<1, kThreads, 0, st>>>(g.red, g.nred, g.n, ctl);   // the tree needs all kThreads threads
+    if (f32) {
+      k_source<float><<<grid_of(g.n), kThreads, 0, st>>>((const float*)q, g.n, aos, g.red + g.nred, g.grav, g.phi,
+                                                          ctl);
+    } else {
+      k_source<double><<<grid_of(g.n), kThreads, 0, st>>>((const double*)q, g.n, aos, g.red + g.nred, g.grav, g.phi,
+                                                          ctl);
+    }
   }
   if (cufftExecD2Z(g.fwd, g.phi, g.spec) != CUFFT_SUCCESS) {
     set_error_message("cufftExecD2Z failed");
@@ -364,7 +392,13 @@ int evora_gravpotential(const double* q, double* phi) {
       return sync_status("evora_gravpotential");
     dq = D.q;
   }
-  if ((rc = grav_potential(D.plan, dq, false, EVORA_NQ, 1, nullptr))) return rc;
+  // the source of the current parameters, a from evora_settime
+  D.plan.comoving = P.supercomoving != 0;
+  D.plan.grav = D.plan.comoving ? P.gravc : 8.38553911e-7;
+  D.plan.fb = P.fb;
+  CosmoTime s;
+  if (!dropin_time(&s)) return EVORA_ERR_ARG;
+  if ((rc = grav_potential(D.plan, dq, false, EVORA_NQ, 1, nullptr, s.cosmo))) return rc;
   double* out = pdev ? phi : D.phi;
   k_real_to_complex<<<grid_of(D.n), kThreads>>>(D.plan.phi, out, D.n);
   if (!pdev && cudaMemcpy(phi, D.phi, sizeof(double) * 2 * D.n, cudaMemcpyDeviceToHost) != cudaSuccess)

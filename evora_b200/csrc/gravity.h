@@ -1,5 +1,5 @@
-// gravity.h -- self-gravity of the hydro state on the device: the
-// non-comoving branch of gravitation.f90 (gravpotential, multigreen,
+// gravity.h -- self-gravity of the hydro state on the device:
+// gravitation.f90 (gravpotential with both source terms, multigreen,
 // gravintegration, grav_force) with cuFFT.
 #pragma once
 
@@ -16,7 +16,9 @@ struct GravPlan {
   int nx = 0, ny = 0, nz = 0;
   int64_t n = 0;          // cells
   int64_t nh = 0;         // complex coefficients of the half spectrum
-  double grav = 0.0;      // 4 pi G (global.f90:101) without comoving coordinates
+  bool comoving = false;  // source cosmo grav (rho / fb - 1) (gravitation.f90:36-37)
+  double grav = 0.0;      // 4 pi G (global.f90:101), or 1.5 omega0 when comoving
+  double fb = 1.0;
   double dx2inv = 0.0, dy2inv = 0.0, dz2inv = 0.0;   // 0.5 / dx ...
   cufftHandle fwd = 0, inv = 0;                       // D2Z, Z2D over (nz, ny, nx)
   double* phi = nullptr;                              // potential, n (real)
@@ -36,8 +38,9 @@ void grav_plan_free(GravPlan* g);
 void grav_set_stream(GravPlan* g, cudaStream_t st);
 
 // gravpotential (gravitation.f90:26-53): phi from the density of the state
-// (SoA with nf fields of type f32 or f64, or the reference AoS q(6, n)).
-int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const GridCtl* ctl);
+// (SoA with nf fields of type f32 or f64, or the reference AoS q(6, n)); the
+// comoving source takes cosmo from ctl, or cosmo_host when ctl is null.
+int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const GridCtl* ctl, double cosmo_host);
 
 // gravintegration (gravitation.f90:170-194) with the forces of grav_force
 // (196-243), in place on the state, with the step's dt from ctl (or dt_host

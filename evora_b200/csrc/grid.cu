@@ -20,11 +20,13 @@
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
 #include "common.h"
+#include "cosmology.cuh"
 #include "dropin_api.h"
 #include "fused.h"
 #include "gravity.h"
 #include "conduction.h"
 #include "chem.h"
+#include "expansion.h"
 
 using namespace evora;
 
@@ -67,6 +69,9 @@ struct evora_grid {
   CondPlan cond{};
   // pressure floors after each step (params.tempfloor / jeansfloor)
   bool floors = false;
+  // comoving coordinates: expansion terms after each step (params.supercomoving
+  // and not atomic)
+  bool expansion = false;
   bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
 };
 
@@ -100,10 +105,13 @@ __global__ void k_step_begin(GridCtl* ctl, int use_next) {
   ctl->errnext = 0u;
   ctl->snext[0] = ctl->snext[1] = ctl->snext[2] = 0ull;
   ctl->vcond = ordered_bits(1e99);   // thermalstep's initial v (timestep.f90:82)
-  ctl->active = (ctl->go != 0 && ctl->err == 0) ? 1 : 0;
+  // a raised dump holds the grid until the host has read it
+  ctl->active = (ctl->go != 0 && ctl->err == 0 && ctl->dump == 0) ? 1 : 0;
 }
 
-// hydrostep part 2 + updatetime (timestep.f90:26-57, 147-171).
+// hydrostep part 2 (timestep.f90:26-57), thermalstep's limit, and the
+// master block of main.f90:124-137: cosmostep and compcosmo (comoving),
+// updatetime, and compunits (comoving).
 __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   if (!ctl->active || ctl->err) {
     ctl->active = 0;
@@ -113,23 +121,74 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   for (int i = 0; i < 3; ++i) sm[i] = __longlong_as_double((long long)ctl->smax[i]);
   unsigned e = 0;
   double dt = cfl_dt(P, sm[0], sm[1], sm[2], 1e99, e);
-  if (!e && P.conduction) dt = thermal_dt(P, __longlong_as_double((long long)ctl->vcond), dt, e);
+  if (!e && P.conduction) dt = thermal_dt(P, units_of(P, ctl), __longlong_as_double((long long)ctl->vcond), dt, e);
   if (e) {
     ctl->err |= e;
     ctl->active = 0;
     return;
   }
-  double t = ctl->t;
-  int go = ctl->go;
-  update_time(ctl->tend, t, dt, go);
-  ctl->t = t;
-  ctl->dt = dt;
+  CosmoTime s{ctl->t, dt, ctl->cosmo, ctl->oldcosmo, ctl->cosmodot, ctl->expand, ctl->redshift};
+  if (P.supercomoving) {
+    cosmostep(P, s, e);
+    if (!e) compcosmo(P, s);
+  }
+  int go = ctl->go, dump = 0;
+  if (!e) updatetime(P, ctl->tend, ctl->dump_redshift, s, go, dump, ctl->k4, e);
+  if (e) {
+    ctl->err |= e;
+    ctl->active = 0;
+    return;
+  }
+  ctl->t = s.t;
+  ctl->dt = s.dt;
   ctl->go = go;
+  if (P.supercomoving) {
+    ctl->cosmo = s.cosmo;
+    ctl->oldcosmo = s.oldcosmo;
+    ctl->cosmodot = s.cosmodot;
+    ctl->expand = s.expand;
+    ctl->redshift = s.redshift;
+    const Units u = comoving_units(P, s.cosmo);
+    ctl->temp0 = u.temp0;
+    ctl->temp0inv = u.temp0inv;
+    ctl->kappa0 = u.kappa0;
+    if (dump) {   // main.f90:197-202: dump number k4, then k4 + 1
+      ctl->dump = ctl->k4;
+      ctl->k4 += 1;
+    }
+  }
 }
 
 __global__ void k_step_end(GridCtl* ctl) {
   if (ctl->active && ctl->err == 0) ctl->k += 1;
 }
+
+// The control block at the start of a run: t = tstart, go, and with
+// supercomoving cosmostart's a, da/dt and redshift, the units at that a and
+// the first dump index k4 = 1 (main.f90:33, 52-62).
+void init_ctl(const evora_grid* g, GridCtl* c) {
+  std::memset(c, 0, sizeof *c);
+  CosmoTime s;
+  start_time(&g->params, g->P, &s);
+  c->t = s.t;
+  c->tend = g->params.tend;
+  c->go = 1;
+  c->cosmo = s.cosmo;
+  c->oldcosmo = s.oldcosmo;
+  c->cosmodot = s.cosmodot;
+  c->expand = s.expand;
+  c->redshift = s.redshift;
+  c->temp0 = g->P.temp0;
+  c->temp0inv = g->P.temp0inv;
+  c->kappa0 = g->P.kappa0;
+  c->k4 = 1;
+  std::memcpy(c->dump_redshift, g->params.dump_redshift, sizeof c->dump_redshift);
+}
+
+// Own kernels of one gravity substep: the mean density (two), the source,
+// the Green's function and the integration; the comoving source needs no
+// mean.
+int grav_launches(const evora_grid* g) { return g->gravity ? (g->grav.comoving ? 3 : 5) : 0; }
 
 void drop_graphs(evora_grid* g) {
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
@@ -167,7 +226,7 @@ int enqueue_reference_step(evora_grid* g) {
   if (g->P.secondorder) o.compevo(g->P, g->w, g->evo, g->s, 0.0, g->ctl, st);
   o.sweep(g->P, g->w, g->q_aos, g->evo, g->s, 0.0, &g->ctl->err, g->ctl, st);
   if (g->gravity) {
-    int rc = grav_potential(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl);
+    int rc = grav_potential(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl, 1.0);
     if (!rc) rc = grav_integrate(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl, 0.0);
     if (rc) return rc;
   }
@@ -190,10 +249,10 @@ int enqueue_fused_step(evora_grid* g) {
   fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
   if (g->gravity) {
     // gravpotential + gravintegration on the updated state (main.f90:158-165)
-    int rc = grav_potential(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl);
+    int rc = grav_potential(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 1.0);
     if (!rc) rc = grav_integrate(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 0.0);
     if (rc) return rc;
-    g->launches += 5;   // own kernels; cuFFT adds its own
+    g->launches += grav_launches(g);   // own kernels; cuFFT adds its own
   }
   if (g->floors) {
     // chem(q) of the plain build: pressure floors (main.f90:167)
@@ -206,6 +265,12 @@ int enqueue_fused_step(evora_grid* g) {
     int rc = cond_step(g->cond, g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, g->ctl, 0.0, st);
     if (rc) return rc;
     g->launches += 2;
+  }
+  if (g->expansion) {
+    // expansion terms of E and S (main.f90:178)
+    int rc = expansion_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->ctl, st);
+    if (rc) return rc;
+    g->launches += 1;
   }
   mark(g);
   k_step_end<<<1, 1, 0, st>>>(g->ctl);
@@ -346,11 +411,17 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
       return rc;
     }
   }
+  if (p->supercomoving) {
+    if (reference_backend(g)) {
+      free_grid(g);
+      return EVORA_ERR_ARG;   // the comoving terms run on the resident SoA state
+    }
+    g->expansion = g->P.expansion != 0;
+    g->plan.cfl_fused = 0;     // the expansion terms change the state after the update
+  }
   {
-    GridCtl c{};
-    c.t = p->tstart;
-    c.tend = p->tend;
-    c.go = 1;
+    GridCtl c;
+    init_ctl(g, &c);
     if (cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream) != cudaSuccess) goto nomem;
     if (cudaStreamSynchronize(g->stream) != cudaSuccess) goto nomem;
   }
@@ -406,10 +477,8 @@ int evora_grid_set_q(evora_grid* g, const double* q) {
     fused_from_aos(g->plan, src, g->qbuf[0], g->stream);
   }
   g->cfl_fresh = false;
-  GridCtl c{};
-  c.t = g->params.tstart;
-  c.tend = g->params.tend;
-  c.go = 1;
+  GridCtl c;
+  init_ctl(g, &c);
   CU(cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream));
   CU(cudaStreamSynchronize(g->stream));
   return 0;
@@ -498,8 +567,8 @@ int graph_steps(evora_grid* g, int nsteps) {
     } else {
       g->cur = start ^ (nsteps & 1);
       const bool fused = g->plan.cfl_fused != 0;
-      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + (g->gravity ? 5 : 0) + (g->conduction ? 2 : 0) +
-                                       (g->floors ? 1 : 0)) +
+      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + grav_launches(g) + (g->conduction ? 2 : 0) +
+                                       (g->floors ? 1 : 0) + (g->expansion ? 1 : 0)) +
                      (fused && !fresh ? 1 : 0);
       g->cfl_fresh = fused;
     }
@@ -520,6 +589,29 @@ int evora_grid_time(evora_grid* g, double* t, double* dt, int32_t* go, int64_t* 
   if (dt) *dt = c.dt;
   if (go) *go = c.go;
   if (k) *k = c.k;
+  return 0;
+}
+
+int evora_grid_cosmo(evora_grid* g, evora_time* s, int32_t* dump) {
+  if (!g) return EVORA_ERR_ARG;
+  GridCtl c;
+  CU(cudaMemcpyAsync(&c, g->ctl, sizeof c, cudaMemcpyDeviceToHost, g->stream));
+  CU(cudaStreamSynchronize(g->stream));
+  if (s) {
+    s->t = c.t;
+    s->dt = c.dt;
+    s->cosmo = c.cosmo;
+    s->oldcosmo = c.oldcosmo;
+    s->cosmodot = c.cosmodot;
+    s->expand = c.expand;
+    s->redshift = c.redshift;
+  }
+  if (dump) *dump = c.dump;
+  if (c.dump) {
+    const int zero = 0;
+    CU(cudaMemcpyAsync(&g->ctl->dump, &zero, sizeof zero, cudaMemcpyHostToDevice, g->stream));
+    CU(cudaStreamSynchronize(g->stream));
+  }
   return 0;
 }
 

@@ -40,6 +40,13 @@ struct GridCtl {
   unsigned long long smax[3];   // CFL maxima of |u_d| + a (ordered bits)
   unsigned long long snext[3];  // the same, over the state the update wrote
   unsigned long long vcond;     // thermalstep: min over cells of rho / kappa (ordered bits)
+  // comoving coordinates: the time scalars of module global (global.f90:86)
+  double cosmo, oldcosmo, cosmodot, expand, redshift;
+  // the units compunits derives from cosmo (units.f90:46-63), current step
+  double temp0, temp0inv, kappa0;
+  int dump;      // dump_redshift index whose dump the last step raised (0: none)
+  int k4;        // the next dump_redshift index updatetime tests (main.f90:33)
+  double dump_redshift[EVORA_NDUMP];
 };
 
 __device__ __forceinline__ bool ctl_skip(const GridCtl* ctl) {
@@ -59,7 +66,28 @@ struct HydroParams {
   // pressure floors (chem, chemistry.f90:92-121, plain build)
   int tempfloor, jeansfloor;
   double temp_fl, temp0inv, jeansfloor0;
+  // comoving coordinates (cosmology.f90, timestep.f90:59-70, 147-226)
+  int supercomoving;
+  int expansion;                  // supercomoving and not atomic (main.f90:178)
+  double omega0, lambda0, c_cosmo, zstart, zend;
+  double g35;                     // 3g - 5 (parameter.f90:231)
+  double gravc;                   // grav = 1.5 omega0 (parameter.f90:236-238)
+  double fb;
+  // a-independent factors of the comoving units (units.f90:32-63): l0^2,
+  // t0^2, m0, t0^3, d0, l0^4 and kappa_coef
+  double u_l02, u_t02, u_m0, u_t03, u_d0, u_l04, u_kcoef;
 };
+
+// The units a kernel uses: the grid's current ones when the run is comoving
+// (compunits after every compcosmo, main.f90:132-136), else the constants.
+struct Units {
+  double temp0, temp0inv, kappa0;
+};
+
+__host__ __device__ __forceinline__ Units units_of(const HydroParams& P, const GridCtl* ctl) {
+  if (P.supercomoving && ctl != nullptr) return Units{ctl->temp0, ctl->temp0inv, ctl->kappa0};
+  return Units{P.temp0, P.temp0inv, P.kappa0};
+}
 
 template <typename T>
 __host__ __device__ __forceinline__ T fmin2(T a, T b) { return (b < a) ? b : a; }

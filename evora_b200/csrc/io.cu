@@ -14,6 +14,7 @@
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
 #include "common.h"
+#include "cosmology.cuh"
 #include "fortran_fmt.h"
 
 namespace evora {
@@ -227,7 +228,11 @@ int snapshot_text(const evora_params* p, const Geometry& G, const CellView& v, c
   return 0;
 }
 
-// writebovhead (write.f90:66-104) for a non-comoving run.
+// The TIME entry of writebovhead (write.f90:89-93): the redshift with
+// supercomoving, else t.
+double bov_time(const evora_params* p, const evora_units* u) { return p->supercomoving ? u->redshift : u->t; }
+
+// writebovhead (write.f90:66-104); t is the TIME entry.
 bool bov_head(const evora_params* p, const Geometry& G, double t, const std::string& name, const char* var,
               const char* dir) {
   std::string file2 = name + "." + var + ".bovdata";
@@ -345,34 +350,71 @@ int evora_read_dump(const char* path, int32_t header[6], double* q, int64_t capa
   return rc;
 }
 
-void evora_units_noncomoving(double t, double g, double fb, evora_units* u) {
-  // units.f90:26-73 with supercomoving false: h = d0 = t0 = l0 = 1, m0 = kb,
-  // cosmo = 1; module global's pi and the default-real literals are single
-  // precision (global.f90:98).
-  const double kb = 1.3806200e-16, megapc = 3.08568025e24, pi = (double)3.1415927f;
-  const double cosmo = 1.0, d0 = 1.0, t0 = 1.0, l0 = 1.0, m0 = kb;
+}  // extern "C"
+
+namespace {
+
+// compunits (units.f90:46-72) from the bases h, d0, t0, l0, m0 at expansion
+// factor cosmo; module global's pi and the default-real literals are single
+// precision (global.f90:98), x**2.0 is x*x (as gcc folds pow(x, 2.0)).
+void units_at(const double b[5], double g, double fb, double t, double cosmo, double redshift, evora_units* u) {
+  const double pi = (double)3.1415927f;
+  const double d0 = b[1], t0 = b[2], l0 = b[3], m0 = b[4];
   const double g1 = g - 1.0;
   std::memset(u, 0, sizeof *u);
   u->t = t;
   u->cosmo = cosmo;
-  u->redshift = 0.0;
+  u->redshift = redshift;
   u->density0 = d0 / std::pow(cosmo, 3.0);
   u->length0 = l0 * cosmo;
-  u->time0 = t0 * std::pow(cosmo, 2.0);
+  u->time0 = t0 * (cosmo * cosmo);
   u->velocity0 = l0 / cosmo / t0;
-  u->temp0 = std::pow(l0, 2.0) / std::pow(cosmo, 2.0) / std::pow(t0, 2.0) * m0 / kb;
+  u->temp0 = (l0 * l0) / (cosmo * cosmo) / (t0 * t0) * m0 / kKb;
   u->press0 = d0 * l0 * l0 / (t0 * t0) / std::pow(cosmo, 5.0);
   u->number0 = d0 / std::pow(cosmo, 3.0) / m0;
   u->chem0 = d0 * t0 / cosmo / m0;
-  u->photo0 = t0 * std::pow(cosmo, 2.0);
-  u->cool0 = g1 * std::pow(t0, 3.0) * cosmo * d0 / std::pow(l0, 2.0) / (m0 * m0);
-  u->heat0 = g1 * std::pow(t0, 3.0) * std::pow(cosmo, 4.0) / std::pow(l0, 2.0) / m0;
-  const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
-  u->kappa0 = std::pow(cosmo, 5.0) * std::pow(t0, 3.0) / d0 / std::pow(l0, 4.0) * 0.5 * kappa_coef;
-  const double mfp_coef = (double)0.023f * megapc * 1e-16 * 1e-3;
-  u->meanfreepath0 = std::pow(cosmo, 2.0) * m0 / l0 / d0 * 0.5 * (double)4.2f * mfp_coef;
+  u->photo0 = t0 * (cosmo * cosmo);
+  u->cool0 = g1 * std::pow(t0, 3.0) * cosmo * d0 / (l0 * l0) / (m0 * m0);
+  u->heat0 = g1 * std::pow(t0, 3.0) * std::pow(cosmo, 4.0) / (l0 * l0) / m0;
+  u->kappa0 = std::pow(cosmo, 5.0) * std::pow(t0, 3.0) / d0 / std::pow(l0, 4.0) * 0.5 * kappa_coef();
+  const double mfp_coef = (double)0.023f * kMegapc * 1e-16 * 1e-3;
+  u->meanfreepath0 = (cosmo * cosmo) * m0 / l0 / d0 * 0.5 * (double)4.2f * mfp_coef;
   u->jeans0 = std::sqrt(pi * g * fb);
   u->jeansfloor0 = 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void evora_units_noncomoving(double t, double g, double fb, evora_units* u) {
+  // supercomoving false: h = d0 = t0 = l0 = 1, m0 = kb, cosmo = 1
+  const double b[5] = {1.0, 1.0, 1.0, 1.0, kKb};
+  units_at(b, g, fb, t, 1.0, 0.0, u);
+}
+
+int evora_compunits(const evora_params* p, const evora_time* s, evora_units* u) {
+  if (!p || !u) return EVORA_ERR_ARG;
+  evora_derived d;
+  int rc = evora_compparameter(p, &d);
+  if (rc) return rc;
+  double b[5];
+  unit_bases(p, b);
+  double t = p->tstart, cosmo = 1.0, redshift = 0.0;
+  if (s) {
+    t = s->t;
+    cosmo = s->cosmo;
+    redshift = s->redshift;
+  } else if (p->supercomoving) {
+    cosmo = 1.0 / (1.0 + p->zstart);   // cosmostart (cosmology.f90:32-33)
+    redshift = p->zstart;
+  }
+  units_at(b, d.g, p->fb, t, cosmo, redshift, u);
+  if (p->jeansfloor) {   // units.f90:66-71
+    const double r = d.dx / u->jeans0 / p->c_jeans;
+    u->jeansfloor0 = r * r;
+  }
+  return 0;
 }
 
 int evora_write_units(const char* path, const evora_units* u) {
@@ -417,7 +459,8 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
   rc = snapshot_text(p, G, v, u, k3, what, dir);
   if (rc || !(what & EVORA_SNAP_BOV)) return rc;
   const std::string name = ft::I0(k3, 3);
-  if (!bov_head(p, G, u->t, name, "dens", dir) || !bov_head(p, G, u->t, name, "temp", dir)) return EVORA_ERR_IO;
+  if (!bov_head(p, G, bov_time(p, u), name, "dens", dir) || !bov_head(p, G, bov_time(p, u), name, "temp", dir))
+    return EVORA_ERR_IO;
   const HostGas c = host_gas(p, G);
   const size_t n = (size_t)p->nx * p->ny * p->nz;
   std::vector<float> dens(n), temp(n);
@@ -464,7 +507,8 @@ int evora_grid_snapshot(evora_grid* g, const evora_units* u, int32_t k3, int32_t
   }
   if (!(what & EVORA_SNAP_BOV)) return 0;
   const std::string name = ft::I0(k3, 3);
-  if (!bov_head(p, G, u->t, name, "dens", dir) || !bov_head(p, G, u->t, name, "temp", dir)) return EVORA_ERR_IO;
+  if (!bov_head(p, G, bov_time(p, u), name, "dens", dir) || !bov_head(p, G, bov_time(p, u), name, "temp", dir))
+    return EVORA_ERR_IO;
   const size_t n = (size_t)nx * ny * nz;
   std::vector<float> dens(n), temp(n);
   if ((rc = grid_bov(g, u->temp0, dens.data(), temp.data()))) return rc;

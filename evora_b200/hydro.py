@@ -21,7 +21,7 @@ import ctypes
 
 import numpy as np
 
-from ._native import EvoraDerived, EvoraError, EvoraParams, check, lib
+from ._native import NDUMP, EvoraDerived, EvoraError, EvoraParams, EvoraTime, check, lib
 
 FP64 = 0
 FP32 = 1
@@ -32,14 +32,31 @@ REFERENCE_KERNELS = 4
 
 # ------------------------------------------------------------- parameters --
 def default_params(**overrides) -> EvoraParams:
-    """readparameter defaults (parameter.f90:41-82), then keyword overrides."""
+    """readparameter defaults (parameter.f90:41-82), then keyword overrides.
+    dump_redshift takes a sequence (the rest stays -1, parameter.f90:82)."""
     p = EvoraParams()
     lib().evora_params_default(ctypes.byref(p))
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(f"unknown parameter {k!r}")
+        if k == "dump_redshift":
+            v = list(v)
+            if len(v) > NDUMP:
+                raise ValueError(f"at most {NDUMP} dump redshifts")
+            for i in range(NDUMP):
+                p.dump_redshift[i] = float(v[i]) if i < len(v) else -1.0
+            continue
         setattr(p, k, v)
     return p
+
+
+def _time(s) -> EvoraTime:
+    if isinstance(s, EvoraTime):
+        return s
+    t = EvoraTime()
+    for k, v in dict(s).items():
+        setattr(t, k, float(v))
+    return t
 
 
 def derived(p: EvoraParams) -> EvoraDerived:
@@ -163,6 +180,45 @@ class DropIn:
         check(lib().evora_gravintegration(_ptr(q, self.shape["q"]), self._phi_ptr(phi), float(dt)),
               "gravintegration")
 
+    # comoving time scalars: dicts with the fields of evora_time
+    def cosmostart(self) -> dict:
+        """cosmostart (cosmology.f90:26-36) after compparameter: the time
+        scalars at the start of the run."""
+        s = EvoraTime()
+        check(lib().evora_cosmostart(ctypes.byref(s)), "cosmostart")
+        return s.as_dict()
+
+    def cosmostep(self, s) -> dict:
+        """cosmostep (timestep.f90:59-70): dt = min(a / (da/dt) c_cosmo, dt)."""
+        t = _time(s)
+        check(lib().evora_cosmostep(ctypes.byref(t)), "cosmostep")
+        return t.as_dict()
+
+    def compcosmo(self, s) -> dict:
+        """compcosmo (cosmology.f90:38-51): a advanced over dt."""
+        t = _time(s)
+        check(lib().evora_compcosmo(ctypes.byref(t)), "compcosmo")
+        return t.as_dict()
+
+    def updatetime_cosmo(self, go: bool, s, k: int = 1):
+        """updatetime(go,dump,k), timestep.f90:147-171, both branches;
+        returns (go, dump, time scalars)."""
+        t = _time(s)
+        g, d, kk = ctypes.c_int32(1 if go else 0), ctypes.c_int32(0), ctypes.c_int32(k)
+        check(lib().evora_updatetime_cosmo(ctypes.byref(g), ctypes.byref(d), ctypes.byref(kk),
+                                           ctypes.byref(t)), "updatetime")
+        return bool(g.value), bool(d.value), t.as_dict()
+
+    def settime(self, s):
+        """The time scalars the routines read from module global (dt and
+        expand for expansion, a for the comoving gravity source and the
+        comoving units)."""
+        check(lib().evora_settime(ctypes.byref(_time(s))), "settime")
+
+    def expansion(self, q):
+        """expansion(q), cosmology.f90:53-72, with dt and expand of settime."""
+        check(lib().evora_expansion(_ptr(q, self.shape["q"])), "expansion")
+
 
 # ---------------------------------------------------------- resident grid --
 class Grid:
@@ -251,14 +307,29 @@ class Grid:
                                       ctypes.byref(la)), "grid_timing")
         return dict(update_ms=up.value, cfl_ms=cf.value, steps=n.value, launches=la.value)
 
-    def run(self, max_steps: int = 1 << 30, chunk: int = 64):
-        """Advances until updatetime clears go (or max_steps)."""
+    def cosmo(self):
+        """The time scalars and the pending dump: (dict, k) with k the
+        dump_redshift index whose dump the last step raised (0: none).  A
+        pending dump holds the grid; this call clears it."""
+        s, d = EvoraTime(), ctypes.c_int32()
+        check(lib().evora_grid_cosmo(self._h, ctypes.byref(s), ctypes.byref(d)), "grid_cosmo")
+        return s.as_dict(), d.value
+
+    def run(self, max_steps: int = 1 << 30, chunk: int = 64, on_dump=None):
+        """Advances until updatetime clears go (or max_steps).  With
+        comoving dumps the grid stops at each one: on_dump(grid, k) is called
+        there (the state is the dump's), then the run goes on."""
+        k_start = self.time()["k"]
         done = 0
         while done < max_steps:
-            n = min(chunk, max_steps - done)
-            self.step(n, sync=True)
-            done += n
-            if not self.time()["go"]:
+            self.step(min(chunk, max_steps - done), sync=True)
+            if self.params.supercomoving:
+                _, dump = self.cosmo()
+                if dump and on_dump is not None:
+                    on_dump(self, dump)
+            tm = self.time()
+            done = tm["k"] - k_start   # steps taken (held ones do not count)
+            if not tm["go"]:
                 break
         return self.time()
 

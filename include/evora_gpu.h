@@ -55,7 +55,8 @@ enum evora_status {
   EVORA_ERR_CUDA = 256,           /* CUDA runtime error (see evora_last_error) */
   EVORA_ERR_NOMEM = 512,          /* device allocation failed */
   EVORA_ERR_TIMEOUT = 1024,       /* a bounded host or device wait gave up */
-  EVORA_ERR_IO = 2048             /* a file could not be opened, written or read */
+  EVORA_ERR_IO = 2048,            /* a file could not be opened, written or read */
+  EVORA_ERR_COSMO = 4096          /* timestepiteration did not converge, timestep.f90:220-223 */
 };
 
 /* Number of conserved / primitive / flux fields of the plain build
@@ -63,6 +64,8 @@ enum evora_status {
  * rho*w, E, S = p/rho^(g-1); of w: rho, u, v, w, p. */
 #define EVORA_NQ 6
 #define EVORA_NW 5
+/* Length of dump_redshift (global.f90:137: ndump = 100). */
+#define EVORA_NDUMP 100
 
 /* ------------------------------------------------------------ parameters -- */
 /* The hydro subset of namelist &para (parameter.f90:30-37). */
@@ -93,6 +96,17 @@ typedef struct evora_params {
   double temp_fl;       /* temperature of the floor                         */
   double c_jeans;       /* Jeans floor factor (units.f90:66-71)             */
   double fb;            /* baryon fraction (units: jeans0 = sqrt(pi g fb))  */
+  /* comoving coordinates (cosmology.f90; main.f90:58, 124-136, 178, 184-185) */
+  int32_t supercomoving;  /* Fortran logical: expansion factor a(t) integrated
+                             with the step, comoving units, the expansion
+                             terms (unless atomic) and the comoving source
+                             of gravity                                      */
+  double c_cosmo;         /* expansion time-step factor (cosmostep)          */
+  double omega0, lambda0; /* density and cosmological-constant parameters    */
+  double hubble0, box;    /* H0 in km/s/Mpc; box size in Mpc/h (units)       */
+  double zstart, zend;    /* first and last redshift                         */
+  double dump_redshift[EVORA_NDUMP]; /* redshifts of the intermediate dumps,
+                             in the order they are reached; -1 = unused      */
 } evora_params;
 
 /* The derived constants of compparameter (parameter.f90:164-265) that the
@@ -186,10 +200,12 @@ int evora_thermalconduction(double* q, const double* w, double dt);
  * corrected by the pressure change. */
 int evora_chem(double* q);
 
-/* gravpotential(q,phi), gravitation.f90:26-53, non-comoving branch: the
- * potential of the density of q (FFT Poisson solve with the reference's
- * discrete Green's function).  phi is the reference's complex(8)
- * phi(nx,ny,nz) (interleaved re, im); the imaginary part is written as 0. */
+/* gravpotential(q,phi), gravitation.f90:26-53: the potential of the
+ * density of q (FFT Poisson solve with the reference's discrete Green's
+ * function), from the source 4 pi G (rho - mean rho), or with supercomoving
+ * a (3/2 omega0) (rho / fb - 1) with a from evora_settime.  phi is the
+ * reference's complex(8) phi(nx,ny,nz) (interleaved re, im); the imaginary
+ * part is written as 0. */
 int evora_gravpotential(const double* q, double* phi);
 
 /* gravintegration(q,phi,...), gravitation.f90:170-243, for one process:
@@ -200,8 +216,56 @@ int evora_gravintegration(double* q, const double* phi, double dt);
 /* updatetime(go,dump,k), timestep.f90:147-171, non-comoving branch:
  * if tend - t <= dt then dt = tend - t, go = false; then t = t + dt.
  * dump and k are accepted for signature parity (they only matter in the
- * supercomoving branch, which is outside the hydro path). */
+ * supercomoving branch: evora_updatetime_cosmo). */
 int evora_updatetime(int32_t* go, int32_t* dump, int32_t* k, double* t, double* dt);
+
+/* The time scalars of module global (global.f90:86) that the reference
+ * broadcasts after each time step (bcasttime, parallel.f90:71-95), plus
+ * oldcosmo and cosmodot. */
+typedef struct evora_time {
+  double t, dt;
+  double cosmo;      /* expansion factor a (1 without comoving coordinates) */
+  double oldcosmo;   /* a before the last compcosmo                         */
+  double cosmodot;   /* da/dt                                               */
+  double expand;     /* a da/dt                                             */
+  double redshift;   /* 1/a - 1                                             */
+} evora_time;
+
+/* The comoving time routines of cosmology.f90 and timestep.f90 on the host
+ * (scalar work; the resident layer runs the same arithmetic on the device):
+ *   evora_cosmostart    cosmostart (cosmology.f90:26-36): t = tstart,
+ *                       redshift = zstart, a = 1/(1+zstart), da/dt; without
+ *                       supercomoving a = 1 (compparameter) and the rest 0
+ *   evora_cosmostep     cosmostep (timestep.f90:59-70):
+ *                       dt = min(a / (da/dt) c_cosmo, dt); EVORA_ERR_DT if <= 0
+ *   evora_compcosmo     compcosmo (cosmology.f90:38-51): a advanced over dt by
+ *                       the reference's Runge-Kutta step (rungekutta,
+ *                       cosmology.f90:136-163, including its last stage at
+ *                       the unadvanced a), then da/dt, expand, redshift
+ *   evora_updatetime_cosmo  updatetime (timestep.f90:147-171), both branches;
+ *                       with supercomoving the step is shortened onto zend
+ *                       (go = false) or onto dump_redshift(k) (dump = true)
+ *                       by timestepiteration (timestep.f90:173-226);
+ *                       EVORA_ERR_COSMO if that does not converge.
+ * Parameters come from evora_set_params. */
+int evora_cosmostart(evora_time* s);
+int evora_cosmostep(evora_time* s);
+int evora_compcosmo(evora_time* s);
+int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s);
+
+/* Set the time scalars the drop-in routines read from module global: dt and
+ * expand for evora_expansion, a for the comoving source of
+ * evora_gravpotential, and (with supercomoving) the units that depend on a
+ * (compunits, units.f90:26-73: temp0 for the floors of evora_chem and for
+ * conduction, kappa0).  The reference recomputes them after every
+ * compcosmo (main.f90:132-136). */
+int evora_settime(const evora_time* s);
+
+/* expansion(q), cosmology.f90:53-72: for every cell, pressure(q) (with its
+ * dual-energy write-back), then E -= dt (3g-5) expand p / (g-1) and
+ * S -= dt (3g-5) expand S, with dt and expand from evora_settime.  main.f90
+ * calls it after conduction when supercomoving and not atomic. */
+int evora_expansion(double* q);
 
 /* compevo(w,evo,s), muscl.f90:45-113, with comp_slope (115-169).
  * Fills the slopes s and the half-step predictor evo over the interior plus
@@ -264,6 +328,13 @@ int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync);
 
 /* Time, last step size, go flag and step count (synchronises the stream). */
 int evora_grid_time(evora_grid* g, double* t, double* dt, int32_t* go, int64_t* k);
+
+/* The grid's time scalars (synchronises the stream), and the dump the last
+ * step raised: with supercomoving, a step that updatetime shortened onto
+ * dump_redshift(k) sets *dump = k (1-based; the reference then writes dump
+ * number k, main.f90:197-202), otherwise *dump = 0.  While a dump is
+ * pending the grid does not step; this call clears it. */
+int evora_grid_cosmo(evora_grid* g, evora_time* s, int32_t* dump);
 
 /* Accumulated device error mask (synchronises the stream). */
 int evora_grid_status(evora_grid* g);

@@ -56,6 +56,15 @@ typedef struct evora_units {
  * the parameter file gives it, fb the baryon fraction (default 1). */
 void evora_units_noncomoving(double t, double g, double fb, evora_units* u);
 
+/* compunits (units.f90:26-73), both branches, for the parameters p at the
+ * time state s (t, cosmo, redshift; NULL = tstart, a = 1, z = 0): with
+ * supercomoving the cosmological units at expansion factor a (h =
+ * hubble0/100, d0 = omega0 rhoc h^2, t0 = 1/H0, l0 = box Mpc/h), and the
+ * Jeans floor jeansfloor0 = (dx / jeans0 / c_jeans)^2 when it is on.  g is
+ * the gas constant after compparameter (5/3 with atomic).  EVORA_ERR_ARG for
+ * parameters compparameter rejects. */
+int evora_compunits(const evora_params* p, const evora_time* s, evora_units* u);
+
 /* writeunits (units.f90:76-113) and readunits (units.f90:115-159). */
 int evora_write_units(const char* path, const evora_units* u);
 int evora_read_units(const char* path, evora_units* u);

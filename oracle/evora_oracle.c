@@ -53,7 +53,20 @@ static struct {
   double c_cond, kappa0, temp0;
   int tempfloor, jeansfloor;
   double temp_fl, temp0inv, jeansfloor0;
+  /* comoving coordinates (global.f90:55-57, 86, 137-138) */
+  int supercomoving, atomic;
+  double c_cosmo, omega0, lambda0, zstart, zend, g35;
+  double dump_redshift[EVORA_NDUMP];
+  double u_d0, u_t0, u_l0, u_m0;        /* compunits' d0, t0, l0, m0 */
 } G;
+
+/* The time scalars of module global (global.f90:86): t, dt, cosmo,
+ * oldcosmo, cosmodot, expand, redshift (evora_time's order). */
+static struct {
+  double t, dt, cosmo, oldcosmo, cosmodot, expand, redshift;
+} T;
+
+static const double kKb = 1.3806200e-16;   /* global.f90:103 */
 
 static int orc_err = 0;
 
@@ -85,6 +98,168 @@ int orc_max_threads(void) {
 static inline double fmin2(double a, double b) { return (b < a) ? b : a; }
 static inline double fmax2(double a, double b) { return (b > a) ? b : a; }
 
+/* ------------------------------------------------------------ cosmology -- */
+static inline size_t iq(int i, int j, int k);
+static double orc_pressure(double* q);
+
+/* adot2(a), cosmology.f90:101-109 (a**2.0 = a*a, as gcc folds pow(a, 2.0)). */
+static double adot2(double a) { return G.omega0 * (1.0 / a - 1.0) + G.lambda0 * (a * a - 1.0) + 1.0; }
+
+/* dcosmodt(t, a), cosmology.f90:111-120 (t is not used). */
+static double dcosmodt(double a) { return (a * a) * sqrt(adot2(a)); }
+
+/* rungekutta(f, x, dx, dcosmodt), cosmology.f90:136-163, including its last
+ * stage taken at the unadvanced f. */
+static void rungekutta(double* f, double dx) {
+  const double dfdx1 = dcosmodt(*f);
+  const double dx2 = 0.5 * dx;
+  double ff = *f + dx2 * dfdx1;
+  double dfdx2 = dcosmodt(ff);
+  ff = *f + dx2 * dfdx2;
+  double dfdx3 = dcosmodt(ff);
+  dfdx3 = dfdx2 + dfdx3;
+  dfdx2 = dcosmodt(*f);
+  *f = *f + (dfdx1 + dfdx2 + 2.0 * dfdx3) * dx / 6;
+}
+
+/* cosmostart, cosmology.f90:26-36. */
+static void orc_cosmostart_(void) {
+  T.redshift = G.zstart;
+  T.cosmo = 1 / (1 + G.zstart);
+  T.cosmodot = dcosmodt(T.cosmo);
+}
+
+/* compcosmo, cosmology.f90:38-51. */
+static void orc_compcosmo_(void) {
+  T.oldcosmo = T.cosmo;
+  rungekutta(&T.cosmo, T.dt);
+  T.cosmodot = dcosmodt(T.cosmo);
+  T.expand = T.cosmo * T.cosmodot;
+  T.redshift = 1.0 / T.cosmo - 1.0;
+}
+
+/* cosmostep, timestep.f90:59-70. */
+static void orc_cosmostep_(void) {
+  T.dt = fmin2(T.cosmo / T.cosmodot * G.c_cosmo, T.dt);
+  if (T.dt <= 0.0) set_err(EVORA_ERR_DT);
+}
+
+/* timestepiteration(targetredshift), timestep.f90:173-226. */
+static void orc_timestepiteration_(double targetredshift) {
+  const int cosmoend_nit = 10;
+  const double cosmoend_tol = 1e-20;
+  const double targetcosmo = 1.0 / (1.0 + targetredshift);
+  double l = 0.0, r = T.dt;
+  double fl = targetcosmo - T.oldcosmo, fr = targetcosmo - T.cosmo;
+  int s = 0;
+  for (int i = 1; i <= cosmoend_nit; ++i) {
+    const double m = (fr * l - fl * r) / (fr - fl);
+    if (fabs(r - l) < cosmoend_tol * fabs(r + l)) break;
+    T.dt = m;
+    T.cosmo = T.oldcosmo;
+    orc_compcosmo_();
+    const double fm = targetcosmo - T.cosmo;
+    if (fabs(fm) < cosmoend_tol) break;
+    if (fm * fr > 0.0) {
+      r = m; fr = fm;
+      if (s == -1) fl = fl * 0.5;
+      s = -1;
+    } else if (fl * fm > 0.0) {
+      l = m; fl = fm;
+      if (s == 1) fr = fr * 0.5;
+      s = 1;
+    } else {
+      break;
+    }
+    if (i == cosmoend_nit) set_err(EVORA_ERR_COSMO);
+  }
+}
+
+/* compunits, units.f90:46-63: the units the hydro path reads (temp0,
+ * temp0inv, kappa0) at the current cosmo. */
+static void orc_compunits_(void) {
+  const double c = T.cosmo, t0 = G.u_t0, l0 = G.u_l0;
+  G.temp0 = (l0 * l0) / (c * c) / (t0 * t0) * G.u_m0 / kKb;
+  G.temp0inv = 1.0 / G.temp0;
+  const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
+  G.kappa0 = pow(c, 5.0) * pow(t0, 3.0) / G.u_d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
+}
+
+/* The exported forms: s holds the 7 time scalars (evora_time's order). */
+static void get_time(double* s) {
+  s[0] = T.t; s[1] = T.dt; s[2] = T.cosmo; s[3] = T.oldcosmo; s[4] = T.cosmodot; s[5] = T.expand;
+  s[6] = T.redshift;
+}
+static void put_time(const double* s) {
+  T.t = s[0]; T.dt = s[1]; T.cosmo = s[2]; T.oldcosmo = s[3]; T.cosmodot = s[4]; T.expand = s[5];
+  T.redshift = s[6];
+}
+void orc_get_time(double* s) { get_time(s); }
+void orc_cosmostep(double* s) { put_time(s); orc_cosmostep_(); get_time(s); }
+void orc_compcosmo(double* s) { put_time(s); orc_compcosmo_(); get_time(s); }
+
+/* updatetime(go,dump,k), timestep.f90:147-171, both branches. */
+static void orc_updatetime_(int* go, int* dump, int k) {
+  if (G.supercomoving) {
+    if (T.redshift <= G.zend) {
+      orc_timestepiteration_(G.zend);
+      *go = 0;
+    } else if (k <= EVORA_NDUMP && T.redshift < G.dump_redshift[k - 1]) {
+      orc_timestepiteration_(G.dump_redshift[k - 1]);
+      *dump = 1;
+    }
+  } else if (G.tend - T.t <= T.dt) {
+    T.dt = G.tend - T.t;
+    *go = 0;
+  }
+  T.t = T.t + T.dt;
+}
+
+void orc_updatetime_cosmo(int* go, int* dump, int k, double* s) {
+  put_time(s);
+  orc_updatetime_(go, dump, k);
+  get_time(s);
+}
+
+/* compunits at the scalars s (the units of the step after compcosmo). */
+void orc_settime(const double* s) {
+  put_time(s);
+  orc_compunits_();
+}
+
+void orc_get_units(double* out) {
+  out[0] = G.temp0; out[1] = G.temp0inv; out[2] = G.kappa0;
+}
+
+/* The time scalars at the start of a run: t = tstart, cosmo = 1
+ * (parameter.f90:232-234), cosmostart with supercomoving (main.f90:58), then
+ * compunits (main.f90:62). */
+static void start_time_(void) {
+  memset(&T, 0, sizeof T);
+  T.t = G.tstart;
+  T.cosmo = 1.0;
+  if (G.supercomoving) orc_cosmostart_();
+  orc_compunits_();
+}
+
+/* expansion(q), cosmology.f90:53-72, with dt and expand of the time
+ * scalars. */
+static void orc_expansion_(double* q) {
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double* c = &q[iq(ix, iy, iz)];
+        const double press = orc_pressure(c);
+        c[4] = c[4] - T.dt * G.g35 * T.expand * press / G.g1;
+        c[5] = c[5] - T.dt * G.g35 * T.expand * c[5];
+      }
+}
+
+void orc_expansion(double* q, const double* s) {
+  put_time(s);
+  orc_expansion_(q);
+}
+
 /* compparameter, parameter.f90:164-265 (hydro subset). */
 int orc_compparameter(const evora_params* p) {
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return EVORA_ERR_ARG;
@@ -107,14 +282,22 @@ int orc_compparameter(const evora_params* p) {
   G.conduction = p->conduction != 0;
   G.simplekappa = p->simplekappa != 0;
   G.c_cond = p->c_cond;
-  {
-    /* compunits, units.f90:26-73, without comoving coordinates:
-     * cosmo = h = d0 = t0 = l0 = 1, m0 = kb */
-    const double kb = 1.3806200e-16, cosmo = 1.0, t0 = 1.0, d0 = 1.0, l0 = 1.0, m0 = kb;
-    G.temp0 = pow(l0, 2.0) / pow(cosmo, 2.0) / pow(t0, 2.0) * m0 / kb;
-    const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
-    G.kappa0 = pow(cosmo, 5.0) * pow(t0, 3.0) / d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
-    G.temp0inv = 1.0 / G.temp0;
+  G.supercomoving = p->supercomoving != 0;
+  G.atomic = p->atomic != 0;
+  G.c_cosmo = p->c_cosmo; G.omega0 = p->omega0; G.lambda0 = p->lambda0;
+  G.zstart = p->zstart; G.zend = p->zend;
+  memcpy(G.dump_redshift, p->dump_redshift, sizeof G.dump_redshift);
+  if (G.supercomoving) {
+    /* compunits' bases, units.f90:32-38 (0.01 is single precision) */
+    const double rhoc = 1.88e-29, megapc = 3.08568025e24, kilometer = 1e5, atomicmass = 1.660538782e-24;
+    const double h = p->hubble0 * (double)0.01f;
+    G.u_d0 = p->omega0 * rhoc * pow(h, 2.0);
+    G.u_t0 = 1.0 / (p->hubble0 * kilometer / megapc);
+    G.u_l0 = p->box * megapc / h;
+    G.u_m0 = atomicmass;
+  } else {
+    /* units.f90:39-44: h = d0 = t0 = l0 = 1, m0 = kb */
+    G.u_d0 = 1.0; G.u_t0 = 1.0; G.u_l0 = 1.0; G.u_m0 = kKb;
   }
   G.tempfloor = p->tempfloor != 0;
   G.jeansfloor = p->jeansfloor != 0;
@@ -151,6 +334,8 @@ int orc_compparameter(const evora_params* p) {
     const double jeans0 = sqrt((double)3.1415927f * G.g * p->fb);
     G.jeansfloor0 = p->jeansfloor ? (G.dx / jeans0 / p->c_jeans) * (G.dx / jeans0 / p->c_jeans) : 0.0;
   }
+  G.g35 = 3.0 * G.g - 5.0;                              /* parameter.f90:231 */
+  start_time_();
   return 0;
 }
 
@@ -774,12 +959,16 @@ void orc_updatetime(int* go, double* t, double* dt) {
 }
 
 /* ------------------------------------------------------------- driver -- */
-/* The hydro subset of the time loop of main.f90:109-203 (no gravity,
- * chemistry, expansion, output; thermal conduction when enabled).  Runs until go is cleared,
- * max_steps is reached or an error is raised.  Arrays w, evo, s are
- * scratch of orc_array_sizes() elements, allocated here.  Returns the error
- * mask; *t and *steps report the end state, *dt_last the last step. */
-int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, int* go_out) {
+/* The time loop of main.f90:109-203 without gravity, chemistry species and
+ * output: hydro, the comoving time scalars (cosmostep, compcosmo,
+ * updatetime, compunits), the pressure floors, thermal conduction and the
+ * expansion terms when enabled.  Runs until go is cleared, max_steps is
+ * reached or an error is raised.  Arrays w, evo, s are scratch of
+ * orc_array_sizes() elements, allocated here.  trace (optional) receives 8
+ * values per step: the 7 time scalars after updatetime and the dump number
+ * the step raised (0: none).  Returns the error mask; *t and *steps report
+ * the end state, *dt_last the last step. */
+int orc_run_trace(double* q, int max_steps, double* trace, double* t, int* steps, double* dt_last, int* go_out) {
   int64_t nq, nw, ne, ns;
   orc_array_sizes(&nq, &nw, &ne, &ns);
   double* w = (double*)calloc((size_t)nw, sizeof(double));
@@ -789,34 +978,52 @@ int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, in
     free(w); free(evo); free(s);
     return EVORA_ERR_NOMEM;
   }
-  int go = 1, k = 0;
-  double dt = 0.0;
-  *t = G.tstart;
+  int go = 1, k = 0, k4 = 1;
+  start_time_();
   orc_err = 0;
   while (go && k < max_steps) {
     orc_primitive(w, q);
     orc_bound(w);
-    dt = 1e99;
-    dt = orc_hydrostep(w, dt);
-    if (G.conduction) dt = orc_thermalstep(q, w, dt);      /* main.f90:121 */
-    orc_updatetime(&go, t, &dt);
+    T.dt = 1e99;
+    T.dt = orc_hydrostep(w, T.dt);
+    if (G.conduction) T.dt = orc_thermalstep(q, w, T.dt);  /* main.f90:121 */
     if (orc_err) break;
-    if (G.secondorder) orc_compevo(w, evo, s, dt);
-    orc_sweep(w, q, evo, s, dt);
+    if (G.supercomoving) {                                  /* main.f90:125-128 */
+      orc_cosmostep_();
+      if (orc_err) break;
+      orc_compcosmo_();
+    }
+    int dump = 0;
+    orc_updatetime_(&go, &dump, k4);                        /* main.f90:130 */
+    if (orc_err) break;
+    if (G.supercomoving) orc_compunits_();                  /* main.f90:132-133 */
+    if (G.secondorder) orc_compevo(w, evo, s, T.dt);
+    orc_sweep(w, q, evo, s, T.dt);
     if (G.tempfloor || G.jeansfloor) orc_chem(q);           /* main.f90:167 */
     if (G.conduction) {                                     /* main.f90:169-175 */
       orc_primitive(w, q);
       orc_bound(w);
-      orc_thermalconduction(q, w, dt);
+      orc_thermalconduction(q, w, T.dt);
     }
+    if (G.supercomoving && !G.atomic) orc_expansion_(q);    /* main.f90:178 */
+    if (trace) {
+      get_time(trace + 8 * k);
+      trace[8 * k + 7] = dump ? k4 : 0;
+    }
+    if (dump) k4 = k4 + 1;                                  /* main.f90:197-202 */
     ++k;
     if (orc_err) break;
   }
   free(w); free(evo); free(s);
   *steps = k;
-  *dt_last = dt;
+  *t = T.t;
+  *dt_last = T.dt;
   if (go_out) *go_out = go;
   return orc_err;
+}
+
+int orc_run(double* q, int max_steps, double* t, int* steps, double* dt_last, int* go_out) {
+  return orc_run_trace(q, max_steps, NULL, t, steps, dt_last, go_out);
 }
 
 /* ------------------------------------------------------------------ ICs -- */

@@ -44,12 +44,19 @@ def green(nx: int, ny: int, nz: int, dx: float) -> np.ndarray:
     return g
 
 
-def gravpotential(q: np.ndarray, dx: float) -> np.ndarray:
-    """q of C shape (nz, ny, nx, 6) -> real potential, C shape (nz, ny, nx)."""
+def gravpotential(q: np.ndarray, dx: float, comoving=None) -> np.ndarray:
+    """q of C shape (nz, ny, nx, 6) -> real potential, C shape (nz, ny, nx).
+    comoving = (cosmo, omega0, fb) takes the comoving source
+    cosmo * grav * (rho / fb - 1) with grav = 1.5 omega0 (gravitation.f90:36-37,
+    parameter.f90:236-238)."""
     nz, ny, nx = q.shape[:3]
     rho = q[..., 0]
-    mean = rho.sum() / (nx * ny * nz)
-    src = FOURPIG * (rho - mean)
+    if comoving is not None:
+        cosmo, omega0, fb = comoving
+        src = cosmo * (1.5 * omega0) * (rho / fb - 1.0)
+    else:
+        mean = rho.sum() / (nx * ny * nz)
+        src = FOURPIG * (rho - mean)
     spec = np.fft.fftn(src)
     spec = spec / float(nx * ny * nz) * green(nx, ny, nz, dx)
     # FFTW's backward transform is unnormalised: n3 * numpy's ifftn

@@ -31,6 +31,8 @@ c_int = ctypes.c_int
 c_double = ctypes.c_double
 c_i64 = ctypes.c_int64
 _dp = ctypes.POINTER(ctypes.c_double)
+NDUMP = 100   # EVORA_NDUMP (global.f90:137)
+TIME_FIELDS = ("t", "dt", "cosmo", "oldcosmo", "cosmodot", "expand", "redshift")
 
 
 class OracleParams(ctypes.Structure):
@@ -41,7 +43,7 @@ class OracleParams(ctypes.Structure):
         ("solver", ctypes.c_int32), ("limiter", ctypes.c_int32),
         ("boundtype", ctypes.c_int32), ("secondorder", ctypes.c_int32),
         ("dualenergy", ctypes.c_int32), ("atomic", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("gravity", ctypes.c_int32),
         ("g", c_double), ("cfl", c_double), ("de_thresh", c_double),
         ("xmin", c_double), ("xmax", c_double), ("ymin", c_double),
         ("ymax", c_double), ("zmin", c_double), ("zmax", c_double),
@@ -49,6 +51,9 @@ class OracleParams(ctypes.Structure):
         ("conduction", ctypes.c_int32), ("simplekappa", ctypes.c_int32), ("c_cond", c_double),
         ("tempfloor", ctypes.c_int32), ("jeansfloor", ctypes.c_int32), ("temp_fl", c_double), ("c_jeans", c_double),
         ("fb", c_double),
+        ("supercomoving", ctypes.c_int32), ("c_cosmo", c_double), ("omega0", c_double), ("lambda0", c_double),
+        ("hubble0", c_double), ("box", c_double), ("zstart", c_double), ("zend", c_double),
+        ("dump_redshift", c_double * NDUMP),
     ]
 
 
@@ -93,6 +98,15 @@ def lib():
             L.orc_thermalstep.restype = c_double
             L.orc_thermalconduction.argtypes = [_dp, _dp, c_double]
             L.orc_chem.argtypes = [_dp]
+            L.orc_run_trace.argtypes = [_dp, c_int, _dp, _dp, ctypes.POINTER(c_int), _dp,
+                                        ctypes.POINTER(c_int)]
+            L.orc_get_time.argtypes = [_dp]
+            L.orc_cosmostep.argtypes = [_dp]
+            L.orc_compcosmo.argtypes = [_dp]
+            L.orc_updatetime_cosmo.argtypes = [ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_int, _dp]
+            L.orc_settime.argtypes = [_dp]
+            L.orc_get_units.argtypes = [_dp]
+            L.orc_expansion.argtypes = [_dp, _dp]
             _lib = L
     return _lib
 
@@ -117,7 +131,15 @@ def make_params(**kw) -> OracleParams:
     p.tstart, p.tend = 0.0, 1.0
     p.conduction, p.simplekappa, p.c_cond = 0, 0, float(np.float32(0.1))
     p.tempfloor, p.jeansfloor, p.temp_fl, p.c_jeans, p.fb = 0, 0, 0.0, 0.0, 1.0
+    p.supercomoving, p.c_cosmo = 0, float(np.float32(0.1))
+    p.omega0, p.lambda0, p.hubble0, p.box, p.zstart, p.zend = 1.0, 0.0, 50.0, 1.0, 99.0, 0.0
+    for i in range(NDUMP):
+        p.dump_redshift[i] = -1.0
     for k, v in kw.items():
+        if k == "dump_redshift":
+            for i, z in enumerate(v):
+                p.dump_redshift[i] = float(z)
+            continue
         setattr(p, k, v)
     return p
 
@@ -217,14 +239,59 @@ class Oracle:
         self.L.orc_riemann_single(_ptr(wl), _ptr(wr), _ptr(f), int(direction))
         return f
 
-    def run(self, q, max_steps: int):
-        """The hydro loop of main.f90:109-155 on q (in place).
-        Returns dict(t, steps, dt, go, status)."""
+    def run(self, q, max_steps: int, trace: bool = False):
+        """The loop of main.f90:109-203 on q (in place): hydro, and the
+        comoving time scalars, floors, conduction and expansion terms when
+        enabled.  Returns dict(t, steps, dt, go, status), plus with trace an
+        array (steps, 8): the time scalars after each updatetime (TIME_FIELDS)
+        and the dump number the step raised."""
         t, dt = c_double(0.0), c_double(0.0)
         steps, go = c_int(0), c_int(0)
-        st = self.L.orc_run(_ptr(q), int(max_steps), ctypes.byref(t), ctypes.byref(steps),
-                            ctypes.byref(dt), ctypes.byref(go))
-        return dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), status=int(st))
+        tr = np.zeros((max(int(max_steps), 1), 8)) if trace else None
+        st = self.L.orc_run_trace(_ptr(q), int(max_steps), _ptr(tr) if trace else None, ctypes.byref(t),
+                                  ctypes.byref(steps), ctypes.byref(dt), ctypes.byref(go))
+        out = dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), status=int(st))
+        if trace:
+            out["trace"] = tr[:steps.value].copy()
+        return out
+
+    # -- comoving time scalars (7 values in TIME_FIELDS order) ---------------
+    def time(self):
+        s = np.zeros(7)
+        self.L.orc_get_time(_ptr(s))
+        return s
+
+    def cosmostep(self, s):
+        s = np.array(s, dtype=np.float64)
+        self.L.orc_cosmostep(_ptr(s))
+        return s
+
+    def compcosmo(self, s):
+        s = np.array(s, dtype=np.float64)
+        self.L.orc_compcosmo(_ptr(s))
+        return s
+
+    def updatetime_cosmo(self, go: bool, s, k: int = 1):
+        s = np.array(s, dtype=np.float64)
+        g, d = c_int(1 if go else 0), c_int(0)
+        self.L.orc_updatetime_cosmo(ctypes.byref(g), ctypes.byref(d), int(k), _ptr(s))
+        return bool(g.value), bool(d.value), s
+
+    def settime(self, s):
+        """Sets the time scalars and recomputes the units (compunits)."""
+        s = np.array(s, dtype=np.float64)
+        self.L.orc_settime(_ptr(s))
+
+    def units(self):
+        """(temp0, temp0inv, kappa0) of the last compunits."""
+        u = np.zeros(3)
+        self.L.orc_get_units(_ptr(u))
+        return u
+
+    def expansion(self, q, s):
+        """expansion(q), cosmology.f90:53-72, at the time scalars s."""
+        s = np.array(s, dtype=np.float64)
+        self.L.orc_expansion(_ptr(q), _ptr(s))
 
     # -- initial conditions -------------------------------------------------
     def ic_shocktube(self, dl, ul, pl, dr, ur, pr, x_diss, direction=1):

@@ -5,9 +5,11 @@ TEST INFRASTRUCTURE ONLY.  No Fortran compiler exists on this image, so the
 reference cannot be built as is.  This script reads the reference's own
 sources (module global, compparameter, decomposition, q2w, pressure,
 coordinates, w2n, press2temp, muscl.f90, riemann.f90, boundary.f90,
-hydrostep, updatetime, thermalstep, conduction.f90, compunits, temp2press,
-chem and the shocktube / Kelvin-Helmholtz ICs) and translates the Fortran 90 subset
-they use into C, statement by statement, keeping Fortran semantics:
+hydrostep, cosmostep, updatetime, timestepiteration, thermalstep,
+conduction.f90, compunits, temp2press, chem, the comoving-time routines of
+cosmology.f90 and the shocktube / Kelvin-Helmholtz ICs) and translates the
+Fortran 90 subset they use into C, statement by statement, keeping Fortran
+semantics:
 
   * default-real literals (0.5, 1e6, 3.1415927) are C floats, d-exponent
     literals doubles, so mixed-mode promotion is the Fortran one;
@@ -18,7 +20,10 @@ they use into C, statement by statement, keeping Fortran semantics:
   * arrays are column-major with their declared lower bounds; array-section
     assignments become loops; actual arguments are passed by reference
     (sections by the address of their first element);
-  * MIN/MAX take the next argument when it is smaller/larger.
+  * MIN/MAX take the next argument when it is smaller/larger;
+  * real(8) functions become C functions returning double; an `external`
+    dummy procedure becomes a function pointer, and a function named as an
+    actual argument is passed as one; `exit` leaves the innermost DO.
 
 The output is compiled with gcc -O2 -ffp-contract=off (gfortran -O3 on x86-64
 emits no FMA) together with oracle/ref/harness.c into oracle/_ref/.  Any
@@ -42,7 +47,8 @@ UNITS = [
     ("source/muscl.f90", None, {}),
     ("source/riemann.f90", None, {}),
     ("source/boundary.f90", None, {}),
-    ("source/timestep.f90", ["hydrostep", "updatetime", "thermalstep"], {}),
+    ("source/timestep.f90", ["hydrostep", "cosmostep", "updatetime", "timestepiteration", "thermalstep"], {}),
+    ("source/cosmology.f90", ["cosmostart", "compcosmo", "expansion", "adot2", "dcosmodt", "rungekutta"], {}),
     ("source/conduction.f90", None, {}),
     ("source/units.f90", ["compunits"], {}),
     ("source/chemistry.f90", ["chem"], {}),
@@ -51,8 +57,8 @@ UNITS = [
 ]
 
 # Routines called by the translated code but not translated: the harness
-# provides them (error stop, MPI broadcast no-ops, comoving-time iteration).
-EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "timestepiteration", "cie", "ncie"}
+# provides them (error stop, MPI broadcast no-ops, the species solvers).
+EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "cie", "ncie"}
 
 
 class F2CError(Exception):
@@ -375,8 +381,9 @@ def parse_expr(s):
 
 # ------------------------------------------------------------- symbols ---
 class Sym:
-    def __init__(self, name, ftype, dims=None, param=None, scope="local", dummy=False):
+    def __init__(self, name, ftype, dims=None, param=None, scope="local", dummy=False, external=False):
         self.name = name
+        self.external = external    # a procedure (real(8), external :: f)
         self.ftype = ftype          # int, long, double, float, logical, char, complex
         self.dims = dims or []      # list of (lo_node, hi_node)
         self.param = param          # constant expression node for parameters
@@ -458,13 +465,15 @@ def parse_decl(stmt):
     else:
         attrs_s, ents_s = "", rest
     attrs = split_top(attrs_s.lstrip(","))
-    dims, is_param = None, False
+    dims, is_param, is_ext = None, False, False
     for a in attrs:
         a = a.strip().lower()
         if a.startswith("dimension"):
             dims = parse_dims(a[a.index("(") + 1:a.rindex(")")])
         elif a == "parameter":
             is_param = True
+        elif a == "external":
+            is_ext = True
         elif a.startswith("intent") or a == "allocatable" or a == "save":
             pass
         else:
@@ -483,13 +492,14 @@ def parse_decl(stmt):
         else:
             nm = e
         ents.append((nm.lower(), edims, init))
-    return ftype, is_param, ents
+    return ftype, is_param, ents, is_ext
 
 
 # ----------------------------------------------------------- emitter ---
 class Unit:
-    def __init__(self, name, args, body, renames):
+    def __init__(self, name, args, body, renames, rtype=None):
         self.name = name
+        self.rtype = rtype          # None: subroutine; else the function's result type
         self.args = args
         self.body = body
         self.renames = renames
@@ -500,6 +510,7 @@ class Translator:
         self.module = {}         # name -> Sym
         self.units = []          # Unit
         self.unit_names = set()
+        self.functions = {}      # function unit name -> result type
         self.out = []
         self.tmp = 0
 
@@ -519,7 +530,9 @@ class Translator:
             d = parse_decl(s)
             if not d:
                 raise F2CError(f"module statement {s}")
-            ftype, is_param, ents = d
+            ftype, is_param, ents, is_ext = d
+            if is_ext:
+                raise F2CError(f"external in module {s}")
             for nm, dims, init in ents:
                 self.module[nm] = Sym(nm, ftype, dims, parse_expr(init) if (is_param and init) else None,
                                       scope="module")
@@ -531,20 +544,28 @@ class Translator:
         i = 0
         while i < len(stmts):
             s = stmts[i]
-            m = re.match(r"^subroutine\s+(\w+)\s*(\((.*)\))?\s*$", s, re.I)
+            m = re.match(r"^(?:(real\(8\)|double\s+precision)\s+)?(subroutine|function)\s+(\w+)\s*(\((.*)\))?\s*$",
+                         s, re.I)
             if not m:
                 i += 1
                 continue
-            name = m.group(1).lower()
-            args = [a.strip().lower() for a in (m.group(3) or "").split(",") if a.strip()]
+            kind = m.group(2).lower()
+            if kind == "function" and not m.group(1):
+                raise F2CError(f"function without a real(8) result: {s}")
+            rtype = "double" if kind == "function" else None
+            name = m.group(3).lower()
+            args = [a.strip().lower() for a in (m.group(5) or "").split(",") if a.strip()]
             j = i + 1
             body = []
-            while not re.match(r"^end\s*subroutine\b", stmts[j], re.I) and stmts[j].lower() != "end":
+            while not re.match(r"^end\s*(subroutine|function)\b", stmts[j], re.I) and stmts[j].lower() != "end":
                 body.append(stmts[j])
                 j += 1
             if take is None or name in take:
-                self.units.append(Unit(renames.get(name, name), args, body, renames))
-                self.unit_names.add(renames.get(name, name))
+                uname = renames.get(name, name)
+                self.units.append(Unit(uname, args, body, renames, rtype))
+                self.unit_names.add(uname)
+                if rtype:
+                    self.functions[uname] = rtype
             i = j + 1
 
     # ---- expression typing / emission
@@ -586,6 +607,10 @@ class Translator:
             if s and s.is_array:
                 return s.ftype
             fn = node.name
+            if s and s.external:
+                return s.ftype
+            if fn in self.functions and not s:
+                return self.functions[fn]
             if fn in ("sqrt", "exp", "sin", "cos", "abs"):
                 t = self.etype(node.args[0], local)
                 return "double" if t in ("double",) else ("float" if t == "float" else t)
@@ -657,6 +682,8 @@ class Translator:
                 raise F2CError(f"unknown {node.name}")
             if s.is_array:
                 raise F2CError(f"whole array {node.name} in scalar context")
+            if s.external:
+                raise F2CError(f"procedure {node.name} in an expression")
             if s.dummy:
                 return f"(*v_{s.name})"
             return self.base(s)
@@ -669,6 +696,8 @@ class Translator:
                 lm = loopmap[:len(ranges)] if ranges else None
                 return f"{self.base(s)}[{self.index_expr(s, node.args, lm, local)}]"
             fn = node.name
+            if (s and s.external) or (not s and fn in self.functions):
+                return self.fcall(node, local, loopmap)
             if fn == "sum":
                 # SUM of a whole one-dimensional array, accumulated in
                 # element order (no reassociation without -ffast-math)
@@ -786,20 +815,26 @@ class Translator:
                 execs.append(s)
         nml = {k[6:]: v for k, v in local.items() if k.startswith("__nml_")}
         local = {k: v for k, v in local.items() if not k.startswith("__nml_")}
-        for ftype, is_param, ents in decls:
+        for ftype, is_param, ents, is_ext in decls:
             for nm, dims, init in ents:
                 local[nm] = Sym(nm, ftype, dims, parse_expr(init) if is_param and init else None,
-                                dummy=nm in u.args)
+                                dummy=nm in u.args, external=is_ext)
+        if u.rtype and local.get(u.name) is None:
+            local[u.name] = Sym(u.name, u.rtype)       # the function's result variable
         for a in u.args:
             if local.get(a) is None:
                 raise F2CError(f"undeclared dummy {a} in {u.name}")
         params = []
         for a in u.args:
             s = local[a]
-            params.append(f"{CTYPE[s.ftype]} *v_{a}")
-        self.emit(f"void ref_{u.name}({', '.join(params) or 'void'}) {{", 0)
+            if s.external:
+                params.append(f"{CTYPE[s.ftype]} (*v_{a})()")
+            else:
+                params.append(f"{CTYPE[s.ftype]} *v_{a}")
+        ret = CTYPE[u.rtype] if u.rtype else "void"
+        self.emit(f"{ret} ref_{u.name}({', '.join(params) or 'void'}) {{", 0)
         for nm, s in local.items():
-            if s.dummy:
+            if s.dummy or s.external:
                 continue
             if s.ftype == "char":
                 continue
@@ -817,6 +852,8 @@ class Translator:
             else:
                 self.emit(f"{ct} v_{nm};", 1)
         self.block(execs, local, nml, 1)
+        if u.rtype:
+            self.emit(f"return v_{u.name};", 1)
         self.emit("}", 0)
         self.emit("", 0)
 
@@ -916,6 +953,9 @@ class Translator:
         if low.startswith("print") or low.startswith("write"):
             self.emit("/* " + s.replace("*/", "* /") + " */", ind)
             return
+        if low == "exit":
+            self.emit("break;", ind)
+            return
         if low == "stop" or low.startswith("stop "):
             self.emit("ref_stop();", ind)
             return
@@ -980,6 +1020,9 @@ class Translator:
                 s = self.sym(node.name, local)
                 if s is None:
                     raise F2CError(f"unknown actual {node.name}")
+                if s.external:
+                    args.append(self.proc(s))
+                    continue
                 if s.is_array or s.dummy:
                     args.append(self.base(s) if not s.dummy else f"v_{s.name}")
                 else:
@@ -1003,6 +1046,46 @@ class Translator:
             self.emit("}", ind)
         else:
             self.emit(f"ref_{target}({', '.join(args)});", ind)
+
+    def proc(self, s):
+        """A procedure name as a C function (pointer)."""
+        if s.dummy:
+            return f"v_{s.name}"
+        if s.name not in self.functions:
+            raise F2CError(f"external {s.name} is not a translated function")
+        return f"ref_{s.name}"
+
+    def fcall(self, node, local, loopmap):
+        """A function reference: arguments by address, expressions through
+        compound literals (evaluated before the call, as Fortran does)."""
+        s = self.sym(node.name, local)
+        target = self.proc(s) if s else f"ref_{node.name}"
+        args = []
+        for a in node.args:
+            if isinstance(a, Range):
+                raise F2CError(f"array section passed to function {node.name}")
+            if isinstance(a, Name):
+                sa = self.sym(a.name, local)
+                if sa is None:
+                    raise F2CError(f"unknown actual {a.name}")
+                if sa.external:
+                    args.append(self.proc(sa))
+                    continue
+                if sa.is_array:
+                    args.append(self.base(sa))
+                    continue
+                args.append(f"v_{sa.name}" if sa.dummy else f"&{self.base(sa)}")
+                continue
+            if isinstance(a, Ref):
+                sa = self.sym(a.name, local)
+                if sa and sa.is_array:
+                    if any(isinstance(x, Range) for x in a.args):
+                        raise F2CError(f"array section passed to function {node.name}")
+                    args.append(f"&{self.c(a, local, loopmap)}")
+                    continue
+            t = CTYPE[self.etype(a, local)]
+            args.append(f"&({t}){{{self.c(a, local, loopmap)}}}")
+        return f"{target}({', '.join(args)})"
 
     # ---- whole program
     def module_c(self):
@@ -1049,7 +1132,6 @@ def translate(ref_root):
         "void ref_stop(void);",
         "void ref_cleanstop(void);",
         "void ref_bcastdouble(double*);",
-        "void ref_timestepiteration(double*);",
         "void ref_namelist_ic_para(double*, double*, double*, double*, double*, double*, double*, int*);",
         "static inline double ref_min_double(double a, double b) { return (b < a) ? b : a; }",
         "static inline double ref_max_double(double a, double b) { return (b > a) ? b : a; }",

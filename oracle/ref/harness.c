@@ -3,10 +3,10 @@
  * translation of the reference's Fortran (oracle/_ref/evora_ref.c, made by
  * oracle/ref/f2c.py from the reference sources) the way main.f90 does:
  * namelist values -> compparameter -> decomposition, then the hydro subset
- * of the time loop (main.f90:109-155).  The routines the translation calls
+ * of the time loop (main.f90:109-203).  The routines the translation calls
  * but that are not part of the hydro path (cleanstop, MPI broadcasts, the
- * comoving time iteration) are provided here; a Fortran `stop` returns to
- * the caller through longjmp with a nonzero status.
+ * species solvers) are provided here; a Fortran `stop` returns to the caller
+ * through longjmp with a nonzero status.
  */
 #include <setjmp.h>
 #include <stdint.h>
@@ -25,7 +25,6 @@ void ref_stop(void) {
 }
 void ref_cleanstop(void) { ref_stop(); }
 void ref_bcastdouble(double* x) { (void)x; }
-void ref_timestepiteration(double* z) { (void)z; ref_stop(); }
 /* the species solvers of chem (not reached without chemistry) */
 void ref_cie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
 void ref_ncie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
@@ -64,8 +63,9 @@ int ref_setup_c(const evora_params* p) {
   G_boundtype = p->boundtype;
   G_gravity = 0;
   G_tstart = p->tstart; G_tend = p->tend;
-  G_supercomoving = 0; G_c_cosmo = 0.1f; G_omega0 = 1.0f; G_lambda0 = 0.0f; G_hubble0 = 50.0f;
-  G_fb = 1.0f; G_box = 1.0f; G_zstart = 99.0f; G_zend = 0.0f;
+  G_supercomoving = p->supercomoving; G_c_cosmo = p->c_cosmo; G_omega0 = p->omega0; G_lambda0 = p->lambda0;
+  G_hubble0 = p->hubble0; G_box = p->box; G_zstart = p->zstart; G_zend = p->zend;
+  for (int i = 0; i < EVORA_NDUMP; ++i) G_dump_redshift[i] = p->dump_redshift[i];
   G_chemistry = 0; G_noncie = 0; G_cooling = 0; G_background = 0;
   G_conduction = p->conduction; G_simplekappa = p->simplekappa; G_c_cond = p->c_cond;
   G_tempfloor = p->tempfloor; G_temp_fl = p->temp_fl; G_jeansfloor = p->jeansfloor; G_c_jeans = p->c_jeans;
@@ -73,10 +73,34 @@ int ref_setup_c(const evora_params* p) {
   G_dualenergy = p->dualenergy; G_de_thresh = p->de_thresh;
   G_mpisize = 1; G_mpirank = 0; G_master = 1; G_parallel = 0;
   G_local_x_start = 0; G_local_nx = p->nz;
-  G_redshift = 0.0;
-  GUARD(ref_compparameter(); ref_decomposition(); ref_compunits());
+  /* the time scalars a fresh program starts with (static storage) */
+  G_dt = 0.0; G_redshift = 0.0; G_oldcosmo = 0.0; G_cosmodot = 0.0; G_expand = 0.0;
+  /* main.f90:52-62: compparameter, cosmostart (comoving), compunits */
+  GUARD(ref_compparameter(); ref_decomposition(); if (G_supercomoving) ref_cosmostart(); ref_compunits());
   return 0;
 }
+
+/* The time scalars (evora_time's order) and the units of module global. */
+void ref_get_time_c(double* s) {
+  s[0] = G_t; s[1] = G_dt; s[2] = G_cosmo; s[3] = G_oldcosmo; s[4] = G_cosmodot; s[5] = G_expand;
+  s[6] = G_redshift;
+}
+static void put_time(const double* s) {
+  G_t = s[0]; G_dt = s[1]; G_cosmo = s[2]; G_oldcosmo = s[3]; G_cosmodot = s[4]; G_expand = s[5];
+  G_redshift = s[6];
+}
+void ref_get_units_c(double* u) { u[0] = G_temp0; u[1] = G_temp0inv; u[2] = G_kappa0; }
+
+int ref_cosmostep_c(double* s) { put_time(s); GUARD(ref_cosmostep()); ref_get_time_c(s); return 0; }
+int ref_compcosmo_c(double* s) { put_time(s); GUARD(ref_compcosmo()); ref_get_time_c(s); return 0; }
+int ref_updatetime_cosmo_c(int* go, int* dump, int k, double* s) {
+  put_time(s);
+  GUARD(ref_updatetime(go, dump, &k));
+  ref_get_time_c(s);
+  return 0;
+}
+int ref_settime_c(double* s) { put_time(s); GUARD(ref_compunits()); return 0; }
+int ref_expansion_c(double* q, double* s) { put_time(s); GUARD(ref_expansion(q)); return 0; }
 
 void ref_sizes_c(int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
   *nq = (int64_t)G_nq * G_nx * G_ny * G_nz;
@@ -130,9 +154,12 @@ int ref_thermalconduction_c(double* q, double* w, double dt) {
   return 0;
 }
 
-/* main.f90:109-203 without cooling, gravity, chemistry, expansion or
- * output: hydro and, when enabled, thermal conduction (121, 169-175). */
-int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* go_out) {
+/* main.f90:109-203 without cooling, gravity, chemistry species or output:
+ * hydro and, when enabled, the comoving time scalars (125-136), the
+ * pressure floors (167), thermal conduction (121, 169-175) and the
+ * expansion terms (178).  trace (optional): 8 values per step, the time
+ * scalars after updatetime and the dump number the step raised. */
+int ref_run_trace_c(double* q, int max_steps, double* trace, double* t, int* steps, double* dt, int* go_out) {
   int64_t nq, nw, ne, ns;
   ref_sizes_c(&nq, &nw, &ne, &ns);
   double* w = calloc((size_t)nw, sizeof(double));
@@ -140,19 +167,27 @@ int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* 
   double* s = calloc((size_t)ns, sizeof(double));
   int go = 1, dump = 0, k = 0, k4 = 1, rc = 0;
   G_t = G_tstart;
+  G_cosmo = 1.0; G_oldcosmo = 0.0; G_cosmodot = 0.0; G_expand = 0.0; G_redshift = 0.0;
   if (setjmp(g_jmp)) {
     g_armed = 0;
     rc = 1;
     goto done;
   }
   g_armed = 1;
+  if (G_supercomoving) ref_cosmostart();
+  ref_compunits();
   while (go && k < max_steps) {
     ref_primitive(w, q);
     ref_bound(w);
     G_dt = 1e99;
     if (G_hydro) ref_hydrostep(w);
     if (G_conduction) ref_thermalstep(q, w);
+    if (G_supercomoving) {
+      ref_cosmostep();
+      ref_compcosmo();
+    }
     ref_updatetime(&go, &dump, &k4);
+    if (G_supercomoving) ref_compunits();
     if (G_secondorder) ref_compevo(w, evo, s);
     if (G_hydro) ref_sweep(w, q, evo, s);
     if (G_chemistry || G_tempfloor || G_jeansfloor) ref_chem(q);
@@ -160,6 +195,15 @@ int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* 
       ref_primitive(w, q);
       ref_bound(w);
       ref_thermalconduction(q, w);
+    }
+    if (G_supercomoving && !G_atomic) ref_expansion(q);
+    if (trace) {
+      ref_get_time_c(trace + 8 * k);
+      trace[8 * k + 7] = dump ? k4 : 0;
+    }
+    if (dump) {
+      dump = 0;
+      k4 = k4 + 1;
     }
     k = k + 1;
   }
@@ -184,4 +228,8 @@ int ref_ic_kh_c(double* q) { GUARD(ref_ic_kevinhelmholtz(q)); return 0; }
 int ref_riemann_c(double* wl, double* wr, double* f, int dir) {
   GUARD(ref_riemannsolver(wl, wr, f, &dir));
   return 0;
+}
+
+int ref_run_c(double* q, int max_steps, double* t, int* steps, double* dt, int* go_out) {
+  return ref_run_trace_c(q, max_steps, NULL, t, steps, dt, go_out);
 }

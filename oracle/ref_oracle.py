@@ -51,6 +51,14 @@ def lib():
         L.ref_thermalstep_c.argtypes = [_dp, _dp, _dp]
         L.ref_chem_c.argtypes = [_dp]
         L.ref_thermalconduction_c.argtypes = [_dp, _dp, ctypes.c_double]
+        L.ref_run_trace_c.argtypes = [_dp, ctypes.c_int, _dp, _dp, _ip, _dp, _ip]
+        L.ref_get_time_c.argtypes = [_dp]
+        L.ref_get_units_c.argtypes = [_dp]
+        L.ref_cosmostep_c.argtypes = [_dp]
+        L.ref_compcosmo_c.argtypes = [_dp]
+        L.ref_updatetime_cosmo_c.argtypes = [_ip, _ip, ctypes.c_int, _dp]
+        L.ref_settime_c.argtypes = [_dp]
+        L.ref_expansion_c.argtypes = [_dp, _dp]
         _lib = L
     return _lib
 
@@ -136,12 +144,53 @@ class RefOracle:
         st = self.L.ref_riemann_c(_p(wl), _p(wr), _p(f), int(direction))
         return f, st
 
-    def run(self, q, max_steps):
+    def run(self, q, max_steps, trace=False):
         t, dt = ctypes.c_double(), ctypes.c_double()
         steps, go = ctypes.c_int(), ctypes.c_int()
-        st = self.L.ref_run_c(_p(q), int(max_steps), ctypes.byref(t), ctypes.byref(steps),
-                              ctypes.byref(dt), ctypes.byref(go))
-        return dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), stopped=int(st))
+        tr = np.zeros((max(int(max_steps), 1), 8)) if trace else None
+        st = self.L.ref_run_trace_c(_p(q), int(max_steps), _p(tr) if trace else None, ctypes.byref(t),
+                                    ctypes.byref(steps), ctypes.byref(dt), ctypes.byref(go))
+        out = dict(t=t.value, steps=steps.value, dt=dt.value, go=bool(go.value), stopped=int(st))
+        if trace:
+            out["trace"] = tr[:steps.value].copy()
+        return out
+
+    # -- comoving time scalars (t, dt, cosmo, oldcosmo, cosmodot, expand, redshift)
+    def time(self):
+        s = np.zeros(7)
+        self.L.ref_get_time_c(_p(s))
+        return s
+
+    def units(self):
+        """(temp0, temp0inv, kappa0) of module global."""
+        u = np.zeros(3)
+        self.L.ref_get_units_c(_p(u))
+        return u
+
+    def cosmostep(self, s):
+        s = np.array(s, dtype=np.float64)
+        st = self.L.ref_cosmostep_c(_p(s))
+        return s, st
+
+    def compcosmo(self, s):
+        s = np.array(s, dtype=np.float64)
+        st = self.L.ref_compcosmo_c(_p(s))
+        return s, st
+
+    def updatetime_cosmo(self, go, s, k=1):
+        s = np.array(s, dtype=np.float64)
+        g, d = ctypes.c_int(1 if go else 0), ctypes.c_int(0)
+        st = self.L.ref_updatetime_cosmo_c(ctypes.byref(g), ctypes.byref(d), int(k), _p(s))
+        return bool(g.value), bool(d.value), s, st
+
+    def settime(self, s):
+        """Sets the time scalars and runs compunits."""
+        s = np.array(s, dtype=np.float64)
+        return self.L.ref_settime_c(_p(s))
+
+    def expansion(self, q, s):
+        s = np.array(s, dtype=np.float64)
+        return self.L.ref_expansion_c(_p(q), _p(s))
 
     def ic_shocktube(self, dl, ul, pl, dr, ur, pr, x_diss, direction=1):
         q = self.zeros_q()

@@ -4,6 +4,7 @@ reference (readparameter defaults, compparameter).  No GPU needed."""
 import ctypes
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -34,8 +35,34 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(ev.EvoraParams) == 10 * 4 + 11 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8
+    assert ctypes.sizeof(ev.EvoraParams) == 10 * 4 + 11 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8 + 8 + 7 * 8 + 100 * 8
     assert ctypes.sizeof(ev.EvoraDerived) == 16 * 8 + 2 * 4
+    assert ctypes.sizeof(_native.EvoraTime) == 7 * 8
+
+
+def test_struct_layouts_match_the_c_header(tmp_path):
+    """sizeof and field offsets of the ctypes mirrors against the C compiler's
+    view of include/evora_gpu.h."""
+    checks = {"evora_params": (_native.EvoraParams, ["nz", "gravity", "g", "tend", "fb", "supercomoving",
+                                                     "c_cosmo", "zend", "dump_redshift"]),
+              "evora_time": (_native.EvoraTime, ["t", "redshift"]),
+              "evora_derived": (ev.EvoraDerived, ["volume", "twodimension"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER_DIR}/evora_gpu.h"', "int main(void) {"]
+    for st, (_, fields) in checks.items():
+        lines.append(f'  printf("%zu\\n", sizeof({st}));')
+        for f in fields:
+            lines.append(f'  printf("%zu\\n", offsetof({st}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = []
+    for st, (cls, fields) in checks.items():
+        want.append(ctypes.sizeof(cls))
+        want += [getattr(cls, f).offset for f in fields]
+    assert got == want
 
 
 def test_defaults_follow_readparameter():

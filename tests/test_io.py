@@ -226,8 +226,10 @@ def test_driver_reads_namelist_and_writes_parameter_copy(tmp_path, group):
 def test_driver_refuses_unknown_or_unsupported(tmp_path):
     r = run_print(para_file(tmp_path / "p1", "nx = 8, bogus = 3"))
     assert r.returncode != 0 and "bogus" in r.stderr
-    r = eio.run(para_file(tmp_path / "p2", "nx = 8, ny = 1, nz = 1\nsupercomoving = .true."), tmp_path)
-    assert r.returncode != 0 and "supercomoving" in r.stderr
+    r = eio.run(para_file(tmp_path / "p2", "nx = 8, ny = 1, nz = 1\nchemistry = .true."), tmp_path)
+    assert r.returncode != 0 and "chemistry" in r.stderr
+    r = run_print(para_file(tmp_path / "p3", "nx = 8, dump_redshift = 3.0, x2.0"))
+    assert r.returncode != 0 and "dump_redshift" in r.stderr
     r = eio.run(tmp_path / "missing", tmp_path)
     assert r.returncode != 0 and "not found" in r.stdout
 
