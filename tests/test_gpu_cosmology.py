@@ -221,6 +221,10 @@ def test_driver_comoving_run_writes_the_dumps(cuda_device, tmp_path):
     np.testing.assert_array_equal(out[..., :5], q_end[..., :5])
     u = eio.read_units(tmp_path / "data" / "out.units")
     assert abs(u.redshift - 9.6) < 1e-6
+    # screen fires when tsnap = a * nsnap passes k1, once per step: a = 1/11
+    # at the start gives the lines k1 = 0..9 on steps 1..10
     log = (tmp_path / "data" / "log").read_text().splitlines()
-    assert log and all(len(line) == 4 + 6 + 12 + 12 + 12 + 12 for line in log)
-    assert log[-1].endswith("9.60")
+    assert len(log) == 10 and all(len(line) == 4 + 6 + 12 + 12 + 12 + 12 for line in log)
+    for i, line in enumerate(log):
+        assert int(line[:4]) == i and int(line[4:10]) == i + 1
+        assert abs(float(line[34:46]) - tr[i, 2]) <= 0.5e-4 and abs(float(line[46:58]) - tr[i, 6]) <= 0.5e-2
