@@ -49,10 +49,10 @@ BYTES_PER_CELL = {"f32": 40, "f64": 80}   # 5 fields read + written once
 WORKLOAD = "3D Kelvin-Helmholtz 256^3 periodic, gamma=5/3, HLLC, minmod, CFL 0.5"
 
 
-def kh_params(ev, nz=None, gravity=0, conduction=0, box=1.0):
+def kh_params(ev, nz=None, gravity=0, conduction=0, box=1.0, **extra):
     return ev.default_params(nx=NX, ny=NY, nz=nz or NZ, g=GAMMA, cfl=CFL, boundtype=2, solver=2,
                              limiter=1, tend=1.0e6, gravity=gravity, conduction=conduction,
-                             simplekappa=conduction, xmax=box, ymax=box, zmax=box)
+                             simplekappa=conduction, xmax=box, ymax=box, zmax=box, **extra)
 
 
 def measured_peaks():
@@ -168,9 +168,9 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
-def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0, conduction=0, box=1.0):
+def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0, conduction=0, box=1.0, **extra):
     """Device-timed resident steps; returns (ms_total, kernel timing, grid)."""
-    g = ev.Grid(kh_params(ev, gravity=gravity, conduction=conduction, box=box), precision)
+    g = ev.Grid(kh_params(ev, gravity=gravity, conduction=conduction, box=box, **extra), precision)
     g.set_stream(stream)
     g.set_q(q)
     g.tuning = g.autotune(reps=3) if AUTOTUNE else (0, [])
@@ -378,15 +378,23 @@ COND_BYTES = {"f32": (20 + 8) + (8 + 4 + 4 + 4), "f64": (40 + 8) + (8 + 8 + 8 + 
 # KH box edge for the conduction workload: kappa_eff = 1/(g-1) is explicit,
 # and a 640-unit box keeps its diffusion number near 0.1 at the hydro step
 COND_BOX = 640.0
+# comoving substeps: gravity from the comoving source (no mean-density pass)
+# and the expansion terms (read rho, m, E, write E)
+COMOV_BYTES = {"f32": GRAV_BYTES["f32"] - 4 + (20 + 4), "f64": GRAV_BYTES["f64"] - 8 + (40 + 8)}
+# a comoving run from z = 99 (omega0 = 1): the expansion's step limit
+# (cosmostep) stays far above the hydro step, so both grids take the same dt
+COMOVING = dict(supercomoving=1, omega0=1.0, lambda0=0.0, zstart=99.0, zend=0.0, gravity=1)
 
 
 def run_physics(args, kind):
-    """The KH workload with one more physics substep after every hydro step:
-    gravity (gravitation.f90, non-comoving: FFT Poisson solve with cuFFT
-    D2Z/Z2D in FP64 and the force update) or thermal conduction
-    (conduction.f90 simplekappa, with thermalstep in the CFL kernel).
-    Reports cell-updates/s of whole steps and the substep's time (grid with
-    it minus grid without, same box) against its algorithmic bytes."""
+    """The KH workload with more physics after every hydro step: gravity
+    (gravitation.f90, non-comoving: FFT Poisson solve with cuFFT D2Z/Z2D in
+    FP64 and the force update), thermal conduction (conduction.f90
+    simplekappa, with thermalstep in the CFL kernel), or comoving coordinates
+    (the expansion factor integrated in the control kernel, gravity from the
+    comoving source and the expansion terms, main.f90:124-178).  Reports
+    cell-updates/s of whole steps and the substeps' time (grid with them
+    minus grid without, same box) against their algorithmic bytes."""
     import torch
     import evora_b200 as ev
     world, rank, local = dist_setup(args.gpus)
@@ -394,9 +402,9 @@ def run_physics(args, kind):
     q = ev.ic.kh3d(kh_params(ev), seed=42, amp=0.01)
     n = NX * NY * NZ
     peak, peak_kind = measured_peaks()
-    nbytes = GRAV_BYTES if kind == "gravity" else COND_BYTES
-    box = 1.0 if kind == "gravity" else COND_BOX
-    extra = {"gravity": 1} if kind == "gravity" else {"conduction": 1}
+    nbytes = {"gravity": GRAV_BYTES, "conduction": COND_BYTES, "comoving": COMOV_BYTES}[kind]
+    box = COND_BOX if kind == "conduction" else 1.0
+    extra = {"gravity": {"gravity": 1}, "conduction": {"conduction": 1}, "comoving": COMOVING}[kind]
     out = {}
     barrier(world)
     with ClockSampler(local) as clk:
@@ -418,8 +426,10 @@ def run_physics(args, kind):
                          "gpu_launches": kt_x["launches"]}
     if rank == 0:
         v = out["f32"]
-        what = ("self-gravity after every step (FFT Poisson solve, FP64)" if kind == "gravity" else
-                f"thermal conduction after every step (simplekappa, box {COND_BOX:g})")
+        what = {"gravity": "self-gravity after every step (FFT Poisson solve, FP64)",
+                "conduction": f"thermal conduction after every step (simplekappa, box {COND_BOX:g})",
+                "comoving": "comoving coordinates from z = 99 (omega0 = 1): expansion factor, comoving "
+                            "gravity and expansion terms with every step"}[kind]
         line = {"metric": METRIC, "value": v["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": v["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -546,9 +556,11 @@ def main():
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
-    ap.add_argument("--workload", default="kh3d", choices=["kh3d", "tubes", "serving", "gravity", "conduction"],
+    ap.add_argument("--workload", default="kh3d",
+                    choices=["kh3d", "tubes", "serving", "gravity", "conduction", "comoving"],
                     help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes; serving: request "
-                         "mix; gravity / conduction: the KH benchmark with that substep after every step")
+                         "mix; gravity / conduction / comoving: the KH benchmark with those substeps after every "
+                         "step")
     ap.add_argument("--ntubes", type=int, default=4096)
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--nrequests", type=int, default=400)
@@ -563,7 +575,7 @@ def main():
         return run_tubes(args)
     if args.workload == "serving":
         return run_serving(args)
-    if args.workload in ("gravity", "conduction"):
+    if args.workload in ("gravity", "conduction", "comoving"):
         return run_physics(args, args.workload)
     if args.impl == "reference":
         return run_reference(args)

@@ -54,8 +54,7 @@ __global__ void k_floors(T* __restrict__ q, int64_t n, int nf, HydroParams P, co
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6];
-    for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
-    if (nf == 5) v[5] = 0.0;   // not carried: the S terms are dropped
+    load_cell(q, n, nf, i, v);   // S not carried (nf = 5): the S terms are dropped
     floor_cell(v, P, temp0inv, c, e);
     q[4 * n + i] = (T)v[4];
     if (nf == 6) q[5 * n + i] = (T)v[5];

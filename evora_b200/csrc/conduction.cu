@@ -53,7 +53,7 @@ __global__ void k_cond_prim(T* __restrict__ q, int64_t n, int nf, HydroParams P,
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6], w[5];
-    for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+    load_cell(q, n, nf, i, v);
     q2w(v, w, c, de, e);
     if (de) {
       q[4 * n + i] = (T)v[4];

@@ -47,8 +47,7 @@ __global__ void k_expansion(T* __restrict__ q, int64_t n, int nf, HydroParams P,
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6];
-    for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
-    if (nf == 5) v[5] = 0.0;   // not carried: S never feeds back without dual energy
+    load_cell(q, n, nf, i, v);   // S not carried (nf = 5): it never feeds back without dual energy
     expand_cell(v, k, P, c, e);
     q[4 * n + i] = (T)v[4];
     if (nf == 6) q[5 * n + i] = (T)v[5];

@@ -129,13 +129,14 @@ template <typename T>
 __global__ void k_to_aos(const T* __restrict__ q, double* __restrict__ aos, int64_t n, int nf, double g1) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6];
-    for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+    load_cell(q, n, nf, i, v);
     if (nf == 5) {
       double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
       double kin = 0.5 * m2 / v[0];
       double p = g1 * (v[4] - kin);
       v[5] = p / pow(v[0], g1);
     }
+#pragma unroll
     for (int f = 0; f < EVORA_NQ; ++f) aos[EVORA_NQ * i + f] = v[f];
   }
 }
@@ -150,7 +151,7 @@ __global__ void k_totals_part(const T* __restrict__ q, int64_t n, int nf, int ao
     if (aos) {
       for (int f = 0; f < 6; ++f) v[f] = (double)q[6 * i + f];
     } else {
-      for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+      load_cell(q, n, nf, i, v);
       if (nf == 5) {
         double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
         double p = g1 * (v[4] - 0.5 * m2 / v[0]);
@@ -193,7 +194,7 @@ __device__ __forceinline__ void cell_load(const T* q, int64_t n, int nf, int aos
     for (int f = 0; f < 6; ++f) v[f] = (double)q[6 * i + f];
     return;
   }
-  for (int f = 0; f < nf; ++f) v[f] = (double)q[f * n + i];
+  load_cell(q, n, nf, i, v);
   if (nf == 5) {
     double m2 = (v[1] * v[1]) + (v[2] * v[2]) + (v[3] * v[3]);
     double kin = 0.5 * m2 / v[0];

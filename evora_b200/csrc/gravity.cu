@@ -119,13 +119,17 @@ __global__ void k_green(cufftDoubleComplex* __restrict__ spec, int nxh, int ny, 
 
 // gravintegration + grav_force (gravitation.f90:170-243): periodic centred
 // differences of phi; E gains dt (m . f) with the momentum before its
-// update, then m gains dt rho f.
-template <typename T>
+// update, then m gains dt rho f.  With EXPAND (a comoving step whose next
+// substep is expansion(q), cosmology.f90:53-72, with nothing in between)
+// the cell's expansion terms follow in the same pass: pressure() of the
+// updated cell, E -= dt g35 expand p / g1, S -= dt g35 expand S -- the same
+// per-cell arithmetic as the separate pass, without its trip through HBM.
+template <typename T, bool EXPAND>
 __global__ void k_integrate(T* __restrict__ q, int64_t n, int nf, int aos, const double* __restrict__ phi, int nx,
                             int ny, int nz, double dx2inv, double dy2inv, double dz2inv, const GridCtl* ctl,
-                            double dt_host) {
-  // (the entropy field, when carried, is not touched: gravintegration
-  // updates E and m only)
+                            double dt_host, HydroParams P) {
+  // (the entropy field, when carried, is not touched by gravintegration:
+  // it updates E and m only)
   // 3D launch: x by threads, one (y, z) row per block row
   if (ctl_skip(ctl)) return;
   const double dt = ctl ? ctl->dt : dt_host;
@@ -146,18 +150,30 @@ __global__ void k_integrate(T* __restrict__ q, int64_t n, int nf, int aos, const
       const int zp = iz + 1 == nz ? 0 : iz + 1, zm = iz == 0 ? nz - 1 : iz - 1;
       f3 = -(phi[i + (int64_t)(zp - iz) * nxy] - phi[i + (int64_t)(zm - iz) * nxy]) * dz2inv;
     }
-    double v[5];
+    double v[6];
+#pragma unroll
     for (int f = 0; f < 5; ++f) v[f] = aos ? (double)q[6 * i + f] : (double)q[f * n + i];
     v[4] = v[4] + dt * (v[1] * f1 + v[2] * f2 + v[3] * f3);
     v[1] = v[1] + dt * v[0] * f1;
     v[2] = v[2] + dt * v[0] * f2;
     v[3] = v[3] + dt * v[0] * f3;
+    if (EXPAND) {
+      // grid states only (aos = 0); S is 0 when not carried
+      v[5] = nf == 6 ? (double)q[5 * n + i] : 0.0;
+      unsigned err = 0;
+      const double press = pressure(v, Gas<double>::make(P), P.dualenergy != 0, err);
+      const double k = dt * P.g35 * ctl->expand;
+      v[4] = v[4] - k * press / P.g1;
+      v[5] = v[5] - k * v[5];
+      if (nf == 6) q[5 * n + i] = (T)v[5];
+      if (err) atomicOr(const_cast<unsigned*>(&ctl->err), err);
+    }
+#pragma unroll
     for (int f = 1; f < 5; ++f) {
       if (aos) q[6 * i + f] = (T)v[f];
       else q[f * n + i] = (T)v[f];
     }
   }
-  (void)nf;
 }
 
 }  // namespace
@@ -288,15 +304,20 @@ int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const 
   return 0;
 }
 
-int grav_integrate(GravPlan& g, void* q, bool f32, int nf, int aos, const GridCtl* ctl, double dt_host) {
+int grav_integrate(GravPlan& g, void* q, bool f32, int nf, int aos, const GridCtl* ctl, double dt_host,
+                   const HydroParams* expand) {
   cudaStream_t st = g.stream;
   const dim3 rows((g.nx + kRow - 1) / kRow, g.ny, g.nz);
+  if (expand && (aos || !ctl)) return EVORA_ERR_ARG;   // the fused expansion reads dt, expand from a grid
+  const HydroParams P = expand ? *expand : HydroParams{};
   if (f32) {
-    k_integrate<float><<<rows, kRow, 0, st>>>((float*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv,
-                                              g.dz2inv, ctl, dt_host);
+    auto k = expand ? k_integrate<float, true> : k_integrate<float, false>;
+    k<<<rows, kRow, 0, st>>>((float*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv, g.dz2inv, ctl,
+                             dt_host, P);
   } else {
-    k_integrate<double><<<rows, kRow, 0, st>>>((double*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv,
-                                               g.dz2inv, ctl, dt_host);
+    auto k = expand ? k_integrate<double, true> : k_integrate<double, false>;
+    k<<<rows, kRow, 0, st>>>((double*)q, g.n, nf, aos, g.phi, g.nx, g.ny, g.nz, g.dx2inv, g.dy2inv, g.dz2inv, ctl,
+                             dt_host, P);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

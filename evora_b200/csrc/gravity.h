@@ -44,7 +44,10 @@ int grav_potential(GravPlan& g, const void* q, bool f32, int nf, int aos, const 
 
 // gravintegration (gravitation.f90:170-194) with the forces of grav_force
 // (196-243), in place on the state, with the step's dt from ctl (or dt_host
-// when ctl is null).
-int grav_integrate(GravPlan& g, void* q, bool f32, int nf, int aos, const GridCtl* ctl, double dt_host);
+// when ctl is null).  With `expand` (a grid's parameters; SoA state and ctl
+// required) the comoving step's expansion terms (cosmology.f90:53-72) are
+// applied to each cell in the same pass.
+int grav_integrate(GravPlan& g, void* q, bool f32, int nf, int aos, const GridCtl* ctl, double dt_host,
+                   const HydroParams* expand = nullptr);
 
 }  // namespace evora

@@ -190,6 +190,12 @@ void init_ctl(const evora_grid* g, GridCtl* c) {
 // mean.
 int grav_launches(const evora_grid* g) { return g->gravity ? (g->grav.comoving ? 3 : 5) : 0; }
 
+// The expansion terms run inside the gravity integration's pass when they
+// follow it directly (main.f90:157-178 with neither chem nor conduction).
+bool fused_expansion(const evora_grid* g) {
+  return g->expansion && g->gravity && !g->floors && !g->conduction && !reference_backend(g);
+}
+
 void drop_graphs(evora_grid* g) {
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   g->graphs.clear();
@@ -248,9 +254,13 @@ int enqueue_fused_step(evora_grid* g) {
   mark(g);
   fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
   if (g->gravity) {
-    // gravpotential + gravintegration on the updated state (main.f90:158-165)
+    // gravpotential + gravintegration on the updated state (main.f90:158-165);
+    // with the expansion terms next (no floors or conduction between), they
+    // ride in the integration's pass over the cells
     int rc = grav_potential(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 1.0);
-    if (!rc) rc = grav_integrate(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 0.0);
+    if (!rc)
+      rc = grav_integrate(g->grav, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, 0, g->ctl, 0.0,
+                          fused_expansion(g) ? &g->P : nullptr);
     if (rc) return rc;
     g->launches += grav_launches(g);   // own kernels; cuFFT adds its own
   }
@@ -266,7 +276,7 @@ int enqueue_fused_step(evora_grid* g) {
     if (rc) return rc;
     g->launches += 2;
   }
-  if (g->expansion) {
+  if (g->expansion && !fused_expansion(g)) {
     // expansion terms of E and S (main.f90:178)
     int rc = expansion_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->ctl, st);
     if (rc) return rc;
@@ -568,7 +578,7 @@ int graph_steps(evora_grid* g, int nsteps) {
       g->cur = start ^ (nsteps & 1);
       const bool fused = g->plan.cfl_fused != 0;
       g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + grav_launches(g) + (g->conduction ? 2 : 0) +
-                                       (g->floors ? 1 : 0) + (g->expansion ? 1 : 0)) +
+                                       (g->floors ? 1 : 0) + (g->expansion && !fused_expansion(g) ? 1 : 0)) +
                      (fused && !fresh ? 1 : 0);
       g->cfl_fresh = fused;
     }

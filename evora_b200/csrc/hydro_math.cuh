@@ -99,6 +99,16 @@ __device__ __forceinline__ float dpow(float a, float b) { return std::pow(a, b);
 __device__ __forceinline__ double dsqrt(double a) { return std::sqrt(a); }
 __device__ __forceinline__ float dsqrt(float a) { return std::sqrt(a); }
 
+// The nf (5 or 6) fields of cell i of a SoA state (field stride n) in FP64;
+// a sixth field that is not carried reads as 0.  Fully unrolled, so that v
+// stays in registers (a loop bounded by the runtime nf would index v
+// dynamically and put it in local memory).
+template <typename T>
+__device__ __forceinline__ void load_cell(const T* __restrict__ q, int64_t n, int nf, int64_t i, double v[6]) {
+#pragma unroll
+  for (int f = 0; f < 6; ++f) v[f] = (f < nf) ? (double)q[f * n + i] : 0.0;
+}
+
 // Gas constants in the working precision.
 template <typename T>
 struct Gas {

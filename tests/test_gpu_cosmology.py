@@ -167,6 +167,38 @@ def test_grid_comoving_gravity_step_matches_oracle(cuda_device):
     assert np.max(np.abs(ref[..., 1:4] - q1[..., 1:4])) > 1e-6 * np.max(np.abs(q1[..., 1:4]))
 
 
+@pytest.mark.parametrize("dualenergy", [0, 1], ids=["plain", "dual-energy"])
+def test_grid_comoving_gravity_with_expansion_matches_oracle(cuda_device, dualenergy):
+    """Gravity followed directly by the expansion terms (the grid applies them
+    in the integration's pass): the oracle's hydro step (the step's dt is the
+    hydro limit here, far below cosmostep's), the numpy potential from the
+    comoving source, then the oracle's expansion(q) at the step's time
+    scalars."""
+    from helpers import oracle_step
+    cfg = dict(nx=16, ny=12, nz=10, boundtype=2, dualenergy=dualenergy, de_thresh=0.3)
+    kw = kw_of(cfg, omega0=0.3, lambda0=0.7, fb=0.8)
+    o = Oracle(make_params(**kw))
+    q0 = random_q(o, np.random.default_rng(8))
+    tr = o.run(q0.copy(), 1, trace=True)["trace"]
+    s1 = tr[0, :7]
+    o_h = Oracle(make_params(**{k: v for k, v in kw.items() if k not in COS}, tend=1e6))
+    q1, dt, _ = oracle_step(o_h, q0)
+    assert dt == s1[1]
+    p = ev.default_params(**kw, gravity=1)
+    d = ev.derived(p)
+    ref = go.gravintegration(q1, go.gravpotential(q1, d.dx, comoving=(s1[2], 0.3, 0.8)), dt, d.dx, d.dy, d.dz)
+    o.expansion(ref, s1)
+    with ev.Grid(p, ev.FP64, ev.STRICT | ev.CARRY_ENTROPY) as g:
+        g.set_q(q0)
+        g.step(1)
+        s, _ = g.cosmo()
+        q = g.get_q()
+    np.testing.assert_array_equal([s[f] for f in TIME_FIELDS], s1)
+    np.testing.assert_array_equal(q[..., 0], ref[..., 0])
+    for f in range(6):
+        assert np.max(np.abs(q[..., f] - ref[..., f])) <= 1e-12 * np.max(np.abs(ref[..., f])), f
+
+
 def test_fp32_comoving_grid_tracks_fp64(cuda_device):
     kw = kw_of(dict(nx=32, ny=32, nz=32, boundtype=2))
     o = Oracle(make_params(**kw))
