@@ -131,6 +131,7 @@ def _declare(L):
         "evora_grid_set_tile": ([G, c_int32], c_int32),
         "evora_grid_set_timing": ([G, c_int32], c_int32),
         "evora_grid_timing": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], c_int32),
+        "evora_grid_timing_split": ([G, _dp, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], c_int32),
         "evora_grid_cosmo": ([G, T, ctypes.POINTER(c_int32)], c_int32),
         "evora_cosmostart": ([T], c_int32),
         "evora_cosmostep": ([T], c_int32),
@@ -138,6 +139,7 @@ def _declare(L):
         "evora_updatetime_cosmo": ([ctypes.POINTER(c_int32)] * 3 + [T], c_int32),
         "evora_settime": ([T], c_int32),
         "evora_expansion": ([c_void_p], c_int32),
+        "evora_peebles": ([T, _dp], c_int32),
     }
     optional = set()
     for name, (args, res) in sig.items():

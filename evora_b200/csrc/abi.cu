@@ -458,6 +458,16 @@ int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s
   return (int)e;
 }
 
+int evora_peebles(const evora_time* s, double* fpeebles) {
+  if (!s || !fpeebles) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return EVORA_ERR_ARG;
+  if (!(s->cosmo > 1e-8)) return EVORA_ERR_ARG;   // the integral starts at a = 1e-8
+  *fpeebles = peebles(S.P, s->cosmo);
+  return 0;
+}
+
 int evora_settime(const evora_time* s) {
   if (!s) return EVORA_ERR_ARG;
   DropinState& S = ds();

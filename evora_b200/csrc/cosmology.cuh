@@ -158,6 +158,38 @@ __host__ __device__ inline void updatetime(const HydroParams& P, double tend, co
   s.t = s.t + s.dt;
 }
 
+// peeblesint(a) = adot2(a)^(-3/2) (cosmology.f90:122-132).
+inline double peeblesint(const HydroParams& P, double a) { return std::pow(adot2(P, a), -1.5); }
+
+// trapezoid(int, a, b, delta, f) (cosmology.f90:165-191): steps of delta
+// from a, the last one shortened to end at b.
+template <class F>
+double trapezoid(double a, double b, double delta, F f) {
+  double sum = 0.0, x = a, dx = delta;
+  double fr = f(x);
+  while (x < b) {
+    const double fl = fr;
+    if (x + dx > b) {
+      dx = b - x;
+      x = b;
+    } else {
+      x = x + dx;
+    }
+    fr = f(x);
+    sum = sum + 0.5 * dx * (fl + fr);
+  }
+  return sum;
+}
+
+// peebles(fpeebles) (cosmology.f90:76-97): the linear growth rate
+// d ln D / d ln a at a = cosmo, from the growing mode D ~ adot int da/adot^3.
+inline double peebles(const HydroParams& P, double cosmo) {
+  const double f1 = (P.lambda0 * (cosmo * cosmo) - 0.5 * P.omega0 / cosmo) / adot2(P, cosmo);
+  const double integral = trapezoid(1e-8, cosmo, 1e-8, [&](double a) { return peeblesint(P, a); });
+  const double f2 = cosmo * peeblesint(P, cosmo) / integral;
+  return f1 + f2 - 1.0;
+}
+
 // h, d0, t0, l0, m0 of compunits (units.f90:32-44): the cosmological
 // bases with supercomoving (hubble0 * 0.01 with a single-precision 0.01),
 // else 1, 1, 1, 1, kb.

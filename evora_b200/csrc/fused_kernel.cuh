@@ -90,13 +90,38 @@ __device__ __forceinline__ T ld(const T* p) {
 
 // Primitive variables from conserved ones.  For FP64 this is q2w itself.
 // For FP32 state the pressure p = (g-1)(E - kin) is recovered in FP64 when
-// kin > E/2, where FP32 cancellation would lose more than one bit.
+// kin > E/2, where FP32 cancellation would lose more than one bit; with dual
+// energy pressure() (comp.f90:45-85) runs with kin, the kin/E switch, E - kin
+// and the resynchronised E in FP64, and rho^(g-1) in FP32 (the entropy
+// branch has no cancellation; S is an FP32 field), its write-back rounded to
+// FP32 (q holds 6 fields then).
 template <typename T>
 __device__ __forceinline__ void prim(T* q, T* w, const Gas<T>& c, const HydroParams& P, bool de,
                                      unsigned& err) {
   if constexpr (sizeof(T) == 8) {
     q2w(q, w, c, de, err);
   } else {
+    if (de) {
+      const double m2 = ((double)q[1] * q[1] + (double)q[2] * q[2]) + (double)q[3] * q[3];
+      const double kin = 0.5 * m2 / (double)q[0];
+      const double rg = (double)powf(q[0], c.g1);
+      double pd;
+      if (kin / (double)q[4] > P.de_thresh1) {      // S system
+        pd = (double)q[5] * rg;
+        q[4] = (T)(kin + pd * P.g1inv);
+      } else {                                       // E system
+        pd = P.g1 * ((double)q[4] - kin);
+        q[5] = (T)(pd / rg);
+      }
+      if (pd <= 0.0) err |= EVORA_ERR_PRESSURE;
+      const T densinv = (T)1.0 / q[0];
+      w[0] = q[0];
+      w[1] = q[1] * densinv;
+      w[2] = q[2] * densinv;
+      w[3] = q[3] * densinv;
+      w[4] = (T)pd;
+      return;
+    }
     T densinv = (T)1.0 / q[0];
     w[0] = q[0];
     w[1] = q[1] * densinv;

@@ -52,7 +52,7 @@ struct evora_grid {
   double* aos_stage = nullptr;  // device staging for q in reference layout
   // kernel timing
   bool timing = false;
-  std::vector<cudaEvent_t> events;  // 4 per timed step
+  std::vector<cudaEvent_t> events;  // 5 per timed step
   size_t ev_used = 0;
   int64_t launches = 0;
   // multi-step CUDA graphs, key = 4 * steps + 2 * (CFL maxima fresh) +
@@ -231,6 +231,7 @@ int enqueue_reference_step(evora_grid* g) {
   mark(g);
   if (g->P.secondorder) o.compevo(g->P, g->w, g->evo, g->s, 0.0, g->ctl, st);
   o.sweep(g->P, g->w, g->q_aos, g->evo, g->s, 0.0, &g->ctl->err, g->ctl, st);
+  mark(g);
   if (g->gravity) {
     int rc = grav_potential(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl, 1.0);
     if (!rc) rc = grav_integrate(g->grav, g->q_aos, false, EVORA_NQ, 1, g->ctl, 0.0);
@@ -253,6 +254,7 @@ int enqueue_fused_step(evora_grid* g) {
   k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
   mark(g);
   fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
+  mark(g);
   if (g->gravity) {
     // gravpotential + gravintegration on the updated state (main.f90:158-165);
     // with the expansion terms next (no floors or conduction between), they
@@ -360,10 +362,6 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
   if (reference_backend(g) && precision != EVORA_FP64) {
     delete g;
     return EVORA_ERR_ARG;
-  }
-  if (!reference_backend(g) && p->dualenergy && precision == EVORA_FP32) {
-    delete g;
-    return EVORA_ERR_ARG;  // the dual-energy switch is evaluated in FP64 only
   }
   cudaGetDevice(&g->device);
   g->stream = astream;
@@ -702,25 +700,37 @@ int evora_grid_set_timing(evora_grid* g, int32_t on) {
   return 0;
 }
 
-int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps, int64_t* launches) {
+int evora_grid_timing_split(evora_grid* g, double* cfl_ms, double* update_ms, double* physics_ms, int64_t* steps,
+                            int64_t* launches) {
   if (!g) return EVORA_ERR_ARG;
   CU(cudaStreamSynchronize(g->stream));
-  double up = 0.0, cf = 0.0;
-  const size_t nstep = g->ev_used / 4;
+  // 5 events per timed step: begin | CFL | control | update | physics | end
+  double up = 0.0, cf = 0.0, ph = 0.0;
+  const size_t nstep = g->ev_used / 5;
   for (size_t i = 0; i < nstep; ++i) {
-    float a = 0.f, b = 0.f;
-    CU(cudaEventElapsedTime(&a, g->events[4 * i + 0], g->events[4 * i + 1]));
-    CU(cudaEventElapsedTime(&b, g->events[4 * i + 2], g->events[4 * i + 3]));
+    float a = 0.f, b = 0.f, c = 0.f;
+    CU(cudaEventElapsedTime(&a, g->events[5 * i + 0], g->events[5 * i + 1]));
+    CU(cudaEventElapsedTime(&b, g->events[5 * i + 2], g->events[5 * i + 3]));
+    CU(cudaEventElapsedTime(&c, g->events[5 * i + 3], g->events[5 * i + 4]));
     cf += a;
     up += b;
+    ph += c;
   }
-  if (update_ms) *update_ms = up;
   if (cfl_ms) *cfl_ms = cf;
+  if (update_ms) *update_ms = up;
+  if (physics_ms) *physics_ms = ph;
   if (steps) *steps = (int64_t)nstep;
   if (launches) *launches = g->launches;
   g->ev_used = 0;
   g->launches = 0;
   return 0;
+}
+
+int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps, int64_t* launches) {
+  double up = 0.0, ph = 0.0;
+  const int rc = evora_grid_timing_split(g, cfl_ms, &up, &ph, steps, launches);
+  if (!rc && update_ms) *update_ms = up + ph;
+  return rc;
 }
 
 static int plane_args(evora_grid* g, int32_t axis, int32_t index, PlaneMap* m) {

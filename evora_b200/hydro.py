@@ -209,6 +209,12 @@ class DropIn:
                                            ctypes.byref(t)), "updatetime")
         return bool(g.value), bool(d.value), t.as_dict()
 
+    def peebles(self, s) -> float:
+        """peebles(fpeebles), cosmology.f90:76-97: d ln D / d ln a at s's a."""
+        f = ctypes.c_double()
+        check(lib().evora_peebles(ctypes.byref(_time(s)), ctypes.byref(f)), "peebles")
+        return f.value
+
     def settime(self, s):
         """The time scalars the routines read from module global (dt and
         expand for expansion, a for the comoving gravity source and the
@@ -301,11 +307,14 @@ class Grid:
         check(lib().evora_grid_set_timing(self._h, 1 if on else 0), "grid_set_timing")
 
     def timing(self):
-        up, cf = ctypes.c_double(), ctypes.c_double()
+        """Summed event times since timing was switched on: update_ms is the
+        update and the physics after it (fused_ms and physics_ms apart)."""
+        cf, up, ph = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         n, la = ctypes.c_int64(), ctypes.c_int64()
-        check(lib().evora_grid_timing(self._h, ctypes.byref(up), ctypes.byref(cf), ctypes.byref(n),
-                                      ctypes.byref(la)), "grid_timing")
-        return dict(update_ms=up.value, cfl_ms=cf.value, steps=n.value, launches=la.value)
+        check(lib().evora_grid_timing_split(self._h, ctypes.byref(cf), ctypes.byref(up), ctypes.byref(ph),
+                                            ctypes.byref(n), ctypes.byref(la)), "grid_timing")
+        return dict(update_ms=up.value + ph.value, fused_ms=up.value, physics_ms=ph.value, cfl_ms=cf.value,
+                    steps=n.value, launches=la.value)
 
     def cosmo(self):
         """The time scalars and the pending dump: (dict, k) with k the

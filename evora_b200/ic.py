@@ -135,3 +135,82 @@ def random_tubes(ntubes, seed=7, nmin=128, nmax=4096, gamma=5.0 / 3.0):
         q[:, 5] = p / d ** g1
         parts.append(q)
     return [int(x) for x in lengths], np.ascontiguousarray(np.concatenate(parts))
+
+
+def _kvalue(n):
+    """kvalue (comp.f90:241-252) over the FFT index order: 0, 1, ..., then
+    the negative wavenumbers above the Nyquist index max(n/2, 1)."""
+    nyq = max(n // 2, 1)
+    i = np.arange(1, n + 1)
+    return np.where(i <= nyq, i - 1, -(n - (i - 1))).astype(np.float64)
+
+
+def _sin2(n):
+    """sin^2(kf/2 k) of multigreen (gravitation.f90:55-84), kf = 2 pi / n with
+    module global's single-precision pi (global.f90:98)."""
+    pi = float(np.float32(3.1415927))
+    return np.sin((2.0 * pi / n) * 0.5 * _kvalue(n)) ** 2
+
+
+def cosmo_zeldovich(p: EvoraParams, seed=5, slope=-2.0, sigma=0.05, temp_k=100.0):
+    """A comoving box in the Zel'dovich approximation, built as ic/cosmo.f90
+    builds it (25-180) with a seeded power law in place of its tabulated
+    spectrum:
+
+      white noise / sqrt(n3) -> FFT -> times sqrt(P(k)), P = k^slope with
+      k = |k| 2 pi / box (multipower, gravitation.f90:90-168, k = 0 removed)
+      -> inverse FFT -> density contrast delta, scaled to rms `sigma`;
+      rho = fb (1 + delta) (the baryon fraction applied as ic/pancake.f90:89
+      does, so that the comoving source rho/fb - 1 is delta);
+      phi from delta with multigreen's discrete Green's function;
+      v = fpeebles adot/a (-grad phi), centred periodic differences
+      (grav_force, gravitation.f90:196-243; peebles, cosmology.f90:76-97);
+      T = temp_k (rho/fb)^(g-1) Kelvin, p = rho T / temp0 at the start
+      (press2temp, comp.f90:87-102).
+
+    p must enable supercomoving; the FFTs are numpy's (real-to-complex, which
+    is the reference's complex transform of a real field).  Returns q of shape
+    (nz, ny, nx, 6)."""
+    import ctypes
+
+    from . import _native
+    from ._native import check
+    from .hydro import DropIn
+    if not p.supercomoving:
+        raise ValueError("cosmo_zeldovich needs supercomoving = 1")
+    d = derived(p)
+    nz, ny, nx = p.nz, p.ny, p.nx
+    n3 = nx * ny * nz
+    rng = np.random.default_rng(seed)
+    white = rng.standard_normal((nz, ny, nx)) / np.sqrt(float(n3))
+    spec = np.fft.rfftn(white)
+    kx, ky, kz = _kvalue(nx)[: nx // 2 + 1], _kvalue(ny), _kvalue(nz)
+    k2 = (kx[None, None, :] ** 2 + ky[None, :, None] ** 2) + kz[:, None, None] ** 2
+    kk = np.sqrt(k2) * (2.0 * np.pi / p.box)
+    with np.errstate(divide="ignore"):
+        pk = np.where(k2 > 0, kk ** (0.5 * slope), 0.0)
+    delta = np.fft.irfftn(spec * pk, s=(nz, ny, nx))
+    delta *= sigma / np.sqrt(np.mean(delta * delta))
+    rho = p.fb * (1.0 + delta)
+    green = np.zeros_like(k2)
+    den = (_sin2(nx)[: nx // 2 + 1][None, None, :] + _sin2(ny)[None, :, None]) + _sin2(nz)[:, None, None]
+    green[k2 > 0] = -(d.dx * d.dx / 4.0) / den[k2 > 0]
+    phi = np.fft.irfftn(np.fft.rfftn(delta) * green, s=(nz, ny, nx))
+    drop = DropIn(p)
+    s = drop.cosmostart()
+    vscale = drop.peebles(s) * s["cosmodot"] / s["cosmo"]
+    vel = np.zeros((nz, ny, nx, 3))
+    for ax, (n, h) in enumerate(((nx, d.dx), (ny, d.dy), (nz, d.dz))):
+        if n > 1:
+            axis = 2 - ax
+            vel[..., ax] = -vscale * (np.roll(phi, -1, axis) - np.roll(phi, 1, axis)) * (0.5 / h)
+    u = _native.EvoraUnits()
+    check(_native.lib().evora_compunits(ctypes.byref(p), None, ctypes.byref(u)), "compunits")
+    temp = temp_k * (rho / p.fb) ** d.g1
+    pres = rho * temp / u.temp0
+    q = np.zeros((nz, ny, nx, 6))
+    q[..., 0] = rho
+    q[..., 1:4] = rho[..., None] * vel
+    q[..., 4] = 0.5 * rho * (vel ** 2).sum(-1) + pres / d.g1
+    q[..., 5] = pres / rho ** d.g1
+    return q

@@ -253,6 +253,12 @@ int evora_cosmostep(evora_time* s);
 int evora_compcosmo(evora_time* s);
 int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s);
 
+/* peebles(fpeebles), cosmology.f90:76-97: the linear growth rate
+ * d ln D / d ln a at s->cosmo, by the reference's trapezoid rule (steps of
+ * 1e-8 in a from 1e-8).  The cosmological initial conditions scale their
+ * Zel'dovich velocities with it (ic/cosmo.f90:91-92, ic/pancake.f90:65-66). */
+int evora_peebles(const evora_time* s, double* fpeebles);
+
 /* Set the time scalars the drop-in routines read from module global: dt and
  * expand for evora_expansion, a for the comoving source of
  * evora_gravpotential, and (with supercomoving) the units that depend on a
@@ -353,13 +359,18 @@ int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms
 int evora_grid_set_tile(evora_grid* g, int32_t tile);
 
 /* Kernel timing (no counterpart in the reference): when on, every step
- * records CUDA events around its CFL kernel and its update kernel on the
+ * records CUDA events around its CFL kernel, its update kernel and the
+ * physics after the update (gravity, floors, conduction, expansion) on the
  * grid's stream.  evora_grid_timing synchronises, returns the summed event
- * times in ms, the number of timed steps and the number of kernels the grid
- * launched since timing was switched on, and clears the record. */
+ * times in ms (update_ms: the update and the physics after it), the number
+ * of timed steps and the number of kernels the grid launched since timing
+ * was switched on, and clears the record; evora_grid_timing_split returns
+ * the update and the physics separately. */
 int evora_grid_set_timing(evora_grid* g, int32_t on);
 int evora_grid_timing(evora_grid* g, double* update_ms, double* cfl_ms, int64_t* steps,
                       int64_t* launches);
+int evora_grid_timing_split(evora_grid* g, double* cfl_ms, double* update_ms, double* physics_ms,
+                            int64_t* steps, int64_t* launches);
 
 /* ------------------------------------------------------- batched tubes -- */
 /* No counterpart in the reference (a one-run CLI): many independent 1D

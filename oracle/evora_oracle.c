@@ -122,6 +122,35 @@ static void rungekutta(double* f, double dx) {
   *f = *f + (dfdx1 + dfdx2 + 2.0 * dfdx3) * dx / 6;
 }
 
+/* peeblesint(a), cosmology.f90:122-132. */
+static double peeblesint(double a) { return pow(adot2(a), -1.5); }
+
+/* trapezoid(int, a, b, delta, f), cosmology.f90:165-191. */
+static double trapezoid(double a, double b, double delta, double (*f)(double)) {
+  double sum = 0.0, x = a, dx = delta, fl, fr = f(x);
+  while (x < b) {
+    fl = fr;
+    if (x + dx > b) {
+      dx = b - x;
+      x = b;
+    } else {
+      x = x + dx;
+    }
+    fr = f(x);
+    sum = sum + 0.5 * dx * (fl + fr);
+  }
+  return sum;
+}
+
+/* peebles(fpeebles), cosmology.f90:76-97, at the time scalars s. */
+double orc_peebles(const double* s) {
+  const double cosmo = s[2];
+  const double f1 = (G.lambda0 * (cosmo * cosmo) - 0.5 * G.omega0 / cosmo) / adot2(cosmo);
+  const double integral = trapezoid(1e-8, cosmo, 1e-8, peeblesint);
+  const double f2 = cosmo * peeblesint(cosmo) / integral;
+  return f1 + f2 - 1.0;
+}
+
 /* cosmostart, cosmology.f90:26-36. */
 static void orc_cosmostart_(void) {
   T.redshift = G.zstart;

@@ -107,6 +107,8 @@ def lib():
             L.orc_settime.argtypes = [_dp]
             L.orc_get_units.argtypes = [_dp]
             L.orc_expansion.argtypes = [_dp, _dp]
+            L.orc_peebles.argtypes = [_dp]
+            L.orc_peebles.restype = c_double
             _lib = L
     return _lib
 
@@ -287,6 +289,11 @@ class Oracle:
         u = np.zeros(3)
         self.L.orc_get_units(_ptr(u))
         return u
+
+    def peebles(self, s) -> float:
+        """peebles(fpeebles), cosmology.f90:76-97, at the time scalars s."""
+        s = np.array(s, dtype=np.float64)
+        return float(self.L.orc_peebles(_ptr(s)))
 
     def expansion(self, q, s):
         """expansion(q), cosmology.f90:53-72, at the time scalars s."""

@@ -48,7 +48,8 @@ UNITS = [
     ("source/riemann.f90", None, {}),
     ("source/boundary.f90", None, {}),
     ("source/timestep.f90", ["hydrostep", "cosmostep", "updatetime", "timestepiteration", "thermalstep"], {}),
-    ("source/cosmology.f90", ["cosmostart", "compcosmo", "expansion", "adot2", "dcosmodt", "rungekutta"], {}),
+    ("source/cosmology.f90", ["cosmostart", "compcosmo", "expansion", "peebles", "adot2", "dcosmodt", "peeblesint",
+                              "rungekutta", "trapezoid"], {}),
     ("source/conduction.f90", None, {}),
     ("source/units.f90", ["compunits"], {}),
     ("source/chemistry.f90", ["chem"], {}),
@@ -899,13 +900,12 @@ class Translator:
                 i = j + 1
                 continue
             m_do = re.match(r"^do\s+(\w+)\s*=\s*(.*)$", low)
-            if m_do:
-                var = m_do.group(1)
-                lo, hi = split_top(m_do.group(2))
+            m_while = re.match(r"^do\s+while\s*\(", low)
+            if m_do or m_while:
                 depth, j, seg = 0, i + 1, []
                 while True:
                     t = execs[j].lower()
-                    if re.match(r"^do\s+\w+\s*=", t):
+                    if re.match(r"^do\s+\w+\s*=", t) or re.match(r"^do\s+while\s*\(", t):
                         depth += 1
                     if re.match(r"^end\s*do$", t):
                         if depth == 0:
@@ -913,8 +913,17 @@ class Translator:
                         depth -= 1
                     seg.append(execs[j])
                     j += 1
-                v = self.c(Name(var), local)
-                self.emit(f"for ({v} = {self.c(parse_expr(lo), local)}; {v} <= {self.c(parse_expr(hi), local)}; ++{v}) {{", ind)
+                if m_while:
+                    cond, rest = self.split_if(s[s.lower().index("while"):].replace("while", "if", 1))
+                    if rest:
+                        raise F2CError(f"text after do while: {s}")
+                    self.emit(f"while ({self.c(parse_expr(cond), local)}) {{", ind)
+                else:
+                    var = m_do.group(1)
+                    lo, hi = split_top(m_do.group(2))
+                    v = self.c(Name(var), local)
+                    self.emit(f"for ({v} = {self.c(parse_expr(lo), local)}; {v} <= {self.c(parse_expr(hi), local)}; ++{v}) {{",
+                              ind)
                 self.block(seg, local, nml, ind + 1)
                 self.emit("}", ind)
                 i = j + 1

@@ -100,6 +100,7 @@ int ref_updatetime_cosmo_c(int* go, int* dump, int k, double* s) {
   return 0;
 }
 int ref_settime_c(double* s) { put_time(s); GUARD(ref_compunits()); return 0; }
+int ref_peebles_c(double* s, double* f) { put_time(s); GUARD(ref_peebles(f)); return 0; }
 int ref_expansion_c(double* q, double* s) { put_time(s); GUARD(ref_expansion(q)); return 0; }
 
 void ref_sizes_c(int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {

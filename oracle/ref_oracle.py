@@ -59,6 +59,7 @@ def lib():
         L.ref_updatetime_cosmo_c.argtypes = [_ip, _ip, ctypes.c_int, _dp]
         L.ref_settime_c.argtypes = [_dp]
         L.ref_expansion_c.argtypes = [_dp, _dp]
+        L.ref_peebles_c.argtypes = [_dp, _dp]
         _lib = L
     return _lib
 
@@ -187,6 +188,12 @@ class RefOracle:
         """Sets the time scalars and runs compunits."""
         s = np.array(s, dtype=np.float64)
         return self.L.ref_settime_c(_p(s))
+
+    def peebles(self, s):
+        s = np.array(s, dtype=np.float64)
+        f = ctypes.c_double()
+        st = self.L.ref_peebles_c(_p(s), ctypes.byref(f))
+        return f.value, st
 
     def expansion(self, q, s):
         s = np.array(s, dtype=np.float64)

@@ -85,6 +85,25 @@ def test_time_scalars_match_reference_bitwise(cfg):
 
 
 @needs_ref
+@pytest.mark.parametrize("cfg", COSMO)
+def test_peebles_matches_reference_bitwise(cfg):
+    """peebles (cosmology.f90:76-97, with trapezoid and peeblesint): oracle
+    against the translation, and the library's evora_peebles against the
+    oracle, at the start and at a later a."""
+    o, r = Oracle(cparams(cfg)), RefOracle(cparams(cfg))
+    drop = DropIn(_lib_params(cfg))
+    for a in (1.0 / (1.0 + cfg["zstart"]), 0.05):
+        s = o.time()
+        s[2] = a
+        f_o = o.peebles(s)
+        f_r, st = r.peebles(s)
+        assert st == 0 and f_o == f_r
+        assert drop.peebles(dict(zip(TIME_FIELDS, s))) == f_o
+        if cfg["lambda0"] == 0.0:
+            assert abs(f_o - 1.0) < 1e-4          # Einstein-de Sitter: D ~ a
+
+
+@needs_ref
 @pytest.mark.parametrize("cfg", COSMO[:2])
 def test_expansion_matches_reference_bitwise(cfg):
     for de in (0, 1):

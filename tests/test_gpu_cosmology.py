@@ -199,6 +199,39 @@ def test_grid_comoving_gravity_with_expansion_matches_oracle(cuda_device, dualen
         assert np.max(np.abs(q[..., f] - ref[..., f])) <= 1e-12 * np.max(np.abs(ref[..., f])), f
 
 
+def _low_mode_amplitude(delta):
+    """Sum of |FFT| over the six |k| = 1 modes of a periodic box."""
+    f = np.abs(np.fft.fftn(delta))
+    return sum(f[i] for i in ((0, 0, 1), (0, 0, -1), (0, 1, 0), (0, -1, 0), (1, 0, 0), (-1, 0, 0)))
+
+
+@pytest.mark.parametrize("precision", [ev.FP64, ev.FP32], ids=["fp64", "fp32"])
+def test_zeldovich_box_grows_as_linear_theory(cuda_device, precision):
+    """A cold comoving box from the Zel'dovich IC (ic/cosmo.f90's
+    construction, growing mode) in an Einstein-de Sitter universe, run with
+    comoving gravity and the expansion terms from z = 50 to z = 20: the
+    largest modes of the density contrast grow as the linear growth factor
+    D = a, mass is conserved, and the run stops on zend."""
+    # cold gas (100 K at z = 50): the entropy system of dual energy keeps the
+    # pressure positive where E - kin is below a thousandth of E
+    kw = dict(nx=32, ny=32, nz=32, boundtype=2, g=5 / 3, cfl=0.5, supercomoving=1, gravity=1, omega0=1.0,
+              lambda0=0.0, hubble0=70.0, box=50.0, zstart=50.0, zend=20.0, fb=0.17, c_cosmo=0.02,
+              dualenergy=1, de_thresh=1e-3)
+    p = ev.default_params(**kw)
+    q0 = ev.ic.cosmo_zeldovich(p, seed=3, sigma=0.01)
+    with ev.Grid(p, precision, ev.CARRY_ENTROPY) as g:
+        g.set_q(q0)
+        t = g.run()
+        s, _ = g.cosmo()
+        q = g.get_q()
+    assert not t["go"] and abs(s["redshift"] - 20.0) < 1e-9
+    tol = 1e-12 if precision == ev.FP64 else 1e-5
+    assert abs(q[..., 0].sum() / q0[..., 0].sum() - 1.0) < tol
+    growth = _low_mode_amplitude(q[..., 0] / 0.17 - 1.0) / _low_mode_amplitude(q0[..., 0] / 0.17 - 1.0)
+    expected = (1.0 + 50.0) / (1.0 + 20.0)
+    assert abs(growth / expected - 1.0) < 0.03, (growth, expected, t["k"])
+
+
 def test_fp32_comoving_grid_tracks_fp64(cuda_device):
     kw = kw_of(dict(nx=32, ny=32, nz=32, boundtype=2))
     o = Oracle(make_params(**kw))
@@ -213,6 +246,32 @@ def test_fp32_comoving_grid_tracks_fp64(cuda_device):
     assert abs(out[ev.FP32][2]["redshift"] - 9.6) < 1e-9
     d = np.abs(out[ev.FP32][0][..., :5] - out[ev.FP64][0][..., :5]).max() / np.abs(out[ev.FP64][0][..., :5]).max()
     assert d < 1e-4
+
+
+@pytest.mark.parametrize("shape", [(32, 24, 16), (48, 40, 1)], ids=["3d", "2d"])
+def test_fp32_dual_energy_tracks_fp64(cuda_device, shape):
+    """FP32 state with dual energy (pressure() in FP64 per cell, the E/S
+    write-back rounded to FP32) against the FP64 dual-energy grid, on a
+    state whose thermal energy is a small fraction of E in part of the box,
+    so both systems of the switch are taken."""
+    nx, ny, nz = shape
+    kw = dict(nx=nx, ny=ny, nz=nz, boundtype=2, g=5 / 3, cfl=0.4, tend=1e6, dualenergy=1, de_thresh=0.05)
+    o = Oracle(make_params(**kw))
+    q0 = random_q(o, np.random.default_rng(4), vel=(-3.0, 3.0), pres=(0.01, 1.0))
+    frac = 1.0 - 0.5 * (q0[..., 1:4] ** 2).sum(-1) / q0[..., 0] / q0[..., 4]
+    assert (frac < 0.05).mean() > 0.05 and (frac > 0.05).mean() > 0.5
+    out = {}
+    for prec in (ev.FP64, ev.FP32):
+        with ev.Grid(ev.default_params(**kw), prec) as g:
+            g.set_q(q0)
+            g.step(10)
+            assert g.status() == 0
+            out[prec] = g.get_q()
+    a, b = out[ev.FP32], out[ev.FP64]
+    l1 = np.abs(a[..., 0] - b[..., 0]).sum() / np.abs(b[..., 0]).sum()
+    assert l1 < 1e-5
+    for f in (4, 5):
+        assert np.abs(a[..., f] - b[..., f]).sum() / np.abs(b[..., f]).sum() < 1e-4, f
 
 
 def test_driver_comoving_run_writes_the_dumps(cuda_device, tmp_path):
