@@ -39,6 +39,9 @@ class EvoraParams(ctypes.Structure):
         ("supercomoving", c_int32), ("c_cosmo", c_double), ("omega0", c_double), ("lambda0", c_double),
         ("hubble0", c_double), ("box", c_double), ("zstart", c_double), ("zend", c_double),
         ("dump_redshift", c_double * NDUMP),
+        ("chemistry", c_int32), ("noncie", c_int32), ("cooling", c_int32), ("background", c_int32),
+        ("bg", c_int32), ("cooldt", c_int32), ("j0", c_double), ("c_chem", c_double), ("substep", c_double),
+        ("rhoh", c_double), ("rhohe", c_double), ("c_cooldt", c_double),
     ]
 
     def as_dict(self):
@@ -80,6 +83,7 @@ class EvoraError(RuntimeError):
         1024: "timeout",
         2048: "file i/o",
         4096: "timestepiteration does not converge (timestep.f90:220-223)",
+        8192: "chemistry: abundances out of range or no electron-density root (chemistry.f90, cie.f90)",
     }
 
     def __init__(self, status: int, where: str = ""):
@@ -140,6 +144,7 @@ def _declare(L):
         "evora_settime": ([T], c_int32),
         "evora_expansion": ([c_void_p], c_int32),
         "evora_peebles": ([T, _dp], c_int32),
+        "evora_initchem": ([c_void_p], c_int32),
     }
     optional = set()
     for name, (args, res) in sig.items():

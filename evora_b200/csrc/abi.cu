@@ -10,6 +10,8 @@
 
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
+#include "chem.h"
+#include "chemistry.cuh"
 #include "common.h"
 #include "cosmology.cuh"
 #include "dropin_api.h"
@@ -63,7 +65,19 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
     P->u_d0 = b[1];
     P->u_l04 = std::pow(l0, 4.0);
     P->u_kcoef = kappa_coef();
+    P->u_t0 = t0;
   }
+  // chemistry (parameter.f90:95-104: without it, no background, cooling or
+  // cooling time step; initchem, chemistry.f90:36-37: chiH = rhoH / mH)
+  P->chemistry = p->chemistry != 0;
+  P->cooling = p->chemistry && p->cooling;
+  P->background = p->chemistry && p->background;
+  P->bg = p->bg;
+  P->j0 = p->j0;
+  P->c_chem = p->c_chem;
+  P->substep = p->substep;
+  P->chiH = p->rhoh / kMH;
+  P->chiHe = p->rhohe / kMHe;
   // compunits (units.f90:26-73) at the start of the run (a = 1/(1+zstart)
   // with supercomoving, main.f90:58-62)
   evora_units u;
@@ -145,6 +159,19 @@ void evora_params_default(evora_params* p) {
   p->zstart = 99.0;
   p->zend = 0.0;
   for (int i = 0; i < EVORA_NDUMP; ++i) p->dump_redshift[i] = -1.0;
+  // parameter.f90:66-77
+  p->chemistry = 0;
+  p->noncie = 0;
+  p->cooling = 0;
+  p->background = 0;
+  p->bg = 0;
+  p->j0 = 1e-21;
+  p->c_chem = (double)0.1f;
+  p->substep = (double)0.1f;
+  p->rhoh = (double)0.76f;
+  p->rhohe = (double)0.24f;
+  p->cooldt = 0;
+  p->c_cooldt = 0.0;
 }
 
 int evora_compparameter(const evora_params* p, evora_derived* d) {
@@ -158,6 +185,11 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
   // density that w2n leaves unset without chemistry, and a gradient before
   // it is assigned: only the simplekappa branch is defined in this build
   if (p->conduction && !p->simplekappa) return EVORA_ERR_ARG;
+  // chemistry: the CIE build only.  The non-equilibrium build advects 12
+  // fields through the whole hydro path; conduction with chemistry reads the
+  // electron density that w2n leaves unset in the CIE build (nw = 5,
+  // comp.f90:121-135); the cooling time-step limit (coolstep) is not built.
+  if (p->chemistry && (p->noncie || p->conduction || p->cooldt)) return EVORA_ERR_ARG;
   // parameter.f90:164-265
   double g = p->atomic ? (double)(5.0f / 3.0f) : p->g;
   d->g = g;
@@ -192,7 +224,7 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
 }
 
 void evora_array_sizes(const evora_params* p, int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
-  if (nq) *nq = (int64_t)EVORA_NQ * p->nx * p->ny * p->nz;
+  if (nq) *nq = (int64_t)(p->chemistry ? EVORA_NQ_CHEM : EVORA_NQ) * p->nx * p->ny * p->nz;
   if (nw) *nw = (int64_t)EVORA_NW * (p->nx + 4) * (p->ny + 4) * (p->nz + 4);
   if (ne) *ne = (int64_t)EVORA_NW * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
   if (ns) *ns = (int64_t)EVORA_NW * 3 * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
@@ -209,6 +241,7 @@ struct DropinState {
   evora_params params{};
   HydroParams P{};
   CosmoTime time{};   // module global's time scalars (evora_settime)
+  ChemCoef coef{};    // the chemistry's rate coefficients (coef, uv)
   int strict = 0;
   int device = -1;
   unsigned* d_err = nullptr;
@@ -312,6 +345,14 @@ bool evora::dropin_time(CosmoTime* s) {
   return true;
 }
 
+bool evora::dropin_coef(ChemCoef* k) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return false;
+  *k = S.coef;
+  return true;
+}
+
 extern "C" {
 
 int evora_set_params(const evora_params* p) {
@@ -324,6 +365,7 @@ int evora_set_params(const evora_params* p) {
   S.params = *p;
   S.P = P;
   start_time(p, P, &S.time);
+  start_coef(P, S.time.cosmo, &S.coef);
   S.have_params = true;
   return 0;
 }
@@ -338,6 +380,7 @@ int evora_set_strict(int32_t strict) {
 int evora_primitive(double* w, double* q) {
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
+  if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
   int64_t nq, nw;
@@ -458,6 +501,37 @@ int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s
   return (int)e;
 }
 
+int evora_initchem(double* q) {
+  if (!q) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params || !S.P.chemistry || is_device_pointer(q)) return EVORA_ERR_ARG;
+  // initchem (chemistry.f90:26-70): fully neutral, n(H) = chiH rho,
+  // n(He) = chiHe rho, the other species at nfloor; the pressure() call
+  // there resynchronises E or S with dual energy
+  const HydroParams& P = S.P;
+  const int64_t n = (int64_t)P.nx * P.ny * P.nz;
+  int rc = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double* c = q + (int64_t)EVORA_NQ_CHEM * i;
+    const double m2 = (c[1] * c[1]) + (c[2] * c[2]) + (c[3] * c[3]);
+    const double kin = 0.5 * m2 / c[0];
+    double press;
+    if (P.dualenergy && kin / c[4] > P.de_thresh1) {
+      press = c[5] * std::pow(c[0], P.g1);
+      c[4] = kin + press * P.g1inv;
+    } else {
+      press = P.g1 * (c[4] - kin);
+      if (P.dualenergy) c[5] = press / std::pow(c[0], P.g1);
+    }
+    if (press <= 0.0) rc |= EVORA_ERR_PRESSURE;
+    for (int s = 0; s < 6; ++s) c[EVORA_NQ + s] = kNfloor;
+    c[EVORA_NQ + 0] = P.chiH * c[0];
+    c[EVORA_NQ + 2] = P.chiHe * c[0];
+  }
+  return rc;
+}
+
 int evora_peebles(const evora_time* s, double* fpeebles) {
   if (!s || !fpeebles) return EVORA_ERR_ARG;
   DropinState& S = ds();
@@ -482,6 +556,7 @@ int evora_settime(const evora_time* s) {
     S.P.temp0 = u.temp0;
     S.P.temp0inv = 1.0 / u.temp0;
     S.P.kappa0 = u.kappa0;
+    if (S.P.chemistry) step_coef(S.P, s->cosmo, s->redshift, &S.coef);   // main.f90:134-135
   }
   return 0;
 }
@@ -507,6 +582,7 @@ int evora_compevo(const double* w, double* evo, double* s, double dt) {
 int evora_sweep(const double* w, double* q, const double* evo, const double* s, double dt) {
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
+  if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
   int64_t nq, nw, ne, ns;

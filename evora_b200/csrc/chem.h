@@ -1,4 +1,5 @@
-// chem.h -- the plain-build chem(q) step (pressure floors) for resident grids.
+// chem.h -- the chem(q) step (pressure floors; with the CIE build, the
+// equilibrium species and the cooling) for resident grids.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,10 +8,15 @@
 
 namespace evora {
 
-// chem(q), chemistry.f90:72-121, without species: pressure() (dual-energy
-// write-back), the temperature and Jeans floors and the E and S
-// corrections, in place on a SoA state (nf fields, f32 or f64); errors of
-// pressure() go to ctl->err.
-int chem_floors(const HydroParams& P, void* q, bool f32, int nf, int64_t n, GridCtl* ctl, cudaStream_t st);
+// chem(q), chemistry.f90:72-121, in place on a SoA state (nf fields, f32 or
+// f64) and, with chemistry, its FP64 species (6 field-major arrays of n
+// cells); dt and the rate coefficients from ctl; errors go to ctl->err.
+int chem_step(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
+              cudaStream_t st);
+
+// The rate coefficients at the start of a run (initchem's compcoef, uv = 0)
+// and after a comoving step's compunits (compbackground, compcoef).
+void start_coef(const HydroParams& P, double cosmo, ChemCoef* k);
+void step_coef(const HydroParams& P, double cosmo, double redshift, ChemCoef* k);
 
 }  // namespace evora

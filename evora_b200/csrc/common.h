@@ -30,6 +30,12 @@ struct CosmoTime;
 // run; then evora_settime).  False if no parameters are set.
 bool dropin_time(CosmoTime* s);
 
+struct ChemCoef;
+
+// The chemistry's rate coefficients of the drop-in layer (evora_set_params:
+// the start of the run; evora_settime with comoving coordinates).
+bool dropin_coef(ChemCoef* k);
+
 // t = tstart and cosmo = 1 (compparameter), then cosmostart with
 // supercomoving (main.f90:52-58).
 void start_time(const evora_params* p, const HydroParams& P, CosmoTime* s);

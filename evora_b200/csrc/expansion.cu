@@ -107,6 +107,7 @@ extern "C" int evora_expansion(double* q) {
   HydroParams P;
   CosmoTime s;
   if (!dropin_params(&P) || !dropin_time(&s)) return EVORA_ERR_ARG;
+  if (P.chemistry) return EVORA_ERR_ARG;   // the drop-in reads q(6, ...); grids take q(12, ...)
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_cuda(e, "evora_expansion");

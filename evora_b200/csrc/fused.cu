@@ -117,16 +117,23 @@ void fused_update(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl
 
 namespace {
 
+// q(nq, cell) -> SoA state; with the chemistry build (nq = 12) the species
+// q(7:12) go to their own FP64 field-major array.
 template <typename T>
-__global__ void k_from_aos(const double* __restrict__ aos, T* __restrict__ q, int64_t n, int nf) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    for (int f = 0; f < nf; ++f) q[f * n + i] = (T)aos[EVORA_NQ * i + f];
+__global__ void k_from_aos(const double* __restrict__ aos, T* __restrict__ q, int64_t n, int nf, int nq,
+                           double* __restrict__ species) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int f = 0; f < nf; ++f) q[f * n + i] = (T)aos[(int64_t)nq * i + f];
+    if (species)
+      for (int s = 0; s < nq - EVORA_NQ; ++s) species[s * n + i] = aos[(int64_t)nq * i + EVORA_NQ + s];
+  }
 }
 
 // Without the entropy field, q(6) = p / rho^(g-1) of the current state
 // (the value pressure() would resynchronise it to, comp.f90:66-68).
 template <typename T>
-__global__ void k_to_aos(const T* __restrict__ q, double* __restrict__ aos, int64_t n, int nf, double g1) {
+__global__ void k_to_aos(const T* __restrict__ q, double* __restrict__ aos, int64_t n, int nf, double g1, int nq,
+                         const double* __restrict__ species) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v[6];
     load_cell(q, n, nf, i, v);
@@ -137,7 +144,9 @@ __global__ void k_to_aos(const T* __restrict__ q, double* __restrict__ aos, int6
       v[5] = p / pow(v[0], g1);
     }
 #pragma unroll
-    for (int f = 0; f < EVORA_NQ; ++f) aos[EVORA_NQ * i + f] = v[f];
+    for (int f = 0; f < EVORA_NQ; ++f) aos[(int64_t)nq * i + f] = v[f];
+    if (species)
+      for (int s = 0; s < nq - EVORA_NQ; ++s) aos[(int64_t)nq * i + EVORA_NQ + s] = species[s * n + i];
   }
 }
 
@@ -288,16 +297,18 @@ void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams&
   else k_bov<double><<<grid_of(n), 256, 0, st>>>((double*)q, n, nf, aos, P, temp0, dens, temp, err);
 }
 
-void fused_from_aos(const FusedPlan& pl, const double* aos, void* q, cudaStream_t st) {
-  if (pl.precision == EVORA_FP32) k_from_aos<float><<<grid_of(pl.n), 256, 0, st>>>(aos, (float*)q, pl.n, pl.nf);
-  else k_from_aos<double><<<grid_of(pl.n), 256, 0, st>>>(aos, (double*)q, pl.n, pl.nf);
+void fused_from_aos(const FusedPlan& pl, const double* aos, void* q, cudaStream_t st, int nq, double* species) {
+  if (pl.precision == EVORA_FP32)
+    k_from_aos<float><<<grid_of(pl.n), 256, 0, st>>>(aos, (float*)q, pl.n, pl.nf, nq, species);
+  else
+    k_from_aos<double><<<grid_of(pl.n), 256, 0, st>>>(aos, (double*)q, pl.n, pl.nf, nq, species);
 }
 
-void fused_to_aos(const FusedPlan& pl, const void* q, double* aos, cudaStream_t st) {
+void fused_to_aos(const FusedPlan& pl, const void* q, double* aos, cudaStream_t st, int nq, const double* species) {
   if (pl.precision == EVORA_FP32)
-    k_to_aos<float><<<grid_of(pl.n), 256, 0, st>>>((const float*)q, aos, pl.n, pl.nf, pl.P.g1);
+    k_to_aos<float><<<grid_of(pl.n), 256, 0, st>>>((const float*)q, aos, pl.n, pl.nf, pl.P.g1, nq, species);
   else
-    k_to_aos<double><<<grid_of(pl.n), 256, 0, st>>>((const double*)q, aos, pl.n, pl.nf, pl.P.g1);
+    k_to_aos<double><<<grid_of(pl.n), 256, 0, st>>>((const double*)q, aos, pl.n, pl.nf, pl.P.g1, nq, species);
 }
 
 static int totals_run(const void* q, bool f32, int64_t n, int nf, int aos, double g1, double* part, int nb,

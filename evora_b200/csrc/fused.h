@@ -55,8 +55,12 @@ void fused_update(const FusedPlan& plan, const void* qin, void* qout, GridCtl* c
 // Layout conversions between the reference q(6, nx, ny, nz) (FP64) and the
 // resident SoA state.  Without the entropy field, q(6) is written as
 // p / rho^(g-1) of the current state.
-void fused_from_aos(const FusedPlan& plan, const double* aos, void* q, cudaStream_t st);
-void fused_to_aos(const FusedPlan& plan, const void* q, double* aos, cudaStream_t st);
+// q(nq, cell) in the reference layout <-> the SoA state; with nq = 12
+// (chemistry) q(7:12) <-> `species` (6 FP64 fields, field-major).
+void fused_from_aos(const FusedPlan& plan, const double* aos, void* q, cudaStream_t st, int nq = EVORA_NQ,
+                    double* species = nullptr);
+void fused_to_aos(const FusedPlan& plan, const void* q, double* aos, cudaStream_t st, int nq = EVORA_NQ,
+                  const double* species = nullptr);
 
 // Sums of q(1..6) over the grid in FP64, deterministic order (synchronises).
 int fused_totals(const FusedPlan& plan, const void* q, double out[6], cudaStream_t st);

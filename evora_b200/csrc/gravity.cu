@@ -360,6 +360,7 @@ DropinGrav& dg() {
 
 int dropin_prepare(DropinGrav& D, HydroParams* P) {
   if (!dropin_params(P)) return EVORA_ERR_ARG;
+  if (P->chemistry) return EVORA_ERR_ARG;   // the drop-in reads q(6, ...); grids take q(12, ...)
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return EVORA_ERR_CUDA;
   const int64_t n = (int64_t)P->nx * P->ny * P->nz;

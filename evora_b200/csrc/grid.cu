@@ -19,6 +19,7 @@
 
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
+#include "chemistry.cuh"
 #include "common.h"
 #include "cosmology.cuh"
 #include "dropin_api.h"
@@ -67,8 +68,10 @@ struct evora_grid {
   // thermal conduction after each step (params.conduction)
   bool conduction = false;
   CondPlan cond{};
-  // pressure floors after each step (params.tempfloor / jeansfloor)
+  // chem(q) after each step (params.chemistry / tempfloor / jeansfloor)
   bool floors = false;
+  // with chemistry: n(H, H+, He, He+, He++, e-), 6 FP64 field-major arrays
+  double* species = nullptr;
   // comoving coordinates: expansion terms after each step (params.supercomoving
   // and not atomic)
   bool expansion = false;
@@ -152,6 +155,10 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
     ctl->temp0 = u.temp0;
     ctl->temp0inv = u.temp0inv;
     ctl->kappa0 = u.kappa0;
+    if (P.chemistry) {   // compbackground and compcoef (main.f90:134-135)
+      const double uv = compbackground(P.background, P.bg, P.j0, s.redshift, s.cosmo, ctl->coef.uv);
+      compcoef(chem_units(P, s.cosmo), uv, ctl->coef);
+    }
     if (dump) {   // main.f90:197-202: dump number k4, then k4 + 1
       ctl->dump = ctl->k4;
       ctl->k4 += 1;
@@ -183,6 +190,7 @@ void init_ctl(const evora_grid* g, GridCtl* c) {
   c->kappa0 = g->P.kappa0;
   c->k4 = 1;
   std::memcpy(c->dump_redshift, g->params.dump_redshift, sizeof c->dump_redshift);
+  if (g->P.chemistry) start_coef(g->P, s.cosmo, &c->coef);
 }
 
 // Own kernels of one gravity substep: the mean density (two), the source,
@@ -267,8 +275,9 @@ int enqueue_fused_step(evora_grid* g) {
     g->launches += grav_launches(g);   // own kernels; cuFFT adds its own
   }
   if (g->floors) {
-    // chem(q) of the plain build: pressure floors (main.f90:167)
-    int rc = chem_floors(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->ctl, st);
+    // chem(q): the CIE species and cooling, and the pressure floors (main.f90:167)
+    int rc = chem_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl,
+                       st);
     if (rc) return rc;
     g->launches += 1;
   }
@@ -320,8 +329,12 @@ void free_grid(evora_grid* g) {
   dfree(g, g->qbuf[0]);
   dfree(g, g->qbuf[1]);
   dfree(g, g->aos_stage);
+  dfree(g, g->species);
   delete g;
 }
+
+// Values per cell of q in the reference layout (12 with chemistry).
+int nq_of(const evora_grid* g) { return g->params.chemistry ? EVORA_NQ_CHEM : EVORA_NQ; }
 
 int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStream_t astream, evora_grid** out);
 int graph_steps(evora_grid* g, int nsteps);
@@ -387,13 +400,14 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
       return rc;
     }
   }
-  if (p->tempfloor || p->jeansfloor) {
+  if (p->chemistry || p->tempfloor || p->jeansfloor) {
     if (reference_backend(g)) {
       free_grid(g);
-      return EVORA_ERR_ARG;   // the floors run on the resident SoA state
+      return EVORA_ERR_ARG;   // chem(q) runs on the resident SoA state
     }
     g->floors = true;
     g->plan.cfl_fused = 0;     // the state changes after the update
+    if (p->chemistry && dalloc(g, (void**)&g->species, sizeof(double) * 6 * ncells(g)) != cudaSuccess) goto nomem;
   }
   if (p->conduction) {
     if (reference_backend(g)) {
@@ -482,7 +496,7 @@ int evora_grid_set_q(evora_grid* g, const double* q) {
       src = g->aos_stage;
     }
     g->cur = 0;
-    fused_from_aos(g->plan, src, g->qbuf[0], g->stream);
+    fused_from_aos(g->plan, src, g->qbuf[0], g->stream, nq_of(g), g->species);
   }
   g->cfl_fresh = false;
   GridCtl c;
@@ -506,7 +520,7 @@ int evora_grid_get_q(evora_grid* g, double* q) {
       if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
       dst = g->aos_stage;
     }
-    fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream);
+    fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream, nq_of(g), g->species);
     if (!dev) CU(cudaMemcpyAsync(q, dst, nq * 8, cudaMemcpyDeviceToHost, g->stream));
   }
   CU(cudaStreamSynchronize(g->stream));

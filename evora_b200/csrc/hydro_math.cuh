@@ -27,6 +27,15 @@
 
 namespace evora {
 
+// coef(ncool, 2) of module global (rates.f90:26-78): c[i][0] = coef(i+1, 1)
+// (chemical), c[i][1] = coef(i+1, 2) (cooling); uv = the background J
+// (compbackground, chemistry.f90:123-157).
+constexpr int kNcool = 13;
+struct ChemCoef {
+  double c[kNcool][2];
+  double uv;
+};
+
 // Step control block of a resident grid, in device memory.  Kernels of a
 // step read dt from here and return at once when the step is inactive
 // (go was already false, or an error was raised earlier).
@@ -47,6 +56,7 @@ struct GridCtl {
   int dump;      // dump_redshift index whose dump the last step raised (0: none)
   int k4;        // the next dump_redshift index updatetime tests (main.f90:33)
   double dump_redshift[EVORA_NDUMP];
+  ChemCoef coef;   // the chemistry's rate coefficients of the current step
 };
 
 __device__ __forceinline__ bool ctl_skip(const GridCtl* ctl) {
@@ -74,8 +84,11 @@ struct HydroParams {
   double gravc;                   // grav = 1.5 omega0 (parameter.f90:236-238)
   double fb;
   // a-independent factors of the comoving units (units.f90:32-63): l0^2,
-  // t0^2, m0, t0^3, d0, l0^4 and kappa_coef
-  double u_l02, u_t02, u_m0, u_t03, u_d0, u_l04, u_kcoef;
+  // t0^2, m0, t0^3, d0, l0^4, kappa_coef and t0
+  double u_l02, u_t02, u_m0, u_t03, u_d0, u_l04, u_kcoef, u_t0;
+  // chemistry of the CIE build (chemistry.f90, cie.f90, rates.f90)
+  int chemistry, cooling, background, bg;
+  double j0, c_chem, substep, chiH, chiHe;
 };
 
 // The units a kernel uses: the grid's current ones when the run is comoving

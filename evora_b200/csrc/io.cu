@@ -449,6 +449,7 @@ int evora_read_units(const char* path, evora_units* u) {
 int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32_t k3, int32_t what,
                    const char* dir) {
   if (!p || !q || !u || k3 < 0) return EVORA_ERR_ARG;
+  if (p->chemistry) return EVORA_ERR_ARG;   // the writers take q(6, ...) and T without species
   Geometry G;
   int rc = geometry(p, &G);
   if (rc) return rc;
@@ -478,6 +479,7 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
 int evora_grid_snapshot(evora_grid* g, const evora_units* u, int32_t k3, int32_t what, const char* dir) {
   if (!g || !u || k3 < 0) return EVORA_ERR_ARG;
   const evora_params* p = grid_params(g);
+  if (p->chemistry) return EVORA_ERR_ARG;   // temperatures without species
   Geometry G;
   int rc = geometry(p, &G);
   if (rc) return rc;

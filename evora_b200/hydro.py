@@ -67,8 +67,11 @@ def derived(p: EvoraParams) -> EvoraDerived:
 
 
 def shapes(p: EvoraParams):
+    """C shapes of the reference arrays: q has 12 values per cell with
+    chemistry (q(7:12) = the species of the CIE build), else 6."""
     nx, ny, nz = p.nx, p.ny, p.nz
-    return dict(q=(nz, ny, nx, 6), w=(nz + 4, ny + 4, nx + 4, 5),
+    nq = 12 if p.chemistry else 6
+    return dict(q=(nz, ny, nx, nq), w=(nz + 4, ny + 4, nx + 4, 5),
                 evo=(nz + 2, ny + 2, nx + 2, 5), s=(nz + 2, ny + 2, nx + 2, 3, 5))
 
 
@@ -157,9 +160,15 @@ class DropIn:
         check(lib().evora_gravpotential(_ptr(q, self.shape["q"], False), self._phi_ptr(phi)), "gravpotential")
 
     def chem(self, q):
-        """chem(q), chemistry.f90:72-121, plain build: pressure() and the
-        temperature / Jeans pressure floors."""
+        """chem(q), chemistry.f90:72-121: pressure(), with chemistry the CIE
+        species and the cooling over the dt of settime, and the temperature /
+        Jeans pressure floors."""
         check(lib().evora_chem(_ptr(q, self.shape["q"])), "chem")
+
+    def initchem(self, q):
+        """initchem(q), chemistry.f90:26-70, on a host q (nz, ny, nx, 12):
+        fully neutral species."""
+        check(lib().evora_initchem(_ptr(q, self.shape["q"])), "initchem")
 
     def thermalstep(self, q, w, dt: float = 1e99) -> float:
         """thermalstep(q,w), timestep.f90:72-104: min(dt, conduction limit);

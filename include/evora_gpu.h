@@ -56,7 +56,10 @@ enum evora_status {
   EVORA_ERR_NOMEM = 512,          /* device allocation failed */
   EVORA_ERR_TIMEOUT = 1024,       /* a bounded host or device wait gave up */
   EVORA_ERR_IO = 2048,            /* a file could not be opened, written or read */
-  EVORA_ERR_COSMO = 4096          /* timestepiteration did not converge, timestep.f90:220-223 */
+  EVORA_ERR_COSMO = 4096,         /* timestepiteration did not converge, timestep.f90:220-223 */
+  EVORA_ERR_CHEM = 8192           /* abundances out of range (ncheck, chemistry.f90:159-176),
+                                     no or no converging electron-density root (cie.f90:131-134,
+                                     164-167), or a cooling update that does not end */
 };
 
 /* Number of conserved / primitive / flux fields of the plain build
@@ -107,7 +110,25 @@ typedef struct evora_params {
   double zstart, zend;    /* first and last redshift                         */
   double dump_redshift[EVORA_NDUMP]; /* redshifts of the intermediate dumps,
                              in the order they are reached; -1 = unused      */
+  /* chemistry and cooling of the CIE build (chemistry.f90, cie.f90,
+   * rates.f90; main.f90:94, 135, 167): with chemistry the state is
+   * q(12, nx, ny, nz), q(7:12) = n(H, H+, He, He+, He++, e-) in equilibrium
+   * (not advected: the CIE build's fluxes are nf = 6, global.f90:31-32).
+   * The non-equilibrium build (noncie) is refused (EVORA_ERR_ARG).          */
+  int32_t chemistry;      /* Fortran logical                                 */
+  int32_t noncie;         /* Fortran logical (refused when set)              */
+  int32_t cooling;        /* Fortran logical: radiative cooling (cie)         */
+  int32_t background;     /* Fortran logical: UV background (implicitcie)     */
+  int32_t bg;             /* background model 1..3 (compbackground)           */
+  int32_t cooldt;         /* Fortran logical: cooling time-step limit (refused) */
+  double j0;              /* background intensity                            */
+  double c_chem, substep; /* cooling sub-cycle factors (cie.f90:41)           */
+  double rhoh, rhohe;     /* H and He mass fractions                          */
+  double c_cooldt;        /* cooling time-step factor                         */
 } evora_params;
+
+/* The chemistry build's layout: EVORA_NQ_CHEM values per cell in q. */
+#define EVORA_NQ_CHEM 12
 
 /* The derived constants of compparameter (parameter.f90:164-265) that the
  * hydro path reads from module global. */
@@ -193,12 +214,22 @@ int evora_thermalstep(double* q, const double* w, double* dt);
  * bound), updating E and S of q in place. */
 int evora_thermalconduction(double* q, const double* w, double dt);
 
-/* chem(q), chemistry.f90:72-121, in the plain build (no species):
- * pressure() with its dual-energy write-back, then the temperature floor
- * (tempfloor: press = max(press, temp_fl rho / temp0)) and the Jeans floor
- * (jeansfloor: press = max(press, jeansfloor0 rho^2)) with E and S
- * corrected by the pressure change. */
+/* chem(q), chemistry.f90:72-121: pressure() with its dual-energy
+ * write-back; with chemistry (q(12, ...)) the CIE abundances q(7:12) and,
+ * with cooling, the pressure advanced over dt by the sub-cycled cooling
+ * update (cie.f90:26-56; dt and, comoving, the units and UV background from
+ * evora_settime); then the temperature floor (tempfloor: press = max(press,
+ * temp_fl rho / temp0), or temp_fl sum(n) / temp0 with chemistry) and the
+ * Jeans floor (jeansfloor: press = max(press, jeansfloor0 rho^2)), with E and
+ * S corrected by the pressure change when cooling or a floor is on. */
 int evora_chem(double* q);
+
+/* initchem(q), chemistry.f90:26-70, on a host q(12, nx, ny, nz) (the
+ * chemistry build's layout): fully neutral species, n(H) = rho rhoH / mH,
+ * n(He) = rho rhoHe / mHe, the others at nfloor = 1e-40; pressure() runs on
+ * every cell as there (resynchronising E or S with dual energy).
+ * EVORA_ERR_ARG without chemistry or for a device pointer. */
+int evora_initchem(double* q);
 
 /* gravpotential(q,phi), gravitation.f90:26-53: the potential of the
  * density of q (FFT Poisson solve with the reference's discrete Green's

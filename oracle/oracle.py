@@ -54,6 +54,10 @@ class OracleParams(ctypes.Structure):
         ("supercomoving", ctypes.c_int32), ("c_cosmo", c_double), ("omega0", c_double), ("lambda0", c_double),
         ("hubble0", c_double), ("box", c_double), ("zstart", c_double), ("zend", c_double),
         ("dump_redshift", c_double * NDUMP),
+        ("chemistry", ctypes.c_int32), ("noncie", ctypes.c_int32), ("cooling", ctypes.c_int32),
+        ("background", ctypes.c_int32), ("bg", ctypes.c_int32), ("cooldt", ctypes.c_int32),
+        ("j0", c_double), ("c_chem", c_double), ("substep", c_double), ("rhoh", c_double), ("rhohe", c_double),
+        ("c_cooldt", c_double),
     ]
 
 
@@ -137,6 +141,9 @@ def make_params(**kw) -> OracleParams:
     p.omega0, p.lambda0, p.hubble0, p.box, p.zstart, p.zend = 1.0, 0.0, 50.0, 1.0, 99.0, 0.0
     for i in range(NDUMP):
         p.dump_redshift[i] = -1.0
+    p.chemistry = p.noncie = p.cooling = p.background = p.bg = p.cooldt = 0
+    p.j0, p.c_chem, p.substep = 1e-21, float(np.float32(0.1)), float(np.float32(0.1))
+    p.rhoh, p.rhohe, p.c_cooldt = float(np.float32(0.76)), float(np.float32(0.24)), 0.0
     for k, v in kw.items():
         if k == "dump_redshift":
             for i, z in enumerate(v):

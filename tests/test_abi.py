@@ -35,7 +35,8 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(ev.EvoraParams) == 10 * 4 + 11 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8 + 8 + 7 * 8 + 100 * 8
+    assert ctypes.sizeof(ev.EvoraParams) == (10 * 4 + 11 * 8 + 2 * 4 + 8 + 2 * 4 + 3 * 8 + 8 + 7 * 8 + 100 * 8
+                                             + 6 * 4 + 6 * 8)
     assert ctypes.sizeof(ev.EvoraDerived) == 16 * 8 + 2 * 4
     assert ctypes.sizeof(_native.EvoraTime) == 7 * 8
 
@@ -44,7 +45,8 @@ def test_struct_layouts_match_the_c_header(tmp_path):
     """sizeof and field offsets of the ctypes mirrors against the C compiler's
     view of include/evora_gpu.h."""
     checks = {"evora_params": (_native.EvoraParams, ["nz", "gravity", "g", "tend", "fb", "supercomoving",
-                                                     "c_cosmo", "zend", "dump_redshift"]),
+                                                     "c_cosmo", "zend", "dump_redshift", "chemistry", "cooldt",
+                                                     "j0", "c_cooldt"]),
               "evora_time": (_native.EvoraTime, ["t", "redshift"]),
               "evora_derived": (ev.EvoraDerived, ["volume", "twodimension"])}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER_DIR}/evora_gpu.h"', "int main(void) {"]
