@@ -189,13 +189,13 @@ def cosmo_zeldovich(p: EvoraParams, seed=5, slope=-2.0, sigma=0.05, temp_k=100.0
     kk = np.sqrt(k2) * (2.0 * np.pi / p.box)
     with np.errstate(divide="ignore"):
         pk = np.where(k2 > 0, kk ** (0.5 * slope), 0.0)
-    delta = np.fft.irfftn(spec * pk, s=(nz, ny, nx))
+    delta = np.fft.irfftn(spec * pk, s=(nz, ny, nx), axes=(0, 1, 2))
     delta *= sigma / np.sqrt(np.mean(delta * delta))
     rho = p.fb * (1.0 + delta)
     green = np.zeros_like(k2)
     den = (_sin2(nx)[: nx // 2 + 1][None, None, :] + _sin2(ny)[None, :, None]) + _sin2(nz)[:, None, None]
     green[k2 > 0] = -(d.dx * d.dx / 4.0) / den[k2 > 0]
-    phi = np.fft.irfftn(np.fft.rfftn(delta) * green, s=(nz, ny, nx))
+    phi = np.fft.irfftn(np.fft.rfftn(delta) * green, s=(nz, ny, nx), axes=(0, 1, 2))
     drop = DropIn(p)
     s = drop.cosmostart()
     vscale = drop.peebles(s) * s["cosmodot"] / s["cosmo"]
@@ -207,10 +207,18 @@ def cosmo_zeldovich(p: EvoraParams, seed=5, slope=-2.0, sigma=0.05, temp_k=100.0
     u = _native.EvoraUnits()
     check(_native.lib().evora_compunits(ctypes.byref(p), None, ctypes.byref(u)), "compunits")
     temp = temp_k * (rho / p.fb) ** d.g1
-    pres = rho * temp / u.temp0
-    q = np.zeros((nz, ny, nx, 6))
+    if p.chemistry:
+        # temp2press (comp.f90:104-119) with the neutral abundances initchem
+        # sets: T sum(n) / temp0, n(H) = rho rhoH / mH, n(He) = rho rhoHe / mHe
+        mh, mhe = float(np.float32(1.00794)), float(np.float32(4.002602))
+        pres = temp * (rho * (p.rhoh / mh) + rho * (p.rhohe / mhe)) / u.temp0
+    else:
+        pres = rho * temp / u.temp0
+    q = np.zeros((nz, ny, nx, 12 if p.chemistry else 6))
     q[..., 0] = rho
     q[..., 1:4] = rho[..., None] * vel
     q[..., 4] = 0.5 * rho * (vel ** 2).sum(-1) + pres / d.g1
     q[..., 5] = pres / rho ** d.g1
+    if p.chemistry:
+        drop.initchem(q)   # q(7:12): fully neutral (initchem, chemistry.f90:26-70)
     return q

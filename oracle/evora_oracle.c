@@ -58,6 +58,13 @@ static struct {
   double c_cosmo, omega0, lambda0, zstart, zend, g35;
   double dump_redshift[EVORA_NDUMP];
   double u_d0, u_t0, u_l0, u_m0;        /* compunits' d0, t0, l0, m0 */
+  /* chemistry of the CIE build (global.f90:29-35, 63-67, 131-133): q holds
+   * nq = 12 values per cell, q(7:12) the species */
+  int nq;
+  int chemistry, cooling, background, bg;
+  double j0, c_chem, substep, chiH, chiHe;
+  double chem0, photo0, cool0, heat0;   /* compunits (units.f90:56-60) */
+  double coef[13][2], uv;               /* compcoef (rates.f90), compbackground */
 } G;
 
 /* The time scalars of module global (global.f90:86): t, dt, cosmo,
@@ -204,14 +211,228 @@ static void orc_timestepiteration_(double targetredshift) {
   }
 }
 
-/* compunits, units.f90:46-63: the units the hydro path reads (temp0,
- * temp0inv, kappa0) at the current cosmo. */
+/* compunits, units.f90:46-63: the units the hydro path and the chemistry
+ * read (temp0, temp0inv, kappa0, chem0, photo0, cool0, heat0) at the
+ * current cosmo. */
 static void orc_compunits_(void) {
-  const double c = T.cosmo, t0 = G.u_t0, l0 = G.u_l0;
-  G.temp0 = (l0 * l0) / (c * c) / (t0 * t0) * G.u_m0 / kKb;
+  const double c = T.cosmo, t0 = G.u_t0, l0 = G.u_l0, d0 = G.u_d0, m0 = G.u_m0;
+  G.temp0 = (l0 * l0) / (c * c) / (t0 * t0) * m0 / kKb;
   G.temp0inv = 1.0 / G.temp0;
   const double kappa_coef = 4.6e13 * 1e-20 / (double)(37.8f / 40.0f);
-  G.kappa0 = pow(c, 5.0) * pow(t0, 3.0) / G.u_d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
+  G.kappa0 = pow(c, 5.0) * pow(t0, 3.0) / d0 / pow(l0, 4.0) * 0.5 * kappa_coef;
+  G.chem0 = d0 * t0 / c / m0;
+  G.photo0 = t0 * (c * c);
+  G.cool0 = G.g1 * pow(t0, 3.0) * c * d0 / (l0 * l0) / (m0 * m0);
+  G.heat0 = G.g1 * pow(t0, 3.0) * pow(c, 4.0) / (l0 * l0) / m0;
+}
+
+/* ---------------------------------------------------- chemistry (CIE) -- */
+/* The CIE build: n = q(7:12) = H, H+, He, He+, He++, e- (global.f90:29-35,
+ * 121-133).  Default-real literals are single precision, as in the
+ * Fortran. */
+static const double kNfloor = 1.0e-40, kRatefloor = 1.0e-40, kCieTol = 1e-10;
+static const int kCieNit = 1000;
+
+/* compcoef, rates.f90:26-78 (entries it never sets stay 0). */
+static void orc_compcoef_(void) {
+  memset(G.coef, 0, sizeof G.coef);
+  const double uv = G.uv;
+  G.coef[0][0] = G.chem0 * 5.85e-11;   G.coef[0][1] = G.cool0 * 1.27e-21;
+  G.coef[1][0] = G.chem0 * 2.38e-11;   G.coef[1][1] = G.cool0 * 9.38e-22;
+  G.coef[2][0] = G.chem0 * 5.68e-12;   G.coef[2][1] = G.cool0 * 4.95e-22;
+  G.coef[3][0] = G.chem0 * 8.4e-11;    G.coef[3][1] = G.cool0 * 8.7e-27;
+  G.coef[4][0] = G.chem0 * 1.5e-10;    G.coef[4][1] = G.cool0 * 1.55e-26;
+  G.coef[5][0] = G.chem0 * 3.36e-10;   G.coef[5][1] = G.cool0 * 3.48e-26;
+  G.coef[6][0] = G.chem0 * 1.9e-3;     G.coef[6][1] = G.cool0 * 1.24e-13;
+  G.coef[7][1] = G.cool0 * 7.5e-19;
+  G.coef[8][1] = G.cool0 * 5.54e-17;
+  G.coef[9][1] = G.cool0 * 1.42e-27 * 1.5;                 /* gff */
+  G.coef[10][0] = G.photo0 * 2.54e8 * uv;  G.coef[10][1] = G.heat0 * 2.54e8 * 7.75e-12 * uv;
+  G.coef[11][0] = G.photo0 * 2.49e8 * uv;  G.coef[11][1] = G.heat0 * 2.49e8 * 2.19e-11 * uv;
+  G.coef[12][0] = G.photo0 * 1.60e7 * uv;  G.coef[12][1] = G.heat0 * 1.60e7 * 3.10e-11 * uv;
+}
+
+/* compbackground, chemistry.f90:123-157. */
+static void orc_compbackground_(void) {
+  if (!G.background) return;
+  const double z = T.redshift, j0 = G.j0;
+  if (G.bg == 1) {
+    G.uv = j0;
+  } else if (G.bg == 2) {
+    if (z < 6 && z > 3) G.uv = j0 * 4.0 * T.cosmo;
+    else if (z <= 3 && z > 1) G.uv = j0;
+    else G.uv = 0.0;
+  } else if (G.bg == 3) {
+    if (z > 8.0) G.uv = 1e-5 * j0;
+    else if (z <= 8.0 && z > 6.0) G.uv = 0.5 * j0 * pow(10.0, (-z + 6.0) * (double)0.35f);
+    else if (z <= 6.0 && z > 3.0) G.uv = j0 * pow(10.0, (-z + 3.0) * (double)0.1f);
+    else if (z <= 3.0 && z > 1.0) G.uv = j0;
+    else if (z <= 1.0) G.uv = j0 * (double)0.1f * pow(10.0, z);
+  }
+}
+
+/* comprates, rates.f90:80-158: chemical rates r[9], cooling rates cr[13]. */
+static void orc_comprates(double temp, double* r, double* cr) {
+  const double temproot = sqrt(temp), tempinv = 1.0 / temp, temp15 = pow(temp, -1.5);
+  const double fec = 1.0 / (1.0 + sqrt(temp * 1e-5));
+  const double fc1 = temproot * fec;
+  const double e1 = exp(-((double)157809.1f * tempinv));
+  const double e2 = exp(-((double)286335.4f * tempinv));
+  const double e3 = exp(-((double)631515.0f * tempinv));
+  const double fr = pow(temp * 1e-3, (double)(-0.2f)) / (1.0 + pow(temp * 1e-6, (double)0.7f));
+  const double fr1 = fr / temproot, fr2 = fr * temproot;
+  const float p3 = 0.3f * (-94000.0f);
+  const double edr = exp((double)(-470000.0f) * tempinv) * (1.0 + (double)p3 * tempinv);
+  const double (*k)[2] = G.coef;
+  r[0] = k[0][0] * fc1 * e1;
+  r[1] = k[1][0] * fc1 * e2;
+  r[2] = k[2][0] * fc1 * e3;
+  r[3] = k[3][0] * fr1;
+  r[4] = k[4][0] * pow(temp, (double)(-0.6353f)) + k[6][0] * temp15 * edr;
+  r[5] = k[5][0] * fr1;
+  r[6] = G.background ? k[10][0] : 0.0;
+  r[7] = G.background ? k[11][0] : 0.0;
+  r[8] = G.background ? k[12][0] : 0.0;
+  if (G.cooling) {
+    cr[0] = k[0][1] * fc1 * e1;
+    cr[1] = k[1][1] * fc1 * e2;
+    cr[2] = k[2][1] * fc1 * e3;
+    cr[3] = k[3][1] * fr2;
+    cr[4] = k[4][1] * pow(temp, (double)0.3647f);
+    cr[5] = k[5][1] * fr2;
+    cr[6] = k[6][1] * temp15 * edr;
+    cr[7] = k[7][1] * fec * exp((double)(-118348.0f) * tempinv);
+    cr[8] = k[8][1] * pow(temp, (double)(-0.397f)) * fec * exp((double)(-473638.0f) * tempinv);
+    cr[9] = k[9][1] * temproot;
+    cr[10] = G.background ? k[10][1] : 0.0;
+    cr[11] = G.background ? k[11][1] : 0.0;
+    cr[12] = G.background ? k[12][1] : 0.0;
+  }
+}
+
+/* cool, rates.f90:160-189. */
+static void orc_cool(const double* n, const double* cr, double* lambda, double* gamma) {
+  double l = cr[0] * n[0] + cr[1] * n[2] + cr[2] * n[3] + cr[3] * n[1] + cr[4] * n[3] + cr[5] * n[4] +
+             cr[6] * n[3] + cr[7] * n[0] + cr[8] * n[3] + cr[9] * (n[1] + n[3] + 4.0 * n[4]);
+  *lambda = l * n[5];
+  *gamma = G.background ? n[0] * cr[10] + n[2] * cr[11] + n[3] * cr[12] : 0.0;
+}
+
+/* cieions, cie.f90:194-217. */
+static void orc_cieions(double nH, double nHe, double ne, const double* r, double* nHII, double* nHeII,
+                        double* nHeIII) {
+  const double ion1 = r[0] * ne + r[6], ion2 = r[1] * ne + r[7], ion3 = r[2] * ne + r[8];
+  if (ion1 < kRatefloor) *nHII = kNfloor;
+  else *nHII = nH / (1.0 + r[3] * ne / ion1);
+  if (ion2 < kRatefloor) {
+    *nHeII = kNfloor;
+    *nHeIII = kNfloor;
+  } else {
+    const double xi2 = r[4] * ne / ion2;
+    if (ion3 < kRatefloor) {
+      *nHeIII = kNfloor;
+      *nHeII = nHe / (1.0 + xi2);
+    } else {
+      const double xi3 = r[5] * ne / ion3;
+      *nHeIII = nHe / (1.0 + (xi2 + 1.0) * xi3);
+      *nHeII = nHe / (1.0 + xi2 + 1.0 / xi3);
+    }
+  }
+}
+
+/* fne, cie.f90:181-192. */
+static double orc_fne(double nH, double nHe, double ne, const double* r) {
+  double a, b, c;
+  orc_cieions(nH, nHe, ne, r, &a, &b, &c);
+  return a + b + 2 * c - ne;
+}
+
+/* rf_cie, cie.f90:114-179. */
+static double orc_rf_cie(double nH, double nHe, double in1, double in2, const double* r) {
+  double l = in1, rr = in2, fl = orc_fne(nH, nHe, l, r), fr = orc_fne(nH, nHe, rr, r), m = 0.0;
+  if (fl * fr > 0.0) {
+    set_err(EVORA_ERR_CHEM);
+    return m;
+  }
+  int s = 0;
+  for (int i = 1; i <= kCieNit; ++i) {
+    m = (fr * l - fl * rr) / (fr - fl);
+    if (fabs(rr - l) < kCieTol * fabs(rr + l)) break;
+    const double fm = orc_fne(nH, nHe, m, r);
+    if (fm * fr > 0.0) {
+      rr = m; fr = fm;
+      if (s == -1) fl = fl * 0.5;
+      s = -1;
+    } else if (fl * fm > 0.0) {
+      l = m; fl = fm;
+      if (s == 1) fr = fr * 0.5;
+      s = 1;
+    } else {
+      break;
+    }
+    if (i == kCieNit) set_err(EVORA_ERR_CHEM);
+  }
+  return m;
+}
+
+/* cieabundance with implicitcie, cie.f90:58-112, and ncheck
+ * (chemistry.f90:159-176). */
+static void orc_cieabundance(double nH, double nHe, double* n, const double* r) {
+  if (G.background && G.uv > 0.0) {
+    const double ne = orc_rf_cie(nH, nHe, kNfloor, nH + 2 * nHe, r);
+    double a, b, c;
+    orc_cieions(nH, nHe, ne, r, &a, &b, &c);
+    n[0] = nH - a; n[1] = a; n[2] = nHe - b - c; n[3] = b; n[4] = c; n[5] = ne;
+    for (int i = 0; i < 6; ++i) n[i] = fmax2(n[i], kNfloor);
+  } else {
+    const double fracH = r[0] / r[3], fracHe1 = r[1] / r[4], fracHe2 = r[2] / r[5];
+    n[0] = nH / (1.0 + fracH);
+    n[1] = n[0] * fracH;
+    n[2] = nHe / (1.0 + fracHe1 * (1.0 + fracHe2));
+    n[3] = n[2] * fracHe1;
+    n[4] = n[3] * fracHe2;
+    n[5] = n[1] + n[3] + 2 * n[4];
+  }
+  for (int i = 0; i < 5; ++i)
+    if (!(n[i] >= 0.0 && n[i] <= 1e20)) set_err(EVORA_ERR_CHEM);
+  for (int i = 0; i < 6; ++i) n[i] = fmax2(n[i], kNfloor);
+}
+
+static double nsum(const double* n) { return n[0] + n[1] + n[2] + n[3] + n[4] + n[5]; }
+
+/* cie(rho, press, n), cie.f90:26-56, over the step T.dt. */
+static void orc_cie(double rho, double* press, double* n) {
+  const double nH = G.chiH * rho, nHe = G.chiHe * rho;
+  double r[9], cr[13];
+  if (G.cooling) {
+    double ct = 0.0;
+    long cycles = 0;
+    while (ct < T.dt) {
+      if (++cycles > (1L << 20)) {   /* the library's bound (the reference has none) */
+        set_err(EVORA_ERR_CHEM);
+        break;
+      }
+      const double temp = *press / nsum(n) * G.temp0;
+      orc_comprates(temp, r, cr);
+      orc_cieabundance(nH, nHe, n, r);
+      double lambda, gamma;
+      orc_cool(n, cr, &lambda, &gamma);
+      const double coolio = gamma - lambda;
+      const double cooltime = fabs(*press / coolio);
+      const double cdt = fmin2(fmin2(G.c_chem * cooltime, T.dt - ct), T.dt * G.substep);
+      ct = ct + cdt;
+      *press = (*press + cdt * gamma) / (1.0 + cdt * lambda / *press);
+    }
+  } else {
+    const double temp = *press / nsum(n) * G.temp0;
+    orc_comprates(temp, r, cr);
+    orc_cieabundance(nH, nHe, n, r);
+  }
+}
+
+void orc_get_coef(double* out) {
+  memcpy(out, G.coef, sizeof G.coef);
+  out[26] = G.uv;
 }
 
 /* The exported forms: s holds the 7 time scalars (evora_time's order). */
@@ -254,6 +475,10 @@ void orc_updatetime_cosmo(int* go, int* dump, int k, double* s) {
 void orc_settime(const double* s) {
   put_time(s);
   orc_compunits_();
+  if (G.supercomoving && G.chemistry) {   /* main.f90:134-135 */
+    orc_compbackground_();
+    orc_compcoef_();
+  }
 }
 
 void orc_get_units(double* out) {
@@ -269,6 +494,8 @@ static void start_time_(void) {
   T.cosmo = 1.0;
   if (G.supercomoving) orc_cosmostart_();
   orc_compunits_();
+  G.uv = 0.0;                            /* no compbackground before the loop */
+  if (G.chemistry) orc_compcoef_();      /* initchem, chemistry.f90:38 */
 }
 
 /* expansion(q), cosmology.f90:53-72, with dt and expand of the time
@@ -311,6 +538,18 @@ int orc_compparameter(const evora_params* p) {
   G.conduction = p->conduction != 0;
   G.simplekappa = p->simplekappa != 0;
   G.c_cond = p->c_cond;
+  /* the CIE build (parameter.f90:95-104: no background, cooling or cooling
+   * time step without chemistry; initchem: chiH = rhoH / mH with module
+   * global's single-precision mH, mHe) */
+  if (p->chemistry && (p->noncie || p->conduction || p->cooldt)) return EVORA_ERR_ARG;
+  G.chemistry = p->chemistry != 0;
+  G.nq = G.chemistry ? 12 : 6;
+  G.cooling = G.chemistry && p->cooling;
+  G.background = G.chemistry && p->background;
+  G.bg = p->bg;
+  G.j0 = p->j0; G.c_chem = p->c_chem; G.substep = p->substep;
+  G.chiH = p->rhoh / (double)1.00794f;
+  G.chiHe = p->rhohe / (double)4.002602f;
   G.supercomoving = p->supercomoving != 0;
   G.atomic = p->atomic != 0;
   G.c_cosmo = p->c_cosmo; G.omega0 = p->omega0; G.lambda0 = p->lambda0;
@@ -380,7 +619,7 @@ void orc_get_derived(evora_derived* d) {
 /* --------------------------------------------------------- array index -- */
 /* q(nq, 1:nx, 1:ny, 1:nz) */
 static inline size_t iq(int i, int j, int k) {
-  return (size_t)NQ * ((size_t)(i - 1) + (size_t)G.nx * ((size_t)(j - 1) + (size_t)G.ny * (size_t)(k - 1)));
+  return (size_t)G.nq * ((size_t)(i - 1) + (size_t)G.nx * ((size_t)(j - 1) + (size_t)G.ny * (size_t)(k - 1)));
 }
 /* w(nw, -1:nx+2, -1:ny+2, -1:nz+2) */
 static inline size_t iw(int i, int j, int k) {
@@ -396,7 +635,7 @@ static inline size_t is_(int d, int i, int j, int k) {
 }
 
 void orc_array_sizes(int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
-  *nq = (int64_t)NQ * G.nx * G.ny * G.nz;
+  *nq = (int64_t)G.nq * G.nx * G.ny * G.nz;
   *nw = (int64_t)NW * (G.nx + 4) * (G.ny + 4) * (G.nz + 4);
   *ne = (int64_t)NW * (G.nx + 2) * (G.ny + 2) * (G.nz + 2);
   *ns = (int64_t)NW * 3 * (G.nx + 2) * (G.ny + 2) * (G.nz + 2);
@@ -954,9 +1193,10 @@ void orc_thermalconduction(double* q, const double* w, double dt) {
   }
 }
 
-/* chem(q), chemistry.f90:72-121, plain build (no species): pressure()
- * with its dual-energy write-back, the temperature and Jeans pressure
- * floors, E and S corrected by the pressure change. */
+/* chem(q), chemistry.f90:72-121: pressure() with its dual-energy
+ * write-back; with chemistry the CIE species q(7:12) and the cooling over
+ * T.dt (cie); the temperature and Jeans pressure floors; E and S corrected
+ * by the pressure change when cooling or a floor is on. */
 void orc_chem(double* q) {
   for (int iz = 1; iz <= G.nz; ++iz)
     for (int iy = 1; iy <= G.ny; ++iy)
@@ -964,17 +1204,39 @@ void orc_chem(double* q) {
         double* c = &q[iq(ix, iy, iz)];
         double press = orc_pressure(c);
         double oldpress = press;
-        if (G.tempfloor) {
-          double pfloor = G.temp_fl * c[0] * G.temp0inv;   /* temp2press, comp.f90:104-119 */
-          press = fmax2(press, pfloor);
+        if (G.chemistry) orc_cie(c[0], &press, c + 6);
+        if (G.cooling || G.tempfloor || G.jeansfloor) {
+          if (G.tempfloor) {
+            /* temp2press, comp.f90:104-119 */
+            double pfloor = G.chemistry ? G.temp_fl * nsum(c + 6) * G.temp0inv : G.temp_fl * c[0] * G.temp0inv;
+            press = fmax2(press, pfloor);
+          }
+          if (G.jeansfloor) {
+            double pfloor = G.jeansfloor0 * c[0] * c[0];
+            press = fmax2(press, pfloor);
+          }
+          double dpress = press - oldpress;
+          c[4] = c[4] + dpress * G.g1inv;
+          c[5] = c[5] + dpress / pow(c[0], G.g1);
         }
-        if (G.jeansfloor) {
-          double pfloor = G.jeansfloor0 * c[0] * c[0];
-          press = fmax2(press, pfloor);
-        }
-        double dpress = press - oldpress;
-        c[4] = c[4] + dpress * G.g1inv;
-        c[5] = c[5] + dpress / pow(c[0], G.g1);
+      }
+}
+
+/* chem(q) at the time scalars s (dt for the cooling). */
+void orc_chem_at(double* q, const double* s) {
+  put_time(s);
+  orc_chem(q);
+}
+
+/* initchem(q), chemistry.f90:26-70: fully neutral. */
+void orc_initchem(double* q) {
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double* c = &q[iq(ix, iy, iz)];
+        const double nH = G.chiH * c[0], nHe = G.chiHe * c[0];
+        (void)orc_pressure(c);
+        for (int i = 7; i <= G.nq; ++i) c[i - 1] = (i == 7) ? nH : (i == 9 ? nHe : kNfloor);
       }
 }
 
@@ -1025,10 +1287,16 @@ int orc_run_trace(double* q, int max_steps, double* trace, double* t, int* steps
     int dump = 0;
     orc_updatetime_(&go, &dump, k4);                        /* main.f90:130 */
     if (orc_err) break;
-    if (G.supercomoving) orc_compunits_();                  /* main.f90:132-133 */
+    if (G.supercomoving) {                                  /* main.f90:132-136 */
+      orc_compunits_();
+      if (G.chemistry) {
+        orc_compbackground_();
+        orc_compcoef_();
+      }
+    }
     if (G.secondorder) orc_compevo(w, evo, s, T.dt);
     orc_sweep(w, q, evo, s, T.dt);
-    if (G.tempfloor || G.jeansfloor) orc_chem(q);           /* main.f90:167 */
+    if (G.chemistry || G.tempfloor || G.jeansfloor) orc_chem(q);   /* main.f90:167 */
     if (G.conduction) {                                     /* main.f90:169-175 */
       orc_primitive(w, q);
       orc_bound(w);

@@ -113,6 +113,9 @@ def lib():
             L.orc_expansion.argtypes = [_dp, _dp]
             L.orc_peebles.argtypes = [_dp]
             L.orc_peebles.restype = c_double
+            L.orc_chem_at.argtypes = [_dp, _dp]
+            L.orc_initchem.argtypes = [_dp]
+            L.orc_get_coef.argtypes = [_dp]
             _lib = L
     return _lib
 
@@ -173,7 +176,7 @@ class Oracle:
     @property
     def shape_q(self):
         p = self.p
-        return (p.nz, p.ny, p.nx, 6)
+        return (p.nz, p.ny, p.nx, 12 if p.chemistry else 6)
 
     @property
     def shape_w(self):
@@ -296,6 +299,22 @@ class Oracle:
         u = np.zeros(3)
         self.L.orc_get_units(_ptr(u))
         return u
+
+    # -- chemistry (the CIE build: q of shape (nz, ny, nx, 12)) -------------
+    def initchem(self, q):
+        """initchem(q), chemistry.f90:26-70: fully neutral."""
+        self.L.orc_initchem(_ptr(q))
+
+    def chem_at(self, q, s):
+        """chem(q) with the time scalars s (dt for the cooling)."""
+        s = np.array(s, dtype=np.float64)
+        self.L.orc_chem_at(_ptr(q), _ptr(s))
+
+    def coef(self):
+        """coef(13, 2) of compcoef as a (13, 2) array, and uv."""
+        out = np.zeros(27)
+        self.L.orc_get_coef(_ptr(out))
+        return out[:26].reshape(13, 2), out[26]
 
     def peebles(self, s) -> float:
         """peebles(fpeebles), cosmology.f90:76-97, at the time scalars s."""

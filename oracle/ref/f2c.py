@@ -59,7 +59,14 @@ UNITS = [
 
 # Routines called by the translated code but not translated: the harness
 # provides them (error stop, MPI broadcast no-ops, the species solvers).
-EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "cie", "ncie"}
+EXTERNAL_STUBS = {"cleanstop", "bcastdouble", "bcastcoef", "cie", "ncie"}
+
+# The CIE build adds the equilibrium chemistry and cooling.
+CIE_UNITS = [
+    ("source/chemistry.f90", ["initchem", "compbackground", "ncheck"], {}),
+    ("source/cie.f90", ["cie", "cieabundance", "implicitcie", "rf_cie", "fne", "cieions"], {}),
+    ("source/rates.f90", ["compcoef", "comprates", "cool"], {}),
+]
 
 
 class F2CError(Exception):
@@ -67,8 +74,13 @@ class F2CError(Exception):
 
 
 # --------------------------------------------------------------- lexing ---
+# Macros of the build being translated: none for the plain build, {"CIE"}
+# for the equilibrium-chemistry build (global.f90:29-36).
+DEFINES: set = set()
+
+
 def preprocess(text):
-    """#ifdef/#elif/#else/#endif with no macro defined (the plain build)."""
+    """#ifdef/#elif/#else/#endif with the macros of DEFINES."""
     out, stack = [], []   # stack of (taking, any_taken)
     for line in text.splitlines():
         s = line.strip()
@@ -76,10 +88,13 @@ def preprocess(text):
             d = s[1:].split()
             kw = d[0]
             if kw in ("ifdef", "if"):
-                stack.append([False, False])
+                on = d[1] in DEFINES
+                stack.append([on, on])
             elif kw == "elif":
                 top = stack[-1]
-                top[0] = False
+                on = (not top[1]) and d[1] in DEFINES
+                top[0] = on
+                top[1] = top[1] or on
             elif kw == "else":
                 top = stack[-1]
                 top[0] = not top[1]
@@ -1117,7 +1132,10 @@ class Translator:
 
 def translate(ref_root):
     tr = Translator()
-    for rel, take, ren in UNITS:
+    units = UNITS + (CIE_UNITS if "CIE" in DEFINES else [])
+    if "CIE" in DEFINES:
+        EXTERNAL_STUBS.discard("cie")
+    for rel, take, ren in units:
         text = open(os.path.join(ref_root, rel)).read()
         st = statements(text)
         if rel.endswith("global.f90"):
@@ -1158,7 +1176,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", required=True)
+    ap.add_argument("--define", action="append", default=[], help="build macro (CIE)")
     a = ap.parse_args()
+    DEFINES.update(a.define)
     try:
         src = translate(a.ref)
     except F2CError as e:

@@ -14,7 +14,11 @@
 #include <string.h>
 
 #include "../../include/evora_gpu.h"
+#ifdef REF_CIE
+#include "../_ref/evora_ref_cie.c"   /* the build with -DCIE: nq = 12 */
+#else
 #include "../_ref/evora_ref.c"
+#endif
 
 static jmp_buf g_jmp;
 static int g_armed = 0;
@@ -25,8 +29,15 @@ void ref_stop(void) {
 }
 void ref_cleanstop(void) { ref_stop(); }
 void ref_bcastdouble(double* x) { (void)x; }
-/* the species solvers of chem (not reached without chemistry) */
+void ref_bcastcoef(void) {}
+/* the species solvers of chem that this build does not contain */
+#ifndef REF_CIE
 void ref_cie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
+/* the plain build has no chemistry coefficients or background to compute */
+static void ref_compcoef(void) {}
+static void ref_compbackground(void) {}
+static void ref_initchem(double* q) { (void)q; ref_stop(); }
+#endif
 void ref_ncie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
 
 /* &ic_para of ic/shocktube.f90:39 */
@@ -66,7 +77,11 @@ int ref_setup_c(const evora_params* p) {
   G_supercomoving = p->supercomoving; G_c_cosmo = p->c_cosmo; G_omega0 = p->omega0; G_lambda0 = p->lambda0;
   G_hubble0 = p->hubble0; G_box = p->box; G_zstart = p->zstart; G_zend = p->zend;
   for (int i = 0; i < EVORA_NDUMP; ++i) G_dump_redshift[i] = p->dump_redshift[i];
-  G_chemistry = 0; G_noncie = 0; G_cooling = 0; G_background = 0;
+  G_chemistry = p->chemistry; G_noncie = p->noncie; G_cooling = p->cooling; G_background = p->background;
+  G_bg = p->bg; G_j0 = p->j0; G_c_chem = p->c_chem; G_substep = p->substep; G_rhoh = p->rhoh;
+  G_rhohe = p->rhohe; G_cooldt = p->cooldt; G_c_cooldt = p->c_cooldt;
+  if (!G_chemistry) { G_background = 0; G_cooling = 0; G_cooldt = 0; }   /* parameter.f90:95-104 */
+  G_uv = 0.0;
   G_conduction = p->conduction; G_simplekappa = p->simplekappa; G_c_cond = p->c_cond;
   G_tempfloor = p->tempfloor; G_temp_fl = p->temp_fl; G_jeansfloor = p->jeansfloor; G_c_jeans = p->c_jeans;
   G_fb = p->fb;
@@ -76,7 +91,8 @@ int ref_setup_c(const evora_params* p) {
   /* the time scalars a fresh program starts with (static storage) */
   G_dt = 0.0; G_redshift = 0.0; G_oldcosmo = 0.0; G_cosmodot = 0.0; G_expand = 0.0;
   /* main.f90:52-62: compparameter, cosmostart (comoving), compunits */
-  GUARD(ref_compparameter(); ref_decomposition(); if (G_supercomoving) ref_cosmostart(); ref_compunits());
+  GUARD(ref_compparameter(); ref_decomposition(); if (G_supercomoving) ref_cosmostart(); ref_compunits();
+        if (G_chemistry) { G_chih = G_rhoh / G_mh; G_chihe = G_rhohe / G_mhe; ref_compcoef(); });
   return 0;
 }
 
@@ -99,7 +115,12 @@ int ref_updatetime_cosmo_c(int* go, int* dump, int k, double* s) {
   ref_get_time_c(s);
   return 0;
 }
-int ref_settime_c(double* s) { put_time(s); GUARD(ref_compunits()); return 0; }
+int ref_settime_c(double* s) {
+  put_time(s);
+  GUARD(ref_compunits(); if (G_supercomoving && G_background) ref_compbackground();
+        if (G_supercomoving && G_chemistry) ref_compcoef());
+  return 0;
+}
 int ref_peebles_c(double* s, double* f) { put_time(s); GUARD(ref_peebles(f)); return 0; }
 int ref_expansion_c(double* q, double* s) { put_time(s); GUARD(ref_expansion(q)); return 0; }
 
@@ -143,6 +164,14 @@ int ref_sweep_c(double* w, double* q, double* evo, double* s, double dt) {
 }
 
 int ref_chem_c(double* q) { GUARD(ref_chem(q)); return 0; }
+int ref_chem_at_c(double* q, double* s) { put_time(s); GUARD(ref_chem(q)); return 0; }
+int ref_initchem_c(double* q) { GUARD(ref_initchem(q)); return 0; }
+/* coef(13, 2) as [13][2] rows, then uv */
+void ref_get_coef_c(double* out) {
+  for (int i = 0; i < 13; ++i)
+    for (int j = 0; j < 2; ++j) out[2 * i + j] = G_coef[i + 13 * j];
+  out[26] = G_uv;
+}
 int ref_thermalstep_c(double* q, double* w, double* dt) {
   G_dt = *dt;
   GUARD(ref_thermalstep(q, w));
@@ -177,6 +206,8 @@ int ref_run_trace_c(double* q, int max_steps, double* trace, double* t, int* ste
   g_armed = 1;
   if (G_supercomoving) ref_cosmostart();
   ref_compunits();
+  G_uv = 0.0;
+  if (G_chemistry) ref_compcoef();   /* initchem's coefficients (main.f90:94) */
   while (go && k < max_steps) {
     ref_primitive(w, q);
     ref_bound(w);
@@ -188,7 +219,11 @@ int ref_run_trace_c(double* q, int max_steps, double* trace, double* t, int* ste
       ref_compcosmo();
     }
     ref_updatetime(&go, &dump, &k4);
-    if (G_supercomoving) ref_compunits();
+    if (G_supercomoving) {   /* main.f90:132-136 */
+      ref_compunits();
+      if (G_background) ref_compbackground();
+      if (G_chemistry) ref_compcoef();
+    }
     if (G_secondorder) ref_compevo(w, evo, s);
     if (G_hydro) ref_sweep(w, q, evo, s);
     if (G_chemistry || G_tempfloor || G_jeansfloor) ref_chem(q);

@@ -19,8 +19,10 @@ from .oracle import OracleParams, make_params  # noqa: F401  (re-exported for te
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libevora_ref.so")
+# the equilibrium-chemistry build (the reference compiled with -DCIE)
+LIB_PATH_CIE = os.path.join(_HERE, "_ref", "libevora_ref_cie.so")
 REF_SOURCES = "/root/reference/source"
-_lib = None
+_libs = {}
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 
@@ -29,12 +31,11 @@ def available() -> bool:
     return os.path.exists(LIB_PATH) or os.path.isdir(REF_SOURCES)
 
 
-def lib():
-    global _lib
-    if _lib is None:
+def lib(cie: bool = False):
+    if cie not in _libs:
         if os.path.isdir(REF_SOURCES):
             subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref")], check=True)
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH_CIE if cie else LIB_PATH)
         L.ref_setup_c.argtypes = [ctypes.POINTER(OracleParams)]
         L.ref_sizes_c.argtypes = [ctypes.POINTER(ctypes.c_int64)] * 4
         L.ref_derived_c.argtypes = [_dp]
@@ -60,8 +61,11 @@ def lib():
         L.ref_settime_c.argtypes = [_dp]
         L.ref_expansion_c.argtypes = [_dp, _dp]
         L.ref_peebles_c.argtypes = [_dp, _dp]
-        _lib = L
-    return _lib
+        L.ref_chem_at_c.argtypes = [_dp, _dp]
+        L.ref_initchem_c.argtypes = [_dp]
+        L.ref_get_coef_c.argtypes = [_dp]
+        _libs[cie] = L
+    return _libs[cie]
 
 
 def _p(a):
@@ -73,7 +77,7 @@ class RefOracle:
     """The translated reference for one grid (module global state)."""
 
     def __init__(self, params: OracleParams | None = None, **kw):
-        self.L = lib()
+        self.L = lib(cie=bool(getattr(params if params is not None else make_params(**kw), "chemistry", 0)))
         self.p = params if params is not None else make_params(**kw)
         if self.L.ref_setup_c(ctypes.byref(self.p)):
             raise ValueError("the reference stopped in compparameter/decomposition")
@@ -84,7 +88,7 @@ class RefOracle:
 
     @property
     def shape_q(self):
-        return (self.p.nz, self.p.ny, self.p.nx, 6)
+        return (self.p.nz, self.p.ny, self.p.nx, 12 if self.p.chemistry else 6)
 
     @property
     def shape_w(self):
@@ -198,6 +202,21 @@ class RefOracle:
     def expansion(self, q, s):
         s = np.array(s, dtype=np.float64)
         return self.L.ref_expansion_c(_p(q), _p(s))
+
+    # -- chemistry (the CIE build: q of shape (nz, ny, nx, 12)) -------------
+    def initchem(self, q):
+        return self.L.ref_initchem_c(_p(q))
+
+    def chem_at(self, q, s):
+        """chem(q) with the time scalars s (dt for the cooling)."""
+        s = np.array(s, dtype=np.float64)
+        return self.L.ref_chem_at_c(_p(q), _p(s))
+
+    def coef(self):
+        """coef(13, 2) as a (13, 2) array, and uv."""
+        out = np.zeros(27)
+        self.L.ref_get_coef_c(_p(out))
+        return out[:26].reshape(13, 2), out[26]
 
     def ic_shocktube(self, dl, ul, pl, dr, ur, pr, x_diss, direction=1):
         q = self.zeros_q()

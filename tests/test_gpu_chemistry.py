@@ -1,0 +1,111 @@
+"""The CIE chemistry build on the GPU against the oracle (itself pinned bit
+for bit to the reference's Fortran translated with -DCIE): the drop-in
+initchem and chem(q), grids with q(12) whose steps run the species and the
+sub-cycled cooling after the hydro update, comoving coefficients per step.
+The rates go through the device's exp, pow and sqrt, so results are
+compared to a relative tolerance; the time scalars of comoving runs stay
+bit-exact while the cooling does not change the step."""
+import numpy as np
+import pytest
+
+import evora_b200 as ev
+from helpers import random_q
+from oracle.oracle import TIME_FIELDS, Oracle, make_params
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(supercomoving=1, omega0=0.3, lambda0=0.7, hubble0=70.0, box=1.0, zstart=10.0, zend=9.5,
+            chemistry=1, g=5 / 3, cfl=0.4)
+CASES = [
+    dict(cooling=0),
+    dict(cooling=1),
+    dict(cooling=1, background=1, bg=1, j0=1e-21),
+    dict(cooling=1, background=1, bg=3, j0=1e-21, tempfloor=1, temp_fl=5e3),
+    dict(cooling=1, dualenergy=1, de_thresh=0.01, jeansfloor=1, c_jeans=0.5),
+]
+IDS = ["abundances", "cooling", "cooling-uv1", "cooling-uv3-tempfloor", "cooling-dual-energy-jeans"]
+
+
+def kw_of(cfg, **extra):
+    return dict(BASE, **cfg, **extra)
+
+
+def state(o, seed):
+    q = random_q(o, np.random.default_rng(seed), pres=(1e-5, 1e-2))
+    o.initchem(q)
+    return q
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
+
+
+@pytest.mark.parametrize("cfg", CASES, ids=IDS)
+def test_dropin_initchem_and_chem_match_oracle(cuda_device, cfg):
+    kw = kw_of(cfg, nx=10, ny=8, nz=6)
+    o = Oracle(make_params(**kw))
+    q = random_q(o, np.random.default_rng(2), pres=(1e-5, 1e-2))
+    drop = ev.DropIn(ev.default_params(**kw), strict=True)
+    q_o, q_g = q.copy(), q.copy()
+    o.initchem(q_o)
+    drop.initchem(q_g)
+    np.testing.assert_array_equal(q_g, q_o)
+    s = o.time()
+    for z in (10.0, 4.5):
+        s[2], s[6] = 1.0 / (1.0 + z), z
+        s[1] = 3e-3
+        o.settime(s)
+        drop.settime(dict(zip(TIME_FIELDS, s)))
+        a, b = q_o.copy(), q_o.copy()
+        o.chem_at(a, s)
+        drop.chem(b)
+        assert rel(b[..., :6], a[..., :6]) < 1e-12
+        assert rel(b[..., 6:], a[..., 6:]) < 1e-10
+        assert not np.array_equal(a[..., 6:], q_o[..., 6:])
+
+
+@pytest.mark.parametrize("cfg", CASES[1:4], ids=IDS[1:4])
+def test_grid_comoving_chemistry_run_matches_oracle(cuda_device, cfg):
+    kw = kw_of(cfg, nx=12, ny=10, nz=8, boundtype=2)
+    o = Oracle(make_params(**kw))
+    q0 = state(o, 3)
+    q_o = q0.copy()
+    ref = o.run(q_o, 60, trace=True)
+    assert ref["status"] == 0
+    tr = ref["trace"]
+    with ev.Grid(ev.default_params(**kw), ev.FP64, ev.STRICT | ev.CARRY_ENTROPY) as g:
+        g.set_q(q0)
+        np.testing.assert_array_equal(g.get_q(), q0)          # q(12) round trip
+        for k in range(len(tr)):
+            g.step(1)
+            s, dump = g.cosmo()
+            np.testing.assert_allclose([s[f] for f in TIME_FIELDS], tr[k, :7], rtol=1e-11, atol=0)
+        q = g.get_q()
+    assert q.shape == q_o.shape == (8, 10, 12, 12)
+    assert rel(q[..., :6], q_o[..., :6]) < 1e-9
+    assert rel(q[..., 6:], q_o[..., 6:]) < 1e-8
+
+
+def test_fp32_chemistry_grid_tracks_fp64(cuda_device):
+    kw = kw_of(dict(cooling=1), nx=24, ny=20, nz=16, boundtype=2)
+    o = Oracle(make_params(**kw))
+    q0 = state(o, 4)
+    out = {}
+    for prec in (ev.FP64, ev.FP32):
+        with ev.Grid(ev.default_params(**kw), prec, ev.CARRY_ENTROPY) as g:
+            g.set_q(q0)
+            g.step(20)
+            assert g.status() == 0
+            out[prec] = g.get_q()
+    a, b = out[ev.FP32], out[ev.FP64]
+    assert np.abs(a[..., 0] - b[..., 0]).sum() / np.abs(b[..., 0]).sum() < 1e-5
+    assert np.abs(a[..., 6:] - b[..., 6:]).sum() / np.abs(b[..., 6:]).sum() < 1e-4
+
+
+def test_chemistry_refusals(cuda_device):
+    """Combinations the CIE build leaves undefined or this build does not
+    have are refused at creation."""
+    for extra in (dict(noncie=1), dict(conduction=1, simplekappa=1), dict(cooldt=1)):
+        p = ev.default_params(**kw_of(dict(cooling=1), nx=8, ny=8, nz=8, **extra))
+        with pytest.raises(ev.EvoraError):
+            ev.Grid(p, ev.FP64)
