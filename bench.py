@@ -42,6 +42,7 @@ sys.path.insert(0, ROOT)
 
 NX = NY = NZ = 256
 AUTOTUNE = True
+CHEMISTRY = True   # the cosmological box runs the CIE chemistry and cooling
 GAMMA = 5.0 / 3.0
 CFL = 0.5
 METRIC = "cell-updates/s"
@@ -454,7 +455,8 @@ def cosmo_params(ev):
     thousandth of E, comp.f90:45-85)."""
     return ev.default_params(nx=NX, ny=NY, nz=NZ, g=GAMMA, cfl=CFL, boundtype=2, solver=2, limiter=1,
                              supercomoving=1, gravity=1, omega0=0.3, lambda0=0.7, hubble0=70.0, box=20.0,
-                             zstart=50.0, zend=0.0, fb=0.17, c_cosmo=0.01, dualenergy=1, de_thresh=1e-3)
+                             zstart=50.0, zend=0.0, fb=0.17, c_cosmo=0.01, dualenergy=1, de_thresh=1e-3,
+                             chemistry=int(CHEMISTRY), cooling=int(CHEMISTRY))
 
 
 def run_cosmo(args):
@@ -518,7 +520,9 @@ def run_cosmo(args):
                 "config": {"workload": "3D comoving cosmological box 256^3 periodic, gamma=5/3, Zel'dovich IC from "
                                        "a seeded power law P(k)~k^-2 at z=50 (density rms 0.05), fb=0.17, T=100 K, "
                                        "omega0=0.3, lambda0=0.7, H0=70, 20 Mpc/h; cuFFT comoving gravity and "
-                                       "expansion terms; chemistry/cooling not built",
+                                       "expansion terms; " + ("six species in CIE with FP64 per-cell cooling "
+                                                              "(neutral start)" if CHEMISTRY else
+                                                              "without chemistry (--no-chemistry)"),
                            "cells": n, "l2": "inputs larger than L2"},
                 "roofline": v["roofline"], "cosmo": out, "l1_density_fp32_vs_fp64": l1,
                 "gpu_launches": v["gpu_launches"], "clocks": clk.summary()}
@@ -651,10 +655,12 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--nrequests", type=int, default=400)
     ap.add_argument("--tick-steps", type=int, default=32)
+    ap.add_argument("--no-chemistry", action="store_true", help="cosmo: without the CIE chemistry and cooling")
     args = ap.parse_args()
-    global NX, NY, NZ, AUTOTUNE
+    global NX, NY, NZ, AUTOTUNE, CHEMISTRY
     NX = NY = NZ = args.size
     AUTOTUNE = not args.no_autotune
+    CHEMISTRY = not args.no_chemistry
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "tubes":

@@ -27,6 +27,7 @@ namespace evora {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kChemThreads = 128;
 
 int grid_of(int64_t n) {
   int64_t b = (n + kThreads - 1) / kThreads;
@@ -60,8 +61,11 @@ __device__ __forceinline__ void chem_cell(double* v, double* n, const HydroParam
   }
 }
 
+// The cooling sub-cycles are a long FP64 latency chain per cell (powers,
+// exponentials, divisions): registers are capped for 16 warps per SM.
 template <typename T>
-__global__ void k_chem(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P,
+__global__ void __launch_bounds__(kChemThreads, 4)
+k_chem(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P,
                        const GridCtl* ctl, unsigned* err) {
   if (ctl_skip(ctl)) return;
   const Gas<double> c = Gas<double>::make(P);
@@ -102,8 +106,10 @@ __global__ void k_chem_aos(double* __restrict__ q, int64_t n, int nq, HydroParam
 
 int chem_step(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
               cudaStream_t st) {
-  if (f32) k_chem<float><<<grid_of(n), kThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err);
-  else k_chem<double><<<grid_of(n), kThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err);
+  const int blocks = (int)((n + kChemThreads - 1) / kChemThreads < 148 * 16 ? (n + kChemThreads - 1) / kChemThreads
+                                                                          : 148 * 16);
+  if (f32) k_chem<float><<<blocks, kChemThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err);
+  else k_chem<double><<<blocks, kChemThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_cuda_error(e, "chem");

@@ -118,18 +118,24 @@ __host__ __device__ inline double compbackground(int background, int bg, double 
   return uv;
 }
 
-// comprates (rates.f90:80-158).
+// comprates (rates.f90:80-158).  The six powers of T are taken as
+// exp(c ln T) from one logarithm (ln(T 1e-3) = ln T + ln 1e-3, ...): the
+// sub-cycled cooling evaluates this ~10 times per cell and step, and a power
+// costs about a logarithm plus an exponential; the results stay within a
+// few ulp of the direct powers.
 __host__ __device__ inline void comprates(double temp, const ChemCoef& k, int background, int cooling,
                                           double* chemrate, double* coolrate) {
+  const double lt = std::log(temp);
   const double temproot = std::sqrt(temp);
   const double tempinv = 1.0 / temp;
-  const double temp15 = std::pow(temp, -1.5);
+  const double temp15 = std::exp(-1.5 * lt);
   const double fec = 1.0 / (1.0 + std::sqrt(temp * 1e-5));
   const double fc1 = temproot * fec;
   const double e1 = std::exp(-((double)157809.1f * tempinv));
   const double e2 = std::exp(-((double)286335.4f * tempinv));
   const double e3 = std::exp(-((double)631515.0f * tempinv));
-  const double fr = std::pow(temp * 1e-3, (double)(-0.2f)) / (1.0 + std::pow(temp * 1e-6, (double)0.7f));
+  const double ln1e3 = -6.907755278982137, ln1e6 = -13.815510557964274;   // ln 1e-3, ln 1e-6
+  const double fr = std::exp((double)(-0.2f) * (lt + ln1e3)) / (1.0 + std::exp((double)0.7f * (lt + ln1e6)));
   const double fr1 = fr / temproot;
   const double fr2 = fr * temproot;
   const float c3 = 0.3f * (-94000.0f);   // a product of two default reals
@@ -138,7 +144,7 @@ __host__ __device__ inline void comprates(double temp, const ChemCoef& k, int ba
   chemrate[1] = k.c[1][0] * fc1 * e2;
   chemrate[2] = k.c[2][0] * fc1 * e3;
   chemrate[3] = k.c[3][0] * fr1;
-  chemrate[4] = k.c[4][0] * std::pow(temp, (double)(-0.6353f)) + k.c[6][0] * temp15 * edr;
+  chemrate[4] = k.c[4][0] * std::exp((double)(-0.6353f) * lt) + k.c[6][0] * temp15 * edr;
   chemrate[5] = k.c[5][0] * fr1;
   if (background) {
     chemrate[6] = k.c[10][0];
@@ -152,11 +158,11 @@ __host__ __device__ inline void comprates(double temp, const ChemCoef& k, int ba
     coolrate[1] = k.c[1][1] * fc1 * e2;
     coolrate[2] = k.c[2][1] * fc1 * e3;
     coolrate[3] = k.c[3][1] * fr2;
-    coolrate[4] = k.c[4][1] * std::pow(temp, (double)0.3647f);
+    coolrate[4] = k.c[4][1] * std::exp((double)0.3647f * lt);
     coolrate[5] = k.c[5][1] * fr2;
     coolrate[6] = k.c[6][1] * temp15 * edr;
     coolrate[7] = k.c[7][1] * fec * std::exp((double)(-118348.0f) * tempinv);
-    coolrate[8] = k.c[8][1] * std::pow(temp, (double)(-0.397f)) * fec * std::exp((double)(-473638.0f) * tempinv);
+    coolrate[8] = k.c[8][1] * std::exp((double)(-0.397f) * lt) * fec * std::exp((double)(-473638.0f) * tempinv);
     coolrate[9] = k.c[9][1] * temproot;
     if (background) {
       coolrate[10] = k.c[10][1];
