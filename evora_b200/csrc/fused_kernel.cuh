@@ -316,7 +316,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
   const bool owned = oi < xe && oj < ye;
   const int64_t n = A.n;
   const Gas<T> c = Gas<T>::make(P);
-  const bool de = P.dualenergy != 0;
+  const bool de = NF == 6 && P.dualenergy != 0;   // dual energy carries S (nf = 6)
   unsigned err = 0;
 
   if (ctl_skip(A.ctl)) {
@@ -799,7 +799,7 @@ __device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
     return;
   }
   const Gas<T> c = Gas<T>::make(P);
-  const bool de = P.dualenergy != 0;
+  const bool de = NF == 6 && P.dualenergy != 0;   // dual energy carries S (nf = 6)
   unsigned err = 0;
   const double dtd = A.ctl->dt;
   const T dt2 = (T)(-0.5 * dtd);
