@@ -61,8 +61,12 @@ static struct {
   /* chemistry of the CIE build (global.f90:29-35, 63-67, 131-133): q holds
    * nq = 12 values per cell, q(7:12) the species */
   int nq;
-  int chemistry, cooling, background, bg;
-  double j0, c_chem, substep, chiH, chiHe;
+  int chemistry, cooling, background, bg, cooldt;
+  double j0, c_chem, substep, chiH, chiHe, c_cooldt;
+  /* module global's nH, nHe: chem and initchem set them per cell
+   * (chemistry.f90:50-51, 90-91); coolstep reads them as the last cell of
+   * the last such pass left them */
+  double nH, nHe;
   double chem0, photo0, cool0, heat0;   /* compunits (units.f90:56-60) */
   double coef[13][2], uv;               /* compcoef (rates.f90), compbackground */
 } G;
@@ -541,10 +545,13 @@ int orc_compparameter(const evora_params* p) {
   /* the CIE build (parameter.f90:95-104: no background, cooling or cooling
    * time step without chemistry; initchem: chiH = rhoH / mH with module
    * global's single-precision mH, mHe) */
-  if (p->chemistry && (p->noncie || p->conduction || p->cooldt)) return EVORA_ERR_ARG;
+  if (p->chemistry && (p->noncie || p->conduction)) return EVORA_ERR_ARG;
   G.chemistry = p->chemistry != 0;
   G.nq = G.chemistry ? 12 : 6;
   G.cooling = G.chemistry && p->cooling;
+  G.cooldt = G.cooling && p->cooldt;
+  G.c_cooldt = p->c_cooldt;
+  G.nH = G.nHe = 0.0;
   G.background = G.chemistry && p->background;
   G.bg = p->bg;
   G.j0 = p->j0; G.c_chem = p->c_chem; G.substep = p->substep;
@@ -1129,6 +1136,34 @@ double orc_thermalstep(double* q, const double* w, double dt_in) {
   return dt;
 }
 
+/* coolstep(q,w), timestep.f90:106-143: returns min(dt_in, c_cooldt v), v
+ * the smallest cooling time |p / (Gamma - Lambda)| over the cells (from
+ * 1e6), with T from w's pressure and the cell's species as they stand.  As
+ * in the reference, the equilibrium abundances are computed with module
+ * global's nH and nHe (the last cell of the last chem or initchem, not this
+ * cell's) and written back into q(7:12): they are the start values of the
+ * next chem. */
+double orc_coolstep(double* q, const double* w, double dt_in) {
+  double v = 1e6;
+  for (int iz = 1; iz <= G.nz; ++iz)
+    for (int iy = 1; iy <= G.ny; ++iy)
+      for (int ix = 1; ix <= G.nx; ++ix) {
+        double* c = &q[iq(ix, iy, iz)];
+        const double press = w[iw(ix, iy, iz) + 4];
+        const double temp = press / nsum(c + 6) * G.temp0;     /* press2temp, comp.f90:96-97 */
+        double r[9], cr[13], lambda, gamma;
+        orc_comprates(temp, r, cr);
+        orc_cieabundance(G.nH, G.nHe, c + 6, r);
+        orc_cool(c + 6, cr, &lambda, &gamma);
+        const double coolio = gamma - lambda;
+        const double cooltime = fabs(press / coolio);
+        v = fmin2(v, cooltime);
+      }
+  double dt = fmin2(dt_in, G.c_cooldt * v);
+  if (dt <= 0.0) set_err(EVORA_ERR_DT);
+  return dt;
+}
+
 /* thermalflux, conduction.f90:126-148 (simplekappa) */
 static double orc_thermalflux(double templ, double tempr, double deltainv) {
   double kappa_eff = 1.0 / G.g1;
@@ -1204,7 +1239,11 @@ void orc_chem(double* q) {
         double* c = &q[iq(ix, iy, iz)];
         double press = orc_pressure(c);
         double oldpress = press;
-        if (G.chemistry) orc_cie(c[0], &press, c + 6);
+        if (G.chemistry) {
+          G.nH = G.chiH * c[0];
+          G.nHe = G.chiHe * c[0];
+          orc_cie(c[0], &press, c + 6);
+        }
         if (G.cooling || G.tempfloor || G.jeansfloor) {
           if (G.tempfloor) {
             /* temp2press, comp.f90:104-119 */
@@ -1235,6 +1274,8 @@ void orc_initchem(double* q) {
       for (int ix = 1; ix <= G.nx; ++ix) {
         double* c = &q[iq(ix, iy, iz)];
         const double nH = G.chiH * c[0], nHe = G.chiHe * c[0];
+        G.nH = nH;
+        G.nHe = nHe;
         (void)orc_pressure(c);
         for (int i = 7; i <= G.nq; ++i) c[i - 1] = (i == 7) ? nH : (i == 9 ? nHe : kNfloor);
       }
@@ -1277,6 +1318,7 @@ int orc_run_trace(double* q, int max_steps, double* trace, double* t, int* steps
     orc_bound(w);
     T.dt = 1e99;
     T.dt = orc_hydrostep(w, T.dt);
+    if (G.cooldt) T.dt = orc_coolstep(q, w, T.dt);          /* main.f90:120 */
     if (G.conduction) T.dt = orc_thermalstep(q, w, T.dt);  /* main.f90:121 */
     if (orc_err) break;
     if (G.supercomoving) {                                  /* main.f90:125-128 */

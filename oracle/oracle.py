@@ -101,6 +101,8 @@ def lib():
             L.orc_thermalstep.argtypes = [_dp, _dp, c_double]
             L.orc_thermalstep.restype = c_double
             L.orc_thermalconduction.argtypes = [_dp, _dp, c_double]
+            L.orc_coolstep.argtypes = [_dp, _dp, c_double]
+            L.orc_coolstep.restype = c_double
             L.orc_chem.argtypes = [_dp]
             L.orc_run_trace.argtypes = [_dp, c_int, _dp, _dp, ctypes.POINTER(c_int), _dp,
                                         ctypes.POINTER(c_int)]
@@ -235,6 +237,12 @@ class Oracle:
         """thermalstep(q,w), timestep.f90:72-104 (q resynchronised in place
         with dual energy, as the reference's pressure() call does)."""
         return float(self.L.orc_thermalstep(_ptr(q), _ptr(w), float(dt_in)))
+
+    def coolstep(self, q, w, dt_in=1e99) -> float:
+        """coolstep(q,w), timestep.f90:106-143: min(dt_in, c_cooldt times the
+        smallest cooling time); q(7:12) is overwritten with the equilibrium
+        abundances at the last chem/initchem cell's nH and nHe, as there."""
+        return float(self.L.orc_coolstep(_ptr(q), _ptr(w), float(dt_in)))
 
     def chem(self, q):
         """chem(q), chemistry.f90:72-121, plain build: the pressure floors."""

@@ -6,7 +6,7 @@ reference cannot be built as is.  This script reads the reference's own
 sources (module global, compparameter, decomposition, q2w, pressure,
 coordinates, w2n, press2temp, muscl.f90, riemann.f90, boundary.f90,
 hydrostep, cosmostep, updatetime, timestepiteration, thermalstep,
-conduction.f90, compunits, temp2press, chem, the comoving-time routines of
+coolstep (chemistry build), conduction.f90, compunits, temp2press, chem, the comoving-time routines of
 cosmology.f90 and the shocktube / Kelvin-Helmholtz ICs) and translates the
 Fortran 90 subset they use into C, statement by statement, keeping Fortran
 semantics:
@@ -66,6 +66,7 @@ CIE_UNITS = [
     ("source/chemistry.f90", ["initchem", "compbackground", "ncheck"], {}),
     ("source/cie.f90", ["cie", "cieabundance", "implicitcie", "rf_cie", "fne", "cieions"], {}),
     ("source/rates.f90", ["compcoef", "comprates", "cool"], {}),
+    ("source/timestep.f90", ["coolstep"], {}),
 ]
 
 
@@ -527,6 +528,7 @@ class Translator:
         self.units = []          # Unit
         self.unit_names = set()
         self.functions = {}      # function unit name -> result type
+        self.arity = {}          # unit name -> number of dummy arguments
         self.out = []
         self.tmp = 0
 
@@ -580,6 +582,7 @@ class Translator:
                 uname = renames.get(name, name)
                 self.units.append(Unit(uname, args, body, renames, rtype))
                 self.unit_names.add(uname)
+                self.arity[uname] = len(args)
                 if rtype:
                     self.functions[uname] = rtype
             i = j + 1
@@ -1062,6 +1065,12 @@ class Translator:
             self.tmp += 1
             pre.append(f"{t} {tmpn} = {self.c(node, local)};")
             args.append(f"&{tmpn}")
+        # An external procedure has no explicit interface: surplus actual
+        # arguments reach the callee, which never reads them (coolstep's
+        # cieabundance(q(7:nq,..),chemrate,q(1,..)) against
+        # cieabundance(n,chemrate), timestep.f90:127 / cie.f90:62).
+        if target in self.arity and len(args) > self.arity[target]:
+            args = args[:self.arity[target]]
         if pre:
             self.emit("{", ind)
             for p in pre:

@@ -80,7 +80,8 @@ int ref_setup_c(const evora_params* p) {
   G_chemistry = p->chemistry; G_noncie = p->noncie; G_cooling = p->cooling; G_background = p->background;
   G_bg = p->bg; G_j0 = p->j0; G_c_chem = p->c_chem; G_substep = p->substep; G_rhoh = p->rhoh;
   G_rhohe = p->rhohe; G_cooldt = p->cooldt; G_c_cooldt = p->c_cooldt;
-  if (!G_chemistry) { G_background = 0; G_cooling = 0; G_cooldt = 0; }   /* parameter.f90:95-104 */
+  if (!G_chemistry) { G_background = 0; G_cooling = 0; }   /* parameter.f90:98-103 */
+  if (!G_cooling) G_cooldt = 0;
   G_uv = 0.0;
   G_conduction = p->conduction; G_simplekappa = p->simplekappa; G_c_cond = p->c_cond;
   G_tempfloor = p->tempfloor; G_temp_fl = p->temp_fl; G_jeansfloor = p->jeansfloor; G_c_jeans = p->c_jeans;
@@ -90,6 +91,7 @@ int ref_setup_c(const evora_params* p) {
   G_local_x_start = 0; G_local_nx = p->nz;
   /* the time scalars a fresh program starts with (static storage) */
   G_dt = 0.0; G_redshift = 0.0; G_oldcosmo = 0.0; G_cosmodot = 0.0; G_expand = 0.0;
+  G_nh = 0.0; G_nhe = 0.0;
   /* main.f90:52-62: compparameter, cosmostart (comoving), compunits */
   GUARD(ref_compparameter(); ref_decomposition(); if (G_supercomoving) ref_cosmostart(); ref_compunits();
         if (G_chemistry) { G_chih = G_rhoh / G_mh; G_chihe = G_rhohe / G_mhe; ref_compcoef(); });
@@ -178,17 +180,31 @@ int ref_thermalstep_c(double* q, double* w, double* dt) {
   *dt = G_dt;
   return 0;
 }
+/* coolstep(q,w), timestep.f90:106-143: reads the module's nH and nHe as the
+ * last chem or initchem left them and writes the abundances back into q. */
+int ref_coolstep_c(double* q, double* w, double* dt) {
+#ifdef REF_CIE
+  G_dt = *dt;
+  GUARD(ref_coolstep(q, w));
+  *dt = G_dt;
+  return 0;
+#else
+  (void)q; (void)w; (void)dt;
+  return 1;
+#endif
+}
 int ref_thermalconduction_c(double* q, double* w, double dt) {
   G_dt = dt;
   GUARD(ref_thermalconduction(q, w));
   return 0;
 }
 
-/* main.f90:109-203 without cooling, gravity, chemistry species or output:
- * hydro and, when enabled, the comoving time scalars (125-136), the
- * pressure floors (167), thermal conduction (121, 169-175) and the
- * expansion terms (178).  trace (optional): 8 values per step, the time
- * scalars after updatetime and the dump number the step raised. */
+/* main.f90:109-203 without gravity or output: hydro and, when enabled, the
+ * cooling time-step limit (120, chemistry build), the comoving time scalars
+ * (125-136), chem with the species and the pressure floors (167), thermal
+ * conduction (121, 169-175) and the expansion terms (178).  trace
+ * (optional): 8 values per step, the time scalars after updatetime and the
+ * dump number the step raised. */
 int ref_run_trace_c(double* q, int max_steps, double* trace, double* t, int* steps, double* dt, int* go_out) {
   int64_t nq, nw, ne, ns;
   ref_sizes_c(&nq, &nw, &ne, &ns);
@@ -213,6 +229,9 @@ int ref_run_trace_c(double* q, int max_steps, double* trace, double* t, int* ste
     ref_bound(w);
     G_dt = 1e99;
     if (G_hydro) ref_hydrostep(w);
+#ifdef REF_CIE
+    if (G_cooldt) ref_coolstep(q, w);
+#endif
     if (G_conduction) ref_thermalstep(q, w);
     if (G_supercomoving) {
       ref_cosmostep();

@@ -52,6 +52,7 @@ def lib(cie: bool = False):
         L.ref_thermalstep_c.argtypes = [_dp, _dp, _dp]
         L.ref_chem_c.argtypes = [_dp]
         L.ref_thermalconduction_c.argtypes = [_dp, _dp, ctypes.c_double]
+        L.ref_coolstep_c.argtypes = [_dp, _dp, _dp]
         L.ref_run_trace_c.argtypes = [_dp, ctypes.c_int, _dp, _dp, _ip, _dp, _ip]
         L.ref_get_time_c.argtypes = [_dp]
         L.ref_get_units_c.argtypes = [_dp]
@@ -132,6 +133,13 @@ class RefOracle:
         """thermalstep(q,w) (timestep.f90:72-104): min(dt_in, conduction limit)."""
         d = ctypes.c_double(dt_in)
         st = self.L.ref_thermalstep_c(_p(q), _p(w), ctypes.byref(d))
+        return d.value, st
+
+    def coolstep(self, q, w, dt_in=1e99):
+        """coolstep(q,w) (timestep.f90:106-143), chemistry build: min(dt_in,
+        cooling limit); writes the abundances back into q as there."""
+        d = ctypes.c_double(dt_in)
+        st = self.L.ref_coolstep_c(_p(q), _p(w), ctypes.byref(d))
         return d.value, st
 
     def chem(self, q):

@@ -95,3 +95,62 @@ def test_comoving_runs_with_chemistry_match_reference_bitwise(cfg):
     assert a["status"] == 0 and b["stopped"] == 0 and a["steps"] == b["steps"]
     np.testing.assert_array_equal(a["trace"], b["trace"])
     np.testing.assert_array_equal(q_o, q_r)
+
+
+@pytest.mark.parametrize("cfg", CASES[1:], ids=IDS[1:])
+def test_coolstep_matches_reference_bitwise(cfg):
+    """coolstep(q,w) (timestep.f90:106-143) after initchem and one chem: the
+    limit and the abundances it writes back into q, bit for bit."""
+    p = params(cfg, nx=10, ny=8, nz=6, cooldt=1, c_cooldt=0.3)
+    o, r = Oracle(p), RefOracle(p)
+    q = state(o, 4)
+    q_o, q_r = q.copy(), q.copy()
+    o.initchem(q_o)
+    assert r.initchem(q_r) == 0
+    s = o.time()
+    s[1], s[2], s[6] = 2e-3, 1.0 / 8.0, 7.0
+    o.settime(s)
+    assert r.settime(s) == 0
+    o.chem_at(q_o, s)
+    assert r.chem_at(q_r, s) == 0
+    np.testing.assert_array_equal(q_o, q_r)
+    w = np.zeros(o.shape_w)
+    o.primitive(w, q_o)
+    assert r.primitive(w.copy(), q_r) == 0
+    o.bound(w)
+    before = q_o.copy()
+    dt_o = o.coolstep(q_o, w, 0.7)
+    dt_r, st = r.coolstep(q_r, w.copy(), 0.7)
+    assert st == 0 and o.error() == 0
+    assert dt_o == dt_r and 0.0 < dt_o < 0.7
+    np.testing.assert_array_equal(q_o, q_r)
+    np.testing.assert_array_equal(q_o[..., :6], before[..., :6])
+    # the reference's quirk: every cell's hydrogen total is the last cell's
+    # nH (module global, left by chem), not chiH times the cell's own density
+    h = q_o[..., 6] + q_o[..., 7]
+    np.testing.assert_allclose(h, h.flat[-1], rtol=1e-12)
+    assert not np.allclose(h / q_o[..., 0], h.flat[-1] / q_o[..., 0].flat[-1], rtol=1e-3)
+
+
+@pytest.mark.parametrize("cfg", CASES[1:3], ids=IDS[1:3])
+def test_comoving_runs_with_cooling_timestep_match_reference_bitwise(cfg):
+    """Whole comoving runs with the cooling time-step limit (main.f90:120):
+    dt from coolstep, the abundances it writes back feeding the next chem."""
+    p = params(cfg, nx=12, ny=10, nz=8, boundtype=2, cooldt=1, c_cooldt=0.05)
+    o, r = Oracle(p), RefOracle(p)
+    q = state(o, 3)
+    q_o, q_r = q.copy(), q.copy()
+    o.initchem(q_o)                 # main.f90:94; sets the nH the first coolstep reads
+    assert r.initchem(q_r) == 0
+    a = o.run(q_o, 40, trace=True)
+    b = r.run(q_r, 40, trace=True)
+    assert a["status"] == 0 and b["stopped"] == 0 and a["steps"] == b["steps"] > 10
+    np.testing.assert_array_equal(a["trace"], b["trace"])
+    np.testing.assert_array_equal(q_o, q_r)
+    # the limit binds: the steps are shorter than without it
+    p2 = params(cfg, nx=12, ny=10, nz=8, boundtype=2)
+    q_c = q.copy()
+    o2 = Oracle(p2)
+    o2.initchem(q_c)
+    c = o2.run(q_c, 40, trace=True)
+    assert c["steps"] < a["steps"]
