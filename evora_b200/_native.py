@@ -219,6 +219,7 @@ def _declare_batch(L):
         "evora_gravintegration": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_thermalstep": ([c_void_p, c_void_p, _dp], c_int32),
         "evora_chem": ([c_void_p], c_int32),
+        "evora_coolstep": ([c_void_p, c_void_p, _dp], c_int32),
         "evora_thermalconduction": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),

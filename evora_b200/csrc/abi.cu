@@ -78,6 +78,8 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->substep = p->substep;
   P->chiH = p->rhoh / kMH;
   P->chiHe = p->rhohe / kMHe;
+  P->cooldt = P->cooling && p->cooldt;   // parameter.f90:103
+  P->c_cooldt = p->c_cooldt;
   // compunits (units.f90:26-73) at the start of the run (a = 1/(1+zstart)
   // with supercomoving, main.f90:58-62)
   evora_units u;
@@ -188,8 +190,8 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
   // chemistry: the CIE build only.  The non-equilibrium build advects 12
   // fields through the whole hydro path; conduction with chemistry reads the
   // electron density that w2n leaves unset in the CIE build (nw = 5,
-  // comp.f90:121-135); the cooling time-step limit (coolstep) is not built.
-  if (p->chemistry && (p->noncie || p->conduction || p->cooldt)) return EVORA_ERR_ARG;
+  // comp.f90:121-135).
+  if (p->chemistry && (p->noncie || p->conduction)) return EVORA_ERR_ARG;
   // parameter.f90:164-265
   double g = p->atomic ? (double)(5.0f / 3.0f) : p->g;
   d->g = g;
@@ -242,6 +244,7 @@ struct DropinState {
   HydroParams P{};
   CosmoTime time{};   // module global's time scalars (evora_settime)
   ChemCoef coef{};    // the chemistry's rate coefficients (coef, uv)
+  double nH = 0.0, nHe = 0.0;   // module global's nH, nHe (dropin_set_nh)
   int strict = 0;
   int device = -1;
   unsigned* d_err = nullptr;
@@ -353,6 +356,22 @@ bool evora::dropin_coef(ChemCoef* k) {
   return true;
 }
 
+void evora::dropin_set_nh(double nH, double nHe) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  S.nH = nH;
+  S.nHe = nHe;
+}
+
+bool evora::dropin_nh(double* nH, double* nHe) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.have_params) return false;
+  *nH = S.nH;
+  *nHe = S.nHe;
+  return true;
+}
+
 extern "C" {
 
 int evora_set_params(const evora_params* p) {
@@ -366,6 +385,7 @@ int evora_set_params(const evora_params* p) {
   S.P = P;
   start_time(p, P, &S.time);
   start_coef(P, S.time.cosmo, &S.coef);
+  S.nH = S.nHe = 0.0;   // a fresh program's module global
   S.have_params = true;
   return 0;
 }
@@ -528,6 +548,8 @@ int evora_initchem(double* q) {
     for (int s = 0; s < 6; ++s) c[EVORA_NQ + s] = kNfloor;
     c[EVORA_NQ + 0] = P.chiH * c[0];
     c[EVORA_NQ + 2] = P.chiHe * c[0];
+    S.nH = c[EVORA_NQ + 0];   // module global's nH, nHe: the last cell's stay
+    S.nHe = c[EVORA_NQ + 2];
   }
   return rc;
 }

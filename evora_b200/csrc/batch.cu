@@ -242,8 +242,9 @@ int evora_batch_create(const evora_params* p, int32_t ntubes, const int32_t* n, 
   if (precision != EVORA_FP32 && precision != EVORA_FP64) return EVORA_ERR_ARG;
   *out = nullptr;
   // the tubes run the hydro step alone: the substeps after it (gravity,
-  // floors, conduction, comoving terms) belong to resident grids
-  if (p->gravity || p->tempfloor || p->jeansfloor || p->conduction || p->supercomoving) return EVORA_ERR_ARG;
+  // chemistry and floors, conduction, comoving terms) belong to resident grids
+  if (p->gravity || p->chemistry || p->tempfloor || p->jeansfloor || p->conduction || p->supercomoving)
+    return EVORA_ERR_ARG;
   int nmax = 0;
   long long ntot = 0;
   for (int i = 0; i < ntubes; ++i) {

@@ -14,6 +14,13 @@ namespace evora {
 int chem_step(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
               cudaStream_t st);
 
+// coolstep (timestep.f90:106-143) part 1 on the state at the start of a
+// step (nf fields, f32 or f64) and its species: the smallest cooling time
+// into ctl->vcool (preset by the step's first kernel), the equilibrium
+// abundances written back to the species as the reference's call does.
+int cool_step(const HydroParams& P, const void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
+              cudaStream_t st);
+
 // The rate coefficients at the start of a run (initchem's compcoef, uv = 0)
 // and after a comoving step's compunits (compbackground, compcoef).
 void start_coef(const HydroParams& P, double cosmo, ChemCoef* k);

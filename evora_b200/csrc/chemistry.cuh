@@ -334,4 +334,29 @@ __host__ __device__ inline void cie(const ChemParams& C, const ChemCoef& k, doub
   }
 }
 
+// coolstep's cell term (timestep.f90:123-130): the cooling time
+// |press / (Gamma - Lambda)| at T = press / sum(n) temp0, with n replaced in
+// place by the equilibrium abundances at (nH, nHe) -- module global's, the
+// last cell's of the last chem or initchem, not this cell's.
+__host__ __device__ inline double cool_time(const ChemCoef& k, int background, double temp0, double press,
+                                            double nH, double nHe, double* n, unsigned& err) {
+  double chemrate[kNchem], coolrate[kNcool];
+  const double temp = press / nsum(n) * temp0;
+  comprates(temp, k, background, 1, chemrate, coolrate);
+  cieabundance(nH, nHe, n, chemrate, background, k.uv, err);
+  double lambda, gamma;
+  cool(n, coolrate, background, lambda, gamma);
+  const double coolio = gamma - lambda;
+  return std::fabs(press / coolio);
+}
+
+// coolstep's limit (timestep.f90:136-141): min(dt, c_cooldt v) from v, the
+// smallest cooling time (1e6 when no cell is below it).
+__host__ __device__ inline double cool_dt(double c_cooldt, double v, double dt, unsigned& err) {
+  const double lim = c_cooldt * v;
+  if (lim < dt) dt = lim;
+  if (dt <= 0.0) err |= EVORA_ERR_DT;
+  return dt;
+}
+
 }  // namespace evora

@@ -36,6 +36,12 @@ struct ChemCoef;
 // the start of the run; evora_settime with comoving coordinates).
 bool dropin_coef(ChemCoef* k);
 
+// Module global's nH, nHe of the drop-in layer: 0 after evora_set_params,
+// then the last cell's of each evora_initchem or evora_chem with chemistry
+// (chemistry.f90:50-51, 90-91); coolstep reads them.
+void dropin_set_nh(double nH, double nHe);
+bool dropin_nh(double* nH, double* nHe);
+
 // t = tstart and cosmo = 1 (compparameter), then cosmostart with
 // supercomoving (main.f90:52-58).
 void start_time(const evora_params* p, const HydroParams& P, CosmoTime* s);

@@ -108,13 +108,15 @@ __global__ void k_step_begin(GridCtl* ctl, int use_next) {
   ctl->errnext = 0u;
   ctl->snext[0] = ctl->snext[1] = ctl->snext[2] = 0ull;
   ctl->vcond = ordered_bits(1e99);   // thermalstep's initial v (timestep.f90:82)
+  ctl->vcool = ordered_bits(1e6);    // coolstep's initial v (timestep.f90:121)
   // a raised dump holds the grid until the host has read it
   ctl->active = (ctl->go != 0 && ctl->err == 0 && ctl->dump == 0) ? 1 : 0;
 }
 
-// hydrostep part 2 (timestep.f90:26-57), thermalstep's limit, and the
-// master block of main.f90:124-137: cosmostep and compcosmo (comoving),
-// updatetime, and compunits (comoving).
+// hydrostep part 2 (timestep.f90:26-57), the coolstep and thermalstep
+// limits in main.f90:119-121's order, and the master block of
+// main.f90:124-137: cosmostep and compcosmo (comoving), updatetime, and
+// compunits (comoving).
 __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   if (!ctl->active || ctl->err) {
     ctl->active = 0;
@@ -124,6 +126,7 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   for (int i = 0; i < 3; ++i) sm[i] = __longlong_as_double((long long)ctl->smax[i]);
   unsigned e = 0;
   double dt = cfl_dt(P, sm[0], sm[1], sm[2], 1e99, e);
+  if (!e && P.cooldt) dt = cool_dt(P.c_cooldt, __longlong_as_double((long long)ctl->vcool), dt, e);
   if (!e && P.conduction) dt = thermal_dt(P, units_of(P, ctl), __longlong_as_double((long long)ctl->vcond), dt, e);
   if (e) {
     ctl->err |= e;
@@ -258,6 +261,12 @@ int enqueue_fused_step(evora_grid* g) {
   k_step_begin<<<1, 1, 0, st>>>(g->ctl, use_next ? 1 : 0);
   mark(g);
   if (!use_next) fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
+  if (g->P.cooldt) {
+    // coolstep (main.f90:120) on the state the step starts from
+    int rc = cool_step(g->P, g->qbuf[g->cur], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl, st);
+    if (rc) return rc;
+    g->launches += 1;
+  }
   mark(g);
   k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
   mark(g);

@@ -49,6 +49,7 @@ struct GridCtl {
   unsigned long long smax[3];   // CFL maxima of |u_d| + a (ordered bits)
   unsigned long long snext[3];  // the same, over the state the update wrote
   unsigned long long vcond;     // thermalstep: min over cells of rho / kappa (ordered bits)
+  unsigned long long vcool;     // coolstep: min over cells of the cooling time (ordered bits)
   // comoving coordinates: the time scalars of module global (global.f90:86)
   double cosmo, oldcosmo, cosmodot, expand, redshift;
   // the units compunits derives from cosmo (units.f90:46-63), current step
@@ -89,6 +90,9 @@ struct HydroParams {
   // chemistry of the CIE build (chemistry.f90, cie.f90, rates.f90)
   int chemistry, cooling, background, bg;
   double j0, c_chem, substep, chiH, chiHe;
+  // the cooling time-step limit (coolstep, timestep.f90:106-143)
+  int cooldt;
+  double c_cooldt;
 };
 
 // The units a kernel uses: the grid's current ones when the run is comoving

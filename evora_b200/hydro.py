@@ -178,6 +178,16 @@ class DropIn:
                                       ctypes.byref(d)), "thermalstep")
         return d.value
 
+    def coolstep(self, q, w, dt: float = 1e99) -> float:
+        """coolstep(q,w), timestep.f90:106-143: min(dt, c_cooldt times the
+        smallest cooling time).  As in the reference, q(7:12) is overwritten
+        with the equilibrium abundances at the nH, nHe the last chem or
+        initchem left (its last cell's)."""
+        d = ctypes.c_double(dt)
+        check(lib().evora_coolstep(_ptr(q, self.shape["q"]), _ptr(w, self.shape["w"], False),
+                                   ctypes.byref(d)), "coolstep")
+        return d.value
+
     def thermalconduction(self, q, w, dt: float):
         """thermalconduction(q,w), conduction.f90:26-122 (simplekappa)."""
         check(lib().evora_thermalconduction(_ptr(q, self.shape["q"]), _ptr(w, self.shape["w"], False),

@@ -120,7 +120,7 @@ typedef struct evora_params {
   int32_t cooling;        /* Fortran logical: radiative cooling (cie)         */
   int32_t background;     /* Fortran logical: UV background (implicitcie)     */
   int32_t bg;             /* background model 1..3 (compbackground)           */
-  int32_t cooldt;         /* Fortran logical: cooling time-step limit (refused) */
+  int32_t cooldt;         /* Fortran logical: cooling time-step limit        */
   double j0;              /* background intensity                            */
   double c_chem, substep; /* cooling sub-cycle factors (cie.f90:41)           */
   double rhoh, rhohe;     /* H and He mass fractions                          */
@@ -208,6 +208,18 @@ int evora_hydrostep_noalloc(const double* w, double* dt);
  * reference's call does) and rho from w.  EVORA_ERR_DT if dt <= 0,
  * EVORA_ERR_ARG unless conduction and simplekappa are set. */
 int evora_thermalstep(double* q, const double* w, double* dt);
+
+/* coolstep(q,w), timestep.f90:106-143 (chemistry with cooling and cooldt):
+ * dt = min(dt, c_cooldt v), v the smallest cooling time |p / (Gamma -
+ * Lambda)| over the cells (from 1e6), T = w(5) / sum(n) temp0 with the
+ * cell's abundances q(7:12) as they stand, the rates at the coefficients
+ * evora_settime (or evora_set_params) computed.  As in the reference, the
+ * equilibrium abundances this computes are written back into q(7:12), and
+ * they use the n(H), n(He) of module global as the last evora_chem or
+ * evora_initchem left them (its last cell's), not the cell's own.
+ * EVORA_ERR_DT if dt <= 0, EVORA_ERR_CHEM for abundances out of range,
+ * EVORA_ERR_ARG unless cooldt is set. */
+int evora_coolstep(double* q, const double* w, double* dt);
 
 /* thermalconduction(q,w), conduction.f90:26-122 (simplekappa): the x, y
  * and z conduction sweeps over dt from the primitives w (ghosts filled by

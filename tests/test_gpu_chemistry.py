@@ -111,7 +111,61 @@ def test_fp32_chemistry_grid_tracks_fp64(cuda_device):
 def test_chemistry_refusals(cuda_device):
     """Combinations the CIE build leaves undefined or this build does not
     have are refused at creation."""
-    for extra in (dict(noncie=1), dict(conduction=1, simplekappa=1), dict(cooldt=1)):
+    for extra in (dict(noncie=1), dict(conduction=1, simplekappa=1)):
         p = ev.default_params(**kw_of(dict(cooling=1), nx=8, ny=8, nz=8, **extra))
         with pytest.raises(ev.EvoraError):
             ev.Grid(p, ev.FP64)
+
+
+@pytest.mark.parametrize("cfg", CASES[1:], ids=IDS[1:])
+def test_dropin_coolstep_matches_oracle(cuda_device, cfg):
+    """coolstep(q,w) (timestep.f90:106-143) through the C-ABI after initchem
+    and one chem: the limit and the abundances written back into q."""
+    kw = kw_of(cfg, nx=10, ny=8, nz=6, cooldt=1, c_cooldt=0.3)
+    o = Oracle(make_params(**kw))
+    q = random_q(o, np.random.default_rng(4), pres=(1e-5, 1e-2))
+    drop = ev.DropIn(ev.default_params(**kw), strict=True)
+    q_o, q_g = q.copy(), q.copy()
+    o.initchem(q_o)
+    drop.initchem(q_g)
+    s = o.time()
+    s[1], s[2], s[6] = 2e-3, 1.0 / 8.0, 7.0
+    o.settime(s)
+    drop.settime(dict(zip(TIME_FIELDS, s)))
+    o.chem_at(q_o, s)
+    drop.chem(q_g)
+    w = np.zeros(o.shape_w)
+    o.primitive(w, q_o)
+    o.bound(w)
+    q_g[...] = q_o                      # the same state; nH, nHe from each side's chem
+    dt_o = o.coolstep(q_o, w, 0.7)
+    dt_g = drop.coolstep(q_g, w, 0.7)
+    tol = 1e-8 if cfg.get("background") else 1e-10
+    assert 0.0 < dt_o < 0.7 and abs(dt_g - dt_o) <= tol * dt_o
+    np.testing.assert_array_equal(q_g[..., :6], q_o[..., :6])
+    assert rel(q_g[..., 6:], q_o[..., 6:]) < tol
+    h = q_g[..., 6] + q_g[..., 7]        # the last cell's nH in every cell
+    np.testing.assert_allclose(h, h.flat[-1], rtol=1e-12)
+
+
+@pytest.mark.parametrize("cfg", CASES[1:3], ids=IDS[1:3])
+def test_grid_run_with_cooling_timestep_matches_oracle(cuda_device, cfg):
+    """Comoving grid runs with the cooling time-step limit (main.f90:120):
+    every step's dt from coolstep, its abundances feeding the next chem."""
+    kw = kw_of(cfg, nx=12, ny=10, nz=8, boundtype=2, cooldt=1, c_cooldt=0.05)
+    o = Oracle(make_params(**kw))
+    q0 = state(o, 3)
+    q_o = q0.copy()
+    ref = o.run(q_o, 40, trace=True)
+    assert ref["status"] == 0 and ref["steps"] > 10
+    tr = ref["trace"]
+    with ev.Grid(ev.default_params(**kw), ev.FP64, ev.STRICT | ev.CARRY_ENTROPY) as g:
+        g.set_q(q0)
+        for k in range(len(tr)):
+            g.step(1)
+            s, dump = g.cosmo()
+            np.testing.assert_allclose([s[f] for f in TIME_FIELDS], tr[k, :7], rtol=1e-9, atol=0)
+        assert g.status() == 0
+        q = g.get_q()
+    assert rel(q[..., :6], q_o[..., :6]) < 1e-8
+    assert rel(q[..., 6:], q_o[..., 6:]) < 1e-7
