@@ -460,11 +460,11 @@ def cosmo_params(ev):
 
 
 def run_cosmo(args):
-    """The comoving cosmological box (the cosmological-box configuration
-    without its chemistry network, which is not built): Zel'dovich IC from a
+    """The comoving cosmological box: Zel'dovich IC from a
     seeded power law P(k) ~ k^-2 at z = 50 (ic/cosmo.f90's construction,
     density rms 0.05), T = 100 K, 200 steps of hydro + comoving gravity
-    (cuFFT) + expansion terms, FP32 and FP64.  Reports cell-updates/s, the
+    (cuFFT) + expansion terms and, unless --no-chemistry, the six CIE species
+    with FP64 cooling, FP32 and FP64.  Reports cell-updates/s, the
     fused update's share and roofline, the substeps' time, the redshift
     reached and the FP32 density error against FP64."""
     import torch
@@ -485,6 +485,7 @@ def run_cosmo(args):
             g.set_stream(stream)
             g.set_q(q)
             g.step(args.warmup, sync=True)
+            tune = g.autotune(reps=3) if AUTOTUNE else (0, [])
             torch.cuda.synchronize()
             g.set_timing(True)
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -509,7 +510,8 @@ def run_cosmo(args):
                          "redshift_reached": s["redshift"], "steps_timed": g.time()["k"] - args.warmup,
                          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                       "frac": achieved / peak, "peak_kind": peak_kind},
-                         "gpu_launches": kt["launches"]}
+                         "gpu_launches": kt["launches"],
+                         "autotune": {"chosen": tune[0], "ms_per_tile": tune[1]}}
             g.close()
     if rank == 0:
         v = out["f32"]

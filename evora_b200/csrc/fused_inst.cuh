@@ -17,8 +17,8 @@ using TT = EVORA_T;
 
 // Tile table of this precision: (TX, TY, ZC, CTAs per SM).  Entry 0 is the
 // default; evora_grid_autotune times all entries on the grid itself.  The
-// 5-field 3D kernel is instantiated for every entry, the other variants for
-// entry 0 only.
+// 3D kernels are instantiated for every entry, the 1D and 2D ones for entry
+// 0 only.
 template <int I> struct Tile;
 #if EVORA_PRECISION_F32
 template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3; };
@@ -77,7 +77,12 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
   }
   if (dim == 1) return pick_one<6, 1, 0>(tx, ty, zc, smem, threads, minb);
   if (dim == 2) return pick_one<6, 2, 0>(tx, ty, zc, smem, threads, minb);
-  return pick_one<6, 3, 0>(tx, ty, zc, smem, threads, minb);
+  switch (tile) {
+    case 1: return pick_one<6, 3, 1>(tx, ty, zc, smem, threads, minb);
+    case 2: return pick_one<6, 3, 2>(tx, ty, zc, smem, threads, minb);
+    case 3: return pick_one<6, 3, 3>(tx, ty, zc, smem, threads, minb);
+    default: return pick_one<6, 3, 0>(tx, ty, zc, smem, threads, minb);
+  }
 }
 
 // hydrostep part 1 on the SoA state: maxima of |u_d| + a (per cell in the

@@ -164,8 +164,9 @@ def test_autotune_keeps_state_and_time(cuda_device):
     kw = dict(nx=64, ny=48, nz=40, g=5 / 3, cfl=0.5, boundtype=2, tend=100.0)
     p = ev.default_params(**kw)
     q = ev.ic.kh3d(p)
-    for prec in (ev.FP64, ev.FP32):
-        with ev.Grid(p, prec) as g:
+    # 5 fields, and 6 (the entropy carried: the dual-energy kernels)
+    for prec, flags in ((ev.FP64, 0), (ev.FP32, 0), (ev.FP64, ev.CARRY_ENTROPY), (ev.FP32, ev.CARRY_ENTROPY)):
+        with ev.Grid(p, prec, flags) as g:
             g.set_q(q)
             g.step(2)
             before, t0 = g.get_q(), g.time()
@@ -177,7 +178,7 @@ def test_autotune_keeps_state_and_time(cuda_device):
             after = g.get_q()
         # every tile shape gives the same answer bit for bit
         for tile in range(len(ms)):
-            with ev.Grid(p, prec) as g:
+            with ev.Grid(p, prec, flags) as g:
                 g.set_tile(tile)
                 g.set_q(q)
                 g.step(5)
