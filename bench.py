@@ -519,7 +519,7 @@ def run_cosmo(args):
         line = {"metric": METRIC, "value": v["value"], "unit": METRIC, "n_gpus": world, "steps": steps,
                 "warmup": args.warmup, "ms_per_step": v["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "3D comoving cosmological box 256^3 periodic, gamma=5/3, Zel'dovich IC from "
+                "config": {"workload": f"3D comoving cosmological box {NX}^3 periodic, gamma=5/3, Zel'dovich IC from "
                                        "a seeded power law P(k)~k^-2 at z=50 (density rms 0.05), fb=0.17, T=100 K, "
                                        "omega0=0.3, lambda0=0.7, H0=70, 20 Mpc/h; cuFFT comoving gravity and "
                                        "expansion terms; " + ("six species in CIE with FP64 per-cell cooling "
@@ -659,8 +659,9 @@ def main():
     ap.add_argument("--tick-steps", type=int, default=32)
     ap.add_argument("--no-chemistry", action="store_true", help="cosmo: without the CIE chemistry and cooling")
     args = ap.parse_args()
-    global NX, NY, NZ, AUTOTUNE, CHEMISTRY
+    global NX, NY, NZ, AUTOTUNE, CHEMISTRY, WORKLOAD
     NX = NY = NZ = args.size
+    WORKLOAD = WORKLOAD.replace("256^3", f"{NX}^3")
     AUTOTUNE = not args.no_autotune
     CHEMISTRY = not args.no_chemistry
     if args.warmup < 3:
