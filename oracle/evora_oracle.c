@@ -61,7 +61,7 @@ static struct {
   /* chemistry of the CIE build (global.f90:29-35, 63-67, 131-133): q holds
    * nq = 12 values per cell, q(7:12) the species */
   int nq;
-  int chemistry, cooling, background, bg, cooldt;
+  int chemistry, noncie, cooling, background, bg, cooldt;
   double j0, c_chem, substep, chiH, chiHe, c_cooldt;
   /* module global's nH, nHe: chem and initchem set them per cell
    * (chemistry.f90:50-51, 90-91); coolstep reads them as the last cell of
@@ -434,6 +434,85 @@ static void orc_cie(double rho, double* press, double* n) {
   }
 }
 
+/* patankarH (ncie.f90:93-117): the implicit (Patankar) update of n(H),
+ * n(H+) over cdt at the electron density ne. */
+static void orc_patankar_h(double* n, double ne, double cdt, const double* r) {
+  const double p12 = r[3] * ne * cdt;
+  const double p21 = (r[0] * ne + r[6]) * cdt;
+  const double d1inv = 1.0 / (1.0 + p21);
+  const double d2 = 1.0 + p12;
+  const double x2 = (n[1] + p21 * n[0] * d1inv) / (d2 - p21 * p12 * d1inv);
+  const double x1 = (n[0] + p12 * x2) * d1inv;
+  n[0] = x1;
+  n[1] = x2;
+}
+
+/* patankarHe (ncie.f90:119-149): the same for n(He), n(He+), n(He++). */
+static void orc_patankar_he(double* n, double ne, double cdt, const double* r) {
+  const double p34 = r[4] * ne * cdt;
+  const double p43 = (r[1] * ne + r[7]) * cdt;
+  const double p45 = r[5] * ne * cdt;
+  const double p54 = (r[2] * ne + r[8]) * cdt;
+  const double d3inv = 1.0 / (1.0 + p43);
+  const double d4 = 1.0 + p34 + p54;
+  const double d5inv = 1.0 / (1.0 + p45);
+  const double x4 = (n[1] + p43 * n[0] * d3inv + p45 * n[2] * d5inv) / (d4 - p43 * p34 * d3inv - p45 * p54 * d5inv);
+  const double x3 = (n[0] + p34 * x4) * d3inv;
+  const double x5 = (n[2] + p54 * x4) * d5inv;
+  n[0] = x3;
+  n[1] = x4;
+  n[2] = x5;
+}
+
+/* ncie(rho, press, n), ncie.f90:26-90, over the step T.dt: sub-cycles of
+ * cdt = min(dt - ct, c_chem t, dt substep), t the cooling time with cooling,
+ * else the shortest abundance change time max(n / |dn/dt|) (the rates of
+ * the first cycle's T: without cooling they are not recomputed), each a
+ * Patankar update of the H and He ions, then the electron density, ncheck,
+ * the floor and, with cooling, the pressure update. */
+static void orc_ncie(double rho, double* press, double* n) {
+  (void)rho;
+  double r[9], cr[13], lambda = 0.0, gamma = 0.0;
+  double ct = 0.0;
+  long cycles = 0;
+  while (ct < T.dt) {
+    if (++cycles > (1L << 20)) {   /* the library's bound (the reference has none) */
+      set_err(EVORA_ERR_CHEM);
+      break;
+    }
+    if (G.cooling || ct == 0.0) orc_comprates(*press / nsum(n) * G.temp0, r, cr);
+    double cooltime;
+    if (G.cooling) {
+      orc_cool(n, cr, &lambda, &gamma);
+      const double coolio = gamma - lambda;
+      cooltime = fabs(*press / coolio);
+    } else {
+      const double ion1 = (r[0] * n[5] + r[6]) * n[0];
+      const double ion2 = (r[1] * n[5] + r[7]) * n[2];
+      const double ion3 = (r[2] * n[5] + r[8]) * n[3];
+      const double rec1 = r[3] * n[1] * n[5];
+      const double rec2 = r[4] * n[3] * n[5];
+      const double rec3 = r[5] * n[4] * n[5];
+      const double delta[5] = {rec1 - ion1, ion1 - rec1, rec2 - ion2, ion2 - rec2 - ion3 + rec3, ion3 - rec3};
+      cooltime = -HUGE_VAL;   /* maxval, taking an element when it is larger */
+      for (int i = 0; i < 5; ++i) {
+        const double x = n[i] / fabs(delta[i]);
+        if (x > cooltime) cooltime = x;
+      }
+    }
+    const double cdt = fmin2(fmin2(T.dt - ct, G.c_chem * cooltime), T.dt * G.substep);
+    ct = ct + cdt;
+    const double ne = n[5];
+    orc_patankar_h(n, ne, cdt, r);
+    orc_patankar_he(n + 2, ne, cdt, r);
+    n[5] = n[1] + n[3] + 2.0 * n[4];
+    for (int i = 0; i < 5; ++i)   /* ncheck, chemistry.f90:159-176 */
+      if (!(n[i] >= 0.0 && n[i] <= 1e20)) set_err(EVORA_ERR_CHEM);
+    for (int i = 0; i < 6; ++i) n[i] = fmax2(n[i], kNfloor);
+    if (G.cooling) *press = (*press + cdt * gamma) / (1.0 + cdt * lambda / *press);
+  }
+}
+
 void orc_get_coef(double* out) {
   memcpy(out, G.coef, sizeof G.coef);
   out[26] = G.uv;
@@ -545,8 +624,11 @@ int orc_compparameter(const evora_params* p) {
   /* the CIE build (parameter.f90:95-104: no background, cooling or cooling
    * time step without chemistry; initchem: chiH = rhoH / mH with module
    * global's single-precision mH, mHe) */
-  if (p->chemistry && (p->noncie || p->conduction)) return EVORA_ERR_ARG;
+  if (p->chemistry && p->conduction) return EVORA_ERR_ARG;
   G.chemistry = p->chemistry != 0;
+  /* the non-equilibrium build (nf = 12, nw = 11): its chem and initchem
+   * only; the hydro routines here advect 6 fields (orc_run refuses it) */
+  G.noncie = G.chemistry && p->noncie;
   G.nq = G.chemistry ? 12 : 6;
   G.cooling = G.chemistry && p->cooling;
   G.cooldt = G.cooling && p->cooldt;
@@ -1242,7 +1324,8 @@ void orc_chem(double* q) {
         if (G.chemistry) {
           G.nH = G.chiH * c[0];
           G.nHe = G.chiHe * c[0];
-          orc_cie(c[0], &press, c + 6);
+          if (G.noncie) orc_ncie(c[0], &press, c + 6);
+          else orc_cie(c[0], &press, c + 6);
         }
         if (G.cooling || G.tempfloor || G.jeansfloor) {
           if (G.tempfloor) {
@@ -1301,6 +1384,7 @@ void orc_updatetime(int* go, double* t, double* dt) {
  * the step raised (0: none).  Returns the error mask; *t and *steps report
  * the end state, *dt_last the last step. */
 int orc_run_trace(double* q, int max_steps, double* trace, double* t, int* steps, double* dt_last, int* go_out) {
+  if (G.noncie) return EVORA_ERR_ARG;   /* the 12-field hydro update is not restated */
   int64_t nq, nw, ne, ns;
   orc_array_sizes(&nq, &nw, &ne, &ns);
   double* w = (double*)calloc((size_t)nw, sizeof(double));

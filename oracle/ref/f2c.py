@@ -70,13 +70,22 @@ CIE_UNITS = [
 ]
 
 
+# The non-equilibrium build (-DNONCIE: nq = nf = 12, nw = 11) adds the
+# Patankar solver; chem calls both species solvers, so it links the CIE
+# routines as well.
+NCIE_UNITS = [
+    ("source/ncie.f90", ["ncie", "patankarh", "patankarhe"], {}),
+]
+
+
 class F2CError(Exception):
     pass
 
 
 # --------------------------------------------------------------- lexing ---
 # Macros of the build being translated: none for the plain build, {"CIE"}
-# for the equilibrium-chemistry build (global.f90:29-36).
+# for the equilibrium-chemistry build, {"NONCIE"} for the non-equilibrium
+# one (global.f90:29-36).
 DEFINES: set = set()
 
 
@@ -637,6 +646,8 @@ class Translator:
                 return self.promote([self.etype(a, local) for a in node.args])
             if fn == "dble":
                 return "double"
+            if fn == "maxval":
+                return "double"
             if fn == "sum":
                 a = node.args[0]
                 sa = self.sym(a.name, local) if isinstance(a, (Name, Ref)) else None
@@ -717,6 +728,20 @@ class Translator:
             fn = node.name
             if (s and s.external) or (not s and fn in self.functions):
                 return self.fcall(node, local, loopmap)
+            if fn == "maxval":
+                # MAXVAL of a one-dimensional elementwise array expression
+                # (real(8)): a running maximum in element order that takes an
+                # element when it is larger, so NaN elements are passed over
+                a = self.whole(node.args[0], local)
+                sec = self.first_section(a, local)
+                if sec is None:
+                    raise F2CError("maxval of a scalar")
+                ext = self.section_extents(sec, local)
+                if len(ext) != 1:
+                    raise F2CError("maxval over more than one dimension")
+                x = self.c(a, local, ["m_i_"])
+                return (f"({{ double m_ = -HUGE_VAL; for (long m_i_ = 0; m_i_ < {ext[0]}; ++m_i_) "
+                        f"{{ double x_ = {x}; if (x_ > m_) m_ = x_; }} m_; }})")
             if fn == "sum":
                 # SUM of a whole one-dimensional array, accumulated in
                 # element order (no reassociation without -ffast-math)
@@ -798,6 +823,22 @@ class Translator:
             if not (s and s.is_array):
                 return Ref(node.name, [self.whole(a, local) for a in node.args])
         return node
+
+    def first_section(self, node, local):
+        """The first array section (a Ref to an array with a Range) in node."""
+        if isinstance(node, Ref):
+            sa = self.sym(node.name, local)
+            if sa and sa.is_array and any(isinstance(a, Range) for a in node.args):
+                return node
+            for a in node.args:
+                r = self.first_section(a, local)
+                if r is not None:
+                    return r
+        if isinstance(node, Bin):
+            return self.first_section(node.a, local) or self.first_section(node.b, local)
+        if isinstance(node, Un):
+            return self.first_section(node.a, local)
+        return None
 
     def section_extents(self, ref, local):
         s = self.sym(ref.name, local)
@@ -1141,9 +1182,12 @@ class Translator:
 
 def translate(ref_root):
     tr = Translator()
-    units = UNITS + (CIE_UNITS if "CIE" in DEFINES else [])
-    if "CIE" in DEFINES:
+    species = "CIE" in DEFINES or "NONCIE" in DEFINES
+    units = UNITS + (CIE_UNITS if species else []) + (NCIE_UNITS if "NONCIE" in DEFINES else [])
+    if species:
         EXTERNAL_STUBS.discard("cie")
+    if "NONCIE" in DEFINES:
+        EXTERNAL_STUBS.discard("ncie")
     for rel, take, ren in units:
         text = open(os.path.join(ref_root, rel)).read()
         st = statements(text)

@@ -14,7 +14,9 @@
 #include <string.h>
 
 #include "../../include/evora_gpu.h"
-#ifdef REF_CIE
+#if defined(REF_NCIE)
+#include "../_ref/evora_ref_ncie.c"  /* the build with -DNONCIE: nq = nf = 12, nw = 11 */
+#elif defined(REF_CIE)
 #include "../_ref/evora_ref_cie.c"   /* the build with -DCIE: nq = 12 */
 #else
 #include "../_ref/evora_ref.c"
@@ -38,7 +40,9 @@ static void ref_compcoef(void) {}
 static void ref_compbackground(void) {}
 static void ref_initchem(double* q) { (void)q; ref_stop(); }
 #endif
+#ifndef REF_NCIE
 void ref_ncie(double* rho, double* press, double* n) { (void)rho; (void)press; (void)n; ref_stop(); }
+#endif
 
 /* &ic_para of ic/shocktube.f90:39 */
 static double nml_dl = 1.0, nml_ul = 0.0, nml_pl = 1.0, nml_dr = 0.125, nml_ur = 0.0, nml_pr = 0.1,

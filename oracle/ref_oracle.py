@@ -21,6 +21,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libevora_ref.so")
 # the equilibrium-chemistry build (the reference compiled with -DCIE)
 LIB_PATH_CIE = os.path.join(_HERE, "_ref", "libevora_ref_cie.so")
+LIB_PATH_NCIE = os.path.join(_HERE, "_ref", "libevora_ref_ncie.so")
+_PATHS = {False: LIB_PATH, True: LIB_PATH_CIE, "ncie": LIB_PATH_NCIE}
 REF_SOURCES = "/root/reference/source"
 _libs = {}
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -35,7 +37,7 @@ def lib(cie: bool = False):
     if cie not in _libs:
         if os.path.isdir(REF_SOURCES):
             subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref")], check=True)
-        L = ctypes.CDLL(LIB_PATH_CIE if cie else LIB_PATH)
+        L = ctypes.CDLL(_PATHS[cie])
         L.ref_setup_c.argtypes = [ctypes.POINTER(OracleParams)]
         L.ref_sizes_c.argtypes = [ctypes.POINTER(ctypes.c_int64)] * 4
         L.ref_derived_c.argtypes = [_dp]
@@ -78,7 +80,9 @@ class RefOracle:
     """The translated reference for one grid (module global state)."""
 
     def __init__(self, params: OracleParams | None = None, **kw):
-        self.L = lib(cie=bool(getattr(params if params is not None else make_params(**kw), "chemistry", 0)))
+        p_ = params if params is not None else make_params(**kw)
+        chem = bool(getattr(p_, "chemistry", 0))
+        self.L = lib(cie="ncie" if chem and getattr(p_, "noncie", 0) else chem)
         self.p = params if params is not None else make_params(**kw)
         if self.L.ref_setup_c(ctypes.byref(self.p)):
             raise ValueError("the reference stopped in compparameter/decomposition")
