@@ -79,6 +79,7 @@ bool params_to_hydro(const evora_params* p, HydroParams* P, evora_derived* d, in
   P->chiH = p->rhoh / kMH;
   P->chiHe = p->rhohe / kMHe;
   P->cooldt = P->cooling && p->cooldt;   // parameter.f90:103
+  P->noncie = p->chemistry && p->noncie;
   P->c_cooldt = p->c_cooldt;
   // compunits (units.f90:26-73) at the start of the run (a = 1/(1+zstart)
   // with supercomoving, main.f90:58-62)
@@ -187,11 +188,11 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
   // density that w2n leaves unset without chemistry, and a gradient before
   // it is assigned: only the simplekappa branch is defined in this build
   if (p->conduction && !p->simplekappa) return EVORA_ERR_ARG;
-  // chemistry: the CIE build only.  The non-equilibrium build advects 12
-  // fields through the whole hydro path; conduction with chemistry reads the
-  // electron density that w2n leaves unset in the CIE build (nw = 5,
-  // comp.f90:121-135).
-  if (p->chemistry && (p->noncie || p->conduction)) return EVORA_ERR_ARG;
+  // chemistry: conduction with chemistry reads the electron density that
+  // w2n leaves unset in the CIE build (nw = 5, comp.f90:121-135).  The
+  // non-equilibrium build (noncie) is accepted for chem and initchem; the
+  // entry points of its 12-field hydro path refuse it.
+  if (p->chemistry && p->conduction) return EVORA_ERR_ARG;
   // parameter.f90:164-265
   double g = p->atomic ? (double)(5.0f / 3.0f) : p->g;
   d->g = g;
@@ -227,9 +228,11 @@ int evora_compparameter(const evora_params* p, evora_derived* d) {
 
 void evora_array_sizes(const evora_params* p, int64_t* nq, int64_t* nw, int64_t* ne, int64_t* ns) {
   if (nq) *nq = (int64_t)(p->chemistry ? EVORA_NQ_CHEM : EVORA_NQ) * p->nx * p->ny * p->nz;
-  if (nw) *nw = (int64_t)EVORA_NW * (p->nx + 4) * (p->ny + 4) * (p->nz + 4);
-  if (ne) *ne = (int64_t)EVORA_NW * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
-  if (ns) *ns = (int64_t)EVORA_NW * 3 * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+  // nw = 11 primitives in the non-equilibrium build (global.f90:29-36)
+  const int64_t fw = (p->chemistry && p->noncie) ? 11 : EVORA_NW;
+  if (nw) *nw = fw * (p->nx + 4) * (p->ny + 4) * (p->nz + 4);
+  if (ne) *ne = fw * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+  if (ns) *ns = fw * 3 * (p->nx + 2) * (p->ny + 2) * (p->nz + 2);
 }
 
 }  // extern "C"
@@ -301,6 +304,9 @@ int copy_back(double* host, const double* dev, size_t bytes) {
 
 int begin(DropinState& S) {
   if (!S.have_params) return EVORA_ERR_ARG;
+  // the non-equilibrium build carries 11 primitives and advects 12 fields;
+  // these routines take the 5-primitive layout
+  if (S.P.noncie) return EVORA_ERR_ARG;
   int dev = 0;
   CU(cudaGetDevice(&dev));
   if (S.device != dev || !S.d_err) {

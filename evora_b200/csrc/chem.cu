@@ -43,7 +43,8 @@ __device__ __forceinline__ void chem_cell(double* v, double* n, const HydroParam
   const double oldpress = press;
   if (P.chemistry) {
     const ChemParams C{P.cooling, P.background, P.chiH, P.chiHe, P.c_chem, P.substep};
-    cie(C, k, U.temp0, dt, v[0], press, n, err);
+    if (P.noncie) ncie(C, k, U.temp0, dt, press, n, err);
+    else cie(C, k, U.temp0, dt, v[0], press, n, err);
   }
   if (P.cooling || P.tempfloor || P.jeansfloor) {
     if (P.tempfloor) {
@@ -310,7 +311,7 @@ extern "C" int evora_coolstep(double* q, const double* w, double* dt) {
   ChemCoef k;
   double nH, nHe;
   if (!dropin_params(&P) || !dropin_coef(&k) || !dropin_nh(&nH, &nHe)) return EVORA_ERR_ARG;
-  if (!P.cooldt) return EVORA_ERR_ARG;
+  if (!P.cooldt || P.noncie) return EVORA_ERR_ARG;   // w(5, ...) of the CIE build
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_cuda(e, "evora_coolstep");

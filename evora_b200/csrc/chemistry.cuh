@@ -350,6 +350,86 @@ __host__ __device__ inline double cool_time(const ChemCoef& k, int background, d
   return std::fabs(press / coolio);
 }
 
+// patankarH (ncie.f90:93-117): the implicit (Patankar) update of n(H),
+// n(H+) over cdt at the electron density ne.
+__host__ __device__ inline void patankar_h(double* n, double ne, double cdt, const double* r) {
+  const double p12 = r[3] * ne * cdt;
+  const double p21 = (r[0] * ne + r[6]) * cdt;
+  const double d1inv = 1.0 / (1.0 + p21);
+  const double d2 = 1.0 + p12;
+  const double x2 = (n[1] + p21 * n[0] * d1inv) / (d2 - p21 * p12 * d1inv);
+  n[0] = (n[0] + p12 * x2) * d1inv;
+  n[1] = x2;
+}
+
+// patankarHe (ncie.f90:119-149): the same for n(He), n(He+), n(He++).
+__host__ __device__ inline void patankar_he(double* n, double ne, double cdt, const double* r) {
+  const double p34 = r[4] * ne * cdt;
+  const double p43 = (r[1] * ne + r[7]) * cdt;
+  const double p45 = r[5] * ne * cdt;
+  const double p54 = (r[2] * ne + r[8]) * cdt;
+  const double d3inv = 1.0 / (1.0 + p43);
+  const double d4 = 1.0 + p34 + p54;
+  const double d5inv = 1.0 / (1.0 + p45);
+  const double x4 = (n[1] + p43 * n[0] * d3inv + p45 * n[2] * d5inv) / (d4 - p43 * p34 * d3inv - p45 * p54 * d5inv);
+  n[0] = (n[0] + p34 * x4) * d3inv;
+  n[2] = (n[2] + p54 * x4) * d5inv;
+  n[1] = x4;
+}
+
+// ncie (ncie.f90:26-90) for one cell, the non-equilibrium build: sub-cycles
+// of cdt = min(dt - ct, c_chem t, dt substep), t the cooling time with
+// cooling, else max(n / |dn/dt|) over the five ions and atoms at the first
+// cycle's rates (without cooling they are not recomputed); each a Patankar
+// update of H and He at the cycle's electron density, then n(e-), ncheck,
+// the floor and, with cooling, the pressure update.  Bounded like cie.
+__host__ __device__ inline void ncie(const ChemParams& C, const ChemCoef& k, double temp0, double dt,
+                                     double& press, double* n, unsigned& err) {
+  double chemrate[kNchem], coolrate[kNcool];
+  double lambda = 0.0, gamma = 0.0;
+  double ct = 0.0;
+  int cycles = 0;
+  while (ct < dt) {
+    if (++cycles > kCoolMaxCycles) {
+      err |= EVORA_ERR_CHEM;
+      break;
+    }
+    if (C.cooling || ct == 0.0) comprates(press / nsum(n) * temp0, k, C.background, C.cooling, chemrate, coolrate);
+    double tchem;
+    if (C.cooling) {
+      cool(n, coolrate, C.background, lambda, gamma);
+      const double coolio = gamma - lambda;
+      tchem = std::fabs(press / coolio);
+    } else {
+      const double* r = chemrate;
+      const double ion1 = (r[0] * n[5] + r[6]) * n[0];
+      const double ion2 = (r[1] * n[5] + r[7]) * n[2];
+      const double ion3 = (r[2] * n[5] + r[8]) * n[3];
+      const double rec1 = r[3] * n[1] * n[5];
+      const double rec2 = r[4] * n[3] * n[5];
+      const double rec3 = r[5] * n[4] * n[5];
+      const double delta[5] = {rec1 - ion1, ion1 - rec1, rec2 - ion2, ion2 - rec2 - ion3 + rec3, ion3 - rec3};
+      tchem = -HUGE_VAL;   // maxval: an element is taken when it is larger
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const double x = n[i] / std::fabs(delta[i]);
+        if (x > tchem) tchem = x;
+      }
+    }
+    double cdt = dt - ct;   // min(dt - ct, c_chem t, dt substep)
+    const double lim = C.c_chem * tchem, cap = dt * C.substep;
+    if (lim < cdt) cdt = lim;
+    if (cap < cdt) cdt = cap;
+    ct = ct + cdt;
+    const double ne = n[5];
+    patankar_h(n, ne, cdt, chemrate);
+    patankar_he(n + 2, ne, cdt, chemrate);
+    n[5] = n[1] + n[3] + 2.0 * n[4];
+    check_floor(n, err);
+    if (C.cooling) press = (press + cdt * gamma) / (1.0 + cdt * lambda / press);
+  }
+}
+
 // coolstep's limit (timestep.f90:136-141): min(dt, c_cooldt v) from v, the
 // smallest cooling time (1e6 when no cell is below it).
 __host__ __device__ inline double cool_dt(double c_cooldt, double v, double dt, unsigned& err) {

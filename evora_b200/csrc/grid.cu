@@ -410,7 +410,9 @@ int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStr
     }
   }
   if (p->chemistry || p->tempfloor || p->jeansfloor) {
-    if (reference_backend(g)) {
+    // the non-equilibrium build advects the species through the update
+    // (nf = 12); grids advect 5 or 6 fields
+    if (reference_backend(g) || (p->chemistry && p->noncie)) {
       free_grid(g);
       return EVORA_ERR_ARG;   // chem(q) runs on the resident SoA state
     }

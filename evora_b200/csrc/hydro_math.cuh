@@ -92,6 +92,8 @@ struct HydroParams {
   double j0, c_chem, substep, chiH, chiHe;
   // the cooling time-step limit (coolstep, timestep.f90:106-143)
   int cooldt;
+  // the non-equilibrium build's species solver (ncie, ncie.f90:26-149)
+  int noncie;
   double c_cooldt;
 };
 

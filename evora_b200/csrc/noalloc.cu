@@ -136,6 +136,7 @@ extern "C" int evora_hydrostep_noalloc(const double* w, double* dt) {
     evora::set_error_message("evora_hydrostep_noalloc: call evora_set_params first");
     return EVORA_ERR_ARG;
   }
+  if (P.noncie) return EVORA_ERR_ARG;   // w has 11 primitives in that build
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   if (n > kMaxCells) {
     char msg[160];

@@ -68,11 +68,13 @@ def derived(p: EvoraParams) -> EvoraDerived:
 
 def shapes(p: EvoraParams):
     """C shapes of the reference arrays: q has 12 values per cell with
-    chemistry (q(7:12) = the species of the CIE build), else 6."""
+    chemistry (q(7:12) = the species), else 6; w has 11 primitives in the
+    non-equilibrium build (noncie), else 5."""
     nx, ny, nz = p.nx, p.ny, p.nz
     nq = 12 if p.chemistry else 6
-    return dict(q=(nz, ny, nx, nq), w=(nz + 4, ny + 4, nx + 4, 5),
-                evo=(nz + 2, ny + 2, nx + 2, 5), s=(nz + 2, ny + 2, nx + 2, 3, 5))
+    nw = 11 if p.chemistry and p.noncie else 5
+    return dict(q=(nz, ny, nx, nq), w=(nz + 4, ny + 4, nx + 4, nw),
+                evo=(nz + 2, ny + 2, nx + 2, nw), s=(nz + 2, ny + 2, nx + 2, 3, nw))
 
 
 def _ptr(a, shape=None, writable=True):

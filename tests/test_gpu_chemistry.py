@@ -169,3 +169,54 @@ def test_grid_run_with_cooling_timestep_matches_oracle(cuda_device, cfg):
         q = g.get_q()
     assert rel(q[..., :6], q_o[..., :6]) < 1e-8
     assert rel(q[..., 6:], q_o[..., 6:]) < 1e-7
+
+
+NCIE_CASES = [dict(cooling=0), dict(cooling=1), dict(cooling=1, background=1, bg=1, j0=1e-21),
+              dict(cooling=0, background=1, bg=3, j0=1e-21, tempfloor=1, temp_fl=5e3)]
+NCIE_IDS = ["patankar", "patankar-cooling", "patankar-cooling-uv1", "patankar-uv3-tempfloor"]
+
+
+@pytest.mark.parametrize("cfg", NCIE_CASES, ids=NCIE_IDS)
+def test_dropin_noncie_chem_matches_oracle(cuda_device, cfg):
+    """The non-equilibrium build's chem(q) (ncie's Patankar sub-cycles,
+    ncie.f90:26-149) through the C-ABI, three calls in a row, each from the
+    previous one's abundances."""
+    kw = kw_of(dict(cfg, noncie=1), nx=10, ny=8, nz=6)
+    o = Oracle(make_params(**kw))
+    q = random_q(o, np.random.default_rng(6), pres=(1e-5, 1e-2))
+    drop = ev.DropIn(ev.default_params(**kw), strict=True)
+    q_o, q_g = q.copy(), q.copy()
+    o.initchem(q_o)
+    drop.initchem(q_g)
+    np.testing.assert_array_equal(q_g, q_o)
+    s = o.time()
+    s[1], s[2], s[6] = 3e-3, 1.0 / 7.0, 6.0
+    o.settime(s)
+    drop.settime(dict(zip(TIME_FIELDS, s)))
+    for _ in range(3):
+        o.chem_at(q_o, s)
+        drop.chem(q_g)
+        assert o.error() == 0
+        assert rel(q_g[..., :6], q_o[..., :6]) < 1e-10
+        assert rel(q_g[..., 6:], q_o[..., 6:]) < 1e-9
+    assert not np.allclose(q_o[..., 6:8].sum(-1), q_o[..., 6], rtol=1e-3)   # hydrogen ionised
+
+
+def test_noncie_refusals(cuda_device):
+    """The non-equilibrium build advects 12 fields through the hydro update
+    and carries 11 primitives: grids and the routines that take w refuse it;
+    chem and initchem accept it."""
+    kw = kw_of(dict(cooling=1, noncie=1, cooldt=1, c_cooldt=0.1), nx=8, ny=8, nz=8)
+    p = ev.default_params(**kw)
+    with pytest.raises(ev.EvoraError):
+        ev.Grid(p, ev.FP64)
+    drop = ev.DropIn(p, strict=True)
+    o = Oracle(make_params(**kw))
+    q = random_q(o, np.random.default_rng(8), pres=(1e-5, 1e-2))
+    drop.initchem(q)
+    drop.chem(q)
+    w = np.zeros(ev.hydro.shapes(p)["w"])
+    assert w.shape[-1] == 11
+    for call in (lambda: drop.hydrostep(w), lambda: drop.bound(w), lambda: drop.coolstep(q, w)):
+        with pytest.raises(ev.EvoraError):
+            call()
