@@ -114,9 +114,12 @@ typedef struct evora_params {
    * rates.f90; main.f90:94, 135, 167): with chemistry the state is
    * q(12, nx, ny, nz), q(7:12) = n(H, H+, He, He+, He++, e-) in equilibrium
    * (not advected: the CIE build's fluxes are nf = 6, global.f90:31-32).
-   * The non-equilibrium build (noncie) is refused (EVORA_ERR_ARG).          */
+   * The non-equilibrium build (noncie: ncie.f90's Patankar solver, the
+   * species advected, nf = 12, nw = 11) is accepted by evora_chem and
+   * evora_initchem only; grids and the routines that take w refuse it
+   * (EVORA_ERR_ARG).                                                         */
   int32_t chemistry;      /* Fortran logical                                 */
-  int32_t noncie;         /* Fortran logical (refused when set)              */
+  int32_t noncie;         /* Fortran logical: non-equilibrium species (ncie) */
   int32_t cooling;        /* Fortran logical: radiative cooling (cie)         */
   int32_t background;     /* Fortran logical: UV background (implicitcie)     */
   int32_t bg;             /* background model 1..3 (compbackground)           */
@@ -230,7 +233,8 @@ int evora_thermalconduction(double* q, const double* w, double dt);
  * write-back; with chemistry (q(12, ...)) the CIE abundances q(7:12) and,
  * with cooling, the pressure advanced over dt by the sub-cycled cooling
  * update (cie.f90:26-56; dt and, comoving, the units and UV background from
- * evora_settime); then the temperature floor (tempfloor: press = max(press,
+ * evora_settime), or with noncie the abundances advanced over dt by ncie's
+ * Patankar sub-cycles (ncie.f90:26-149), with the same cooling update; then the temperature floor (tempfloor: press = max(press,
  * temp_fl rho / temp0), or temp_fl sum(n) / temp0 with chemistry) and the
  * Jeans floor (jeansfloor: press = max(press, jeansfloor0 rho^2)), with E and
  * S corrected by the pressure change when cooling or a floor is on. */
