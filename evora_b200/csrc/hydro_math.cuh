@@ -338,11 +338,14 @@ __device__ __forceinline__ void riemann(const T* wl, const T* wr, T* f, int dir,
 // Reciprocal.  FP32: the fast-math division of its translation unit.  FP64:
 // Newton-Raphson on a single-precision seed (two iterations: the relative
 // error e of the seed becomes e^2 then e^4, ~2^-92 from 2^-23, i.e. the
-// result is within an ulp).  Valid for |x| in about [1e-37, 1e37], the range
-// of the single-precision seed.
+// result is within an ulp).  The seed and its reciprocal are normal floats
+// for |x| in [2^-126, 2^126]; outside that range (and for 0, inf, NaN) the
+// correctly rounded division is taken instead.
 __device__ __forceinline__ float rcp_fast(float x) { return 1.0f / x; }
 __device__ __forceinline__ double rcp_fast(double x) {
 #if defined(__CUDA_ARCH__)
+  const double a = fabs(x);
+  if (!(a >= 0x1p-126 && a <= 0x1p126)) return 1.0 / x;
   double r = (double)__frcp_rn((float)x);
   double e = fma(-x, r, 1.0);
   r = fma(r, e, r);

@@ -136,7 +136,10 @@ extern "C" int evora_hydrostep_noalloc(const double* w, double* dt) {
     evora::set_error_message("evora_hydrostep_noalloc: call evora_set_params first");
     return EVORA_ERR_ARG;
   }
-  if (P.noncie) return EVORA_ERR_ARG;   // w has 11 primitives in that build
+  if (P.noncie) {
+    evora::set_error_message("evora_hydrostep_noalloc: w has 11 primitives in the non-equilibrium build");
+    return EVORA_ERR_ARG;
+  }
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   if (n > kMaxCells) {
     char msg[160];
@@ -156,8 +159,14 @@ extern "C" int evora_hydrostep_noalloc(const double* w, double* dt) {
   const int nb = (int)((n + kBlock - 1) / kBlock);
   k_partial_max<<<nb, kBlock>>>(P, w, scratch, n);
   k_finish<<<1, 1024>>>(P, scratch, nb, *dt);
+  // a launch that failed would leave the previous call's dt in the array
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    evora::set_cuda_error(e, "evora_hydrostep_noalloc: launch");
+    return EVORA_ERR_CUDA;
+  }
   unsigned long long res[2];
-  cudaError_t e = cudaMemcpy(res, scratch + kSlotDt, sizeof res, cudaMemcpyDeviceToHost);
+  e = cudaMemcpy(res, scratch + kSlotDt, sizeof res, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {
     evora::set_cuda_error(e, "evora_hydrostep_noalloc");
     return EVORA_ERR_CUDA;

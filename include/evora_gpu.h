@@ -166,6 +166,12 @@ const char* evora_last_error(void);
 /* Library version string. */
 const char* evora_version(void);
 
+/* Self-test of the FP64 reciprocal of the fast arithmetic forms (no
+ * counterpart in the reference, which divides): for host arrays x[n],
+ * out[i] = the device's fast reciprocal of x[i] and out[n + i] = the device's
+ * correctly rounded 1.0 / x[i]; out holds 2n doubles. */
+int evora_selftest_rcp(const double* x, double* out, int64_t n);
+
 /* -------------------------------------------------------- drop-in layer -- */
 /* Set the module-global hydro parameters used by the routines below (the
  * analogue of `use global` after compparameter).  Must be called first. */

@@ -46,3 +46,16 @@ def rel_l1(a, b):
     num = np.abs(a - b).sum(axis=0)
     den = np.abs(b).sum(axis=0)
     return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+def oracle_tube_task(task):
+    """One 1D tube through the oracle's time loop, for a spawned worker
+    process: task = (params dict, cells, q of shape (cells, 6)).  Returns
+    (q after the run, run info)."""
+    from oracle.oracle import Oracle, make_params
+    kw, n, q = task
+    o = Oracle(make_params(nx=n, ny=1, nz=1, **kw))
+    o.set_threads(1)
+    qq = np.ascontiguousarray(q, dtype=np.float64).reshape(1, 1, n, 6).copy()
+    r = o.run(qq, 1 << 30)
+    return qq.reshape(n, 6), r

@@ -220,3 +220,11 @@ def test_noncie_refusals(cuda_device):
     for call in (lambda: drop.hydrostep(w), lambda: drop.bound(w), lambda: drop.coolstep(q, w)):
         with pytest.raises(ev.EvoraError):
             call()
+    # the allocation-free CFL step refuses it too, with its own message
+    import ctypes
+    import torch
+    from evora_b200._native import lib
+    wd = torch.zeros(w.shape, dtype=torch.float64, device=cuda_device)
+    dt = ctypes.c_double(1e99)
+    assert lib().evora_hydrostep_noalloc(ctypes.c_void_p(wd.data_ptr()), ctypes.byref(dt)) == 128
+    assert b"non-equilibrium" in lib().evora_last_error()
