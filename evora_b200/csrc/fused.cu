@@ -17,11 +17,12 @@ struct Inst {
   FusedLaunch (*pick)(int, int, int, int*, int*, int*, size_t*, int*, int*);
   int (*tiles)();
   void (*cfl)(const FusedPlan&, const void*, GridCtl*, cudaStream_t);
+  bool (*fits)(const HydroParams&, int, int, int);
 };
 Inst inst_of(int precision, int strict) {
-  if (precision == EVORA_FP32) return {f32::pick, f32::tiles, f32::cfl};
-  if (strict) return {f64s::pick, f64s::tiles, f64s::cfl};
-  return {f64::pick, f64::tiles, f64::cfl};
+  if (precision == EVORA_FP32) return {f32::pick, f32::tiles, f32::cfl, f32::tile_fits};
+  if (strict) return {f64s::pick, f64s::tiles, f64s::cfl, f64s::tile_fits};
+  return {f64::pick, f64::tiles, f64::cfl, f64::tile_fits};
 }
 }  // namespace
 
@@ -59,6 +60,7 @@ int choose_zc(const HydroParams& P, int tx, int ty, int minb, int zc_default) {
 void fused_set_tile(FusedPlan* pl, int tile) {
   const Inst in = inst_of(pl->precision, pl->strict);
   if (tile < 0 || tile >= in.tiles()) tile = 0;
+  if (!in.fits(pl->P, pl->nf, pl->dim, tile)) tile = 0;
   pl->tile = tile;
   pl->launch = in.pick(pl->nf, pl->dim, tile, &pl->tx, &pl->ty, &pl->zc, &pl->smem, &pl->threads, &pl->minb);
   const HydroParams& P = pl->P;

@@ -90,6 +90,7 @@ void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams&
   namespace ns {                                                                             \
   FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb); \
   int tiles();                                                                               \
+  bool tile_fits(const HydroParams& P, int nf, int dim, int tile);                           \
   void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st);                \
   }
 EVORA_DECLARE_FUSED_NS(f64)

@@ -5,33 +5,81 @@
 // EVORA_TX, EVORA_TY, EVORA_ZC.
 #pragma once
 
+#include <cudaTypedefs.h>
+
 #include "batch_kernel.cuh"
 #include "conduction.h"
 #include "fused.h"
 #include "fused_kernel.cuh"
+#include "fused_tma.cuh"
 
 namespace evora {
 namespace EVORA_FNS {
 
 using TT = EVORA_T;
 
-// Tile table of this precision: (TX, TY, ZC, CTAs per SM).  Entry 0 is the
-// default; evora_grid_autotune times all entries on the grid itself.  The
-// 3D kernels are instantiated for every entry, the 1D and 2D ones for entry
-// 0 only.
+// Tile table of this precision: (TX, TY, ZC, CTAs per SM, TMA).  TMA = 1:
+// the tensor-staged 3D kernel of fused_tma.cuh, for grids tiled by whole
+// tiles (the plan falls back to entry 0 elsewhere).  Entry 0 is the default
+// for grids the TMA kernel does not take; evora_grid_autotune times all
+// entries on the grid itself.  The 3D kernels are instantiated for every
+// entry, the 1D and 2D ones for entry 0 only.
 template <int I> struct Tile;
 #if EVORA_PRECISION_F32
-template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3; };
-template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MINB = 3; };
-template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2; };
-template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4; };
+template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 0; };
+template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MINB = 3, TMA = 0; };
+template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 0; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4, TMA = 0; };
+template <> struct Tile<4> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
 #else
-template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3; };
-template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3; };
-template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3; };
-template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3; };
+template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3, TMA = 0; };
+template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3, TMA = 0; };
+template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3, TMA = 0; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3, TMA = 0; };
+template <> struct Tile<4> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
 #endif
-constexpr int kTiles = 4;
+constexpr int kTiles = 5;
+
+// cuTensorMapEncodeTiled from the driver (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The 4D map (x, y, z, field) of an SoA state q[f][z][y][x] with a box of
+// one halo'd plane of all fields, as fused_tma.cuh stages it.
+template <int NF, int TX, int TY>
+bool encode_state_map(const HydroParams& P, const void* q, CUtensorMap* map) {
+  using S = TmaSmem<TT, NF, TX, TY>;
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nz, (cuuint64_t)NF};
+  const cuuint64_t es = sizeof(TT);
+  const cuuint64_t strides[3] = {es * P.nx, es * P.nx * P.ny, es * P.nx * P.ny * P.nz};
+  const cuuint32_t box[4] = {(cuuint32_t)S::SX, (cuuint32_t)S::RY, 1, (cuuint32_t)NF};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, sizeof(TT) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         4, const_cast<void*>(q), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Whether the TMA kernel of this shape takes the grid: whole tiles in x and
+// y, a 3D grid, 16-byte aligned rows.
+template <int TX, int TY>
+bool tma_fits(const HydroParams& P, int dim) {
+  return dim == 3 && P.nx % TX == 0 && P.ny % TY == 0 && ((size_t)P.nx * sizeof(TT)) % 16 == 0;
+}
 
 template <int NF, int DIM, int I>
 void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
@@ -40,7 +88,19 @@ void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cuda
     k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
   } else {
     using C = Tile<I>;
-    k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A);
+    if constexpr (C::TMA && DIM == 3) {
+      CUtensorMap map;
+      if (encode_state_map<NF, C::TX, C::TY>(pl.P, qin, &map)) {
+        k_fused_tma<TT, NF, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A, map);
+        return;
+      }
+      // the map was checked at plan time; should it fail here, the same
+      // tile runs without tensor staging
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>
+          <<<pl.grid, pl.threads, sizeof(FusedSmem<TT, NF, C::TX, C::TY>), st>>>(A);
+    } else {
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A);
+    }
   }
 }
 
@@ -56,11 +116,29 @@ FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads, int*
     auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if constexpr (C::TMA && DIM == 3) {
+      *smem = sizeof(TmaSmem<TT, NF, C::TX, C::TY>);
+      auto kt = k_fused_tma<TT, NF, C::TX, C::TY, C::ZC, C::MINB>;
+      cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+      cudaFuncSetAttribute(kt, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
   }
   return &launch<NF, DIM, I>;
 }
 
 int tiles() { return kTiles; }
+
+// Whether tile entry `tile` can run this grid (TMA entries need whole tiles
+// and an encodable tensor map).
+bool tile_fits(const HydroParams& P, int nf, int dim, int tile) {
+  if (tile != 4) return true;
+  using C = Tile<4>;
+  if (!tma_fits<C::TX, C::TY>(P, dim)) return false;
+  // encode against an aligned dummy address: only shapes and strides are checked
+  CUtensorMap map;
+  const void* fake = reinterpret_cast<const void*>((uintptr_t)1 << 20);
+  return nf == 5 ? encode_state_map<5, C::TX, C::TY>(P, fake, &map) : encode_state_map<6, C::TX, C::TY>(P, fake, &map);
+}
 
 FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb) {
   if (nf == 5 && dim == 3) {
@@ -68,6 +146,7 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
       case 1: return pick_one<5, 3, 1>(tx, ty, zc, smem, threads, minb);
       case 2: return pick_one<5, 3, 2>(tx, ty, zc, smem, threads, minb);
       case 3: return pick_one<5, 3, 3>(tx, ty, zc, smem, threads, minb);
+      case 4: return pick_one<5, 3, 4>(tx, ty, zc, smem, threads, minb);
       default: return pick_one<5, 3, 0>(tx, ty, zc, smem, threads, minb);
     }
   }
@@ -81,6 +160,7 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
     case 1: return pick_one<6, 3, 1>(tx, ty, zc, smem, threads, minb);
     case 2: return pick_one<6, 3, 2>(tx, ty, zc, smem, threads, minb);
     case 3: return pick_one<6, 3, 3>(tx, ty, zc, smem, threads, minb);
+    case 4: return pick_one<6, 3, 4>(tx, ty, zc, smem, threads, minb);
     default: return pick_one<6, 3, 0>(tx, ty, zc, smem, threads, minb);
   }
 }

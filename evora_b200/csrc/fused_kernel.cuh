@@ -249,19 +249,18 @@ __device__ __forceinline__ void cfl_speeds(const T* qs, const HydroParams& P, bo
   s[2] = fabs(w[3]) + a;
 }
 
-// Slopes, predictor and face states of one cell of plane c.  (cx, cy) are
-// coordinates in the halo ring arrays.  DIM = 2 or 3 selects the 2D
-// (muscl.f90:70-88) or 3D (89-111) predictor.
-template <typename T, int DIM, int TX, int TY, typename Sm>
-__device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn, int cx, int cy,
-                                           const HydroParams& P, T dt2, T* wv, T (*face)[2][5]) {
+// Slopes, predictor and face states of one cell.  get(f, dx, dy, dz) reads
+// primitive f of the neighbour at offset (dx, dy, dz) (one axis at a time).
+// DIM = 2 or 3 selects the 2D (muscl.f90:70-88) or 3D (89-111) predictor.
+template <typename T, int DIM, typename Get>
+__device__ __forceinline__ void cell_faces_g(Get get, const HydroParams& P, T dt2, T* wv, T (*face)[2][5]) {
   T sx[5], sy[5], sz[5];
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
-    wv[f] = sm.w[sc][f][cy][cx];
-    sx[f] = slope_k(sm.w[sc][f][cy][cx - 1], wv[f], sm.w[sc][f][cy][cx + 1], P.limiter);
-    sy[f] = slope_k(sm.w[sc][f][cy - 1][cx], wv[f], sm.w[sc][f][cy + 1][cx], P.limiter);
-    if (DIM == 3) sz[f] = slope_k(sm.w[sp][f][cy][cx], wv[f], sm.w[sn][f][cy][cx], P.limiter);
+    wv[f] = get(f, 0, 0, 0);
+    sx[f] = slope_k(get(f, -1, 0, 0), wv[f], get(f, 1, 0, 0), P.limiter);
+    sy[f] = slope_k(get(f, 0, -1, 0), wv[f], get(f, 0, 1, 0), P.limiter);
+    if (DIM == 3) sz[f] = slope_k(get(f, 0, 0, -1), wv[f], get(f, 0, 0, 1), P.limiter);
   }
   if (!P.secondorder) {
     // first-order Godunov: the face states are the cell averages (sweep,
@@ -295,6 +294,20 @@ __device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn,
       face[2][1][f] = face_plus(wv[f], sz[f], evo[f]);
     }
   }
+}
+
+// cell_faces_g on the shared-memory ring: (cx, cy) are coordinates in the
+// halo ring arrays, sp / sc / sn the ring slots of planes c-1, c, c+1.
+template <typename T, int DIM, int TX, int TY, typename Sm>
+__device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn, int cx, int cy,
+                                           const HydroParams& P, T dt2, T* wv, T (*face)[2][5]) {
+  cell_faces_g<T, DIM>(
+      [&](int f, int dx, int dy, int dz) -> T {
+        if (dz < 0) return sm.w[sp][f][cy][cx];
+        if (dz > 0) return sm.w[sn][f][cy][cx];
+        return sm.w[sc][f][cy + dy][cx + dx];
+      },
+      P, dt2, wv, face);
 }
 
 // The tile program of one CTA.  tid in [0, TX*TY); (bx, by, bz) its tile.

@@ -123,3 +123,54 @@ def test_emulated_update_reduces_next_cfl_maxima(emu, case):
     assert err == 0
     np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
     assert cfl_dt(o, smax) == dt_next
+
+
+# The tensor-staged march (fused_tma.cuh) on grids of whole tiles, with the
+# z march split into chunks of zc planes (0: the tile's own), against the
+# oracle bit for bit, and its next-step CFL maxima.
+TMA_CASES = [
+    # nx, ny, nz, boundtype, nf, limiter, solver, tile, secondorder, zc
+    (16, 8, 9, 2, 5, 1, 2, 2, 1, 0),
+    (32, 16, 7, 1, 5, 1, 2, 2, 1, 3),
+    (16, 16, 12, 3, 5, 2, 1, 2, 1, 5),
+    (16, 8, 6, 2, 6, 3, 2, 2, 1, 0),
+    (16, 8, 5, 3, 6, 1, 1, 2, 0, 2),
+    (8, 4, 6, 2, 5, 1, 2, 0, 1, 4),
+    (8, 8, 3, 1, 5, 1, 2, 0, 1, 2),
+]
+
+
+@pytest.fixture(scope="module")
+def emu_tma():
+    subprocess.run(["make", "-s", "-C", EMU], check=True)
+    L = ctypes.CDLL(os.path.join(EMU, "_build", "libfused_emu.so"))
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.emu_fused_update_cfl.argtypes = [ctypes.POINTER(HP), ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int, dp]
+    L.emu_set_pipeline.argtypes = [ctypes.c_int]
+    L.emu_set_zc.argtypes = [ctypes.c_int]
+    L.emu_set_pipeline(2)
+    yield L
+    L.emu_set_zc(0)
+    L.emu_set_pipeline(0)
+
+
+@pytest.mark.parametrize("case", TMA_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-bt{c[3]}-nf{c[4]}-t{c[7]}-zc{c[9]}")
+def test_emulated_tma_march_is_bitwise_oracle(emu_tma, case):
+    nx, ny, nz, bt, nf, lim, sol, tile, so, zc = case
+    o = Oracle(make_params(nx=nx, ny=ny, nz=nz, boundtype=bt, limiter=lim, solver=sol, g=5 / 3, cfl=0.4,
+                           secondorder=so))
+    q = random_q(o, np.random.default_rng(nx * 131 + ny * 7 + nz))
+    q2, dt, _ = oracle_step(o, q)
+    _, dt_next, _ = oracle_step(o, q2)
+    assert o.error() == 0
+    n = nx * ny * nz
+    qin = np.ascontiguousarray(q.reshape(n, 6).T[:nf])
+    qout = np.zeros_like(qin)
+    smax = np.zeros(3)
+    dp = ctypes.POINTER(ctypes.c_double)
+    emu_tma.emu_set_zc(zc)
+    err = emu_tma.emu_fused_update_cfl(ctypes.byref(hp_of(o)), nf, qin.ctypes.data_as(dp), qout.ctypes.data_as(dp),
+                                       dt, tile, smax.ctypes.data_as(dp))
+    assert err == 0
+    np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
+    assert cfl_dt(o, smax) == dt_next
