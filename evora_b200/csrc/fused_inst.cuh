@@ -12,6 +12,9 @@
 #include "fused.h"
 #include "fused_kernel.cuh"
 #include "fused_tma.cuh"
+#if EVORA_PRECISION_F32
+#include "fused_pair.cuh"
+#endif
 
 namespace evora {
 namespace EVORA_FNS {
@@ -31,14 +34,17 @@ template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MIN
 template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 0; };
 template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4, TMA = 0; };
 template <> struct Tile<4> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
+// two cells per thread on packed FP32 pairs (fused_pair.cuh)
+template <> struct Tile<5> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 2; };
+constexpr int kTiles = 6;
 #else
 template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3, TMA = 0; };
 template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3, TMA = 0; };
 template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3, TMA = 0; };
 template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3, TMA = 0; };
 template <> struct Tile<4> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
-#endif
 constexpr int kTiles = 5;
+#endif
 
 // cuTensorMapEncodeTiled from the driver (no link against libcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -88,7 +94,19 @@ void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cuda
     k_fused1d<TT, NF><<<pl.grid, pl.threads, 0, st>>>(A);
   } else {
     using C = Tile<I>;
-    if constexpr (C::TMA && DIM == 3) {
+#if EVORA_PRECISION_F32
+    if constexpr (C::TMA == 2 && DIM == 3 && NF == 5) {
+      CUtensorMap map;
+      if (encode_state_map<5, C::TX, C::TY>(pl.P, qin, &map)) {
+        k_fused_pair<C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A, map);
+        return;
+      }
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, 2>
+          <<<pl.grid, C::TX * C::TY, sizeof(FusedSmem<TT, NF, C::TX, C::TY>), st>>>(A);
+      return;
+    }
+#endif
+    if constexpr (C::TMA == 1 && DIM == 3) {
       CUtensorMap map;
       if (encode_state_map<NF, C::TX, C::TY>(pl.P, qin, &map)) {
         k_fused_tma<TT, NF, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A, map);
@@ -113,10 +131,19 @@ FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads, int*
     *tx = C::TX; *ty = C::TY; *zc = DIM == 3 ? C::ZC : 1; *minb = C::MINB;
     *smem = sizeof(FusedSmem<TT, NF, C::TX, C::TY>);
     *threads = C::TX * C::TY;
-    auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>;
+    auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::TMA == 2 ? 2 : C::MINB>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if constexpr (C::TMA && DIM == 3) {
+#if EVORA_PRECISION_F32
+    if constexpr (C::TMA == 2 && DIM == 3 && NF == 5) {
+      *smem = sizeof(PairSmem<float, C::TX, C::TY>);
+      *threads = C::TX / 2 * C::TY;
+      auto kp = k_fused_pair<C::TX, C::TY, C::ZC, C::MINB>;
+      cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+      cudaFuncSetAttribute(kp, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+#endif
+    if constexpr (C::TMA == 1 && DIM == 3) {
       *smem = sizeof(TmaSmem<TT, NF, C::TX, C::TY>);
       auto kt = k_fused_tma<TT, NF, C::TX, C::TY, C::ZC, C::MINB>;
       cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
@@ -131,6 +158,14 @@ int tiles() { return kTiles; }
 // Whether tile entry `tile` can run this grid (TMA entries need whole tiles
 // and an encodable tensor map).
 bool tile_fits(const HydroParams& P, int nf, int dim, int tile) {
+#if EVORA_PRECISION_F32
+  if (tile == 5) {
+    using C5 = Tile<5>;
+    if (nf != 5 || !pair_config(P) || !tma_fits<C5::TX, C5::TY>(P, dim)) return false;
+    CUtensorMap map;
+    return encode_state_map<5, C5::TX, C5::TY>(P, reinterpret_cast<const void*>((uintptr_t)1 << 20), &map);
+  }
+#endif
   if (tile != 4) return true;
   using C = Tile<4>;
   if (!tma_fits<C::TX, C::TY>(P, dim)) return false;
@@ -147,6 +182,9 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
       case 2: return pick_one<5, 3, 2>(tx, ty, zc, smem, threads, minb);
       case 3: return pick_one<5, 3, 3>(tx, ty, zc, smem, threads, minb);
       case 4: return pick_one<5, 3, 4>(tx, ty, zc, smem, threads, minb);
+#if EVORA_PRECISION_F32
+      case 5: return pick_one<5, 3, 5>(tx, ty, zc, smem, threads, minb);
+#endif
       default: return pick_one<5, 3, 0>(tx, ty, zc, smem, threads, minb);
     }
   }

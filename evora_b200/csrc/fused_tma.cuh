@@ -592,8 +592,8 @@ __device__ __forceinline__ void tma_tile(const FusedArgs<T>& A, const TmaMap& ma
 #if !defined(EVORA_HOST_EMU)
 template <typename T, int NF, int TX, int TY, int ZC, int MINB>
 __global__ void __launch_bounds__(TX* TY, MINB) k_fused_tma(FusedArgs<T> A, const __grid_constant__ CUtensorMap map) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  auto& sm = *reinterpret_cast<TmaSmem<T, NF, TX, TY>*>(smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_staged[];
+  auto& sm = *reinterpret_cast<TmaSmem<T, NF, TX, TY>*>(smem_staged);
   tma_tile<T, NF, TX, TY, ZC>(A, map, sm, threadIdx.x, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 #endif

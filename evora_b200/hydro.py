@@ -28,6 +28,9 @@ FP32 = 1
 CARRY_ENTROPY = 1
 STRICT = 2
 REFERENCE_KERNELS = 4
+# tile entry of the FP32 table that runs two cells per thread on packed FP32
+# pairs (its sums are associated differently from the other FP32 kernels)
+FP32_PAIR_TILE = 5
 
 
 # ------------------------------------------------------------- parameters --
@@ -365,7 +368,8 @@ class Grid:
 
 
 __all__ = ["EvoraError", "EvoraParams", "EvoraDerived", "default_params", "derived", "shapes",
-           "DropIn", "Grid", "Batch", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS"]
+           "DropIn", "Grid", "Batch", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS",
+           "FP32_PAIR_TILE"]
 
 
 # --------------------------------------------------------- batched tubes --

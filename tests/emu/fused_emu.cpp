@@ -9,6 +9,7 @@
 #define EVORA_FNS emu
 #include "../../evora_b200/csrc/fused_kernel.cuh"
 #include "../../evora_b200/csrc/fused_tma.cuh"
+#include "../../evora_b200/csrc/fused_pair.cuh"
 
 #include <cstring>
 #include <memory>
@@ -23,7 +24,9 @@ using namespace evora::emu;
 // 1: the two-barrier pipelined 3D march (the FP32 kernels' schedule),
 // 0: the three-barrier march (the FP64 kernels' schedule),
 // 2: the tensor-staged march of fused_tma.cuh (3D grids of whole tiles; the
-//    tensor load is a copy by the issuing thread)
+//    tensor load is a copy by the issuing thread),
+// 3: the two-cells-per-thread march of fused_pair.cuh (fast-form arithmetic
+//    in FP64 here: equal to the oracle up to rounding, not bit for bit)
 static int g_pipe = 0;
 extern "C" void emu_set_pipeline(int on) { g_pipe = on; }
 // planes per CTA of the 3D march (0: the tile's ZC)
@@ -53,12 +56,41 @@ static void run_tma_tiles(const FusedArgs<double>& A) {
       }
 }
 
+template <int TX, int TY, int ZC>
+static void run_pair_tiles(const FusedArgs<double>& A) {
+  constexpr int NT = TX / 2 * TY;
+  const HydroParams& P = A.P;
+  const int zc = A.zc > 0 ? A.zc : ZC;
+  const int gx = P.nx / TX, gy = P.ny / TY, gz = (P.nz + zc - 1) / zc;
+  auto sm = std::make_unique<PairSmem<double, TX, TY>>();
+  const void* map = nullptr;
+  for (int bz = 0; bz < gz; ++bz)
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) {
+        std::barrier<> bar(NT);
+        std::vector<std::thread> th;
+        th.reserve(NT);
+        for (int t = 0; t < NT; ++t)
+          th.emplace_back([&, t] {
+            evora_emu::tl_barrier = &bar;
+            pair_tile<double, TX, TY, ZC>(A, map, *sm, t, bx, by, bz);
+          });
+        for (auto& x : th) x.join();
+      }
+}
+
 template <int NF, int DIM, int TX, int TY, int ZC>
 static void run_tiles(const FusedArgs<double>& A) {
   if constexpr (DIM == 3) {
     if (g_pipe == 2 && A.P.nx % TX == 0 && A.P.ny % TY == 0) {
       run_tma_tiles<NF, TX, TY, ZC>(A);
       return;
+    }
+    if constexpr (NF == 5 && TX % 16 == 0 && TX / 2 * TY >= 2 * (TX / 2 + TY)) {
+      if (g_pipe == 3 && A.P.nx % TX == 0 && A.P.ny % TY == 0 && pair_config(A.P)) {
+        run_pair_tiles<TX, TY, ZC>(A);
+        return;
+      }
     }
   }
   constexpr int NT = TX * TY;

@@ -174,3 +174,45 @@ def test_emulated_tma_march_is_bitwise_oracle(emu_tma, case):
     assert err == 0
     np.testing.assert_array_equal(qout, q2.reshape(n, 6).T[:nf])
     assert cfl_dt(o, smax) == dt_next
+
+
+# The two-cells-per-thread march (fused_pair.cuh: packed pairs, shuffles,
+# the fast-form arithmetic) emulated in FP64 on grids of whole tiles: equal
+# to the oracle to rounding (its sums are associated differently), with the
+# next-step CFL maxima.
+PAIR_CASES = [
+    # nx, ny, nz, boundtype, tile, zc
+    (16, 8, 9, 2, 2, 0),
+    (32, 16, 7, 1, 2, 3),
+    (16, 16, 12, 3, 2, 5),
+    (32, 8, 6, 2, 1, 4),
+    (32, 4, 5, 3, 1, 2),
+]
+
+
+@pytest.mark.parametrize("case", PAIR_CASES, ids=lambda c: "x".join(map(str, c[:3])) + f"-bt{c[3]}-t{c[4]}-zc{c[5]}")
+def test_emulated_pair_march_matches_oracle(emu_tma, case):
+    nx, ny, nz, bt, tile, zc = case
+    o = Oracle(make_params(nx=nx, ny=ny, nz=nz, boundtype=bt, limiter=1, solver=2, g=5 / 3, cfl=0.4))
+    q = random_q(o, np.random.default_rng(nx * 17 + ny * 5 + nz))
+    q2, dt, _ = oracle_step(o, q)
+    _, dt_next, _ = oracle_step(o, q2)
+    assert o.error() == 0
+    n = nx * ny * nz
+    qin = np.ascontiguousarray(q.reshape(n, 6).T[:5])
+    qout = np.zeros_like(qin)
+    smax = np.zeros(3)
+    dp = ctypes.POINTER(ctypes.c_double)
+    emu_tma.emu_set_pipeline(3)
+    emu_tma.emu_set_zc(zc)
+    try:
+        err = emu_tma.emu_fused_update_cfl(ctypes.byref(hp_of(o)), 5, qin.ctypes.data_as(dp),
+                                           qout.ctypes.data_as(dp), dt, tile, smax.ctypes.data_as(dp))
+    finally:
+        emu_tma.emu_set_pipeline(2)
+    assert err == 0
+    ref = q2.reshape(n, 6).T[:5]
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert np.abs(qout - ref).max() > 0          # the pair schedule ran (fast forms differ in the last bits)
+    np.testing.assert_allclose(qout, ref, rtol=0, atol=1e-12 * scale.max())
+    assert abs(cfl_dt(o, smax) - dt_next) <= 1e-13 * dt_next
