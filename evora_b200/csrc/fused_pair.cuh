@@ -317,15 +317,22 @@ __device__ __forceinline__ void pair_tile(const FusedArgs<S>& A, const TmaMap& m
   // ---- C: x and y solves of a plane (faces from the previous interval)
   V fxl[5], fxr[5];
   auto solves_xy = [&]() {
-    V wl[5], fv[5];
+    // left states of both solves first, then the two solves as one
+    // straight-line block (independent chains the scheduler interleaves)
+    V wl[5], wly[5], fv[5];
 #pragma unroll
     for (int f = 0; f < 5; ++f) wl[f] = xu[f];
     from_left(wl);
-    if (p == 0) {
+    const M2 first{p == 0, p == 0};
 #pragma unroll
-      for (int f = 0; f < 5; ++f) wl[f] = sm.xrl[f][j];
+    for (int f = 0; f < 5; ++f) {
+      wl[f] = sel2(first, sm.xrl[f][j], wl[f]);
+      wly[f] = sm.yu[f][j][p];
     }
     hllc_p<S, 1>(wl, xl, fxl, c, err);
+    hllc_p<S, 2>(wly, yl, fv, c, err);
+#pragma unroll
+    for (int f = 0; f < 5; ++f) sm.fy[f][j][p] = fv[f];
     // the flux right of the pair: .x through (p, p+1), .y through (p+HX,
     // p+HX+1); pair HX-1 takes .x from pair 0's .y and .y from the closing
     // interface (in the update)
@@ -336,11 +343,6 @@ __device__ __forceinline__ void pair_tile(const FusedArgs<S>& A, const TmaMap& m
       fxr[f].x = p < HX - 1 ? fr[f].x : fr[f].y;
       fxr[f].y = fr[f].y;
     }
-#pragma unroll
-    for (int f = 0; f < 5; ++f) wl[f] = sm.yu[f][j][p];
-    hllc_p<S, 2>(wl, yl, fv, c, err);
-#pragma unroll
-    for (int f = 0; f < 5; ++f) sm.fy[f][j][p] = fv[f];
     if (ecl >= 0) {
       V wr[5];
       if (ecl < TY) {
