@@ -192,21 +192,101 @@ def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0, conduct
     return ms, kt, g
 
 
-def time_e2e(ev, torch, q_pinned, out_pinned, precision, steps):
-    """Per step: host->device q, one step, device->host q (public C ABI)."""
-    g = ev.Grid(kh_params(ev), precision)
-    g.set_q(q_pinned)
-    g.step(1)
-    g.get_q(out_pinned)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
+def time_e2e(ev, torch, q_pinned, outs_pinned, precision, steps):
+    """The step through the public API with host buffers: every step uploads
+    q(6, nx, ny, nz) (FP64, pinned host) with set_q, advances it one step and
+    reads it back with get_q.  Two grids on two streams, each driven by its
+    own host thread, alternate the steps, so one grid's upload overlaps the
+    other's download (PCIe is full duplex) and the kernels.  Returns the wall
+    time of all `steps` steps."""
+    import threading
+    k = len(outs_pinned)
+    grids = [ev.Grid(kh_params(ev), precision) for _ in range(k)]
+    streams = [torch.cuda.Stream() for _ in range(k)]
+    for g, st, out in zip(grids, streams, outs_pinned):
+        g.set_stream(st)
         g.set_q(q_pinned)
-        g.step(1, sync=True)
-        g.get_q(out_pinned)
+        g.step(1)
+        g.get_q(out)
+    torch.cuda.synchronize()
+    share = [steps // k + (1 if i < steps % k else 0) for i in range(k)]
+    errors = []
+
+    def work(i):
+        try:
+            for _ in range(share[i]):
+                grids[i].set_q(q_pinned)
+                grids[i].step(1, sync=True)
+                grids[i].get_q(outs_pinned[i])
+        except Exception as e:  # reported after the join
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(k)]
+    t0 = time.perf_counter()
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
     el = time.perf_counter() - t0
-    g.close()
+    for g in grids:
+        g.close()
+    if errors:
+        raise errors[0]
     return el
+
+
+def oracle_errors(q0, steps, results):
+    """Relative L1 per field of GPU results against the oracle (the CPU
+    restatement of the reference, all host threads) after the same steps
+    from the same initial state: {name: [rho, mx, my, mz, E]}."""
+    from oracle.oracle import Oracle, make_params
+    o = Oracle(make_params(nx=NX, ny=NY, nz=NZ, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6))
+    q = q0.copy()
+    r = o.run(q, steps)
+    if r["status"] or r["steps"] != steps:
+        return {"error": f"oracle status {r['status']} after {r['steps']} steps"}
+    out = {}
+    for name, qg in results.items():
+        num = np.abs(qg[..., :5] - q[..., :5]).reshape(-1, 5).sum(0)
+        den = np.abs(q[..., :5]).reshape(-1, 5).sum(0)
+        out[name] = [float(x) for x in np.where(den > 0, num / np.where(den > 0, den, 1.0), num)]
+    return out
+
+
+def reference_serial(budget_s=8.0):
+    """The reference's own hydro path, translated mechanically from its
+    Fortran sources (oracle/_ref), on one host thread: the analogue of one
+    reference MPI rank, on a z-slab of the workload."""
+    try:
+        from oracle.ref_oracle import RefOracle, LIB_PATH
+        if not os.path.exists(LIB_PATH):
+            return None
+        o = RefOracle(nx=NX, ny=NY, nz=2, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6)
+        q = o.zeros_q()
+        q[...] = _kh_slab(2)
+        t0 = time.perf_counter()
+        o.run(q, 1)
+        per_cell = (time.perf_counter() - t0) / (NX * NY * 2)
+        nz_s = int(max(2, min(NZ, budget_s / max(per_cell, 1e-12) / (NX * NY))))
+        o = RefOracle(nx=NX, ny=NY, nz=nz_s, g=GAMMA, cfl=CFL, boundtype=2, tend=1e6)
+        q = o.zeros_q()
+        q[...] = _kh_slab(nz_s)
+        t0 = time.perf_counter()
+        r = o.run(q, 1)
+        el = time.perf_counter() - t0
+        return {"value": NX * NY * nz_s * max(1, r["steps"]) / el, "unit": METRIC, "cores": 1,
+                "kind": "reference",
+                "sample": f"1 step of a {NX}x{NY}x{nz_s} periodic slab of the workload, FP64, the reference's "
+                          f"Fortran hydro path translated to C (oracle/_ref), one thread, {el:.1f} s"}
+    except Exception as e:  # the serial figure is an extra; the line does not depend on it
+        return {"error": str(e)}
+
+
+def _kh_slab(nz_s):
+    """The KH initial state of a slab of nz_s planes (the IC is z-invariant)."""
+    import evora_b200 as ev
+    p = ev.default_params(nx=NX, ny=NY, nz=nz_s, g=GAMMA, cfl=CFL, boundtype=2)
+    return ev.ic.kh3d(p, seed=42, amp=0.01)
 
 
 def cpu_baseline(steps_budget_s=20.0, threads=None):
@@ -644,6 +724,8 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the full-size comparison of both forms with the CPU oracle")
     ap.add_argument("--size", type=int, default=256,
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
@@ -704,8 +786,8 @@ def main():
         return 0
     # accuracy of the FP32 form against FP64 after the same steps
     tune32, tune64 = g32.tuning, g64.tuning
-    r32 = g32.get_q()[..., 0]
-    r64 = g64.get_q()[..., 0]
+    q32_end, q64_end = g32.get_q(), g64.get_q()
+    r32, r64 = q32_end[..., 0], q64_end[..., 0]
     l1 = float(np.abs(r32 - r64).sum() / np.abs(r64).sum())
     g32.close()
     g64.close()
@@ -719,8 +801,12 @@ def main():
         bytes_alg = n * BYTES_PER_CELL[dtype]
         achieved = bytes_alg / (avg_ms * 1e-3) / 1e9
         traffic = profile_traffic(prof)
+        kern = "k_fused_pair (fused MUSCL-Hancock update, two cells per thread)" if "pair" in prof else \
+            "k_fused (fused MUSCL-Hancock update)"
         return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_fused (fused MUSCL-Hancock update)",
+                "traffic": traffic, "traffic_source": f"profiles/{prof} (one ncu capture of this kernel on this "
+                                                      "workload; not measured in this run)",
+                "peak_kind": peak_kind, "kernel": kern,
                 "kernel_ms": avg_ms, "cfl_kernel_ms": kt["cfl_ms"] / max(1, kt["steps"]),
                 "algorithmic_bytes_per_launch": bytes_alg}
 
@@ -731,7 +817,8 @@ def main():
         "config": {"workload": WORKLOAD, "cells": n, "form": "FP32 state, FP64 pressure recovery (kin>E/2) and "
                    "CFL reduction", "l2": "inputs larger than L2 (335 MB FP32 / 671 MB FP64 state per copy)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "roofline": roofline(kt32, "f32", "fused_update_kh256_fp32.md"),
+        "roofline": roofline(kt32, "f32", "fused_pair_kh256_fp32.md" if tune32[0] == ev.FP32_PAIR_TILE
+                             else "fused_update_kh256_fp32.md"),
         "fp64": {"value": value64, "ms_per_step": ms64 / args.steps,
                  "roofline": roofline(kt64, "f64", "fused_update_kh256_fp64.md")},
         "fp32_over_fp64": value32 / value64,
@@ -744,14 +831,25 @@ def main():
     if not args.no_e2e and rank == 0:
         qp = torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy()
         qp[...] = q
-        outp = torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy()
-        e2e_steps = max(3, min(args.steps, 10))
-        el = time_e2e(ev, torch, qp, outp, ev.FP32, e2e_steps)
+        outs = [torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
+        e2e_steps = max(4, min(args.steps, 10))
+        note = (f"per step: q(6,{NX}^3) FP64 from pinned host -> set_q, 1 step, get_q -> pinned host; two grids "
+                "on two streams alternate the steps so uploads overlap downloads")
+        el = time_e2e(ev, torch, qp, outs, ev.FP32, e2e_steps)
         line["e2e"] = {"value": n * e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": q.nbytes,
-                       "d2h_bytes_per_step": q.nbytes, "form": "FP32",
-                       "note": "per step: q(6,256^3) FP64 from pinned host -> set_q, 1 step, get_q -> host"}
+                       "d2h_bytes_per_step": q.nbytes, "form": "FP32", "note": note}
+        el64 = time_e2e(ev, torch, qp, outs, ev.FP64, e2e_steps)
+        line["fp64"]["e2e"] = {"value": n * e2e_steps / el64, "unit": METRIC, "h2d_bytes_per_step": q.nbytes,
+                               "d2h_bytes_per_step": q.nbytes, "form": "FP64", "note": note}
+    if rank == 0 and world == 1 and not args.no_oracle_check:
+        # both forms against the oracle after the same steps (autotune keeps the state)
+        line["l1_vs_oracle"] = {"steps": args.warmup + args.steps, "fields": ["rho", "mx", "my", "mz", "E"],
+                                **oracle_errors(q, args.warmup + args.steps, {"fp32": q32_end, "fp64": q64_end})}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+        serial = reference_serial()
+        if serial:
+            line["cpu_baseline"]["reference_serial"] = serial
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
