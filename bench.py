@@ -235,6 +235,43 @@ def time_e2e(ev, torch, q_pinned, outs_pinned, precision, steps):
     return el
 
 
+def time_dropin_resident(ev, q, mode, steps, warmup):
+    """main.f90:109-155's call order (primitive, bound, hydrostep,
+    updatetime, compevo, sweep) through the drop-in C ABI on host arrays, in
+    resident mode: the state stays on the GPU between the calls, and
+    evora_sync brings q back once at the end.  Returns (ms per step of the
+    loop, ms of the final sync)."""
+    p = kh_params(ev)
+    sh = ev.shapes(p)
+    w, evo, s = np.zeros(sh["w"]), np.zeros(sh["evo"]), np.zeros(sh["s"])
+    qh = q.copy()
+    di = ev.DropIn(p)
+    di.set_resident(mode)
+    t, go = p.tstart, True
+
+    def step():
+        nonlocal t, go
+        di.primitive(w, qh)
+        di.bound(w)
+        dt = di.hydrostep(w, 1e99)
+        go, t, dt = di.updatetime(go, t, dt)
+        di.compevo(w, evo, s, dt)
+        di.sweep(w, qh, evo, s, dt)
+
+    try:
+        for _ in range(warmup):
+            step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        t1 = time.perf_counter()
+        di.sync(qh)
+        t2 = time.perf_counter()
+    finally:
+        di.set_resident(0)
+    return 1e3 * (t1 - t0) / steps, 1e3 * (t2 - t1)
+
+
 def oracle_errors(q0, steps, results):
     """Relative L1 per field of GPU results against the oracle (the CPU
     restatement of the reference, all host threads) after the same steps
@@ -841,6 +878,17 @@ def main():
         el64 = time_e2e(ev, torch, qp, outs, ev.FP64, e2e_steps)
         line["fp64"]["e2e"] = {"value": n * e2e_steps / el64, "unit": METRIC, "h2d_bytes_per_step": q.nbytes,
                                "d2h_bytes_per_step": q.nbytes, "form": "FP64", "note": note}
+    if not args.no_e2e and rank == 0:
+        # the unmodified driver's call sequence with host arrays, state resident
+        line["dropin_resident"] = {}
+        for mode, name, ms_grid in ((ev.RESIDENT_FP32, "fp32", ms32 / args.steps),
+                                    (ev.RESIDENT_FP64, "fp64", ms64 / args.steps)):
+            ms_step, ms_sync = time_dropin_resident(ev, q, mode, args.steps, args.warmup)
+            line["dropin_resident"][name] = {
+                "ms_per_step": ms_step, "grid_ms_per_step": ms_grid, "over_grid": ms_step / ms_grid,
+                "final_sync_ms": ms_sync, "value": n / (ms_step * 1e-3), "unit": METRIC,
+                "note": "host wall time of primitive, bound, hydrostep, updatetime, compevo, sweep per step "
+                        "(main.f90:109-155) on host arrays in resident mode; evora_sync of q once at the end"}
     if rank == 0 and world == 1 and not args.no_oracle_check:
         # both forms against the oracle after the same steps (autotune keeps the state)
         line["l1_vs_oracle"] = {"steps": args.warmup + args.steps, "fields": ["rho", "mx", "my", "mz", "E"],

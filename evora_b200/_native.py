@@ -116,6 +116,9 @@ def _declare(L):
                                ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)], None),
         "evora_set_params": ([P], c_int32),
         "evora_set_strict": ([c_int32], c_int32),
+        "evora_set_resident": ([c_int32], c_int32),
+        "evora_sync": ([c_void_p], c_int32),
+        "evora_invalidate": ([c_void_p], c_int32),
         "evora_primitive": ([c_void_p, c_void_p], c_int32),
         "evora_bound": ([c_void_p], c_int32),
         "evora_hydrostep": ([c_void_p, _dp], c_int32),

@@ -289,6 +289,13 @@ struct DropinState {
   // staging buffers for host arrays: q, w, evo, s
   double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t stage_bytes[4] = {0, 0, 0, 0};
+  // resident mode (evora_set_resident): 0 off, EVORA_RESIDENT_FP64 or
+  // EVORA_RESIDENT_FP32; the grid holding the state of host array rq
+  int resident = 0;
+  evora_grid* rgrid = nullptr;
+  const double* rq = nullptr;
+  bool rq_device_newer = false;   // the grid has steps the host q lacks
+  bool rq_host_newer = false;     // host q changed after the upload
 };
 
 DropinState& ds() {
@@ -370,7 +377,76 @@ int finish(DropinState& S) {
 
 const DropinOps& ops(const DropinState& S) { return S.strict ? evora::strict::kOps : evora::fast::kOps; }
 
+// ---- resident mode
+// The state goes back to host q when the grid has steps q lacks.
+int resident_download(DropinState& S) {
+  if (!S.rgrid || !S.rq || !S.rq_device_newer) return 0;
+  int rc = evora_grid_get_q(S.rgrid, const_cast<double*>(S.rq));
+  if (rc) return rc;
+  S.rq_device_newer = false;
+  return 0;
+}
+
+// Ends the resident grid (after its state went back to the host).
+int resident_close(DropinState& S) {
+  int rc = resident_download(S);
+  if (S.rgrid) evora_grid_destroy(S.rgrid);
+  S.rgrid = nullptr;
+  S.rq = nullptr;
+  S.rq_device_newer = S.rq_host_newer = false;
+  return rc;
+}
+
+// Binds host q to the resident grid (created on first use with the hydro
+// subset of the parameters), uploading q when it is new or changed.
+int resident_bind(DropinState& S, const double* q) {
+  if (!S.rgrid) {
+    evora_params p = S.params;
+    // the grid runs only the hydro routines; the physics after the update
+    // stays with the drop-in routines of the caller's loop
+    p.gravity = 0;
+    p.conduction = 0;
+    p.tempfloor = p.jeansfloor = 0;
+    p.supercomoving = 0;
+    p.tend = 1e300;
+    const int32_t flags = S.strict ? EVORA_STRICT : 0;
+    const int32_t prec = S.resident == EVORA_RESIDENT_FP32 ? EVORA_FP32 : EVORA_FP64;
+    int rc = evora_grid_create(&p, prec, flags, &S.rgrid);
+    if (rc) {
+      S.rgrid = nullptr;
+      return rc;
+    }
+    S.rq = nullptr;
+  }
+  if (q != S.rq || S.rq_host_newer) {
+    if (S.rq && q != S.rq) {
+      int rc = resident_download(S);   // the previous array keeps its steps
+      if (rc) return rc;
+    }
+    int rc = evora_grid_set_q(S.rgrid, q);
+    if (rc) return rc;
+    S.rq = q;
+    S.rq_host_newer = S.rq_device_newer = false;
+  }
+  return 0;
+}
+
 }  // namespace
+
+void evora::dropin_resident_read(const double* q) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.resident && q && q == S.rq) resident_download(S);
+}
+
+void evora::dropin_resident_write(const double* q) {
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.resident && q && q == S.rq) {
+    resident_download(S);
+    S.rq_host_newer = true;
+  }
+}
 
 bool evora::dropin_params(HydroParams* P) {
   DropinState& S = ds();
@@ -421,6 +497,7 @@ int evora_set_params(const evora_params* p) {
   HydroParams P;
   int rc = 0;
   if (!params_to_hydro(p, &P, nullptr, &rc)) return rc;
+  if ((rc = resident_close(S))) return rc;   // a new run: the last state goes home first
   S.params = *p;
   S.P = P;
   start_time(p, P, &S.time);
@@ -433,7 +510,39 @@ int evora_set_params(const evora_params* p) {
 int evora_set_strict(int32_t strict) {
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
+  if ((strict != 0) != (S.strict != 0) && S.rgrid) {
+    int rc = resident_close(S);   // the next primitive builds the grid in the new mode
+    if (rc) return rc;
+  }
   S.strict = strict != 0;
+  return 0;
+}
+
+int evora_set_resident(int32_t mode) {
+  if (mode != 0 && mode != EVORA_RESIDENT_FP64 && mode != EVORA_RESIDENT_FP32) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (mode != S.resident) {
+    int rc = resident_close(S);
+    if (rc) return rc;
+  }
+  S.resident = mode;
+  return 0;
+}
+
+int evora_sync(double* q) {
+  if (!q) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (!S.resident || q != S.rq) return 0;
+  return resident_download(S);
+}
+
+int evora_invalidate(const double* q) {
+  if (!q) return EVORA_ERR_ARG;
+  DropinState& S = ds();
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.resident && q == S.rq) S.rq_host_newer = true;
   return 0;
 }
 
@@ -443,6 +552,12 @@ int evora_primitive(double* w, double* q) {
   if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
+  if (S.resident) {
+    // the primitives are recovered inside the update from the resident
+    // state (w is not written); p <= 0 is reported by hydrostep
+    if (!w || !q || is_device_pointer(q)) return EVORA_ERR_ARG;
+    return resident_bind(S, q);
+  }
   int64_t nq, nw;
   evora_array_sizes(&S.params, &nq, &nw, nullptr, nullptr);
   double *dq, *dw;
@@ -461,6 +576,7 @@ int evora_bound(double* w) {
   std::lock_guard<std::mutex> lk(S.mu);
   int rc = begin(S);
   if (rc) return rc;
+  if (S.resident) return w ? 0 : EVORA_ERR_ARG;   // the ghost map is applied inside the update
   int64_t nw;
   evora_array_sizes(&S.params, nullptr, &nw, nullptr, nullptr);
   double* dw;
@@ -477,6 +593,19 @@ int evora_hydrostep(const double* w, double* dt) {
   std::lock_guard<std::mutex> lk(S.mu);
   int rc = begin(S);
   if (rc) return rc;
+  if (S.resident) {
+    if (!w) return EVORA_ERR_ARG;
+    if (!S.rgrid || !S.rq) {
+      set_error_message("evora_hydrostep: resident mode needs evora_primitive first");
+      return EVORA_ERR_ARG;
+    }
+    double sm[3];
+    const int st = grid_cfl_maxima(S.rgrid, sm);
+    if (st) return st;
+    unsigned e = 0;
+    *dt = cfl_dt(S.P, sm[0], sm[1], sm[2], *dt, e);
+    return (int)e;
+  }
   int64_t nw;
   evora_array_sizes(&S.params, nullptr, &nw, nullptr, nullptr);
   double* dw;
@@ -563,6 +692,7 @@ int evora_updatetime_cosmo(int32_t* go, int32_t* dump, int32_t* k, evora_time* s
 
 int evora_initchem(double* q) {
   if (!q) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
   if (!S.have_params || !S.P.chemistry || is_device_pointer(q)) return EVORA_ERR_ARG;
@@ -628,6 +758,7 @@ int evora_compevo(const double* w, double* evo, double* s, double dt) {
   std::lock_guard<std::mutex> lk(S.mu);
   int rc = begin(S);
   if (rc) return rc;
+  if (S.resident) return (w && evo && s) ? 0 : EVORA_ERR_ARG;   // slopes and predictor run inside the update
   int64_t nw, ne, ns;
   evora_array_sizes(&S.params, nullptr, &nw, &ne, &ns);
   double *dw, *de, *dss;
@@ -647,6 +778,16 @@ int evora_sweep(const double* w, double* q, const double* evo, const double* s, 
   if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
+  if (S.resident) {
+    if (!w || !evo || !s || !q) return EVORA_ERR_ARG;
+    if (!S.rgrid || q != S.rq || S.rq_host_newer) {
+      set_error_message("evora_sweep: resident mode needs evora_primitive on this q first");
+      return EVORA_ERR_ARG;
+    }
+    const int st = grid_update_dt(S.rgrid, dt);
+    S.rq_device_newer = true;
+    return st;
+  }
   int64_t nq, nw, ne, ns;
   evora_array_sizes(&S.params, &nq, &nw, &ne, &ns);
   double *dq, *dw, *de, *dss;

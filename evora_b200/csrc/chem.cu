@@ -268,6 +268,7 @@ cudaError_t record_last_cell(const HydroParams& P, const double* q, bool dev_q, 
 
 extern "C" int evora_chem(double* q) {
   if (!q) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinChem& D = dchem();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;
@@ -305,6 +306,7 @@ extern "C" int evora_chem(double* q) {
 
 extern "C" int evora_coolstep(double* q, const double* w, double* dt) {
   if (!q || !w || !dt) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinChem& D = dchem();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;

@@ -49,6 +49,23 @@ void start_time(const evora_params* p, const HydroParams& P, CosmoTime* s);
 // The parameters a grid was created with.
 const evora_params* grid_params(const evora_grid* g);
 
+// The drop-in layer's resident mode drives a fused-backend grid one routine
+// at a time.  grid_cfl_maxima: the per-axis maxima of |u_d| + a of the
+// current state (from the previous update when it reduced them, else from
+// the CFL kernel) into smax on the host; returns the grid's error word.
+// grid_update_dt: the fused update of the current state with the caller's
+// dt; returns the grid's error word.
+int grid_cfl_maxima(evora_grid* g, double smax[3]);
+int grid_update_dt(evora_grid* g, double dt);
+
+// Host arrays q bound to the resident mode's grid: before a routine that
+// reads q on the host, the newer device state is copied back
+// (dropin_resident_read); before one that also writes it, the device copy is
+// then marked stale so that the next evora_primitive uploads q again
+// (dropin_resident_write).  No-ops for other pointers or with residency off.
+void dropin_resident_read(const double* q);
+void dropin_resident_write(const double* q);
+
 // Per cell FP32 density and temperature of the grid's state into host
 // arrays of nx*ny*nz values (snapshot.f90:317-341); returns 0, an error
 // status of pressure(), or EVORA_ERR_CUDA.

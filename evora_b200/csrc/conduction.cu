@@ -301,6 +301,7 @@ extern "C" {
 
 int evora_thermalstep(double* q, const double* w, double* dt) {
   if (!q || !w || !dt) return EVORA_ERR_ARG;
+  evora::dropin_resident_read(q);
   DropinCond& D = dc();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;
@@ -330,6 +331,7 @@ int evora_thermalstep(double* q, const double* w, double* dt) {
 
 int evora_thermalconduction(double* q, const double* w, double dt) {
   if (!q || !w) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinCond& D = dc();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;

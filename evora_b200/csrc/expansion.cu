@@ -102,6 +102,7 @@ int fail_cuda(cudaError_t e, const char* where) {
 
 extern "C" int evora_expansion(double* q) {
   if (!q) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinExpansion& D = dexp();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;

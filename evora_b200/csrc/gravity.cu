@@ -402,6 +402,7 @@ extern "C" {
 
 int evora_gravpotential(const double* q, double* phi) {
   if (!q || !phi) return EVORA_ERR_ARG;
+  evora::dropin_resident_read(q);
   DropinGrav& D = dg();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;
@@ -430,6 +431,7 @@ int evora_gravpotential(const double* q, double* phi) {
 
 int evora_gravintegration(double* q, const double* phi, double dt) {
   if (!q || !phi) return EVORA_ERR_ARG;
+  evora::dropin_resident_write(q);
   DropinGrav& D = dg();
   std::lock_guard<std::mutex> lk(D.mu);
   HydroParams P;

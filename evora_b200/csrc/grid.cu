@@ -173,6 +173,16 @@ __global__ void k_step_end(GridCtl* ctl) {
   if (ctl->active && ctl->err == 0) ctl->k += 1;
 }
 
+// An update with the caller's dt (the drop-in layer's resident mode): the
+// step is active unless an error was raised; the next step's CFL maxima
+// start from zero.
+__global__ void k_set_dt(GridCtl* ctl, double dt) {
+  ctl->dt = dt;
+  ctl->active = ctl->err == 0 ? 1 : 0;
+  ctl->errnext = 0u;
+  ctl->snext[0] = ctl->snext[1] = ctl->snext[2] = 0ull;
+}
+
 // The control block at the start of a run: t = tstart, go, and with
 // supercomoving cosmostart's a, da/dt and redshift, the units at that a and
 // the first dump index k4 = 1 (main.f90:33, 52-62).
@@ -311,6 +321,42 @@ int enqueue_fused_step(evora_grid* g) {
   g->cfl_fresh = g->plan.cfl_fused != 0;
   return 0;
 }
+
+}  // namespace
+
+namespace evora {
+
+int grid_cfl_maxima(evora_grid* g, double smax[3]) {
+  if (!g || reference_backend(g)) return EVORA_ERR_ARG;
+  cudaStream_t st = g->stream;
+  const bool use_next = g->cfl_fresh;
+  k_step_begin<<<1, 1, 0, st>>>(g->ctl, use_next ? 1 : 0);
+  if (!use_next) fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
+  g->launches += use_next ? 1 : 2;
+  CU(cudaGetLastError());
+  GridCtl c;
+  CU(cudaMemcpyAsync(&c, g->ctl, sizeof c, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  for (int i = 0; i < 3; ++i) std::memcpy(&smax[i], &c.smax[i], sizeof(double));
+  return (int)c.err;
+}
+
+int grid_update_dt(evora_grid* g, double dt) {
+  if (!g || reference_backend(g)) return EVORA_ERR_ARG;
+  cudaStream_t st = g->stream;
+  k_set_dt<<<1, 1, 0, st>>>(g->ctl, dt);
+  fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
+  k_step_end<<<1, 1, 0, st>>>(g->ctl);
+  g->launches += 3;
+  CU(cudaGetLastError());
+  g->cur ^= 1;
+  g->cfl_fresh = g->plan.cfl_fused != 0;
+  return evora_grid_status(g);
+}
+
+}  // namespace evora
+
+namespace {
 
 // Device memory of a grid: cudaMalloc, or stream-ordered on the grid's
 // stream for grids made by evora_grid_create_async.

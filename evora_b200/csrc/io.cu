@@ -315,6 +315,7 @@ extern "C" {
 int evora_write_dump(const char* path, const double* q, int32_t nn, int32_t nx, int32_t ny, int32_t nz, int32_t lz,
                      int32_t mz) {
   if (!path || !q || nn < 1 || nx < 1 || ny < 1 || nz < 1 || lz < 1 || mz < lz || mz > nz) return EVORA_ERR_ARG;
+  evora::dropin_resident_read(q);
   const uint64_t bytes = 8ull * nn * nx * ny * (uint64_t)(mz - lz + 1);
   if (bytes > kMaxRecord) return EVORA_ERR_ARG;
   std::FILE* f = std::fopen(path, "wb");
@@ -450,6 +451,7 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
                    const char* dir) {
   if (!p || !q || !u || k3 < 0) return EVORA_ERR_ARG;
   if (p->chemistry) return EVORA_ERR_ARG;   // the writers take q(6, ...) and T without species
+  evora::dropin_resident_write(q);
   Geometry G;
   int rc = geometry(p, &G);
   if (rc) return rc;

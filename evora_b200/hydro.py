@@ -31,6 +31,9 @@ REFERENCE_KERNELS = 4
 # tile entry of the FP32 table that runs two cells per thread on packed FP32
 # pairs (its sums are associated differently from the other FP32 kernels)
 FP32_PAIR_TILE = 5
+# resident modes of the drop-in layer (evora_set_resident)
+RESIDENT_FP64 = 1
+RESIDENT_FP32 = 2
 
 
 # ------------------------------------------------------------- parameters --
@@ -115,6 +118,20 @@ class DropIn:
 
     def _activate(self):
         check(lib().evora_set_params(ctypes.byref(self.params)), "set_params")
+
+    def set_resident(self, mode: int):
+        """Resident mode (RESIDENT_FP64, RESIDENT_FP32, or 0 to end it): the
+        routines keep the state on the GPU between calls; host q is brought
+        up to date by sync(q) (see evora_set_resident)."""
+        check(lib().evora_set_resident(int(mode)), "set_resident")
+
+    def sync(self, q):
+        """Copies the resident state back into host array q."""
+        check(lib().evora_sync(_ptr(q, self.shape["q"])), "sync")
+
+    def invalidate(self, q):
+        """The caller changed host q: the next primitive uploads it again."""
+        check(lib().evora_invalidate(_ptr(q, self.shape["q"], False)), "invalidate")
 
     def primitive(self, w, q):
         """primitive(w,q), muscl.f90:26-43."""
@@ -369,7 +386,7 @@ class Grid:
 
 __all__ = ["EvoraError", "EvoraParams", "EvoraDerived", "default_params", "derived", "shapes",
            "DropIn", "Grid", "Batch", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS",
-           "FP32_PAIR_TILE"]
+           "FP32_PAIR_TILE", "RESIDENT_FP64", "RESIDENT_FP32"]
 
 
 # --------------------------------------------------------- batched tubes --

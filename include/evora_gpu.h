@@ -182,6 +182,37 @@ int evora_set_params(const evora_params* p);
  * reference bit for bit where libm is not involved). */
 int evora_set_strict(int32_t strict);
 
+/* Resident mode of the drop-in layer (no reference counterpart: the
+ * reference's arrays live in host memory).  With mode EVORA_RESIDENT_FP64
+ * (the arithmetic of evora_set_strict) or EVORA_RESIDENT_FP32 (the FP32
+ * form), the routines that main.f90:109-155 calls keep the fluid state on
+ * the GPU between calls instead of copying the host arrays in and out:
+ *   evora_primitive(w, q)  binds host array q to a resident grid, uploading it
+ *                          when it is new or was invalidated; w is not written
+ *   evora_bound(w), evora_compevo(w, evo, s, dt)   nothing to do (the ghost
+ *                          map, slopes and predictor run inside the update)
+ *   evora_hydrostep(w, dt) dt from the CFL maxima of the resident state; it
+ *                          also reports p <= 0 (which primitive reports
+ *                          without residency)
+ *   evora_sweep(w, q, evo, s, dt)  the fused update with this dt
+ * Host q is brought up to date only by evora_sync(q), and automatically
+ * before any other drop-in routine or file writer takes q (those that
+ * change q make the next evora_primitive upload it again).  w, evo and s are
+ * never written in this mode.  0 ends the mode after copying the state back.
+ * The results equal the non-resident routines' (bit for bit in strict FP64). */
+enum evora_resident_mode { EVORA_RESIDENT_FP64 = 1, EVORA_RESIDENT_FP32 = 2 };
+int evora_set_resident(int32_t mode);
+
+/* Resident mode: copies the resident state of host array q back into q (no
+ * reference counterpart; call it before the driver reads q, e.g. before
+ * evolution, snapshot and writedump, main.f90:191-206).  No-op for arrays
+ * that are not resident. */
+int evora_sync(double* q);
+
+/* Resident mode: the caller changed host q itself; the next evora_primitive
+ * uploads it again (no reference counterpart). */
+int evora_invalidate(const double* q);
+
 /* primitive(w,q), muscl.f90:26-43.  w interior <- q2w(q) for every cell.
  * With dualenergy the routine writes back q(5) or q(6) (comp.f90:60-72). */
 int evora_primitive(double* w, double* q);
