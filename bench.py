@@ -387,6 +387,73 @@ def run_reference(args):
     return 0
 
 
+def front_position(rho, i):
+    """Sub-cell position of the density front around the jump between cells
+    i and i+1: where the profile crosses the mean of the densities three
+    cells either side (linear between cells)."""
+    n = len(rho)
+    a, b = rho[max(i - 3, 0)], rho[min(i + 4, n - 1)]
+    level = 0.5 * (a + b)
+    for k in range(max(i - 3, 0), min(i + 4, n - 1)):
+        if (rho[k] - level) * (rho[k + 1] - level) <= 0 and rho[k + 1] != rho[k]:
+            return k + (level - rho[k]) / (rho[k + 1] - rho[k])
+    return float(i) + 0.5
+
+
+def front_shift(rho, rho_ref, lo=0):
+    """Cells between the largest density jump of rho_ref (beyond index lo)
+    and the same front in rho."""
+    i = lo + int(np.argmax(np.abs(np.diff(rho_ref[lo:]))))
+    return abs(front_position(rho, i) - front_position(rho_ref, i))
+
+
+def run_sod(args):
+    """The 1D Sod shock tube of the reference's shock-tube test (1024 cells
+    on [0, 1], gamma 1.4, (1, 0, 1) | (0.125, 0, 0.1) at x = 0.5, outflow,
+    minmod, HLLC, CFL 0.8, to t = 0.2): each form against the oracle, L1
+    density and the shock position in cells; device time of the whole run."""
+    import torch
+    import evora_b200 as ev
+    from oracle.oracle import Oracle, make_params
+    dist_setup(args.gpus)
+    kw = dict(nx=1024, ny=1, nz=1, g=1.4, cfl=0.8, boundtype=1, solver=2, limiter=1, tend=0.2)
+    p = ev.default_params(**kw)
+    q0 = ev.ic.shocktube(p)
+    o = Oracle(make_params(**kw))
+    qo = q0.copy()
+    r = o.run(qo, 1 << 30)
+    rho_o = qo[0, 0, :, 0]
+    forms = {}
+    for name, prec, flags in (("fp64_strict", ev.FP64, ev.STRICT), ("fp64", ev.FP64, 0), ("fp32", ev.FP32, 0)):
+        stream = torch.cuda.Stream()
+        with ev.Grid(p, prec, flags) as g:
+            g.set_stream(stream)
+            for _ in range(max(3, args.warmup)):   # whole runs from the IC
+                g.set_q(q0)
+                g.run()
+            g.set_q(q0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t = g.run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rho = g.get_q()[0, 0, :, 0]
+        forms[name] = {"steps": t["k"], "t": t["t"], "ms_run": e0.elapsed_time(e1),
+                       "l1_density_vs_oracle": float(np.abs(rho - rho_o).sum() / np.abs(rho_o).sum()),
+                       "shock_shift_cells": float(front_shift(rho, rho_o, lo=int(0.75 * kw["nx"]))),
+                       "bitwise_rho_m_e": bool(np.array_equal(rho, rho_o))}
+    v = forms["fp32"]
+    line = {"metric": METRIC, "value": kw["nx"] * v["steps"] / (v["ms_run"] * 1e-3), "unit": METRIC, "n_gpus": 1,
+            "steps": v["steps"], "warmup": max(3, args.warmup), "ms_per_step": v["ms_run"] / v["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "1D Sod shock tube, 1024 cells, gamma 1.4, outflow, minmod, HLLC, CFL 0.8, "
+                                   "t = 0.2 (one grid; a whole run is timed)"},
+            "oracle": {"steps": r["steps"], "t": r["t"]}, "forms": forms}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_tubes(args):
     """Batched Riemann problems: ntubes independent 1D tubes, lengths uniform
     in [128, 4096], random left/right states (rho, p log-uniform, v uniform,
@@ -447,12 +514,33 @@ def run_tubes(args):
             if out["f32"]["ok"][i] and out["f64"]["ok"][i]:
                 a, b64 = out["f32"]["q"][offs[i]:offs[i + 1], 0], out["f64"]["q"][offs[i]:offs[i + 1], 0]
                 l1.append(np.abs(a - b64).sum() / np.abs(b64).sum())
+        vs_oracle = None
+        if world == 1 and not args.no_oracle_check:
+            # every tube against the oracle (spawned pool over tubes): L1
+            # density and the shift of its largest density jump, in cells
+            from oracle.oracle import run_tubes as oracle_tubes
+            ref = oracle_tubes(dict(g=5.0 / 3.0, cfl=0.8, boundtype=1, solver=solver, tend=0.1), lengths, q)
+            vs_oracle = {}
+            for name in ("f32", "f64"):
+                e, sh, same_steps = [], [], 0
+                for i, (qo, ri) in enumerate(ref):
+                    if ri["status"] or not out[name]["ok"][i]:
+                        continue
+                    a = out[name]["q"][offs[i]:offs[i + 1], 0]
+                    e.append(np.abs(a - qo[:, 0]).sum() / np.abs(qo[:, 0]).sum())
+                    sh.append(front_shift(a, qo[:, 0]))
+                vs_oracle[name] = {"tubes": len(e), "l1_density_median": float(np.median(e)),
+                                   "l1_density_max": float(np.max(e)),
+                                   "front_shift_cells_median": float(np.median(sh)),
+                                   "front_shift_cells_max": float(np.max(sh)),
+                                   "oracle_failed_tubes": sum(1 for _, ri in ref if ri["status"])}
         for v in out.values():
             v.pop("q")
             v.pop("ok")
         res["hllc" if solver == 2 else "hll"] = dict(
             out, l1_density_f32_vs_f64_median=float(np.median(l1)) if l1 else None,
-            l1_density_f32_vs_f64_max=sharding.max_over_ranks(float(np.max(l1)) if l1 else 0.0, dev))
+            l1_density_f32_vs_f64_max=sharding.max_over_ranks(float(np.max(l1)) if l1 else 0.0, dev),
+            vs_oracle=vs_oracle)
     peak, peak_kind = measured_peaks()
     v = res["hllc"]["f32"]
     if rank != 0:
@@ -768,7 +856,7 @@ def main():
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
     ap.add_argument("--workload", default="kh3d",
-                    choices=["kh3d", "tubes", "serving", "gravity", "conduction", "comoving", "cosmo"],
+                    choices=["kh3d", "sod", "tubes", "serving", "gravity", "conduction", "comoving", "cosmo"],
                     help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes; serving: request "
                          "mix; gravity / conduction / comoving: the KH benchmark with those substeps after every "
                          "step; cosmo: the comoving cosmological box (Zel'dovich IC, 200 steps)")
@@ -787,6 +875,8 @@ def main():
         args.warmup = 3
     if args.workload == "tubes":
         return run_tubes(args)
+    if args.workload == "sod":
+        return run_sod(args)
     if args.workload == "serving":
         return run_serving(args)
     if args.workload in ("gravity", "conduction", "comoving"):

@@ -384,7 +384,7 @@ int resident_download(DropinState& S) {
   int rc = evora_grid_get_q(S.rgrid, const_cast<double*>(S.rq));
   if (rc) return rc;
   S.rq_device_newer = false;
-  return 0;
+  return evora_grid_status(S.rgrid);   // errors of the updates since the last wait
 }
 
 // Ends the resident grid (after its state went back to the host).
@@ -784,7 +784,9 @@ int evora_sweep(const double* w, double* q, const double* evo, const double* s, 
       set_error_message("evora_sweep: resident mode needs evora_primitive on this q first");
       return EVORA_ERR_ARG;
     }
-    const int st = grid_update_dt(S.rgrid, dt);
+    // enqueued without a wait: the errors it raises are returned by the
+    // next hydrostep or sync, which wait for the GPU anyway
+    const int st = grid_update_dt(S.rgrid, dt, false);
     S.rq_device_newer = true;
     return st;
   }

@@ -54,9 +54,10 @@ const evora_params* grid_params(const evora_grid* g);
 // current state (from the previous update when it reduced them, else from
 // the CFL kernel) into smax on the host; returns the grid's error word.
 // grid_update_dt: the fused update of the current state with the caller's
-// dt; returns the grid's error word.
+// dt; with sync, waits for it and returns the grid's error word, else only
+// enqueues it (launch errors are returned).
 int grid_cfl_maxima(evora_grid* g, double smax[3]);
-int grid_update_dt(evora_grid* g, double dt);
+int grid_update_dt(evora_grid* g, double dt, bool sync);
 
 // Host arrays q bound to the resident mode's grid: before a routine that
 // reads q on the host, the newer device state is copied back

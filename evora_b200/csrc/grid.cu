@@ -341,7 +341,7 @@ int grid_cfl_maxima(evora_grid* g, double smax[3]) {
   return (int)c.err;
 }
 
-int grid_update_dt(evora_grid* g, double dt) {
+int grid_update_dt(evora_grid* g, double dt, bool sync) {
   if (!g || reference_backend(g)) return EVORA_ERR_ARG;
   cudaStream_t st = g->stream;
   k_set_dt<<<1, 1, 0, st>>>(g->ctl, dt);
@@ -351,7 +351,7 @@ int grid_update_dt(evora_grid* g, double dt) {
   CU(cudaGetLastError());
   g->cur ^= 1;
   g->cfl_fresh = g->plan.cfl_fused != 0;
-  return evora_grid_status(g);
+  return sync ? evora_grid_status(g) : 0;
 }
 
 }  // namespace evora

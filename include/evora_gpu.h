@@ -194,7 +194,9 @@ int evora_set_strict(int32_t strict);
  *   evora_hydrostep(w, dt) dt from the CFL maxima of the resident state; it
  *                          also reports p <= 0 (which primitive reports
  *                          without residency)
- *   evora_sweep(w, q, evo, s, dt)  the fused update with this dt
+ *   evora_sweep(w, q, evo, s, dt)  enqueues the fused update with this dt;
+ *                          errors it raises are returned by the next
+ *                          hydrostep or evora_sync
  * Host q is brought up to date only by evora_sync(q), and automatically
  * before any other drop-in routine or file writer takes q (those that
  * change q make the next evora_primitive upload it again).  w, evo and s are

@@ -351,3 +351,33 @@ class Oracle:
         q = self.zeros_q()
         self.L.orc_ic_kh3d(_ptr(q), int(seed), float(amp))
         return q
+
+
+def run_tube(task):
+    """One 1D tube through the oracle's time loop (for a worker process of a
+    spawned pool): task = (params dict, cells, q of shape (cells, 6)).
+    Returns (q after the run, run info)."""
+    kw, n, q = task
+    o = Oracle(make_params(nx=n, ny=1, nz=1, **kw))
+    o.set_threads(1)
+    qq = np.ascontiguousarray(q, dtype=np.float64).reshape(1, 1, n, 6).copy()
+    r = o.run(qq, 1 << 30)
+    return qq.reshape(n, 6), r
+
+
+def run_tubes(kw, lengths, q, workers=None):
+    """Every tube of a packed batch (tubes concatenated, q of shape (cells,
+    6)) through the oracle, longest first, in a spawned process pool (a
+    broken worker raises instead of being restarted).  Returns a list of
+    (q, info) in tube order."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
+    tasks = [(kw, int(n), q[offs[i]:offs[i + 1]]) for i, n in enumerate(lengths)]
+    order = sorted(range(len(tasks)), key=lambda i: -lengths[i])
+    with cf.ProcessPoolExecutor(workers or os.cpu_count() or 4, mp_context=mp.get_context("spawn")) as pool:
+        res = list(pool.map(run_tube, [tasks[i] for i in order], chunksize=4))
+    out = [None] * len(tasks)
+    for i, r in zip(order, res):
+        out[i] = r
+    return out

@@ -49,13 +49,6 @@ def rel_l1(a, b):
 
 
 def oracle_tube_task(task):
-    """One 1D tube through the oracle's time loop, for a spawned worker
-    process: task = (params dict, cells, q of shape (cells, 6)).  Returns
-    (q after the run, run info)."""
-    from oracle.oracle import Oracle, make_params
-    kw, n, q = task
-    o = Oracle(make_params(nx=n, ny=1, nz=1, **kw))
-    o.set_threads(1)
-    qq = np.ascontiguousarray(q, dtype=np.float64).reshape(1, 1, n, 6).copy()
-    r = o.run(qq, 1 << 30)
-    return qq.reshape(n, 6), r
+    """One 1D tube through the oracle's time loop (spawned worker process)."""
+    from oracle.oracle import run_tube
+    return run_tube(task)

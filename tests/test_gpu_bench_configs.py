@@ -20,16 +20,12 @@ over tubes (one tube per task), so the whole file takes a few minutes.
 Reference path: muscl.f90:171-274, riemann.f90:26-288, boundary.f90:26-113,
 timestep.f90:26-57.
 """
-import concurrent.futures as cf
-import multiprocessing as mp
-import os
-
 import numpy as np
 import pytest
 
 import evora_b200 as ev
 from oracle.oracle import Oracle, make_params
-from helpers import oracle_tube_task, rel_l1
+from helpers import rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -90,17 +86,8 @@ def test_kh256_fp32_vs_oracle(cuda_device, kh_oracle):
 
 
 def _oracle_tubes(kw, lengths, q):
-    offs = np.concatenate([[0], np.cumsum(lengths)])
-    tasks = [(kw, int(n), q[offs[i]:offs[i + 1]]) for i, n in enumerate(lengths)]
-    # longest tubes first so the pool ends together; spawn, not fork
-    order = sorted(range(len(tasks)), key=lambda i: -lengths[i])
-    # a broken worker raises BrokenProcessPool here instead of being respawned
-    with cf.ProcessPoolExecutor(os.cpu_count() or 4, mp_context=mp.get_context("spawn")) as pool:
-        res = list(pool.map(oracle_tube_task, [tasks[i] for i in order], chunksize=4))
-    out = [None] * len(tasks)
-    for i, r in zip(order, res):
-        out[i] = r
-    return out
+    from oracle.oracle import run_tubes
+    return run_tubes(kw, lengths, q)
 
 
 @pytest.mark.parametrize("solver", [2, 1], ids=["hllc", "hll"])
