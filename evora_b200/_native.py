@@ -225,6 +225,13 @@ def _declare_batch(L):
         "evora_chem": ([c_void_p], c_int32),
         "evora_coolstep": ([c_void_p, c_void_p, _dp], c_int32),
         "evora_thermalconduction": ([c_void_p, c_void_p, c_double], c_int32),
+        "evora_multigrid_create": ([c_int32, c_int32, c_void_p, ctypes.POINTER(G)], c_int32),
+        "evora_multigrid_destroy": ([G], c_int32),
+        "evora_multigrid_add": ([G, G], c_int32),
+        "evora_multigrid_remove": ([G, G], c_int32),
+        "evora_multigrid_step": ([G, c_int32, c_int32], c_int32),
+        "evora_multigrid_status": ([G, ctypes.POINTER(G), ctypes.POINTER(c_int32), ctypes.POINTER(ctypes.c_uint32),
+                                    ctypes.POINTER(c_int64), c_int32, ctypes.POINTER(c_int32)], c_int32),
         "evora_server_create": ([ctypes.POINTER(EvoraParams), c_int32, c_int32, c_double, c_int32, c_int32,
                                  c_int32, ctypes.POINTER(G)], c_int32),
         "evora_server_destroy": ([G], c_int32),

@@ -113,6 +113,13 @@ void fused_plan_free(FusedPlan* pl) {
 
 void fused_cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st) { pl.cfl(pl, q, ctl, st); }
 
+MultiLaunch fused_multi_pick(int precision, int strict, int nf, int* tx, int* ty, int* zc, size_t* smem,
+                             int* threads, int* ctas_per_sm) {
+  if (precision == EVORA_FP32) return f32::multi_pick(nf, tx, ty, zc, smem, threads, ctas_per_sm);
+  if (strict) return f64s::multi_pick(nf, tx, ty, zc, smem, threads, ctas_per_sm);
+  return f64::multi_pick(nf, tx, ty, zc, smem, threads, ctas_per_sm);
+}
+
 void fused_update(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cudaStream_t st) {
   pl.launch(pl, qin, qout, ctl, st);
 }

@@ -85,12 +85,39 @@ void state_set_plane(void* q, bool f32, int64_t n, int nf, int aos, const PlaneM
 void state_bov(void* q, bool f32, int64_t n, int nf, int aos, const HydroParams& P, double temp0, float* dens,
                float* temp, unsigned* err, cudaStream_t st);
 
+// One grid of a multi-grid batch (device table): its parameters, its two
+// state buffers (par: the one holding the current state), its control
+// block, cells, planes per 3D tile, 2 or 3 dimensions, and whether the CFL
+// maxima of its current state are in ctl->snext (the previous update reduced
+// them) or in ctl->smax (a CFL kernel filled them before the step).
+struct MultiGridDesc {
+  HydroParams P;
+  void* q[2];
+  GridCtl* ctl;
+  int64_t n;
+  int zc, dim, par, fresh;
+};
+// One work item of a batched update: a tile (bx, by, bz) of grid `grid`.
+struct MultiGridItem {
+  int grid, bx, by, bz;
+};
+// meta[0] grids, meta[1] items, meta[2] the next item to take (reset by the
+// control kernel of each step).
+typedef void (*MultiLaunch)(const MultiGridDesc* grids, const MultiGridItem* items, int* meta, int ctas,
+                            cudaStream_t st);
+
+// The multi-grid update of a precision (tile shape, shared memory, threads
+// and CTAs per SM of its persistent launch).
+MultiLaunch fused_multi_pick(int precision, int strict, int nf, int* tx, int* ty, int* zc, size_t* smem,
+                             int* threads, int* ctas_per_sm);
+
 // Instantiation launchers (fused_f64.cu, fused_f64_strict.cu, fused_f32.cu).
 #define EVORA_DECLARE_FUSED_NS(ns)                                                           \
   namespace ns {                                                                             \
   FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* minb); \
   int tiles();                                                                               \
   bool tile_fits(const HydroParams& P, int nf, int dim, int tile);                           \
+  MultiLaunch multi_pick(int nf, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* ctas_per_sm); \
   void cfl(const FusedPlan& pl, const void* q, GridCtl* ctl, cudaStream_t st);                \
   }
 EVORA_DECLARE_FUSED_NS(f64)

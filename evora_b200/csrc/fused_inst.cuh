@@ -203,6 +203,73 @@ FusedLaunch pick(int nf, int dim, int tile, int* tx, int* ty, int* zc, size_t* s
   }
 }
 
+// ---- multi-grid batches: one persistent launch updates the tiles of many
+// 2D and 3D grids of uneven sizes (the tile program of entry 0), pulling
+// (grid, tile) items from an atomic work queue; each grid keeps its own dt,
+// control block and ping-pong parity (MultiGridDesc).
+template <int NF>
+__global__ void __launch_bounds__(Tile<0>::TX* Tile<0>::TY, Tile<0>::MINB)
+    k_multi(const MultiGridDesc* grids, const MultiGridItem* items, int* meta) {
+  using C = Tile<0>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<FusedSmem<TT, NF, C::TX, C::TY>*>(smem_raw);
+  __shared__ __align__(16) unsigned char a_raw[sizeof(FusedArgs<TT>)];
+  __shared__ int s_item, s_dim, s_bx, s_by, s_bz;
+  auto& A = *reinterpret_cast<FusedArgs<TT>*>(a_raw);
+  const int nitems = meta[1];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int it = atomicAdd(&meta[2], 1);
+      s_item = it;
+      if (it < nitems) {
+        const MultiGridItem w = items[it];
+        const MultiGridDesc& d = grids[w.grid];
+        A.P = d.P;
+        A.qin = (const TT*)d.q[d.par];
+        A.qout = (TT*)d.q[d.par ^ 1];
+        A.ctl = d.ctl;
+        A.n = d.n;
+        A.cfl_next = 1;
+        A.zc = d.zc;
+        s_dim = d.dim;
+        s_bx = w.bx;
+        s_by = w.by;
+        s_bz = w.bz;
+      }
+    }
+    __syncthreads();
+    if (s_item >= nitems) break;
+    if (s_dim == 3) fused_tile<TT, NF, 3, C::TX, C::TY, C::ZC>(A, sm, threadIdx.x, s_bx, s_by, s_bz);
+    else fused_tile<TT, NF, 2, C::TX, C::TY, C::ZC>(A, sm, threadIdx.x, s_bx, s_by, 0);
+    __syncthreads();   // the shared state is reused by the next item
+  }
+}
+
+template <int NF>
+void multi_launch(const MultiGridDesc* grids, const MultiGridItem* items, int* meta, int ctas, cudaStream_t st) {
+  using C = Tile<0>;
+  k_multi<NF><<<ctas, C::TX * C::TY, sizeof(FusedSmem<TT, NF, C::TX, C::TY>), st>>>(grids, items, meta);
+}
+
+MultiLaunch multi_pick(int nf, int* tx, int* ty, int* zc, size_t* smem, int* threads, int* ctas_per_sm) {
+  using C = Tile<0>;
+  *tx = C::TX;
+  *ty = C::TY;
+  *zc = C::ZC;
+  *threads = C::TX * C::TY;
+  *ctas_per_sm = C::MINB;
+  if (nf == 5) {
+    *smem = sizeof(FusedSmem<TT, 5, C::TX, C::TY>);
+    cudaFuncSetAttribute(k_multi<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    cudaFuncSetAttribute(k_multi<5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return &multi_launch<5>;
+  }
+  *smem = sizeof(FusedSmem<TT, 6, C::TX, C::TY>);
+  cudaFuncSetAttribute(k_multi<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  cudaFuncSetAttribute(k_multi<6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  return &multi_launch<6>;
+}
+
 // hydrostep part 1 on the SoA state: maxima of |u_d| + a (per cell in the
 // working precision, cfl_speeds; maxima and dt in FP64).
 template <int NF>

@@ -11,7 +11,9 @@
 //    device-resident arrays in the reference layouts; FP64 only.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
+#include <numeric>
 #include <cstring>
 #include <map>
 #include <new>
@@ -76,6 +78,30 @@ struct evora_grid {
   // and not atomic)
   bool expansion = false;
   bool async_alloc = false;  // memory from cudaMallocAsync on `stream`
+  evora_multigrid* multigrid = nullptr;   // the batch stepping this grid, if any
+};
+
+// A batch of resident 2D and 3D grids stepped together: per step one control
+// kernel (every grid's hydrostep, updatetime), one persistent update launch
+// over the tiles of all grids, one closing control kernel.
+struct evora_multigrid {
+  int precision = EVORA_FP64;
+  int flags = 0;
+  int nf = 5;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<evora_grid*> grids;
+  bool dirty = true;
+  evora::MultiGridDesc* d_desc = nullptr;
+  evora::MultiGridItem* d_items = nullptr;
+  int* d_meta = nullptr;                   // grids, items, next item
+  long long* d_status = nullptr;           // per grid: go | err << 1, then k
+  int cap_grids = 0, cap_items = 0;
+  evora::MultiLaunch launch = nullptr;
+  int tx = 0, ty = 0, zc = 0, threads = 0, ctas = 0;
+  size_t smem = 0;
+  std::map<int, cudaGraphExec_t> graphs;   // by step count
+  long long cell_updates = 0;              // member cells x steps enqueued
 };
 
 namespace {
@@ -95,14 +121,14 @@ int64_t ncells(const evora_grid* g) { return (int64_t)g->P.nx * g->P.ny * g->P.n
 
 size_t elem_size(const evora_grid* g) { return g->precision == EVORA_FP32 ? 4 : 8; }
 
-// use_next: the CFL maxima of this step's state were reduced by the previous
-// step's update (with the errors that computation raised); otherwise a CFL
-// kernel fills smax.
-__global__ void k_step_begin(GridCtl* ctl, int use_next) {
-  if (use_next) {
+// use_next 1: the CFL maxima of this step's state were reduced by the
+// previous step's update (with the errors that computation raised); 0: a CFL
+// kernel fills smax after this; 2: a CFL kernel filled smax before this.
+__device__ __forceinline__ void step_begin(GridCtl* ctl, int use_next) {
+  if (use_next == 1) {
     ctl->err |= ctl->errnext;
     for (int i = 0; i < 3; ++i) ctl->smax[i] = ctl->snext[i];
-  } else {
+  } else if (use_next == 0) {
     ctl->smax[0] = ctl->smax[1] = ctl->smax[2] = 0ull;
   }
   ctl->errnext = 0u;
@@ -113,11 +139,13 @@ __global__ void k_step_begin(GridCtl* ctl, int use_next) {
   ctl->active = (ctl->go != 0 && ctl->err == 0 && ctl->dump == 0) ? 1 : 0;
 }
 
+__global__ void k_step_begin(GridCtl* ctl, int use_next) { step_begin(ctl, use_next); }
+
 // hydrostep part 2 (timestep.f90:26-57), the coolstep and thermalstep
 // limits in main.f90:119-121's order, and the master block of
 // main.f90:124-137: cosmostep and compcosmo (comoving), updatetime, and
 // compunits (comoving).
-__global__ void k_step_time(HydroParams P, GridCtl* ctl) {
+__device__ __forceinline__ void step_time(const HydroParams& P, GridCtl* ctl) {
   if (!ctl->active || ctl->err) {
     ctl->active = 0;
     return;
@@ -169,8 +197,35 @@ __global__ void k_step_time(HydroParams P, GridCtl* ctl) {
   }
 }
 
-__global__ void k_step_end(GridCtl* ctl) {
+__global__ void k_step_time(HydroParams P, GridCtl* ctl) { step_time(P, ctl); }
+
+__device__ __forceinline__ void step_end(GridCtl* ctl) {
   if (ctl->active && ctl->err == 0) ctl->k += 1;
+}
+
+__global__ void k_step_end(GridCtl* ctl) { step_end(ctl); }
+
+// Control of a multi-grid step, one thread per grid: hydrostep part 2 and
+// updatetime (as k_step_begin + k_step_time), and after the update the step
+// count, the ping-pong parity and a compact status word.
+__global__ void k_mg_begin(MultiGridDesc* g, int* meta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) meta[2] = 0;
+  if (i >= meta[0]) return;
+  GridCtl* ctl = g[i].ctl;
+  step_begin(ctl, g[i].fresh ? 1 : 2);
+  g[i].fresh = 1;
+  step_time(g[i].P, ctl);
+}
+
+__global__ void k_mg_end(MultiGridDesc* g, const int* meta, long long* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= meta[0]) return;
+  GridCtl* ctl = g[i].ctl;
+  step_end(ctl);
+  g[i].par ^= 1;
+  status[2 * i] = (long long)(ctl->go != 0) | ((long long)ctl->err << 1);
+  status[2 * i + 1] = ctl->k;
 }
 
 // An update with the caller's dt (the drop-in layer's resident mode): the
@@ -518,6 +573,7 @@ extern "C" {
 
 int evora_grid_destroy(evora_grid* g) {
   if (!g) return EVORA_ERR_ARG;
+  if (g->multigrid) evora_multigrid_remove(g->multigrid, g);
   if (g->async_alloc) {
     free_grid(g);   // stream-ordered frees: no device-wide synchronisation
     return 0;
@@ -556,6 +612,7 @@ int evora_grid_set_q(evora_grid* g, const double* q) {
     fused_from_aos(g->plan, src, g->qbuf[0], g->stream, nq_of(g), g->species);
   }
   g->cfl_fresh = false;
+  if (g->multigrid) g->multigrid->dirty = true;   // its table entry (parity, maxima) changes
   GridCtl c;
   init_ctl(g, &c);
   CU(cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream));
@@ -586,6 +643,10 @@ int evora_grid_get_q(evora_grid* g, double* q) {
 
 int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync) {
   if (!g || nsteps < 0) return EVORA_ERR_ARG;
+  if (g->multigrid) {
+    set_error_message("evora_grid_step: the grid is stepped by its multi-grid batch");
+    return EVORA_ERR_ARG;
+  }
   // Several steps on a capturable stream replay graphs of at most 32 steps
   // (instantiating a graph costs with its node count; replays are cheap).
   while (g->stream != nullptr && nsteps >= 2 && !g->timing) {
@@ -903,3 +964,244 @@ int grid_bov(evora_grid* g, double temp0, float* dens, float* temp) {
 }
 
 }  // namespace evora
+
+// ------------------------------------------------------ multi-grid batches --
+namespace {
+
+int mg_rebuild(evora_multigrid* m) {
+  const int n = (int)m->grids.size();
+  std::vector<MultiGridDesc> desc(n);
+  std::vector<MultiGridItem> items3, items2;
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  // larger grids first, so that the last items of a step are small ones
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    const evora_grid* ga = m->grids[a];
+    const evora_grid* gb = m->grids[b];
+    return (int64_t)ga->P.nx * ga->P.ny * ga->P.nz > (int64_t)gb->P.nx * gb->P.ny * gb->P.nz;
+  });
+  for (int i = 0; i < n; ++i) {
+    evora_grid* g = m->grids[i];
+    MultiGridDesc& d = desc[i];
+    d.P = g->P;
+    d.q[0] = g->qbuf[0];
+    d.q[1] = g->qbuf[1];
+    d.ctl = g->ctl;
+    d.n = ncells(g);
+    d.dim = g->plan.dim;
+    d.zc = d.dim == 3 ? std::min(m->zc, g->P.nz) : 1;
+    d.par = g->cur;
+    d.fresh = g->cfl_fresh ? 1 : 0;
+  }
+  for (int i : idx) {
+    const MultiGridDesc& d = desc[i];
+    const int gx = (d.P.nx + m->tx - 1) / m->tx, gy = (d.P.ny + m->ty - 1) / m->ty;
+    const int gz = d.dim == 3 ? (d.P.nz + d.zc - 1) / d.zc : 1;
+    auto& dst = d.dim == 3 ? items3 : items2;
+    for (int bz = 0; bz < gz; ++bz)
+      for (int by = 0; by < gy; ++by)
+        for (int bx = 0; bx < gx; ++bx) dst.push_back(MultiGridItem{i, bx, by, bz});
+  }
+  items3.insert(items3.end(), items2.begin(), items2.end());   // 3D items (ZC planes) before 2D ones
+  const int ni = (int)items3.size();
+  if (n > m->cap_grids || ni > m->cap_items) {
+    CU(cudaStreamSynchronize(m->stream));
+    for (auto& kv : m->graphs) cudaGraphExecDestroy(kv.second);
+    m->graphs.clear();
+    if (n > m->cap_grids) {
+      cudaFree(m->d_desc);
+      cudaFree(m->d_status);
+      m->d_desc = nullptr;
+      m->d_status = nullptr;
+      const int cap = std::max(2 * n, 64);
+      CU(cudaMalloc(&m->d_desc, sizeof(MultiGridDesc) * cap));
+      CU(cudaMalloc(&m->d_status, sizeof(long long) * 2 * cap));
+      m->cap_grids = cap;
+    }
+    if (ni > m->cap_items) {
+      cudaFree(m->d_items);
+      m->d_items = nullptr;
+      const int cap = std::max(2 * ni, 4096);
+      CU(cudaMalloc(&m->d_items, sizeof(MultiGridItem) * cap));
+      m->cap_items = cap;
+    }
+  }
+  const int meta[3] = {n, ni, 0};
+  if (n) CU(cudaMemcpyAsync(m->d_desc, desc.data(), sizeof(MultiGridDesc) * n, cudaMemcpyHostToDevice, m->stream));
+  if (ni) CU(cudaMemcpyAsync(m->d_items, items3.data(), sizeof(MultiGridItem) * ni, cudaMemcpyHostToDevice, m->stream));
+  CU(cudaMemcpyAsync(m->d_meta, meta, sizeof meta, cudaMemcpyHostToDevice, m->stream));
+  // grids without the CFL maxima of their state get them from the CFL kernel
+  for (evora_grid* g : m->grids)
+    if (!g->cfl_fresh) {
+      k_step_begin<<<1, 1, 0, m->stream>>>(g->ctl, 0);
+      fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, m->stream);
+    }
+  CU(cudaGetLastError());
+  // the host copies above must stay alive until enqueued work has read them
+  CU(cudaStreamSynchronize(m->stream));
+  m->dirty = false;
+  return 0;
+}
+
+void mg_enqueue(evora_multigrid* m, int nsteps) {
+  const int cb = (m->cap_grids + 127) / 128;
+  for (int k = 0; k < nsteps; ++k) {
+    k_mg_begin<<<cb, 128, 0, m->stream>>>(m->d_desc, m->d_meta);
+    m->launch(m->d_desc, m->d_items, m->d_meta, m->ctas, m->stream);
+    k_mg_end<<<cb, 128, 0, m->stream>>>(m->d_desc, m->d_meta, m->d_status);
+  }
+}
+
+bool mg_accepts(const evora_multigrid* m, const evora_grid* g) {
+  return !reference_backend(g) && g->precision == m->precision &&
+         (g->flags & ~EVORA_REFERENCE_KERNELS) == m->flags && g->nf == m->nf && g->plan.dim >= 2 &&
+         !g->gravity && !g->conduction && !g->floors && !g->expansion && !g->P.supercomoving &&
+         !g->P.chemistry && !g->P.cooldt;
+}
+
+}  // namespace
+
+extern "C" {
+
+int evora_multigrid_create(int32_t precision, int32_t flags, void* stream, evora_multigrid** out) {
+  if (!out || (precision != EVORA_FP32 && precision != EVORA_FP64)) return EVORA_ERR_ARG;
+  if (flags & EVORA_REFERENCE_KERNELS) return EVORA_ERR_ARG;
+  *out = nullptr;
+  evora_multigrid* m = new (std::nothrow) evora_multigrid();
+  if (!m) return EVORA_ERR_NOMEM;
+  m->precision = precision;
+  m->flags = flags;
+  m->nf = (flags & EVORA_CARRY_ENTROPY) ? 6 : 5;
+  m->stream = (cudaStream_t)stream;
+  cudaGetDevice(&m->device);
+  int per_sm = 1, sms = 148;
+  m->launch = fused_multi_pick(precision, (flags & EVORA_STRICT) != 0, m->nf, &m->tx, &m->ty, &m->zc, &m->smem,
+                               &m->threads, &per_sm);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  m->ctas = sms * per_sm;
+  if (cudaMalloc(&m->d_meta, sizeof(int) * 4) != cudaSuccess) {
+    cudaGetLastError();
+    delete m;
+    return EVORA_ERR_NOMEM;
+  }
+  *out = m;
+  return 0;
+}
+
+int evora_multigrid_destroy(evora_multigrid* m) {
+  if (!m) return EVORA_ERR_ARG;
+  cudaStreamSynchronize(m->stream);
+  for (evora_grid* g : m->grids) g->multigrid = nullptr;
+  for (auto& kv : m->graphs) cudaGraphExecDestroy(kv.second);
+  cudaFree(m->d_desc);
+  cudaFree(m->d_items);
+  cudaFree(m->d_meta);
+  cudaFree(m->d_status);
+  delete m;
+  return 0;
+}
+
+int evora_multigrid_add(evora_multigrid* m, evora_grid* g) {
+  if (!m || !g || g->multigrid) return EVORA_ERR_ARG;
+  if (!mg_accepts(m, g)) {
+    set_error_message("evora_multigrid_add: a member is a 2D or 3D fused grid of the batch's precision and "
+                      "flags with no physics after the update");
+    return EVORA_ERR_ARG;
+  }
+  CU(cudaStreamSynchronize(g->stream));   // its set-up work is done
+  m->grids.push_back(g);
+  g->multigrid = m;
+  m->dirty = true;
+  return 0;
+}
+
+int evora_multigrid_remove(evora_multigrid* m, evora_grid* g) {
+  if (!m || !g || g->multigrid != m) return EVORA_ERR_ARG;
+  CU(cudaStreamSynchronize(m->stream));   // no batch work touches it any more
+  m->grids.erase(std::find(m->grids.begin(), m->grids.end(), g));
+  g->multigrid = nullptr;
+  m->dirty = true;
+  return 0;
+}
+
+int evora_multigrid_step(evora_multigrid* m, int32_t nsteps, int32_t sync) {
+  if (!m || nsteps < 0) return EVORA_ERR_ARG;
+  if (m->dirty) {
+    int rc = mg_rebuild(m);
+    if (rc) return rc;
+  }
+  if (m->grids.empty() || nsteps == 0) return 0;
+  int left = nsteps;
+  while (left > 0) {
+    const int chunk = left < 32 ? left : 32;
+    if (m->stream) {
+      auto it = m->graphs.find(chunk);
+      if (it == m->graphs.end()) {
+        cudaGraph_t graph;
+        CU(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+        mg_enqueue(m, chunk);
+        cudaError_t e = cudaStreamEndCapture(m->stream, &graph);
+        if (e != cudaSuccess) {
+          set_cuda_error(e, "evora_multigrid_step: capture");
+          return EVORA_ERR_CUDA;
+        }
+        cudaGraphExec_t exec;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          set_cuda_error(e, "evora_multigrid_step: instantiate");
+          return EVORA_ERR_CUDA;
+        }
+        it = m->graphs.emplace(chunk, exec).first;
+      }
+      CU(cudaGraphLaunch(it->second, m->stream));
+    } else {
+      mg_enqueue(m, chunk);
+    }
+    left -= chunk;
+  }
+  CU(cudaGetLastError());
+  for (evora_grid* g : m->grids) {
+    if (nsteps & 1) g->cur ^= 1;
+    g->cfl_fresh = g->plan.cfl_fused != 0;
+    g->launches += 3LL * nsteps;
+    m->cell_updates += (long long)nsteps * ncells(g);
+  }
+  if (sync) CU(cudaStreamSynchronize(m->stream));
+  return 0;
+}
+
+int evora_multigrid_status(evora_multigrid* m, evora_grid** grids, int32_t* go, uint32_t* err, int64_t* k,
+                           int32_t max, int32_t* n) {
+  if (!m || !n || max < 0) return EVORA_ERR_ARG;
+  CU(cudaStreamSynchronize(m->stream));
+  const int cnt = std::min<int>(max, (int)m->grids.size());
+  *n = cnt;
+  if (cnt == 0) return 0;
+  if (m->dirty) {
+    // not stepped since the last change: read the members' own control blocks
+    for (int i = 0; i < cnt; ++i) {
+      double t, dt;
+      int32_t g_go;
+      int64_t g_k;
+      int rc = evora_grid_time(m->grids[i], &t, &dt, &g_go, &g_k);
+      if (rc) return rc;
+      if (grids) grids[i] = m->grids[i];
+      if (go) go[i] = g_go;
+      if (err) err[i] = (uint32_t)evora_grid_status(m->grids[i]);
+      if (k) k[i] = g_k;
+    }
+    return 0;
+  }
+  std::vector<long long> st(2 * (size_t)cnt);
+  CU(cudaMemcpy(st.data(), m->d_status, sizeof(long long) * 2 * cnt, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < cnt; ++i) {
+    if (grids) grids[i] = m->grids[i];
+    if (go) go[i] = (int32_t)(st[2 * i] & 1);
+    if (err) err[i] = (uint32_t)(st[2 * i] >> 1);
+    if (k) k[i] = st[2 * i + 1];
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -9,8 +9,11 @@
 //   * 1D requests become tubes of one shared pool (a packed arena plus a tube
 //     table) advanced together by one persistent launch of the batched-tube
 //     kernel (batch_kernel.cuh), each tube with its own dt and t;
-//   * 2D and 3D requests become resident grids (grid.cu) stepped on their own
-//     streams, so small grids run concurrently with the tube launch.
+//   * 2D and 3D requests become resident grids (grid.cu) advanced together by
+//     one multi-grid batch (evora_multigrid_*: per step one control kernel,
+//     one persistent update launch over the tiles of all grids, one closing
+//     kernel) on its own stream, concurrently with the tube launch; grids the
+//     batch cannot take step on their own streams.
 // Requests that arrive while others run are admitted at the next tick, as
 // memory and tube slots free up.  Finished requests are read back and their
 // time to solution (submit -> read back) is recorded.  A request's arithmetic
@@ -55,6 +58,7 @@ struct Request {
   int slot = -1;                 // tube slot
   long long off = 0;             // arena offset (tubes)
   evora_grid* grid = nullptr;    // 2D/3D
+  bool batched = false;          // stepped by the server's multi-grid batch
   int stream = 0;                // index into the server's grid streams
   size_t bytes = 0;              // device footprint (grids)
   int64_t steps = 0;
@@ -111,6 +115,9 @@ struct evora_server {
   bool order_dirty = true;
   int active_tubes = 0;
   cudaStream_t tstream = nullptr;
+  cudaStream_t mstream = nullptr;  // the multi-grid batch
+  evora_multigrid* mg = nullptr;
+  int batched_grids = 0;
   std::vector<cudaStream_t> gstreams;
   int next_stream = 0;
   std::vector<double> latencies;
@@ -225,6 +232,8 @@ int admit(evora_server* s, Request& r) {
     }
     r.grid = g;
     r.bytes = bytes;
+    r.batched = s->mg && evora_multigrid_add(s->mg, g) == 0;
+    if (r.batched) s->batched_grids++;
     // time quantum: a round gives each grid about the same device time, so
     // its step count falls with its size (2^20 cell-updates per base step)
     const double quantum = (double)s->steps_per_tick * (double)(1 << 20);
@@ -313,6 +322,8 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
     cudaGetLastError();
   }
   if (cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  if (cudaStreamCreateWithFlags(&s->mstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  if (evora_multigrid_create(precision, flags & ~EVORA_REFERENCE_KERNELS, s->mstream, &s->mg)) s->mg = nullptr;
   if (cudaMalloc(&s->stage2, sizeof(double) * EVORA_NQ * max_tube_cells) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->q, arena_bytes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->tubes, sizeof(TubeState) * max_tubes) != cudaSuccess) goto fail;
@@ -381,6 +392,7 @@ fail:
 int evora_server_destroy(evora_server* s) {
   if (!s) return EVORA_ERR_ARG;
   cudaDeviceSynchronize();
+  if (s->mg) evora_multigrid_destroy(s->mg);
   for (auto& kv : s->reqs)
     if (kv.second.grid) evora_grid_destroy(kv.second.grid);
   cudaFree(s->q);
@@ -393,6 +405,7 @@ int evora_server_destroy(evora_server* s) {
   cudaFree(s->stage2);
   if (s->rstream) cudaStreamDestroy(s->rstream);
   if (s->tstream) cudaStreamDestroy(s->tstream);
+  if (s->mstream) cudaStreamDestroy(s->mstream);
   for (auto st : s->gstreams) cudaStreamDestroy(st);
   delete s;
   return 0;
@@ -446,9 +459,14 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   for (auto& kv : s->reqs)
     if (kv.second.state == REQ_RUNNING && kv.second.grid) {
       grids.push_back(&kv.second);
+      if (kv.second.batched) continue;
       int rc = evora_grid_step(kv.second.grid, kv.second.round_steps, 0);
       if (rc) return rc;
     }
+  if (s->batched_grids > 0) {
+    int rc = evora_multigrid_step(s->mg, s->steps_per_tick, 0);
+    if (rc) return rc;
+  }
   mark(0);
   // 3. while the GPU works: read back what finished in the previous round
   for (auto& kv : s->reqs) {
@@ -489,7 +507,9 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   mark(2);
   // 4. wait for the round
   CU(cudaStreamSynchronize(s->tstream));
-  for (Request* r : grids) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+  CU(cudaStreamSynchronize(s->mstream));
+  for (Request* r : grids)
+    if (!r->batched) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
   mark(3);
   // 5. grids read back above can go now (their streams are idle)
   for (Request* r : s->to_free) {
@@ -515,7 +535,34 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       s->order_dirty = true;
     }
   }
+  if (s->batched_grids > 0) {
+    // one read of the batch's status words; finished grids leave the batch
+    // and are read back on their own streams during the next round
+    const int nb = s->batched_grids;
+    std::vector<evora_grid*> gs(nb);
+    std::vector<int32_t> go(nb);
+    std::vector<uint32_t> er(nb);
+    std::vector<int64_t> kk(nb);
+    int32_t n = 0;
+    int rc = evora_multigrid_status(s->mg, gs.data(), go.data(), er.data(), kk.data(), nb, &n);
+    if (rc) return rc;
+    std::map<evora_grid*, int> done;
+    for (int i = 0; i < n; ++i)
+      if (!go[i] || er[i]) done[gs[i]] = i;
+    for (Request* r : grids) {
+      if (!r->batched) continue;
+      auto it = done.find(r->grid);
+      if (it == done.end()) continue;
+      r->steps = kk[it->second];
+      r->err = er[it->second];
+      r->state = REQ_FINISHING;
+      evora_multigrid_remove(s->mg, r->grid);
+      r->batched = false;
+      s->batched_grids--;
+    }
+  }
   for (Request* r : grids) {
+    if (r->batched || r->state != REQ_RUNNING) continue;
     double t, dt;
     int32_t go;
     int64_t k;

@@ -384,9 +384,62 @@ class Grid:
         return self.time()
 
 
+class MultiGrid:
+    """Resident 2D and 3D grids of uneven sizes advanced together: per step
+    one control kernel, one persistent update launch over the tiles of all
+    member grids, one closing control kernel (evora_multigrid_*)."""
+
+    def __init__(self, precision: int = FP32, flags: int = 0, stream=None):
+        h = ctypes.c_void_p()
+        raw = getattr(stream, "cuda_stream", stream) if stream is not None else None
+        check(lib().evora_multigrid_create(precision, flags, ctypes.c_void_p(int(raw) if raw else 0),
+                                           ctypes.byref(h)), "multigrid_create")
+        self._h = h
+        self.members = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().evora_multigrid_destroy(self._h)
+            self._h = None
+            self.members = []
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, grid: "Grid"):
+        check(lib().evora_multigrid_add(self._h, grid._h), "multigrid_add")
+        self.members.append(grid)
+
+    def remove(self, grid: "Grid"):
+        check(lib().evora_multigrid_remove(self._h, grid._h), "multigrid_remove")
+        self.members.remove(grid)
+
+    def step(self, nsteps: int = 1, sync: bool = True):
+        check(lib().evora_multigrid_step(self._h, int(nsteps), 1 if sync else 0), "multigrid_step")
+
+    def status(self):
+        """[(go, err, k)] in member order (waits for the batch)."""
+        n = len(self.members)
+        go = (ctypes.c_int32 * max(n, 1))()
+        err = (ctypes.c_uint32 * max(n, 1))()
+        k = (ctypes.c_int64 * max(n, 1))()
+        cnt = ctypes.c_int32()
+        check(lib().evora_multigrid_status(self._h, None, go, err, k, n, ctypes.byref(cnt)), "multigrid_status")
+        return [(bool(go[i]), int(err[i]), int(k[i])) for i in range(cnt.value)]
+
+
 __all__ = ["EvoraError", "EvoraParams", "EvoraDerived", "default_params", "derived", "shapes",
            "DropIn", "Grid", "Batch", "FP64", "FP32", "CARRY_ENTROPY", "STRICT", "REFERENCE_KERNELS",
-           "FP32_PAIR_TILE", "RESIDENT_FP64", "RESIDENT_FP32"]
+           "FP32_PAIR_TILE", "RESIDENT_FP64", "RESIDENT_FP32", "MultiGrid"]
 
 
 # --------------------------------------------------------- batched tubes --

@@ -371,6 +371,7 @@ int evora_sweep(const double* w, double* q, const double* evo, const double* s, 
 
 /* ------------------------------------------------------- resident layer -- */
 typedef struct evora_grid evora_grid;
+typedef struct evora_multigrid evora_multigrid;
 
 enum evora_precision { EVORA_FP64 = 0, EVORA_FP32 = 1 };
 
@@ -434,6 +435,36 @@ int evora_grid_status(evora_grid* g);
 /* Sums of q(1..6) over the interior in FP64 (the totals of evolution,
  * snapshot.f90:159-193, before the multiplication by the cell volume). */
 int evora_grid_totals(evora_grid* g, double out[6]);
+
+/* ------------------------------------------------ multi-grid batches -- */
+/* Many resident 2D and 3D grids of uneven sizes advanced together (no
+ * counterpart in the reference, which runs one grid per process).  Each step
+ * of all member grids is three launches: one control kernel (every grid's
+ * hydrostep and updatetime, timestep.f90:26-57, 147-171, with its own dt and
+ * t), one persistent update launch whose CTAs pull (grid, tile) work items
+ * from a queue (largest first) and run the fused update of muscl.f90:171-290
+ * on them, and one closing control kernel; steps are replayed from CUDA
+ * graphs.  A member's results equal those of the grid stepped alone (bit for
+ * bit).  Members share precision and flags, are 2D or 3D, and carry no
+ * physics after the update (gravity, conduction, floors, chemistry,
+ * comoving coordinates): EVORA_ERR_ARG otherwise.  While a grid is a member
+ * it is stepped only through its batch; set_q, get_q, time and status work
+ * between batch steps, after a step with sync or evora_multigrid_status.
+ * The batch works on `stream` (NULL: the default stream). */
+int evora_multigrid_create(int32_t precision, int32_t flags, void* stream, evora_multigrid** out);
+/* Releases the batch (its member grids stay, stepped alone again). */
+int evora_multigrid_destroy(evora_multigrid* m);
+int evora_multigrid_add(evora_multigrid* m, evora_grid* g);
+int evora_multigrid_remove(evora_multigrid* m, evora_grid* g);
+/* Advances every member nsteps steps (members whose run has ended, or that
+ * raised an error, pass their state through unchanged).  Asynchronous unless
+ * sync != 0. */
+int evora_multigrid_step(evora_multigrid* m, int32_t nsteps, int32_t sync);
+/* Waits for the batch and reports, in member order, up to max members: the
+ * grid, its go flag, its error mask and its step count; *n = members
+ * reported. */
+int evora_multigrid_status(evora_multigrid* m, evora_grid** grids, int32_t* go, uint32_t* err, int64_t* k,
+                           int32_t max, int32_t* n);
 
 /* Tile autotuner (no counterpart in the reference): times every tile shape
  * of the fused update kernel (`reps` launches each) on the grid's own state
