@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -46,12 +47,21 @@ using Clock = std::chrono::steady_clock;
 // running).
 enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3, REQ_FINISHING = 4 };
 
+// A host buffer of doubles from the server's pool of page-locked buffers
+// (so that uploads and read-backs are direct DMA), or pageable memory when
+// page-locked memory could not be had.
+struct HostBuf {
+  double* p = nullptr;
+  size_t cap = 0;      // doubles
+  bool pinned = false;
+};
+
 struct Request {
   int64_t id = 0;
   int nx = 0, ny = 0, nz = 0;
   double tend = 0.0;
   int bt = 0;                    // boundary type (0: the server's)
-  std::vector<double> q0;        // initial state (host copy), freed at admission
+  HostBuf q0;                    // initial state (host copy), released at admission
   double t_submit = 0.0, t_done = 0.0;
   int state = REQ_PENDING;
   bool tube = false;
@@ -64,7 +74,8 @@ struct Request {
   int64_t steps = 0;
   int round_steps = 1;           // steps per round (grids)
   unsigned err = 0;
-  std::vector<double> result;
+  HostBuf result;                // read back state, released when delivered
+  size_t result_n = 0;
   long long cells() const { return (long long)nx * ny * nz; }
 };
 
@@ -124,6 +135,8 @@ struct evora_server {
   long long grid_cell_updates = 0;
   double first_submit = -1.0, last_done = 0.0;
   size_t fixed = 0;              // arena and staging
+  // page-locked host buffers by size class (powers of two of doubles)
+  std::map<int, std::vector<HostBuf>> free_bufs;
   // host time per round phase: launch, read-back, admission, wait, free, detect
   double phase_s[6] = {0, 0, 0, 0, 0, 0};
   long long rounds = 0;
@@ -133,6 +146,43 @@ struct evora_server {
 };
 
 namespace {
+
+HostBuf buf_get(evora_server* s, size_t n) {
+  int cls = 10;
+  while (((size_t)1 << cls) < n) ++cls;
+  auto& fl = s->free_bufs[cls];
+  if (!fl.empty()) {
+    HostBuf b = fl.back();
+    fl.pop_back();
+    return b;
+  }
+  HostBuf b;
+  b.cap = (size_t)1 << cls;
+  if (cudaHostAlloc((void**)&b.p, b.cap * sizeof(double), cudaHostAllocDefault) == cudaSuccess) {
+    b.pinned = true;
+  } else {
+    cudaGetLastError();
+    b.p = static_cast<double*>(std::malloc(b.cap * sizeof(double)));
+    b.pinned = false;
+  }
+  if (!b.p) b.cap = 0;
+  return b;
+}
+
+void buf_put(evora_server* s, HostBuf& b) {
+  if (!b.p) return;
+  int cls = 10;
+  while (((size_t)1 << cls) < b.cap) ++cls;
+  s->free_bufs[cls].push_back(b);
+  b = HostBuf{};
+}
+
+void buf_free(HostBuf& b) {
+  if (!b.p) return;
+  if (b.pinned) cudaFreeHost(b.p);
+  else std::free(b.p);
+  b = HostBuf{};
+}
 
 bool alloc_segment(evora_server* s, long long n, long long* off) {
   for (size_t i = 0; i < s->free_seg.size(); ++i) {
@@ -184,7 +234,7 @@ int admit(evora_server* s, Request& r) {
     s->slot_req[slot] = r.id;
     // on the read-back stream: the running tube launch never touches a free
     // slot or a free arena segment, so the upload overlaps it
-    CU(cudaMemcpyAsync(s->stage, r.q0.data(), sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->rstream));
+    CU(cudaMemcpyAsync(s->stage, r.q0.p, sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->rstream));
     tube_from_aos(s->stage, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->rstream);
     TubeState ts{};
     ts.offset = off;
@@ -224,7 +274,7 @@ int admit(evora_server* s, Request& r) {
     if (rc) return rc == EVORA_ERR_NOMEM ? 1 : rc;
     s->free_streams.pop_back();
     r.stream = si;
-    rc = evora_grid_set_q(g, r.q0.data());
+    rc = evora_grid_set_q(g, r.q0.p);
     if (rc) {
       evora_grid_destroy(g);
       s->free_streams.push_back(si);
@@ -241,7 +291,7 @@ int admit(evora_server* s, Request& r) {
     s->used += bytes;
   }
   r.state = REQ_RUNNING;
-  std::vector<double>().swap(r.q0);
+  buf_put(s, r.q0);   // the upload has completed (both paths waited for it)
   return 0;
 }
 
@@ -393,8 +443,13 @@ int evora_server_destroy(evora_server* s) {
   if (!s) return EVORA_ERR_ARG;
   cudaDeviceSynchronize();
   if (s->mg) evora_multigrid_destroy(s->mg);
-  for (auto& kv : s->reqs)
+  for (auto& kv : s->reqs) {
     if (kv.second.grid) evora_grid_destroy(kv.second.grid);
+    buf_free(kv.second.q0);
+    buf_free(kv.second.result);
+  }
+  for (auto& kv : s->free_bufs)
+    for (auto& b : kv.second) buf_free(b);
   cudaFree(s->q);
   cudaFree(s->tubes);
   cudaFree(s->order);
@@ -425,10 +480,16 @@ int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, dou
   r.tend = tend;
   r.bt = boundtype;
   r.tube = tube;
-  r.q0.assign(q0, q0 + (size_t)EVORA_NQ * nx * ny * nz);
+  const size_t nq = (size_t)EVORA_NQ * nx * ny * nz;
+  r.q0 = buf_get(s, nq);
+  if (!r.q0.p) return EVORA_ERR_NOMEM;
+  std::memcpy(r.q0.p, q0, nq * sizeof(double));
   r.t_submit = s->now();
   if (s->first_submit < 0) s->first_submit = r.t_submit;
-  if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) return EVORA_ERR_ARG;  // could never fit
+  if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) {   // could never fit
+    buf_put(s, r.q0);
+    return EVORA_ERR_ARG;
+  }
   *id = r.id;
   s->pending.push_back(r.id);
   s->reqs.emplace(r.id, std::move(r));
@@ -472,17 +533,19 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   for (auto& kv : s->reqs) {
     Request& r = kv.second;
     if (r.state != REQ_FINISHING) continue;
-    r.result.resize((size_t)EVORA_NQ * r.cells());
+    r.result_n = (size_t)EVORA_NQ * r.cells();
+    r.result = buf_get(s, r.result_n);
+    if (!r.result.p) return EVORA_ERR_NOMEM;
     int rc = 0;
     if (r.tube) {
       tube_to_aos(s->q, s->stage2, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->rstream);
-      CU(cudaMemcpyAsync(r.result.data(), s->stage2, sizeof(double) * r.result.size(), cudaMemcpyDeviceToHost,
+      CU(cudaMemcpyAsync(r.result.p, s->stage2, sizeof(double) * r.result_n, cudaMemcpyDeviceToHost,
                          s->rstream));
       CU(cudaStreamSynchronize(s->rstream));
       free_segment(s, r.off, r.nx);
       s->slot_req[r.slot] = 0;
     } else {
-      rc = evora_grid_get_q(r.grid, r.result.data());
+      rc = evora_grid_get_q(r.grid, r.result.p);
       s->grid_cell_updates += (long long)r.steps * r.cells();
       s->to_free.push_back(&r);
     }
@@ -596,9 +659,12 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
   if (r.state != REQ_DONE && r.state != REQ_FAILED) return 0;
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (steps) *steps = r.steps;
-  if (q_out && !r.result.empty()) std::memcpy(q_out, r.result.data(), sizeof(double) * r.result.size());
+  if (q_out && r.result.p) std::memcpy(q_out, r.result.p, sizeof(double) * r.result_n);
   const int err = (int)r.err;
-  if (q_out) s->reqs.erase(it);   // delivered
+  if (q_out) {   // delivered
+    buf_put(s, r.result);
+    s->reqs.erase(it);
+  }
   return err;
 }
 
