@@ -345,9 +345,6 @@ int copy_back(double* host, const double* dev, size_t bytes) {
 
 int begin(DropinState& S) {
   if (!S.have_params) return EVORA_ERR_ARG;
-  // the non-equilibrium build carries 11 primitives and advects 12 fields;
-  // these routines take the 5-primitive layout
-  if (S.P.noncie) return EVORA_ERR_ARG;
   int dev = 0;
   CU(cudaGetDevice(&dev));
   if (S.device != dev || !S.d_err) {
@@ -375,7 +372,12 @@ int finish(DropinState& S) {
   return (int)e;
 }
 
-const DropinOps& ops(const DropinState& S) { return S.strict ? evora::strict::kOps : evora::fast::kOps; }
+// The kernels of the parameters' array layouts (global.f90:30-36).
+const DropinOps& ops(const DropinState& S) {
+  if (S.P.chemistry && S.P.noncie) return S.strict ? evora::strict::kOpsNcie : evora::fast::kOpsNcie;
+  if (S.P.chemistry) return S.strict ? evora::strict::kOpsCie : evora::fast::kOpsCie;
+  return S.strict ? evora::strict::kOps : evora::fast::kOps;
+}
 
 // ---- resident mode
 // The state goes back to host q when the grid has steps q lacks.
@@ -549,12 +551,12 @@ int evora_invalidate(const double* q) {
 int evora_primitive(double* w, double* q) {
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
-  if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
   if (S.resident) {
     // the primitives are recovered inside the update from the resident
     // state (w is not written); p <= 0 is reported by hydrostep
+    if (S.P.chemistry) return EVORA_ERR_ARG;   // resident grids keep q(6) (species apart)
     if (!w || !q || is_device_pointer(q)) return EVORA_ERR_ARG;
     return resident_bind(S, q);
   }
@@ -775,11 +777,10 @@ int evora_compevo(const double* w, double* evo, double* s, double dt) {
 int evora_sweep(const double* w, double* q, const double* evo, const double* s, double dt) {
   DropinState& S = ds();
   std::lock_guard<std::mutex> lk(S.mu);
-  if (S.P.chemistry) return EVORA_ERR_ARG;   // the drop-in kernels read q(6, ...); grids take q(12, ...)
   int rc = begin(S);
   if (rc) return rc;
   if (S.resident) {
-    if (!w || !evo || !s || !q) return EVORA_ERR_ARG;
+    if (!w || !evo || !s || !q || S.P.chemistry) return EVORA_ERR_ARG;
     if (!S.rgrid || q != S.rq || S.rq_host_newer) {
       set_error_message("evora_sweep: resident mode needs evora_primitive on this q first");
       return EVORA_ERR_ARG;

@@ -22,7 +22,10 @@ struct DropinOps {
                 double dt, unsigned* err, const GridCtl* ctl, cudaStream_t);
 };
 
-namespace fast { extern const DropinOps kOps; }
-namespace strict { extern const DropinOps kOps; }
+// kOps: the plain build's layouts; kOpsCie: q(12) with species carried (the
+// equilibrium-chemistry build); kOpsNcie: q(12) and w(11) with 12 advected
+// fields (the non-equilibrium build).
+namespace fast { extern const DropinOps kOps, kOpsCie, kOpsNcie; }
+namespace strict { extern const DropinOps kOps, kOpsCie, kOpsNcie; }
 
 }  // namespace evora

@@ -18,19 +18,22 @@ namespace evora {
 namespace EVORA_NS {
 
 // Reference array indexing, 1-based interior indices as in the Fortran.
+// NQ, NW: the leading dimensions of q and of w, evo, s (global.f90:30-36:
+// 6 and 5 in the plain build, 12 and 5 with -DCIE, 12 and 11 with -DNONCIE).
+template <int NQ = EVORA_NQ, int NW = EVORA_NW>
 struct RefLayout {
   int nx, ny, nz;
-  __device__ __forceinline__ int64_t q(int i, int j, int k) const {   // q(6, 1:nx, 1:ny, 1:nz)
-    return (int64_t)EVORA_NQ * ((int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)ny * (k - 1)));
+  __device__ __forceinline__ int64_t q(int i, int j, int k) const {   // q(nq, 1:nx, 1:ny, 1:nz)
+    return (int64_t)NQ * ((int64_t)(i - 1) + (int64_t)nx * ((int64_t)(j - 1) + (int64_t)ny * (k - 1)));
   }
-  __device__ __forceinline__ int64_t w(int i, int j, int k) const {   // w(5, -1:nx+2, ...)
-    return (int64_t)EVORA_NW * ((int64_t)(i + 1) + (int64_t)(nx + 4) * ((int64_t)(j + 1) + (int64_t)(ny + 4) * (k + 1)));
+  __device__ __forceinline__ int64_t w(int i, int j, int k) const {   // w(nw, -1:nx+2, ...)
+    return (int64_t)NW * ((int64_t)(i + 1) + (int64_t)(nx + 4) * ((int64_t)(j + 1) + (int64_t)(ny + 4) * (k + 1)));
   }
-  __device__ __forceinline__ int64_t e(int i, int j, int k) const {   // evo(5, 0:nx+1, ...)
-    return (int64_t)EVORA_NW * ((int64_t)i + (int64_t)(nx + 2) * ((int64_t)j + (int64_t)(ny + 2) * k));
+  __device__ __forceinline__ int64_t e(int i, int j, int k) const {   // evo(nw, 0:nx+1, ...)
+    return (int64_t)NW * ((int64_t)i + (int64_t)(nx + 2) * ((int64_t)j + (int64_t)(ny + 2) * k));
   }
-  __device__ __forceinline__ int64_t s(int d, int i, int j, int k) const {  // s(5, 3, 0:nx+1, ...)
-    return (int64_t)EVORA_NW * ((int64_t)(d - 1) + 3 * ((int64_t)i + (int64_t)(nx + 2) * ((int64_t)j + (int64_t)(ny + 2) * k)));
+  __device__ __forceinline__ int64_t s(int d, int i, int j, int k) const {  // s(nw, 3, 0:nx+1, ...)
+    return (int64_t)NW * ((int64_t)(d - 1) + 3 * ((int64_t)i + (int64_t)(nx + 2) * ((int64_t)j + (int64_t)(ny + 2) * k)));
   }
 };
 
@@ -38,11 +41,13 @@ __device__ __forceinline__ void flush_err(unsigned* err, unsigned e) {
   if (e) atomicOr(err, e);
 }
 
-// primitive(w,q), muscl.f90:26-43: one thread per interior cell.
+// primitive(w,q), muscl.f90:26-43: one thread per interior cell; with nw =
+// 11 the species per unit mass w(6:11) = q(7:12) / rho (comp.f90:40-42).
+template <int NQ, int NW>
 __global__ void k_primitive(HydroParams P, double* __restrict__ w, double* __restrict__ q,
                             unsigned* err, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<NQ, NW> L{P.nx, P.ny, P.nz};
   const Gas<double> c = Gas<double>::make(P);
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   unsigned e = 0;
@@ -52,7 +57,7 @@ __global__ void k_primitive(HydroParams P, double* __restrict__ w, double* __res
     int j = (int)((idx / P.nx) % P.ny) + 1;
     int k = (int)(idx / ((int64_t)P.nx * P.ny)) + 1;
     double* qc = q + L.q(i, j, k);
-    double qv[EVORA_NQ], wv[EVORA_NW];
+    double qv[EVORA_NQ], wv[NW];
 #pragma unroll
     for (int f = 0; f < EVORA_NQ; ++f) qv[f] = qc[f];
     q2w(qv, wv, c, P.dualenergy != 0, e);
@@ -60,9 +65,14 @@ __global__ void k_primitive(HydroParams P, double* __restrict__ w, double* __res
       qc[4] = qv[4];
       qc[5] = qv[5];
     }
+    if (NW > 5) {
+      const double densinv = 1.0 / qv[0];
+#pragma unroll
+      for (int f = 5; f < NW; ++f) wv[f] = qc[f + 1] * densinv;
+    }
     double* wc = w + L.w(i, j, k);
 #pragma unroll
-    for (int f = 0; f < EVORA_NW; ++f) wc[f] = wv[f];
+    for (int f = 0; f < NW; ++f) wc[f] = wv[f];
   }
   flush_err(err, e);
 }
@@ -70,76 +80,81 @@ __global__ void k_primitive(HydroParams P, double* __restrict__ w, double* __res
 // bound(w), boundary.f90:26-113.  One launch per axis, in the reference's
 // order x, y, z, each over the full ghost-inclusive extent of the other two
 // axes, so edges and corners end up as the reference leaves them.
+template <int NW>
 __device__ __forceinline__ void copy_cell(double* w, int64_t dst, int64_t src, bool reflect) {
   w[dst + 0] = w[src + 0];
   w[dst + 1] = reflect ? -w[src + 1] : w[src + 1];
   w[dst + 2] = reflect ? -w[src + 2] : w[src + 2];
   w[dst + 3] = reflect ? -w[src + 3] : w[src + 3];
-  w[dst + 4] = w[src + 4];
+#pragma unroll
+  for (int f = 4; f < NW; ++f) w[dst + f] = w[src + f];
 }
 
+template <int NW>
 __global__ void k_bound_x(HydroParams P, double* __restrict__ w, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<EVORA_NQ, NW> L{P.nx, P.ny, P.nz};
   const int ny4 = P.ny + 4, nz4 = P.nz + 4, nx = P.nx, bt = P.boundtype;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ny4 * nz4; idx += gridDim.x * blockDim.x) {
     int j = idx % ny4 - 1, k = idx / ny4 - 1;
     if (bt == 1 || bt == 3) {              // lower: zero gradient (41-48 unreachable)
-      copy_cell(w, L.w(-1, j, k), L.w(2, j, k), false);
-      copy_cell(w, L.w(0, j, k), L.w(1, j, k), false);
+      copy_cell<NW>(w, L.w(-1, j, k), L.w(2, j, k), false);
+      copy_cell<NW>(w, L.w(0, j, k), L.w(1, j, k), false);
     } else if (bt == 2) {
-      copy_cell(w, L.w(-1, j, k), L.w(nx - 1, j, k), false);
-      copy_cell(w, L.w(0, j, k), L.w(nx, j, k), false);
+      copy_cell<NW>(w, L.w(-1, j, k), L.w(nx - 1, j, k), false);
+      copy_cell<NW>(w, L.w(0, j, k), L.w(nx, j, k), false);
     }
     if (bt == 1) {
-      copy_cell(w, L.w(nx + 2, j, k), L.w(nx - 1, j, k), false);
-      copy_cell(w, L.w(nx + 1, j, k), L.w(nx, j, k), false);
+      copy_cell<NW>(w, L.w(nx + 2, j, k), L.w(nx - 1, j, k), false);
+      copy_cell<NW>(w, L.w(nx + 1, j, k), L.w(nx, j, k), false);
     } else if (bt == 2) {
-      copy_cell(w, L.w(nx + 2, j, k), L.w(2, j, k), false);
-      copy_cell(w, L.w(nx + 1, j, k), L.w(1, j, k), false);
+      copy_cell<NW>(w, L.w(nx + 2, j, k), L.w(2, j, k), false);
+      copy_cell<NW>(w, L.w(nx + 1, j, k), L.w(1, j, k), false);
     } else if (bt == 3) {                  // reflecting upper x face
-      copy_cell(w, L.w(nx + 1, j, k), L.w(nx, j, k), true);
-      copy_cell(w, L.w(nx + 2, j, k), L.w(nx - 1, j, k), true);
+      copy_cell<NW>(w, L.w(nx + 1, j, k), L.w(nx, j, k), true);
+      copy_cell<NW>(w, L.w(nx + 2, j, k), L.w(nx - 1, j, k), true);
     }
   }
 }
 
+template <int NW>
 __global__ void k_bound_y(HydroParams P, double* __restrict__ w, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<EVORA_NQ, NW> L{P.nx, P.ny, P.nz};
   const int nx4 = P.nx + 4, nz4 = P.nz + 4, ny = P.ny, bt = P.boundtype;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nx4 * nz4; idx += gridDim.x * blockDim.x) {
     int i = idx % nx4 - 1, k = idx / nx4 - 1;
     if (bt == 1 || bt == 3) {
-      copy_cell(w, L.w(i, -1, k), L.w(i, 2, k), false);
-      copy_cell(w, L.w(i, 0, k), L.w(i, 1, k), false);
-      copy_cell(w, L.w(i, ny + 2, k), L.w(i, ny - 1, k), false);
-      copy_cell(w, L.w(i, ny + 1, k), L.w(i, ny, k), false);
+      copy_cell<NW>(w, L.w(i, -1, k), L.w(i, 2, k), false);
+      copy_cell<NW>(w, L.w(i, 0, k), L.w(i, 1, k), false);
+      copy_cell<NW>(w, L.w(i, ny + 2, k), L.w(i, ny - 1, k), false);
+      copy_cell<NW>(w, L.w(i, ny + 1, k), L.w(i, ny, k), false);
     } else if (bt == 2) {
-      copy_cell(w, L.w(i, -1, k), L.w(i, ny - 1, k), false);
-      copy_cell(w, L.w(i, 0, k), L.w(i, ny, k), false);
-      copy_cell(w, L.w(i, ny + 2, k), L.w(i, 2, k), false);
-      copy_cell(w, L.w(i, ny + 1, k), L.w(i, 1, k), false);
+      copy_cell<NW>(w, L.w(i, -1, k), L.w(i, ny - 1, k), false);
+      copy_cell<NW>(w, L.w(i, 0, k), L.w(i, ny, k), false);
+      copy_cell<NW>(w, L.w(i, ny + 2, k), L.w(i, 2, k), false);
+      copy_cell<NW>(w, L.w(i, ny + 1, k), L.w(i, 1, k), false);
     }
   }
 }
 
+template <int NW>
 __global__ void k_bound_z(HydroParams P, double* __restrict__ w, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<EVORA_NQ, NW> L{P.nx, P.ny, P.nz};
   const int nx4 = P.nx + 4, ny4 = P.ny + 4, nz = P.nz, bt = P.boundtype;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nx4 * ny4; idx += gridDim.x * blockDim.x) {
     int i = idx % nx4 - 1, j = idx / nx4 - 1;
     if (bt == 1 || bt == 3) {
-      copy_cell(w, L.w(i, j, -1), L.w(i, j, 2), false);
-      copy_cell(w, L.w(i, j, 0), L.w(i, j, 1), false);
-      copy_cell(w, L.w(i, j, nz + 2), L.w(i, j, nz - 1), false);
-      copy_cell(w, L.w(i, j, nz + 1), L.w(i, j, nz), false);
+      copy_cell<NW>(w, L.w(i, j, -1), L.w(i, j, 2), false);
+      copy_cell<NW>(w, L.w(i, j, 0), L.w(i, j, 1), false);
+      copy_cell<NW>(w, L.w(i, j, nz + 2), L.w(i, j, nz - 1), false);
+      copy_cell<NW>(w, L.w(i, j, nz + 1), L.w(i, j, nz), false);
     } else if (bt == 2) {
-      copy_cell(w, L.w(i, j, -1), L.w(i, j, nz - 1), false);
-      copy_cell(w, L.w(i, j, 0), L.w(i, j, nz), false);
-      copy_cell(w, L.w(i, j, nz + 2), L.w(i, j, 2), false);
-      copy_cell(w, L.w(i, j, nz + 1), L.w(i, j, 1), false);
+      copy_cell<NW>(w, L.w(i, j, -1), L.w(i, j, nz - 1), false);
+      copy_cell<NW>(w, L.w(i, j, 0), L.w(i, j, nz), false);
+      copy_cell<NW>(w, L.w(i, j, nz + 2), L.w(i, j, 2), false);
+      copy_cell<NW>(w, L.w(i, j, nz + 1), L.w(i, j, 1), false);
     }
   }
 }
@@ -150,10 +165,11 @@ __global__ void k_bound_z(HydroParams P, double* __restrict__ w, const GridCtl* 
 // dx/max(|u|+a) exactly, so the reduction keeps maxima and divides once.
 // smax[0..2] hold the maxima as ordered u64 bit patterns (NaN speeds are
 // skipped, as MIN skips them).
+template <int NW>
 __global__ void k_cfl(HydroParams P, const double* __restrict__ w, unsigned long long* smax,
                       const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<EVORA_NQ, NW> L{P.nx, P.ny, P.nz};
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   double m0 = 0.0, m1 = 0.0, m2 = 0.0;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < n;
@@ -197,11 +213,12 @@ __global__ void k_cfl(HydroParams P, const double* __restrict__ w, unsigned long
 
 // compevo(w,evo,s), muscl.f90:45-113: one thread per cell of the interior
 // plus one ghost layer (lx1:mx1 ...), with the 1D, 2D and 3D variants.
+template <int NW>
 __global__ void k_compevo(HydroParams P, const double* __restrict__ w, double* __restrict__ evo,
                           double* __restrict__ s, double dt, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
   if (ctl) dt = ctl->dt;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<EVORA_NQ, NW> L{P.nx, P.ny, P.nz};
   const double dt2 = -0.5 * dt;
   const int ex = P.nx + 2;
   const int ey = P.onedimension ? 1 : P.ny + 2;
@@ -215,32 +232,35 @@ __global__ void k_compevo(HydroParams P, const double* __restrict__ w, double* _
     if (P.onedimension) j = 1;
     if (P.twodimension) k = 1;
     const double* wc = w + L.w(i, j, k);
-    double wv[5];
+    double wv[NW];
 #pragma unroll
-    for (int f = 0; f < 5; ++f) wv[f] = wc[f];
+    for (int f = 0; f < NW; ++f) wv[f] = wc[f];
     const int ndim = P.onedimension ? 1 : (P.twodimension ? 2 : 3);
-    double a[3][5];
+    double a[3][NW];
     for (int d = 1; d <= ndim; ++d) {
       const double* wm = w + (d == 1 ? L.w(i - 1, j, k) : d == 2 ? L.w(i, j - 1, k) : L.w(i, j, k - 1));
       const double* wp = w + (d == 1 ? L.w(i + 1, j, k) : d == 2 ? L.w(i, j + 1, k) : L.w(i, j, k + 1));
-      double sv[5];
+      double sv[NW];
 #pragma unroll
-      for (int f = 0; f < 5; ++f) sv[f] = slope1(wm[f], wv[f], wp[f], P.limiter);
+      for (int f = 0; f < NW; ++f) sv[f] = slope1(wm[f], wv[f], wp[f], P.limiter);
       double* sd = s + L.s(d, i, j, k);
 #pragma unroll
-      for (int f = 0; f < 5; ++f) sd[f] = sv[f];
+      for (int f = 0; f < NW; ++f) sd[f] = sv[f];
       predictor_term(wv, sv, d, P.g, a[d - 1]);
+      // species rows: the advection term alone (muscl.f90:62, 73-74, 92-94)
+#pragma unroll
+      for (int f = 5; f < NW; ++f) a[d - 1][f] = wv[d] * sv[f];
     }
     double* e = evo + L.e(i, j, k);
     if (ndim == 1) {
 #pragma unroll
-      for (int f = 0; f < 5; ++f) e[f] = dt2 * a[0][f] * P.dxinv;           // 68
+      for (int f = 0; f < NW; ++f) e[f] = dt2 * a[0][f] * P.dxinv;           // 68
     } else if (ndim == 2) {
 #pragma unroll
-      for (int f = 0; f < 5; ++f) e[f] = dt2 * (a[0][f] * P.dxinv + a[1][f] * P.dyinv);  // 86
+      for (int f = 0; f < NW; ++f) e[f] = dt2 * (a[0][f] * P.dxinv + a[1][f] * P.dyinv);  // 86
     } else {
 #pragma unroll
-      for (int f = 0; f < 5; ++f)
+      for (int f = 0; f < NW; ++f)
         e[f] = dt2 * (a[0][f] * P.dxinv + a[1][f] * P.dyinv + a[2][f] * P.dzinv);  // 106-107
     }
   }
@@ -252,12 +272,13 @@ __global__ void k_compevo(HydroParams P, const double* __restrict__ w, double* _
 // reference reuses fr as the next cell's fl; the values are identical).
 // The x, y, z contributions are added in that order (integration,
 // muscl.f90:276-290).
+template <int NQ, int NW, int NF>
 __global__ void k_sweep(HydroParams P, const double* __restrict__ w, double* __restrict__ q,
                         const double* __restrict__ evo, const double* __restrict__ s, double dt,
                         unsigned* err, const GridCtl* ctl) {
   if (ctl_skip(ctl)) return;
   if (ctl) dt = ctl->dt;
-  const RefLayout L{P.nx, P.ny, P.nz};
+  const RefLayout<NQ, NW> L{P.nx, P.ny, P.nz};
   const Gas<double> c = Gas<double>::make(P);
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   const bool so = P.secondorder != 0;
@@ -267,44 +288,44 @@ __global__ void k_sweep(HydroParams P, const double* __restrict__ w, double* __r
     int i = (int)(idx % P.nx) + 1;
     int j = (int)((idx / P.nx) % P.ny) + 1;
     int k = (int)(idx / ((int64_t)P.nx * P.ny)) + 1;
-    double qv[EVORA_NQ];
+    double qv[NF];
     double* qc = q + L.q(i, j, k);
 #pragma unroll
-    for (int f = 0; f < EVORA_NQ; ++f) qv[f] = qc[f];
+    for (int f = 0; f < NF; ++f) qv[f] = qc[f];
     for (int d = 1; d <= 3; ++d) {
       const int nd = d == 1 ? P.nx : d == 2 ? P.ny : P.nz;
       if (nd == 1) continue;
       const double delta = dt * (d == 1 ? P.dxinv : d == 2 ? P.dyinv : P.dzinv);
       const int di = d == 1, dj = d == 2, dk = d == 3;
-      double fl[EVORA_NQ], fr[EVORA_NQ];
+      double fl[NF], fr[NF];
       for (int side = 0; side < 2; ++side) {
         // interface between cells a = (i,j,k) - 1 + side and b = a + 1 along d
         const int ai = i - di + side * di, aj = j - dj + side * dj, ak = k - dk + side * dk;
         const int bi = ai + di, bj = aj + dj, bk = ak + dk;
         const double* wa = w + L.w(ai, aj, ak);
         const double* wb = w + L.w(bi, bj, bk);
-        double wl[5], wr[5];
+        double wl[NW], wr[NW];
         if (so) {
           const double* sa = s + L.s(d, ai, aj, ak);
           const double* sb = s + L.s(d, bi, bj, bk);
           const double* ea = evo + L.e(ai, aj, ak);
           const double* eb = evo + L.e(bi, bj, bk);
 #pragma unroll
-          for (int f = 0; f < 5; ++f) {
+          for (int f = 0; f < NW; ++f) {
             wl[f] = face_plus(wa[f], sa[f], ea[f]);
             wr[f] = face_minus(wb[f], sb[f], eb[f]);
           }
         } else {
 #pragma unroll
-          for (int f = 0; f < 5; ++f) { wl[f] = wa[f]; wr[f] = wb[f]; }
+          for (int f = 0; f < NW; ++f) { wl[f] = wa[f]; wr[f] = wb[f]; }
         }
-        riemann<double, EVORA_NQ>(wl, wr, side == 0 ? fl : fr, d, P.solver, c, e);
+        riemann<double, NF>(wl, wr, side == 0 ? fl : fr, d, P.solver, c, e);
       }
 #pragma unroll
-      for (int f = 0; f < EVORA_NQ; ++f) qv[f] = qv[f] + delta * (fl[f] - fr[f]);
+      for (int f = 0; f < NF; ++f) qv[f] = qv[f] + delta * (fl[f] - fr[f]);
     }
 #pragma unroll
-    for (int f = 0; f < EVORA_NQ; ++f) qc[f] = qv[f];
+    for (int f = 0; f < NF; ++f) qc[f] = qv[f];
   }
   flush_err(err, e);
 }
@@ -316,34 +337,39 @@ inline int grid_for(int64_t n, int block) {
   return (int)(g < 1 ? 1 : g);
 }
 
+template <int NQ, int NW>
 inline void launch_primitive(const HydroParams& P, double* w, double* q, unsigned* err,
                              const GridCtl* ctl, cudaStream_t st) {
   int64_t n = (int64_t)P.nx * P.ny * P.nz;
-  k_primitive<<<grid_for(n, 256), 256, 0, st>>>(P, w, q, err, ctl);
+  k_primitive<NQ, NW><<<grid_for(n, 256), 256, 0, st>>>(P, w, q, err, ctl);
 }
 
+template <int NW>
 inline void launch_bound(const HydroParams& P, double* w, const GridCtl* ctl, cudaStream_t st) {
-  if (P.nx != 1) k_bound_x<<<grid_for((int64_t)(P.ny + 4) * (P.nz + 4), 256), 256, 0, st>>>(P, w, ctl);
-  if (P.ny != 1) k_bound_y<<<grid_for((int64_t)(P.nx + 4) * (P.nz + 4), 256), 256, 0, st>>>(P, w, ctl);
-  if (P.nz != 1) k_bound_z<<<grid_for((int64_t)(P.nx + 4) * (P.ny + 4), 256), 256, 0, st>>>(P, w, ctl);
+  if (P.nx != 1) k_bound_x<NW><<<grid_for((int64_t)(P.ny + 4) * (P.nz + 4), 256), 256, 0, st>>>(P, w, ctl);
+  if (P.ny != 1) k_bound_y<NW><<<grid_for((int64_t)(P.nx + 4) * (P.nz + 4), 256), 256, 0, st>>>(P, w, ctl);
+  if (P.nz != 1) k_bound_z<NW><<<grid_for((int64_t)(P.nx + 4) * (P.ny + 4), 256), 256, 0, st>>>(P, w, ctl);
 }
 
+template <int NW>
 inline void launch_cfl(const HydroParams& P, const double* w, unsigned long long* smax,
                        const GridCtl* ctl, cudaStream_t st) {
   int64_t n = (int64_t)P.nx * P.ny * P.nz;
-  k_cfl<<<grid_for(n, 256), 256, 0, st>>>(P, w, smax, ctl);
+  k_cfl<NW><<<grid_for(n, 256), 256, 0, st>>>(P, w, smax, ctl);
 }
 
+template <int NW>
 inline void launch_compevo(const HydroParams& P, const double* w, double* evo, double* s, double dt,
                            const GridCtl* ctl, cudaStream_t st) {
   int64_t n = (int64_t)(P.nx + 2) * (P.onedimension ? 1 : P.ny + 2) * (P.twodimension ? 1 : P.nz + 2);
-  k_compevo<<<grid_for(n, 128), 128, 0, st>>>(P, w, evo, s, dt, ctl);
+  k_compevo<NW><<<grid_for(n, 128), 128, 0, st>>>(P, w, evo, s, dt, ctl);
 }
 
+template <int NQ, int NW, int NF>
 inline void launch_sweep(const HydroParams& P, const double* w, double* q, const double* evo,
                          const double* s, double dt, unsigned* err, const GridCtl* ctl, cudaStream_t st) {
   int64_t n = (int64_t)P.nx * P.ny * P.nz;
-  k_sweep<<<grid_for(n, 128), 128, 0, st>>>(P, w, q, evo, s, dt, err, ctl);
+  k_sweep<NQ, NW, NF><<<grid_for(n, 128), 128, 0, st>>>(P, w, q, evo, s, dt, err, ctl);
 }
 
 }  // namespace EVORA_NS

@@ -207,7 +207,9 @@ __device__ __forceinline__ void predictor_term(const T* w, const T* s, int d, T 
   a[d] = a[d] + s[4] / w[0];
 }
 
-// flux(w,f,dir), riemann.f90:157-205.  nf = 5 or 6 (the entropy flux).
+// flux(w,f,dir), riemann.f90:157-205.  nf = 5, 6 (the entropy flux) or 12
+// (the non-equilibrium build: the species fluxes f(i) = f(1) w(i-1),
+// riemann.f90:200-204; w then carries 11 primitives).
 template <typename T, int NF>
 __device__ __forceinline__ void flux(const T* w, T* f, int dir, const Gas<T>& c) {
   T u2 = w[1] * w[1] + w[2] * w[2] + w[3] * w[3];
@@ -227,7 +229,9 @@ __device__ __forceinline__ void flux(const T* w, T* f, int dir, const Gas<T>& c)
     f[3] = w[0] * (w[3] * w[3]) + w[4];
   }
   f[4] = ud * ((T)0.5 * w[0] * u2 + c.gg1 * w[4]);
-  if (NF == 6) f[NF - 1] = ud * w[4] / dpow(w[0], c.g1);
+  if (NF >= 6) f[5] = ud * w[4] / dpow(w[0], c.g1);
+#pragma unroll
+  for (int i = 6; i < NF; ++i) f[i] = f[0] * w[i - 1];
 }
 
 // state(w,q), riemann.f90:207-239.
@@ -239,7 +243,9 @@ __device__ __forceinline__ void state(const T* w, T* q, const Gas<T>& c) {
   q[3] = w[0] * w[3];
   T u2 = (w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3]);
   q[4] = (T)0.5 * w[0] * u2 + w[4] / c.g1;
-  if (NF == 6) q[NF - 1] = w[4] / dpow(w[0], c.g1);
+  if (NF >= 6) q[5] = w[4] / dpow(w[0], c.g1);
+#pragma unroll
+  for (int i = 6; i < NF; ++i) q[i] = w[0] * w[i - 1];   // riemann.f90:233-237
 }
 
 // statex(w,qx,s,sm,dir), riemann.f90:241-288.
@@ -252,7 +258,9 @@ __device__ __forceinline__ void statex(const T* w, T* qx, T s, T sm, int dir, co
   qx[3] = (dir == 3 ? sm : w[3]) * qx[0];
   T energy = (T)0.5 * w[0] * ((w[1] * w[1]) + (w[2] * w[2]) + (w[3] * w[3])) + w[4] / c.g1;
   qx[4] = qx[0] * (energy / w[0] + (sm - wd) * (sm + (w[4] / (w[0] * (s - wd)))));
-  if (NF == 6) qx[NF - 1] = qx[0] * w[4] / dpow(w[0], c.g);
+  if (NF >= 6) qx[5] = qx[0] * w[4] / dpow(w[0], c.g);
+#pragma unroll
+  for (int i = 6; i < NF; ++i) qx[i] = qx[0] * w[i - 1];   // riemann.f90:282-286
 }
 
 // hll(wl,wr,f,dir), riemann.f90:47-92.

@@ -69,12 +69,19 @@ class Server:
         lib().evora_server_result(self._h, int(rid), None, None, None, ctypes.byref(st))
         return st.value
 
-    def result(self, rid: int):
-        """(q, latency_s, steps, err) for a finished request, else None."""
+    def result(self, rid: int, out=None):
+        """(q, latency_s, steps, err) for a finished request, else None.  q
+        is written into `out` when given (float64, C-contiguous, the
+        request's shape), else into a new array."""
         st = self.state(rid)
         if st not in (DONE, FAILED):
             return None
-        q = np.empty(self.shapes[rid])
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or out.shape != tuple(self.shapes[rid]):
+                raise ValueError("out must be a C-contiguous float64 array of the request's shape")
+            q = out
+        else:
+            q = np.empty(self.shapes[rid])
         lat, steps, st2 = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int32()
         err = lib().evora_server_result(self._h, int(rid), ctypes.c_void_p(q.ctypes.data), ctypes.byref(lat),
                                         ctypes.byref(steps), ctypes.byref(st2))

@@ -96,16 +96,22 @@ class RefOracle:
         return (self.p.nz, self.p.ny, self.p.nx, 12 if self.p.chemistry else 6)
 
     @property
+    def nw(self):
+        """Primitives per cell: 11 in the non-equilibrium build, else 5
+        (global.f90:30-36)."""
+        return 11 if (self.p.chemistry and self.p.noncie) else 5
+
+    @property
     def shape_w(self):
-        return (self.p.nz + 4, self.p.ny + 4, self.p.nx + 4, 5)
+        return (self.p.nz + 4, self.p.ny + 4, self.p.nx + 4, self.nw)
 
     @property
     def shape_evo(self):
-        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, 5)
+        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, self.nw)
 
     @property
     def shape_s(self):
-        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, 3, 5)
+        return (self.p.nz + 2, self.p.ny + 2, self.p.nx + 2, 3, self.nw)
 
     def zeros_q(self):
         return np.zeros(self.shape_q)

@@ -204,8 +204,9 @@ def test_dropin_noncie_chem_matches_oracle(cuda_device, cfg):
 
 def test_noncie_refusals(cuda_device):
     """The non-equilibrium build advects 12 fields through the hydro update
-    and carries 11 primitives: grids and the routines that take w refuse it;
-    chem and initchem accept it."""
+    and carries 11 primitives: grids, the allocation-free CFL step and the
+    cooling time step (whose CIE abundances it has no use for) refuse it; the
+    drop-in hydro routines, chem and initchem accept it."""
     kw = kw_of(dict(cooling=1, noncie=1, cooldt=1, c_cooldt=0.1), nx=8, ny=8, nz=8)
     p = ev.default_params(**kw)
     with pytest.raises(ev.EvoraError):
@@ -217,9 +218,8 @@ def test_noncie_refusals(cuda_device):
     drop.chem(q)
     w = np.zeros(ev.hydro.shapes(p)["w"])
     assert w.shape[-1] == 11
-    for call in (lambda: drop.hydrostep(w), lambda: drop.bound(w), lambda: drop.coolstep(q, w)):
-        with pytest.raises(ev.EvoraError):
-            call()
+    with pytest.raises(ev.EvoraError):
+        drop.coolstep(q, w)
     # the allocation-free CFL step refuses it too, with its own message
     import ctypes
     import torch
