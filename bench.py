@@ -42,6 +42,7 @@ sys.path.insert(0, ROOT)
 
 NX = NY = NZ = 256
 AUTOTUNE = True
+TILES = None       # (fp32 tile, fp64 tile) pinned by --tiles
 CHEMISTRY = True   # the cosmological box runs the CIE chemistry and cooling
 GAMMA = 5.0 / 3.0
 CFL = 0.5
@@ -169,12 +170,23 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
+def pick_tile(g, precision):
+    """The tile shape of the fused kernel: --tiles pins it (profiling runs
+    reproduce the shape a timed run chose), else autotune, else the default."""
+    import evora_b200 as ev
+    if TILES is not None:
+        t = TILES[0 if precision == ev.FP32 else 1]
+        g.set_tile(t)
+        return t, []
+    return g.autotune(reps=3) if AUTOTUNE else (0, [])
+
+
 def time_grid(ev, torch, q, precision, steps, warmup, stream, gravity=0, conduction=0, box=1.0, **extra):
     """Device-timed resident steps; returns (ms_total, kernel timing, grid)."""
     g = ev.Grid(kh_params(ev, gravity=gravity, conduction=conduction, box=box, **extra), precision)
     g.set_stream(stream)
     g.set_q(q)
-    g.tuning = g.autotune(reps=3) if AUTOTUNE else (0, [])
+    g.tuning = pick_tile(g, precision)
     g.step(warmup, sync=True)
     torch.cuda.synchronize()
     g.set_timing(True)
@@ -690,7 +702,7 @@ def run_cosmo(args):
             g.set_stream(stream)
             g.set_q(q)
             g.step(args.warmup, sync=True)
-            tune = g.autotune(reps=3) if AUTOTUNE else (0, [])
+            tune = pick_tile(g, prec)
             torch.cuda.synchronize()
             g.set_timing(True)
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -903,6 +915,8 @@ def main():
                     help="cells per axis (256 = the benchmark; smaller sizes for ncu captures)")
     ap.add_argument("--forms", default="f32,f64", help="f32,f64 (default) or f32 alone")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shape")
+    ap.add_argument("--tiles", default=None,
+                    help="F32,F64: pin the fused kernel's tile shapes (indices of the tile table) instead of autotune")
     ap.add_argument("--workload", default="kh3d",
                     choices=["kh3d", "sod", "tubes", "serving", "gravity", "conduction", "comoving", "cosmo"],
                     help="kh3d: the benchmark (256^3 KH); tubes: 4096 batched Riemann tubes; serving: request "
@@ -916,10 +930,11 @@ def main():
                     help="serving: measure the capacity with a burst, then latency at 70%% of it")
     ap.add_argument("--no-chemistry", action="store_true", help="cosmo: without the CIE chemistry and cooling")
     args = ap.parse_args()
-    global NX, NY, NZ, AUTOTUNE, CHEMISTRY, WORKLOAD
+    global NX, NY, NZ, AUTOTUNE, CHEMISTRY, WORKLOAD, TILES
     NX = NY = NZ = args.size
     WORKLOAD = WORKLOAD.replace("256^3", f"{NX}^3")
     AUTOTUNE = not args.no_autotune
+    TILES = tuple(int(t) for t in args.tiles.split(",")) if args.tiles else None
     CHEMISTRY = not args.no_chemistry
     if args.warmup < 3:
         args.warmup = 3

@@ -219,6 +219,7 @@ def _declare_batch(L):
         "evora_batch_autotune": ([G, c_int32, ctypes.POINTER(c_int32), ctypes.POINTER(c_int32)], c_int32),
         "evora_hydrostep_noalloc": ([c_void_p, _dp], c_int32),
         "evora_selftest_rcp": ([c_void_p, c_void_p, c_int64], c_int32),
+        "evora_selftest_exp": ([c_void_p, c_void_p, c_int64], c_int32),
         "evora_gravpotential": ([c_void_p, c_void_p], c_int32),
         "evora_gravintegration": ([c_void_p, c_void_p, c_double], c_int32),
         "evora_thermalstep": ([c_void_p, c_void_p, _dp], c_int32),

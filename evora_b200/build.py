@@ -38,7 +38,7 @@ PER_FILE = {
 }
 SOURCES = ["abi.cu", "dropin_fast.cu", "dropin_strict.cu", "grid.cu", "fused.cu",
            "fused_f64.cu", "fused_f64_strict.cu", "fused_f32.cu", "batch.cu", "noalloc.cu", "server.cu",
-           "io.cu", "gravity.cu", "conduction.cu", "chem.cu", "expansion.cu"]
+           "io.cu", "gravity.cu", "conduction.cu", "chem.cu", "chem_fast.cu", "expansion.cu"]
 
 
 def _deps():

@@ -1,18 +1,12 @@
 // chem.cu -- the per-cell step chem(q) of the reference (chemistry.f90:
-// 72-121), after the hydro update and gravity as main.f90:167 orders it:
-//
-//   press = pressure(q)                              (dual-energy write-back)
-//   with chemistry (CIE build): n = q(7:12) in ionisation equilibrium at
-//     (rho, press) and, with cooling, press advanced over dt by the
-//     sub-cycled cooling update (cie, cie.f90:26-56; chemistry.cuh)
-//   press = max(press, temp2press(temp_fl))          (tempfloor)
-//   press = max(press, jeansfloor0 rho rho)          (jeansfloor)
-//   E += dpress / (g-1),  S += dpress / rho^(g-1)   (cooling or a floor)
-//
-// on a resident SoA state (species in their own FP64 array), plus the
-// drop-in chem(q) on the reference layout q(6) or, with chemistry, q(12).
-// Species and cooling are FP64 whatever the state precision.  This
-// translation unit is compiled without FMA contraction.
+// 72-121; the cell update in chem_cell.cuh), after the hydro update and
+// gravity as main.f90:167 orders it, in the reference's order of operations:
+// on a resident SoA state (species in their own FP64 array) for STRICT
+// grids, the drop-in chem(q) on the reference layout q(6) or, with
+// chemistry, q(12), and coolstep (timestep.f90:106-143) for both.  Species
+// and cooling are FP64 whatever the state precision.  This translation unit
+// is compiled without FMA contraction; the default mode's chem(q) is in
+// chem_fast.cu.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -21,6 +15,7 @@
 
 #include "../../include/evora_gpu.h"
 #include "chem.h"
+#include "chem_cell.cuh"
 #include "chemistry.cuh"
 #include "common.h"
 
@@ -35,60 +30,15 @@ int grid_of(int64_t n) {
   return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
 }
 
-// One cell: v holds q(1:6) in FP64 (in place), n the species (in place;
-// read only with chemistry); U the step's units, k its rate coefficients.
-__device__ __forceinline__ void chem_cell(double* v, double* n, const HydroParams& P, const Units& U,
-                                          const ChemCoef& k, double dt, const Gas<double>& c, unsigned& err) {
-  double press = pressure(v, c, P.dualenergy != 0, err);
-  const double oldpress = press;
-  if (P.chemistry) {
-    const ChemParams C{P.cooling, P.background, P.chiH, P.chiHe, P.c_chem, P.substep};
-    if (P.noncie) ncie(C, k, U.temp0, dt, press, n, err);
-    else cie(C, k, U.temp0, dt, v[0], press, n, err);
-  }
-  if (P.cooling || P.tempfloor || P.jeansfloor) {
-    if (P.tempfloor) {
-      // temp2press (comp.f90:104-119): temp sum(n) temp0inv with chemistry,
-      // temp rho temp0inv without
-      const double pfloor = P.chemistry ? P.temp_fl * nsum(n) * U.temp0inv : P.temp_fl * v[0] * U.temp0inv;
-      if (pfloor > press) press = pfloor;   // max(press, pfloor)
-    }
-    if (P.jeansfloor) {
-      const double pfloor = P.jeansfloor0 * v[0] * v[0];
-      if (pfloor > press) press = pfloor;
-    }
-    const double dpress = press - oldpress;
-    v[4] = v[4] + dpress * P.g1inv;
-    v[5] = v[5] + dpress / pow(v[0], P.g1);
-  }
-}
-
-// The cooling sub-cycles are a long FP64 latency chain per cell (powers,
-// exponentials, divisions): registers are capped for 16 warps per SM.
+// chem(q) on the resident SoA state.  The cooling sub-cycles are a long
+// FP64 latency chain per cell (powers, exponentials, divisions): registers
+// are capped for 16 warps per SM.
 template <typename T>
 __global__ void __launch_bounds__(kChemThreads, 4)
 k_chem(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P,
                        const GridCtl* ctl, unsigned* err) {
   if (ctl_skip(ctl)) return;
-  const Gas<double> c = Gas<double>::make(P);
-  const Units U = units_of(P, ctl);
-  const ChemCoef& k = ctl->coef;
-  const double dt = ctl->dt;
-  unsigned e = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double v[6], s[kNs];
-    load_cell(q, n, nf, i, v);   // S not carried (nf = 5): the S terms are dropped
-    if (P.chemistry)
-#pragma unroll
-      for (int j = 0; j < kNs; ++j) s[j] = species[j * n + i];
-    chem_cell(v, s, P, U, k, dt, c, e);
-    q[4 * n + i] = (T)v[4];
-    if (nf == 6) q[5 * n + i] = (T)v[5];
-    if (P.chemistry)
-#pragma unroll
-      for (int j = 0; j < kNs; ++j) species[j * n + i] = s[j];
-  }
-  if (e) atomicOr(err, e);
+  chem_soa(q, n, nf, species, P, ctl, CieExact{}, err);
 }
 
 // coolstep (timestep.f90:106-143) part 1 on a resident SoA state: the
@@ -159,7 +109,7 @@ __global__ void k_chem_aos(double* __restrict__ q, int64_t n, int nq, HydroParam
   unsigned e = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double* cell = q + (int64_t)nq * i;
-    chem_cell(cell, cell + EVORA_NQ, P, U, k, dt, c, e);
+    chem_cell(cell, cell + EVORA_NQ, P, U, k, dt, c, CieExact{}, e);
   }
   if (e) atomicOr(err, e);
 }

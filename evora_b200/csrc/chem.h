@@ -14,6 +14,12 @@ namespace evora {
 int chem_step(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
               cudaStream_t st);
 
+// The same on a grid of the default mode: fewer FP64 operations per cooling
+// sub-cycle (shared powers of T, a table-driven exponential, contracted
+// products), within a few ulp of chem_step per rate (chem_fast.cu).
+int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
+                   cudaStream_t st);
+
 // coolstep (timestep.f90:106-143) part 1 on the state at the start of a
 // step (nf fields, f32 or f64) and its species: the smallest cooling time
 // into ctl->vcool (preset by the step's first kernel), the equilibrium

@@ -1,0 +1,392 @@
+// chem_fast.cu -- chem(q) (chemistry.f90:72-121) of the default (not
+// STRICT) mode on a resident SoA state: the cell update of chem_cell.cuh with
+// the CIE cooling sub-cycles (cie.f90:26-56) evaluating fewer FP64
+// operations per cycle than the reference's order of operations (chem.cu):
+//
+//   * the rates (rates.f90:80-158) share their powers of T: T^-3/2 =
+//     T^-1 T^-1/2 and T^-1/2 = T^-1 sqrt(T) are products instead of an
+//     exponential and a division; T^0.3647 = T T^-0.6353 exp(-2^-25 ln T)
+//     (the single-precision literals 0.3647 and -0.6353 differ by exactly
+//     1 - 2^-25), e^(-2^-25 ln T) by its cubic Taylor polynomial;
+//     T^-0.397 exp(-473638/T) is one exponential of the summed arguments;
+//   * the remaining nine exponentials per cycle use the table-driven method
+//     of Tang (ACM TOMS 15(2), 1989, "Table-driven implementation of the
+//     exponential function in IEEE floating-point arithmetic") with 32
+//     table entries and the degree-6 Taylor polynomial of e^r - 1 on
+//     |r| <= ln2/64 (truncation below 4e-18), about 1 ulp;
+//   * 8 reciprocals (rcp64: the hardware's approximation and two Newton
+//     steps, within an ulp) instead of 12 divisions per cycle: those of p
+//     and sum(n) are shared by T, 1/T and the pressure update, and the
+//     equilibrium abundances take one per element;
+//   * products and sums contract to FMAs (this unit is compiled with them).
+//
+// Results stay within a few ulp of the reference order per rate; the cells'
+// trajectories agree with the oracle to the chemistry tests' tolerances.
+// Species and cooling are FP64 whatever the state precision.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <type_traits>
+
+#include "../../include/evora_gpu.h"
+#include "chem.h"
+#include "chem_cell.cuh"
+#include "chemistry.cuh"
+#include "common.h"
+
+namespace evora {
+namespace {
+
+constexpr int kChemThreads = 128;
+
+// 2^(j/32), j = 0..31, rounded to nearest double (from 60-digit decimal
+// arithmetic).
+__device__ const double kExp2Frac[32] = {
+    0x1.0000000000000p+0, 0x1.059b0d3158574p+0, 0x1.0b5586cf9890fp+0, 0x1.11301d0125b51p+0,
+    0x1.172b83c7d517bp+0, 0x1.1d4873168b9aap+0, 0x1.2387a6e756238p+0, 0x1.29e9df51fdee1p+0,
+    0x1.306fe0a31b715p+0, 0x1.371a7373aa9cbp+0, 0x1.3dea64c123422p+0, 0x1.44e086061892dp+0,
+    0x1.4bfdad5362a27p+0, 0x1.5342b569d4f82p+0, 0x1.5ab07dd485429p+0, 0x1.6247eb03a5585p+0,
+    0x1.6a09e667f3bcdp+0, 0x1.71f75e8ec5f74p+0, 0x1.7a11473eb0187p+0, 0x1.82589994cce13p+0,
+    0x1.8ace5422aa0dbp+0, 0x1.93737b0cdc5e5p+0, 0x1.9c49182a3f090p+0, 0x1.a5503b23e255dp+0,
+    0x1.ae89f995ad3adp+0, 0x1.b7f76f2fb5e47p+0, 0x1.c199bdd85529cp+0, 0x1.cb720dcef9069p+0,
+    0x1.d5818dcfba487p+0, 0x1.dfc97337b9b5fp+0, 0x1.ea4afa2a490dap+0, 0x1.f50765b6e4540p+0,
+};
+
+// exp(x) by Tang's table-driven method: x = (32 m + j) ln2/32 + r with
+// n = 32 m + j = rint(32 x / ln2), so |r| <= ln2/64 (a little more when the
+// product rounds across a half), then exp(x) = 2^m 2^(j/32) (1 + p(r)).
+// ln2/32 is split in a leading and a trailing double so that r is exact to
+// about 2^-100 relative to x.  x is clamped to [-746, 710] (NaN passes
+// through the comparisons), outside of which exp rounds to 0 or overflows;
+// 2^m is applied as two powers of two so that a subnormal result rounds
+// once.  tab: kExp2Frac staged in shared memory.
+struct ExpTable {
+  const double* tab;
+  __device__ __forceinline__ double operator()(double x) const {
+    constexpr double kInvL = 0x1.71547652b82fep+5;     // 32 / ln 2
+    constexpr double kLhi = 0x1.62e42fefa39efp-6;      // ln 2 / 32, leading part
+    constexpr double kLlo = 0x1.abc9e3b39803fp-61;     // ... and trailing part
+    x = x < -746.0 ? -746.0 : x;
+    x = x > 710.0 ? 710.0 : x;
+    const double nd = rint(x * kInvL);
+    const int n = __double2int_rn(nd);
+    double r = fma(-nd, kLhi, x);
+    r = fma(-nd, kLlo, r);
+    // e^r - 1 = r + r^2/2 + ... + r^6/720
+    double p = fma(r, 1.0 / 720.0, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = p * r;
+    const double s = tab[n & 31];
+    const double y = fma(s, p, s);
+    const int m = n >> 5;   // floor(n / 32): -1077 .. 1024 after the clamp (NaN: any; y is NaN)
+    const int m1 = m >> 1, m2 = m - m1;
+    const double s1 = __longlong_as_double((long long)((unsigned long long)(m1 + 1023) << 52));
+    const double s2 = __longlong_as_double((long long)((unsigned long long)(m2 + 1023) << 52));
+    return (y * s1) * s2;
+  }
+};
+
+// 1/x from the hardware's approximate FP64 reciprocal (rcp.approx.ftz.f64,
+// relative error below 2^-22, checked by evora_selftest_exp) and two Newton
+// steps (e -> e^2 -> e^4): within an ulp of the quotient for normal x and
+// results, with no branch to a slow path.  x = +-0, +-inf and NaN give the
+// approximation itself (+-inf, +-0, NaN: the residual is NaN there); a
+// subnormal x (flushed) gives +-inf.
+__device__ __forceinline__ double rcp64(double x) {
+  double r0;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r0) : "d"(x));
+  double e = fma(-x, r0, 1.0);
+  double r = fma(r0, e, r0);
+  e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  return e == e ? r : r0;
+}
+
+// The math library's exp.
+struct ExpLib {
+  __device__ __forceinline__ double operator()(double x) const { return exp(x); }
+};
+
+// The rate coefficients staged in shared memory (c[i][j] at 2 i + j), read
+// where they are used: a volatile load is not hoisted out of the sub-cycle
+// loop, so the 26 coefficients hold no registers across it.
+struct CoefShared {
+  const double* c;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(c + 2 * i + j)));
+    return v;
+  }
+};
+
+// The rate coefficients read from the step's ChemCoef.
+struct CoefRef {
+  const ChemCoef* k;
+  __device__ __forceinline__ double operator()(int i, int j) const { return k->c[i][j]; }
+};
+
+// comprates (rates.f90:80-158) at temperature temp (tempinv = 1/temp) with
+// the shared powers of T described above; the same outputs as
+// chemistry.cuh's comprates.  kc(i, j) = k.c[i][j].
+template <class Exp, class Coef>
+__device__ __forceinline__ void comprates_fast(double temp, double tempinv, const Coef& kc, int background,
+                                               int cooling, const Exp& ex, double* chemrate, double* coolrate) {
+  const double lt = log(temp);
+  const double temproot = sqrt(temp);
+  const double tmhalf = tempinv * temproot;   // T^-1/2
+  const double temp15 = tempinv * tmhalf;     // T^-3/2
+  // sqrt(T 1e-5) = sqrt(T) sqrt(1e-5)
+  const double fec = rcp64(1.0 + temproot * 3.1622776601683794e-3);
+  const double fc1 = temproot * fec;
+  const double e1 = ex(-((double)157809.1f * tempinv));
+  const double e2 = ex(-((double)286335.4f * tempinv));
+  const double e3 = ex(-((double)631515.0f * tempinv));
+  const double ln1e3 = -6.907755278982137, ln1e6 = -13.815510557964274;   // ln 1e-3, ln 1e-6
+  const double fr = ex((double)(-0.2f) * (lt + ln1e3)) * rcp64(1.0 + ex((double)0.7f * (lt + ln1e6)));
+  const double fr1 = fr * tmhalf;
+  const double fr2 = fr * temproot;
+  const float c3 = 0.3f * (-94000.0f);   // a product of two default reals
+  const double edr = ex((double)(-470000.0f) * tempinv) * (1.0 + (double)c3 * tempinv);
+  const double p6353 = ex((double)(-0.6353f) * lt);   // T^-0.6353
+  chemrate[0] = kc(0, 0) * fc1 * e1;
+  chemrate[1] = kc(1, 0) * fc1 * e2;
+  chemrate[2] = kc(2, 0) * fc1 * e3;
+  chemrate[3] = kc(3, 0) * fr1;
+  chemrate[4] = kc(4, 0) * p6353 + kc(6, 0) * temp15 * edr;
+  chemrate[5] = kc(5, 0) * fr1;
+  if (background) {
+    chemrate[6] = kc(10, 0);
+    chemrate[7] = kc(11, 0);
+    chemrate[8] = kc(12, 0);
+  } else {
+    chemrate[6] = chemrate[7] = chemrate[8] = 0.0;
+  }
+  if (cooling) {
+    // T^0.3647 = T T^-0.6353 e^u, u = -2^-25 ln T (|u| < 2.3e-5 for any
+    // finite T > 0): e^u by 1 + u + u^2/2 + u^3/6, error below 2e-20
+    const double u = -0x1p-25 * lt;
+    const double eu = fma(fma(fma(u, 1.0 / 6.0, 0.5), u, 1.0), u, 1.0);
+    coolrate[0] = kc(0, 1) * fc1 * e1;
+    coolrate[1] = kc(1, 1) * fc1 * e2;
+    coolrate[2] = kc(2, 1) * fc1 * e3;
+    coolrate[3] = kc(3, 1) * fr2;
+    coolrate[4] = kc(4, 1) * (temp * p6353 * eu);
+    coolrate[5] = kc(5, 1) * fr2;
+    coolrate[6] = kc(6, 1) * temp15 * edr;
+    coolrate[7] = kc(7, 1) * fec * ex((double)(-118348.0f) * tempinv);
+    coolrate[8] = kc(8, 1) * fec * ex((double)(-0.397f) * lt + (double)(-473638.0f) * tempinv);
+    coolrate[9] = kc(9, 1) * temproot;
+    if (background) {
+      coolrate[10] = kc(10, 1);
+      coolrate[11] = kc(11, 1);
+      coolrate[12] = kc(12, 1);
+    } else {
+      coolrate[10] = coolrate[11] = coolrate[12] = 0.0;
+    }
+  }
+}
+
+// cieabundance (cie.f90:58-85) without a UV background, with one
+// reciprocal per element: n(H) = nH cr3 / (cr0 + cr3), n(H+) = nH cr0 /
+// (cr0 + cr3), and with D = cr4 cr5 + cr1 cr5 + cr1 cr2, n(He) = nHe cr4 cr5
+// / D, n(He+) = nHe cr1 cr5 / D, n(He++) = nHe cr1 cr2 / D (the reference's
+// fractions cr0/cr3, cr1/cr4, cr2/cr5 multiplied out); with a background,
+// chemistry.cuh's (implicitcie's electron-density root).
+__device__ __forceinline__ void cieabundance_fast(double nH, double nHe, double* n, const double* cr,
+                                                  int background, double uv, unsigned& err) {
+  if (background && uv > 0.0) {
+    cieabundance(nH, nHe, n, cr, background, uv, err);
+    return;
+  }
+  const double dH = nH * rcp64(cr[0] + cr[3]);
+  n[0] = cr[3] * dH;
+  n[1] = cr[0] * dH;
+  const double a = cr[4] * cr[5], b = cr[1] * cr[5], c = cr[1] * cr[2];
+  const double dHe = nHe * rcp64(a + b + c);
+  n[2] = a * dHe;
+  n[3] = b * dHe;
+  n[4] = c * dHe;
+  n[5] = n[1] + n[3] + 2 * n[4];
+  check_floor(n, err);
+}
+
+// cie (cie.f90:26-56) with comprates_fast and cieabundance_fast: the same
+// sub-cycle schedule and pressure update as chemistry.cuh's cie, with the
+// reciprocals of p and sum(n) shared: T = p / sum(n) temp0, 1/T =
+// sum(n) / p / temp0, cdt Lambda / p.
+template <class Exp, class Coef>
+struct CieFast {
+  Exp ex;
+  Coef kc;
+  __device__ __forceinline__ void run(const ChemParams& C, const ChemCoef& k, double temp0, double dt, double rho,
+                                      double& press, double* n, unsigned& err) const {
+    const double nH = C.chiH * rho, nHe = C.chiHe * rho;
+    const double temp0inv = rcp64(temp0);
+    double chemrate[kNchem], coolrate[kNcool];
+    if (!C.cooling) {
+      const double ns = nsum(n);
+      comprates_fast(press * rcp64(ns) * temp0, ns * rcp64(press) * temp0inv, kc, C.background, 0, ex,
+                     chemrate, coolrate);
+      cieabundance_fast(nH, nHe, n, chemrate, C.background, k.uv, err);
+      return;
+    }
+    double ct = 0.0;
+    int cycles = 0;
+    while (ct < dt) {
+      if (++cycles > kCoolMaxCycles) {
+        err |= EVORA_ERR_CHEM;
+        break;
+      }
+      const double ns = nsum(n);
+      const double pinv = rcp64(press);
+      comprates_fast(press * rcp64(ns) * temp0, ns * pinv * temp0inv, kc, C.background, 1, ex, chemrate,
+                     coolrate);
+      cieabundance_fast(nH, nHe, n, chemrate, C.background, k.uv, err);
+      double lambda, gamma;
+      cool(n, coolrate, C.background, lambda, gamma);
+      const double coolio = gamma - lambda;
+      const double cooltime = fabs(press * rcp64(coolio));
+      double cdt = C.c_chem * cooltime;
+      const double rest = dt - ct, cap = dt * C.substep;
+      if (rest < cdt) cdt = rest;   // min(c_chem * cooltime, dt - ct, dt * substep)
+      if (cap < cdt) cdt = cap;
+      ct = ct + cdt;
+      press = (press + cdt * gamma) * rcp64(1.0 + cdt * lambda * pinv);
+    }
+  }
+};
+
+// chem(q) on the resident SoA state.  kTable: Tang's exponential (its table
+// staged in shared memory), else the math library's; kSmemCoef: the rate
+// coefficients read from shared memory where they are used.
+template <typename T, int MINB, bool kTable, bool kSmemCoef>
+__global__ void __launch_bounds__(kChemThreads, MINB)
+k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P, const GridCtl* ctl,
+            unsigned* err) {
+  if (ctl_skip(ctl)) return;
+  __shared__ double tab[32];
+  __shared__ double coef[2 * kNcool];
+  if (threadIdx.x < 32) tab[threadIdx.x] = kExp2Frac[threadIdx.x];
+  if (threadIdx.x < 2 * kNcool) coef[threadIdx.x] = ctl->coef.c[threadIdx.x >> 1][threadIdx.x & 1];
+  __syncthreads();
+  using Exp = typename std::conditional<kTable, ExpTable, ExpLib>::type;
+  using Coef = typename std::conditional<kSmemCoef, CoefShared, CoefRef>::type;
+  Exp ex;
+  if constexpr (kTable) ex.tab = tab;
+  Coef kc;
+  if constexpr (kSmemCoef) kc.c = coef;
+  else kc.k = &ctl->coef;
+  chem_soa(q, n, nf, species, P, ctl, CieFast<Exp, Coef>{ex, kc}, err);
+}
+
+// The self-test of the error bounds over x[0..n): out[i] = Tang's exp(x[i]),
+// out[n + i] = rcp64(x[i]), out[2n + i] = the hardware's approximate
+// reciprocal it starts from.
+__global__ void k_math_selftest(const double* __restrict__ x, double* __restrict__ out, int64_t n) {
+  __shared__ double tab[32];
+  if (threadIdx.x < 32) tab[threadIdx.x] = kExp2Frac[threadIdx.x];
+  __syncthreads();
+  const ExpTable ex{tab};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    double r0;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r0) : "d"(v));
+    out[i] = ex(v);
+    out[n + i] = rcp64(v);
+    out[2 * n + i] = r0;
+  }
+}
+
+template <typename T, int MINB, bool kTable, bool kSmemCoef>
+void launch_chem(void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl, int blocks,
+                 cudaStream_t st) {
+  k_chem_fast<T, MINB, kTable, kSmemCoef>
+      <<<blocks, kChemThreads, 0, st>>>((T*)q, n, nf, species, P, ctl, &ctl->err);
+}
+
+// The kernel form: EVORA_CHEM_FAST="minb,table,smem" (minb 4 or 6 blocks of
+// 128 threads per SM; table 1 for Tang's exponential; smem 1 for the
+// coefficients in shared memory), default "4,1,1".
+struct ChemForm {
+  int minb = 4;
+  bool table = true, smem = true, exact = false;
+};
+ChemForm chem_form() {
+  static const ChemForm f = [] {
+    ChemForm c;
+    if (const char* s = std::getenv("EVORA_CHEM_FAST")) {
+      int m = 4, t = 1, k = 1;
+      if (s[0] == 'x') c.exact = true;
+      if (std::sscanf(s, "%d,%d,%d", &m, &t, &k) == 3 && (m == 4 || m == 5 || m == 6)) {
+        c.minb = m;
+        c.table = t != 0;
+        c.smem = k != 0;
+      }
+    }
+    return c;
+  }();
+  return f;
+}
+
+template <typename T, int MINB>
+void launch_minb(const ChemForm& f, void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl,
+                 int blocks, cudaStream_t st) {
+  if (f.table) f.smem ? launch_chem<T, MINB, true, true>(q, n, nf, species, P, ctl, blocks, st)
+                      : launch_chem<T, MINB, true, false>(q, n, nf, species, P, ctl, blocks, st);
+  else f.smem ? launch_chem<T, MINB, false, true>(q, n, nf, species, P, ctl, blocks, st)
+              : launch_chem<T, MINB, false, false>(q, n, nf, species, P, ctl, blocks, st);
+}
+
+template <typename T>
+void launch_form(const ChemForm& f, void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl,
+                 int blocks, cudaStream_t st) {
+  if (f.minb == 6) launch_minb<T, 6>(f, q, n, nf, species, P, ctl, blocks, st);
+  else if (f.minb == 5) launch_minb<T, 5>(f, q, n, nf, species, P, ctl, blocks, st);
+  else launch_minb<T, 4>(f, q, n, nf, species, P, ctl, blocks, st);
+}
+
+}  // namespace
+
+int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
+                   cudaStream_t st) {
+  const ChemForm f = chem_form();
+  if (f.exact) return chem_step(P, q, f32, nf, n, species, ctl, st);
+  const int64_t want = (n + kChemThreads - 1) / kChemThreads, cap = (int64_t)148 * f.minb * 4;
+  const int blocks = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
+  if (f32) launch_form<float>(f, q, n, nf, species, P, ctl, blocks, st);
+  else launch_form<double>(f, q, n, nf, species, P, ctl, blocks, st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "chem");
+    return EVORA_ERR_CUDA;
+  }
+  return 0;
+}
+
+}  // namespace evora
+
+extern "C" int evora_selftest_exp(const double* x, double* out, int64_t n) {
+  if (!x || !out || n < 0) return EVORA_ERR_ARG;
+  if (n == 0) return 0;
+  double *dx = nullptr, *dy = nullptr;
+  cudaError_t e = cudaMalloc(&dx, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&dy, 3 * sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    evora::k_math_selftest<<<148 * 4, 256>>>(dx, dy, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dy, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dy);
+  if (e != cudaSuccess) {
+    evora::set_cuda_error(e, "evora_selftest_exp");
+    return EVORA_ERR_CUDA;
+  }
+  return 0;
+}

@@ -350,8 +350,8 @@ int enqueue_fused_step(evora_grid* g) {
   }
   if (g->floors) {
     // chem(q): the CIE species and cooling, and the pressure floors (main.f90:167)
-    int rc = chem_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl,
-                       st);
+    auto* step = (g->flags & EVORA_STRICT) ? chem_step : chem_step_fast;
+    int rc = step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl, st);
     if (rc) return rc;
     g->launches += 1;
   }

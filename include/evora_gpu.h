@@ -172,6 +172,13 @@ const char* evora_version(void);
  * correctly rounded 1.0 / x[i]; out holds 2n doubles. */
 int evora_selftest_rcp(const double* x, double* out, int64_t n);
 
+/* Self-test of the arithmetic the default mode's chem(q) uses (no
+ * counterpart in the reference, which calls exp and divides): for host
+ * arrays x[n], out[i] = the table-driven exp(x[i]) (Tang's method),
+ * out[n + i] = the Newton-refined reciprocal of x[i] and out[2n + i] = the
+ * hardware's approximate reciprocal it starts from; out holds 3n doubles. */
+int evora_selftest_exp(const double* x, double* out, int64_t n);
+
 /* -------------------------------------------------------- drop-in layer -- */
 /* Set the module-global hydro parameters used by the routines below (the
  * analogue of `use global` after compparameter).  Must be called first. */

@@ -48,3 +48,55 @@ def test_rcp_fast_specials(cuda_device):
     assert fast[0] == np.inf and fast[1] == -np.inf
     assert fast[2] == 0.0 and fast[3] == 0.0 and np.signbit(fast[3])
     assert np.isnan(fast[4])
+
+
+def _chem_math(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(3 * x.size)
+    st = lib().evora_selftest_exp(x.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p), x.size)
+    assert st == 0
+    return out[:x.size], out[x.size:2 * x.size], out[2 * x.size:]
+
+
+def _exp(x):
+    return _chem_math(x)[0]
+
+
+def test_rcp64_within_one_ulp(cuda_device):
+    """The reciprocal of the default mode's chemistry: the hardware's
+    approximation is within 2^-20 relative over normal x (two Newton steps
+    then reach full precision), the refined value within 1 ulp of 1.0 / x,
+    and 0, inf, NaN map to inf, 0, NaN."""
+    rng = np.random.default_rng(7)
+    mag = 10.0 ** rng.uniform(-307, 307, 1 << 20)
+    x = np.concatenate([mag * rng.choice([-1.0, 1.0], mag.size), [1.0, -1.0, 3.0, 0.1, 2.2250738585072014e-308,
+                                                                  1.7976931348623157e308 / 8, 1e-300, 1e300]])
+    _, r, r0 = _chem_math(x)
+    ref = 1.0 / x
+    assert np.max(np.abs(r0 * x - 1.0)) < 2.0 ** -20
+    assert np.all(np.abs(r - ref) <= np.spacing(np.abs(ref)))
+    _, r, _ = _chem_math(np.array([0.0, -0.0, np.inf, -np.inf, np.nan]))
+    assert r[0] == np.inf and r[1] == -np.inf and r[2] == 0.0 and r[3] == 0.0 and np.isnan(r[4])
+
+
+def test_table_exp_within_two_ulp(cuda_device):
+    """Tang's table-driven exponential of the default mode's chemistry
+    against the host's exp (glibc, within 1 ulp of exact): within 2 ulp
+    over normal results, within one subnormal step where exp underflows
+    gradually (x in [-745.2, -708.4]), 0 below, inf above 709.79, NaN
+    through."""
+    rng = np.random.default_rng(6)
+    x = np.concatenate([rng.uniform(-708.0, 709.0, 1 << 20), rng.uniform(-30.0, 30.0, 1 << 18),
+                        rng.uniform(-1e-6, 1e-6, 1 << 12),
+                        np.arange(-20000, 20001) * (np.log(2.0) / 64.0),   # the reduction's half-way points
+                        [0.0, -0.0, 1.0, -1.0, 709.78, -708.39, 5e-324, -5e-324]])
+    y, ref = _exp(x), np.exp(x)
+    assert np.all(np.abs(y - ref) <= 2 * np.spacing(ref))
+    sub = rng.uniform(-745.2, -708.4, 1 << 14)
+    ys, refs = _exp(sub), np.exp(sub)
+    assert np.all(np.abs(ys - refs) <= 5e-324)
+    with np.errstate(over="ignore"):
+        edge = _exp(np.array([-746.0, -800.0, -1e300, -np.inf, 709.8, 710.0, 1e300, np.inf, np.nan]))
+    np.testing.assert_array_equal(edge[:4], 0.0)
+    np.testing.assert_array_equal(edge[4:8], np.inf)
+    assert np.isnan(edge[8])
