@@ -26,8 +26,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <cstdio>
-#include <cstdlib>
 #include <type_traits>
 
 #include "../../include/evora_gpu.h"
@@ -39,7 +37,11 @@
 namespace evora {
 namespace {
 
+// 128-thread blocks, 4 per SM (128 registers per thread, a few spills):
+// measured at 256^3 against 5 and 6 blocks per SM (96 and 80 registers,
+// more spills), which ran about 3 and 2 % slower.
 constexpr int kChemThreads = 128;
+constexpr int kChemMinBlocks = 4;
 
 // 2^(j/32), j = 0..31, rounded to nearest double (from 60-digit decimal
 // arithmetic).
@@ -92,9 +94,9 @@ struct ExpTable {
 };
 
 // 1/x from the hardware's approximate FP64 reciprocal (rcp.approx.ftz.f64,
-// relative error below 2^-22, checked by evora_selftest_exp) and two Newton
-// steps (e -> e^2 -> e^4): within an ulp of the quotient for normal x and
-// results, with no branch to a slow path.  x = +-0, +-inf and NaN give the
+// relative error about 1e-6, checked below 2^-16 by evora_selftest_exp) and
+// two Newton steps (e -> e^2 -> e^4, past 2^-64): within an ulp of the
+// quotient for normal x and results, with no branch to a slow path.  x = +-0, +-inf and NaN give the
 // approximation itself (+-inf, +-0, NaN: the residual is NaN there); a
 // subnormal x (flushed) gives +-inf.
 __device__ __forceinline__ double rcp64(double x) {
@@ -263,7 +265,9 @@ struct CieFast {
 
 // chem(q) on the resident SoA state.  kTable: Tang's exponential (its table
 // staged in shared memory), else the math library's; kSmemCoef: the rate
-// coefficients read from shared memory where they are used.
+// coefficients read from shared memory where they are used (both measured
+// faster in the 256^3 cosmological box: with the library's exp the kernel
+// ran about 14 % slower, with the coefficients in registers about 5 %).
 template <typename T, int MINB, bool kTable, bool kSmemCoef>
 __global__ void __launch_bounds__(kChemThreads, MINB)
 k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P, const GridCtl* ctl,
@@ -302,64 +306,18 @@ __global__ void k_math_selftest(const double* __restrict__ x, double* __restrict
   }
 }
 
-template <typename T, int MINB, bool kTable, bool kSmemCoef>
-void launch_chem(void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl, int blocks,
-                 cudaStream_t st) {
-  k_chem_fast<T, MINB, kTable, kSmemCoef>
-      <<<blocks, kChemThreads, 0, st>>>((T*)q, n, nf, species, P, ctl, &ctl->err);
-}
-
-// The kernel form: EVORA_CHEM_FAST="minb,table,smem" (minb 4 or 6 blocks of
-// 128 threads per SM; table 1 for Tang's exponential; smem 1 for the
-// coefficients in shared memory), default "4,1,1".
-struct ChemForm {
-  int minb = 4;
-  bool table = true, smem = true, exact = false;
-};
-ChemForm chem_form() {
-  static const ChemForm f = [] {
-    ChemForm c;
-    if (const char* s = std::getenv("EVORA_CHEM_FAST")) {
-      int m = 4, t = 1, k = 1;
-      if (s[0] == 'x') c.exact = true;
-      if (std::sscanf(s, "%d,%d,%d", &m, &t, &k) == 3 && (m == 4 || m == 5 || m == 6)) {
-        c.minb = m;
-        c.table = t != 0;
-        c.smem = k != 0;
-      }
-    }
-    return c;
-  }();
-  return f;
-}
-
-template <typename T, int MINB>
-void launch_minb(const ChemForm& f, void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl,
-                 int blocks, cudaStream_t st) {
-  if (f.table) f.smem ? launch_chem<T, MINB, true, true>(q, n, nf, species, P, ctl, blocks, st)
-                      : launch_chem<T, MINB, true, false>(q, n, nf, species, P, ctl, blocks, st);
-  else f.smem ? launch_chem<T, MINB, false, true>(q, n, nf, species, P, ctl, blocks, st)
-              : launch_chem<T, MINB, false, false>(q, n, nf, species, P, ctl, blocks, st);
-}
-
-template <typename T>
-void launch_form(const ChemForm& f, void* q, int64_t n, int nf, double* species, const HydroParams& P, GridCtl* ctl,
-                 int blocks, cudaStream_t st) {
-  if (f.minb == 6) launch_minb<T, 6>(f, q, n, nf, species, P, ctl, blocks, st);
-  else if (f.minb == 5) launch_minb<T, 5>(f, q, n, nf, species, P, ctl, blocks, st);
-  else launch_minb<T, 4>(f, q, n, nf, species, P, ctl, blocks, st);
-}
-
 }  // namespace
 
 int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
                    cudaStream_t st) {
-  const ChemForm f = chem_form();
-  if (f.exact) return chem_step(P, q, f32, nf, n, species, ctl, st);
-  const int64_t want = (n + kChemThreads - 1) / kChemThreads, cap = (int64_t)148 * f.minb * 4;
+  const int64_t want = (n + kChemThreads - 1) / kChemThreads, cap = (int64_t)148 * kChemMinBlocks * 4;
   const int blocks = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
-  if (f32) launch_form<float>(f, q, n, nf, species, P, ctl, blocks, st);
-  else launch_form<double>(f, q, n, nf, species, P, ctl, blocks, st);
+  if (f32)
+    k_chem_fast<float, kChemMinBlocks, true, true>
+        <<<blocks, kChemThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err);
+  else
+    k_chem_fast<double, kChemMinBlocks, true, true>
+        <<<blocks, kChemThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_cuda_error(e, "chem");

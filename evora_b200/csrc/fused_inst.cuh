@@ -21,30 +21,37 @@ namespace EVORA_FNS {
 
 using TT = EVORA_T;
 
-// Tile table of this precision: (TX, TY, ZC, CTAs per SM, TMA).  TMA = 1:
-// the tensor-staged 3D kernel of fused_tma.cuh, for grids tiled by whole
-// tiles (the plan falls back to entry 0 elsewhere).  Entry 0 is the default
-// for grids the TMA kernel does not take; evora_grid_autotune times all
-// entries on the grid itself.  The 3D kernels are instantiated for every
+// Tile table of this precision: (TX, TY, ZC, CTAs per SM, TMA, PIPE).
+// TMA = 1: the tensor-staged 3D kernel of fused_tma.cuh, for grids tiled by
+// whole tiles (the plan falls back to entry 0 elsewhere).  PIPE = 1: the
+// two-barrier pipelined 3D march of fused_kernel.cuh (FP32; in FP64 it
+// measured no faster than the three-barrier march, 3.24 against 3.23 ms per
+// 256^3 launch).  Entry 0 is the
+// default for grids the TMA kernel does not take; evora_grid_autotune times
+// all entries on the grid itself.  The 3D kernels are instantiated for every
 // entry, the 1D and 2D ones for entry 0 only.
 template <int I> struct Tile;
 #if EVORA_PRECISION_F32
-template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 0; };
-template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MINB = 3, TMA = 0; };
-template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 0; };
-template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4, TMA = 0; };
-template <> struct Tile<4> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
+template <> struct Tile<0> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 0, PIPE = 1; };
+template <> struct Tile<1> { static constexpr int TX = 16, TY = 16, ZC = 32, MINB = 3, TMA = 0, PIPE = 1; };
+template <> struct Tile<2> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 0, PIPE = 1; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 4, TMA = 0, PIPE = 1; };
+template <> struct Tile<4> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 2, TMA = 1, PIPE = 1; };
 // two cells per thread on packed FP32 pairs (fused_pair.cuh)
-template <> struct Tile<5> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 2; };
+template <> struct Tile<5> { static constexpr int TX = 32, TY = 8, ZC = 32, MINB = 3, TMA = 2, PIPE = 1; };
 constexpr int kTiles = 6;
 #else
-template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3, TMA = 0; };
-template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3, TMA = 0; };
-template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3, TMA = 0; };
-template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3, TMA = 0; };
-template <> struct Tile<4> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 2, TMA = 1; };
+template <> struct Tile<0> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 3, TMA = 0, PIPE = 0; };
+template <> struct Tile<1> { static constexpr int TX = 32, TY = 4, ZC = 32, MINB = 3, TMA = 0, PIPE = 0; };
+template <> struct Tile<2> { static constexpr int TX = 16, TY = 8, ZC = 16, MINB = 3, TMA = 0, PIPE = 0; };
+template <> struct Tile<3> { static constexpr int TX = 16, TY = 8, ZC = 64, MINB = 3, TMA = 0, PIPE = 0; };
+template <> struct Tile<4> { static constexpr int TX = 16, TY = 8, ZC = 32, MINB = 2, TMA = 1, PIPE = 0; };
 constexpr int kTiles = 5;
 #endif
+
+// The shared-memory layout of the k_fused kernel of entry C.
+template <class C, int NF>
+using TileSmem = FusedSmem<TT, NF, C::TX, C::TY, kSmemDq<TT, C::PIPE != 0>>;
 
 // cuTensorMapEncodeTiled from the driver (no link against libcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -101,8 +108,8 @@ void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cuda
         k_fused_pair<C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A, map);
         return;
       }
-      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, 2>
-          <<<pl.grid, C::TX * C::TY, sizeof(FusedSmem<TT, NF, C::TX, C::TY>), st>>>(A);
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, 2, C::PIPE != 0>
+          <<<pl.grid, C::TX * C::TY, sizeof(TileSmem<C, NF>), st>>>(A);
       return;
     }
 #endif
@@ -114,10 +121,10 @@ void launch(const FusedPlan& pl, const void* qin, void* qout, GridCtl* ctl, cuda
       }
       // the map was checked at plan time; should it fail here, the same
       // tile runs without tensor staging
-      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB>
-          <<<pl.grid, pl.threads, sizeof(FusedSmem<TT, NF, C::TX, C::TY>), st>>>(A);
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB, C::PIPE != 0>
+          <<<pl.grid, pl.threads, sizeof(TileSmem<C, NF>), st>>>(A);
     } else {
-      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB><<<pl.grid, pl.threads, pl.smem, st>>>(A);
+      k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::MINB, C::PIPE != 0><<<pl.grid, pl.threads, pl.smem, st>>>(A);
     }
   }
 }
@@ -129,9 +136,9 @@ FusedLaunch pick_one(int* tx, int* ty, int* zc, size_t* smem, int* threads, int*
   } else {
     using C = Tile<I>;
     *tx = C::TX; *ty = C::TY; *zc = DIM == 3 ? C::ZC : 1; *minb = C::MINB;
-    *smem = sizeof(FusedSmem<TT, NF, C::TX, C::TY>);
+    *smem = sizeof(TileSmem<C, NF>);
     *threads = C::TX * C::TY;
-    auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::TMA == 2 ? 2 : C::MINB>;
+    auto k = k_fused<TT, NF, DIM, C::TX, C::TY, C::ZC, C::TMA == 2 ? 2 : C::MINB, C::PIPE != 0>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 #if EVORA_PRECISION_F32

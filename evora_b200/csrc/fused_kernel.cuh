@@ -185,8 +185,10 @@ __device__ __forceinline__ void prim_k(T* q, T* w, const Gas<T>& c, const HydroP
   prim(q, w, c, P, de, err);
 }
 
-// Shared-memory layout of one CTA (all arrays field-major).
-template <typename T, int NF, int TX, int TY>
+// Shared-memory layout of one CTA (all arrays field-major).  DQ: the
+// pipelined march's staging of the owned cells' state (FP32 state, FP64
+// tiles that run the pipelined march, and the host emulation).
+template <typename T, int NF, int TX, int TY, bool DQ = (sizeof(T) == 4 || kHostEmu)>
 struct FusedSmem {
   static constexpr int RX = TX + 4, RY = TY + 4;
   T w[3][5][RY][RX];          // primitive ring: planes c-1, c, c+1 (+ halo 2)
@@ -197,18 +199,26 @@ struct FusedSmem {
   // maxima of |u_d| + a of the written cells: per thread for FP32 state
   // (whose register budget is tight), per warp otherwise
   T cfl[3][sizeof(T) == 4 ? TX * TY : 32];
-  // FP32 pipelined march: the owned cells' conserved state of the plane
-  // being updated, copied asynchronously one interval ahead of its use
-  T dq[NF][(sizeof(T) == 4 || kHostEmu) ? TX * TY : 1];
+  // pipelined march: the owned cells' conserved state of the plane being
+  // updated, copied asynchronously one interval ahead of its use
+  T dq[NF][DQ ? TX * TY : 1];
 };
 
-// Asynchronous 4-byte global -> shared copy (cp.async), its commit and wait.
+// Whether the shared-memory layout of a march carries dq.
+template <typename T, bool PIPE>
+constexpr bool kSmemDq = PIPE || sizeof(T) == 4 || kHostEmu;
+
+// Asynchronous 4- or 8-byte global -> shared copy (cp.async), its commit
+// and wait.
 template <typename T>
 __device__ __forceinline__ void copy_async(T* dst, const T* src) {
 #if defined(__CUDACC__) && !defined(EVORA_HOST_EMU)
-  static_assert(sizeof(T) == 4, "4-byte copies");
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte copies");
   const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+  if constexpr (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
 #else
   *dst = *src;
 #endif
@@ -311,10 +321,10 @@ __device__ __forceinline__ void cell_faces(const Sm& sm, int sp, int sc, int sn,
 }
 
 // The tile program of one CTA.  tid in [0, TX*TY); (bx, by, bz) its tile.
-// PIPE: the 3D march as a two-barrier software pipeline (faster for FP32
-// state; FP64 tiles, with fewer warps per SM, run the three-barrier march).
+// PIPE: the 3D march as a two-barrier software pipeline (FP32 state, and
+// the FP64 tile entries that select it); else the three-barrier march.
 template <typename T, int NF, int DIM, int TX, int TY, int ZC, bool PIPE = (sizeof(T) == 4)>
-__device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, NF, TX, TY>& sm,
+__device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, NF, TX, TY, kSmemDq<T, PIPE>>& sm,
                                            int tid, int bx, int by, int bz) {
   constexpr int NT = TX * TY;
   constexpr int RX = TX + 4, RY = TY + 4;
@@ -881,12 +891,13 @@ __global__ void __launch_bounds__(128) k_fused1d(FusedArgs<T> A) {
 }
 
 // MINB: CTAs per SM the register allocation must allow (shared memory is
-// sized for the same count; see the tile table in fused_inst.cuh).
-template <typename T, int NF, int DIM, int TX, int TY, int ZC, int MINB>
+// sized for the same count; see the tile table in fused_inst.cuh).  PIPE:
+// the march (fused_tile).
+template <typename T, int NF, int DIM, int TX, int TY, int ZC, int MINB, bool PIPE = (sizeof(T) == 4)>
 __global__ void __launch_bounds__(TX* TY, MINB) k_fused(FusedArgs<T> A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto& sm = *reinterpret_cast<FusedSmem<T, NF, TX, TY>*>(smem_raw);
-  fused_tile<T, NF, DIM, TX, TY, ZC>(A, sm, threadIdx.x, blockIdx.x, blockIdx.y, blockIdx.z);
+  auto& sm = *reinterpret_cast<FusedSmem<T, NF, TX, TY, kSmemDq<T, PIPE>>*>(smem_raw);
+  fused_tile<T, NF, DIM, TX, TY, ZC, PIPE>(A, sm, threadIdx.x, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 #endif
 

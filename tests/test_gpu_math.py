@@ -64,16 +64,16 @@ def _exp(x):
 
 def test_rcp64_within_one_ulp(cuda_device):
     """The reciprocal of the default mode's chemistry: the hardware's
-    approximation is within 2^-20 relative over normal x (two Newton steps
-    then reach full precision), the refined value within 1 ulp of 1.0 / x,
-    and 0, inf, NaN map to inf, 0, NaN."""
+    approximation is within 2^-16 relative over normal x (measured about
+    1e-6; two Newton steps square the error twice, past 2^-64), the refined
+    value within 1 ulp of 1.0 / x, and 0, inf, NaN map to inf, 0, NaN."""
     rng = np.random.default_rng(7)
     mag = 10.0 ** rng.uniform(-307, 307, 1 << 20)
     x = np.concatenate([mag * rng.choice([-1.0, 1.0], mag.size), [1.0, -1.0, 3.0, 0.1, 2.2250738585072014e-308,
                                                                   1.7976931348623157e308 / 8, 1e-300, 1e300]])
     _, r, r0 = _chem_math(x)
     ref = 1.0 / x
-    assert np.max(np.abs(r0 * x - 1.0)) < 2.0 ** -20
+    assert np.max(np.abs(r0 * x - 1.0)) < 2.0 ** -16
     assert np.all(np.abs(r - ref) <= np.spacing(np.abs(ref)))
     _, r, _ = _chem_math(np.array([0.0, -0.0, np.inf, -np.inf, np.nan]))
     assert r[0] == np.inf and r[1] == -np.inf and r[2] == 0.0 and r[3] == 0.0 and np.isnan(r[4])
