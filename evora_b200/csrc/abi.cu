@@ -129,11 +129,14 @@ const char* evora_version(void) { return "evora-b200 0.1 (sm_100a)"; }
 
 namespace {
 // out[i] = the FP64 fast reciprocal of x[i], out[n + i] = the device's
-// correctly rounded 1.0 / x[i].
+// correctly rounded 1.0 / x[i], out[2n + i] = the FP64 fast square root,
+// out[3n + i] = the device's correctly rounded sqrt(x[i]).
 __global__ void k_selftest_rcp(const double* x, double* out, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     out[i] = evora::rcp_fast(x[i]);
     out[n + i] = 1.0 / x[i];
+    out[2 * n + i] = evora::sqrt_fast(x[i]);
+    out[3 * n + i] = sqrt(x[i]);
   }
 }
 }  // namespace
@@ -143,14 +146,14 @@ extern "C" {
 int evora_selftest_rcp(const double* x, double* out, int64_t n) {
   if (!x || !out || n <= 0) return EVORA_ERR_ARG;
   double* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, (size_t)n * 3 * sizeof(double));
+  cudaError_t e = cudaMalloc(&d, (size_t)n * 5 * sizeof(double));
   if (e == cudaSuccess) e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     const int nb = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
     k_selftest_rcp<<<nb, 256>>>(d, d + n, n);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * 2 * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost);
   if (d) cudaFree(d);
   if (e != cudaSuccess) {
     evora::set_cuda_error(e, "evora_selftest_rcp");

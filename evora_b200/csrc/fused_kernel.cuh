@@ -236,7 +236,8 @@ __device__ __forceinline__ void copy_async_wait() {
 
 // hydrostep per cell (timestep.f90:40-43): the signal speeds |u_d| + a of
 // a conserved state, in the working precision.  FP64: q2w and a = sqrt(g p
-// / rho).  FP32 form: its primitives (FP64 pressure recovery where kin >
+// / rho) (in the fast form without dual energy: q2w_fast, the reciprocal
+// and square root of the fast forms).  FP32 form: its primitives (FP64 pressure recovery where kin >
 // E/2) and a in FP32; the maxima over cells and dt are formed in FP64 from
 // these exactly representable values.  The CFL kernel and the fused
 // update's reduction for the next step both call this, so either gives the
@@ -248,8 +249,13 @@ __device__ __forceinline__ void cfl_speeds(const T* qs, const HydroParams& P, bo
   for (int f = 0; f < NF; ++f) q[f] = qs[f];
   T a;
   if constexpr (sizeof(T) == 8) {
-    q2w(q, w, Gas<double>::make(P), de, err);
-    a = sqrt(P.g * w[4] / w[0]);
+    if (kFast && !de) {
+      q2w_fast(q, w, Gas<double>::make(P), err);
+      a = sqrt_fast(P.g * w[4] * rcp_fast(w[0]));
+    } else {
+      q2w(q, w, Gas<double>::make(P), de, err);
+      a = sqrt(P.g * w[4] / w[0]);
+    }
   } else {
     prim(q, w, Gas<float>::make(P), P, de, err);
     a = sqrtf((float)P.g * w[4] / w[0]);

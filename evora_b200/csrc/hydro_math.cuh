@@ -344,23 +344,55 @@ __device__ __forceinline__ void riemann(const T* wl, const T* wr, T* f, int dir,
 // the literal forms).
 
 // Reciprocal.  FP32: the fast-math division of its translation unit.  FP64:
-// Newton-Raphson on a single-precision seed (two iterations: the relative
-// error e of the seed becomes e^2 then e^4, ~2^-92 from 2^-23, i.e. the
-// result is within an ulp).  The seed and its reciprocal are normal floats
-// for |x| in [2^-126, 2^126]; outside that range (and for 0, inf, NaN) the
-// correctly rounded division is taken instead.
+// the hardware's approximate reciprocal (rcp.approx.ftz.f64, relative error
+// about 1e-6) refined by two Newton steps (the error e becomes e^2, then
+// e^4: within an ulp), with no branch: the division's range checks and
+// slow-path branch cut the kernels into blocks the scheduler cannot
+// interleave.  |x| beyond 2^+-1000 is scaled by 2^-+64 first, and the result
+// by the same factor, so that the approximation sees neither a subnormal
+// argument nor a subnormal result; 0, inf and NaN give +-inf, +-0 and NaN
+// (the refinement's residual is NaN there and the approximation is kept).
 __device__ __forceinline__ float rcp_fast(float x) { return 1.0f / x; }
 __device__ __forceinline__ double rcp_fast(double x) {
 #if defined(__CUDA_ARCH__)
   const double a = fabs(x);
-  if (!(a >= 0x1p-126 && a <= 0x1p126)) return 1.0 / x;
-  double r = (double)__frcp_rn((float)x);
-  double e = fma(-x, r, 1.0);
+  const double s = a > 0x1p1000 ? 0x1p-64 : (a < 0x1p-1000 ? 0x1p64 : 1.0);
+  const double xs = x * s;
+  double r0;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r0) : "d"(xs));
+  double e = fma(-xs, r0, 1.0);
+  double r = fma(r0, e, r0);
+  e = fma(-xs, r, 1.0);
   r = fma(r, e, r);
-  e = fma(-x, r, 1.0);
-  return fma(r, e, r);
+  return (e == e ? r : r0) * s;
 #else
   return 1.0 / x;
+#endif
+}
+
+// Square root.  FP32: the fast-math sqrtf.  FP64: the hardware's approximate
+// reciprocal square root (rsqrt.approx.ftz.f64) refined by two Newton steps,
+// then sqrt(x) = x y with one correction, x y + y/2 (x - (x y)^2): within an
+// ulp, with no branch.  x beyond 2^+-1000 is scaled by 2^-+128 (the result
+// by 2^-+64); +-0 and inf return themselves, negative x and NaN give NaN.
+__device__ __forceinline__ float sqrt_fast(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_fast(double x) {
+#if defined(__CUDA_ARCH__)
+  const double si = x > 0x1p1000 ? 0x1p-128 : (x < 0x1p-1000 ? 0x1p128 : 1.0);
+  const double so = x > 0x1p1000 ? 0x1p64 : (x < 0x1p-1000 ? 0x1p-64 : 1.0);
+  const double xs = x * si;
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(xs));
+  double e = fma(-(xs * y), y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-(xs * y), y, 1.0);
+  y = fma(0.5 * y, e, y);
+  double sq = xs * y;
+  const double d = fma(-sq, sq, xs);
+  sq = fma(0.5 * y, d, sq);
+  return sq == sq ? sq * so : ((xs == 0.0 || xs == HUGE_VAL) ? x : sq);
+#else
+  return std::sqrt(x);
 #endif
 }
 
@@ -406,8 +438,8 @@ template <typename T, int NF, int DIR>
 __device__ __forceinline__ void hllc_fast(const T* wl, const T* wr, T* f, const Gas<T>& c, unsigned& err) {
   if (wl[4] <= (T)0 || wr[4] <= (T)0) err |= EVORA_ERR_RIEMANN_PRESSURE;
   const T ril = rcp_fast(wl[0]), rir = rcp_fast(wr[0]);
-  const T al = dsqrt(c.g * wl[4] * ril);
-  const T ar = dsqrt(c.g * wr[4] * rir);
+  const T al = sqrt_fast(c.g * wl[4] * ril);
+  const T ar = sqrt_fast(c.g * wr[4] * rir);
   const T ul = wl[DIR], ur = wr[DIR];
   const T sl = fmin2(ul - al, ur - ar);
   const T sr = fmax2(ul + al, ur + ar);

@@ -166,10 +166,12 @@ const char* evora_last_error(void);
 /* Library version string. */
 const char* evora_version(void);
 
-/* Self-test of the FP64 reciprocal of the fast arithmetic forms (no
- * counterpart in the reference, which divides): for host arrays x[n],
- * out[i] = the device's fast reciprocal of x[i] and out[n + i] = the device's
- * correctly rounded 1.0 / x[i]; out holds 2n doubles. */
+/* Self-test of the FP64 reciprocal and square root of the fast arithmetic
+ * forms (no counterpart in the reference, which divides and calls sqrt): for
+ * host arrays x[n], out[i] = the device's fast reciprocal of x[i],
+ * out[n + i] = the device's correctly rounded 1.0 / x[i], out[2n + i] = the
+ * fast square root and out[3n + i] = the correctly rounded sqrt(x[i]); out
+ * holds 4n doubles. */
 int evora_selftest_rcp(const double* x, double* out, int64_t n);
 
 /* Self-test of the arithmetic the default mode's chem(q) uses (no

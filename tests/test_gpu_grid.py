@@ -165,7 +165,8 @@ def test_autotune_keeps_state_and_time(cuda_device):
     p = ev.default_params(**kw)
     q = ev.ic.kh3d(p)
     # 5 fields, and 6 (the entropy carried: the dual-energy kernels)
-    for prec, flags in ((ev.FP64, 0), (ev.FP32, 0), (ev.FP64, ev.CARRY_ENTROPY), (ev.FP32, ev.CARRY_ENTROPY)):
+    for prec, flags in ((ev.FP64, ev.STRICT), (ev.FP64, ev.STRICT | ev.CARRY_ENTROPY), (ev.FP64, 0), (ev.FP32, 0),
+                        (ev.FP64, ev.CARRY_ENTROPY), (ev.FP32, ev.CARRY_ENTROPY)):
         with ev.Grid(p, prec, flags) as g:
             g.set_q(q)
             g.step(2)
@@ -175,9 +176,11 @@ def test_autotune_keeps_state_and_time(cuda_device):
             np.testing.assert_array_equal(g.get_q(), before)
             assert g.time() == t0
             g.step(3)
-        # every tile shape gives the same answer bit for bit, except the
-        # FP32 packed-pair kernel, whose sums are associated differently:
-        # within FP32 rounding of the others
+        # every tile shape gives the same answer: bit for bit in strict FP64
+        # and with the FP32 state; in default FP64, whose kernels contract
+        # products into FMAs per instantiation, within a few ulp; the FP32
+        # packed-pair kernel, whose sums are associated differently, within
+        # FP32 rounding of the others
         outs = {}
         for tile in range(len(ms)):
             with ev.Grid(p, prec, flags) as g:
@@ -187,7 +190,11 @@ def test_autotune_keeps_state_and_time(cuda_device):
                 outs[tile] = g.get_q()
         plain = [t for t in outs if not (prec == ev.FP32 and t == ev.FP32_PAIR_TILE)]
         for t in plain:
-            np.testing.assert_array_equal(outs[t], outs[plain[0]])
+            if prec == ev.FP64 and not flags & ev.STRICT:
+                a, b = outs[t], outs[plain[0]]
+                assert np.all(np.abs(a - b) <= 8 * np.spacing(np.abs(b))), np.max(np.abs(a - b))
+            else:
+                np.testing.assert_array_equal(outs[t], outs[plain[0]])
         if prec == ev.FP32 and ev.FP32_PAIR_TILE in outs:
             a, b = outs[ev.FP32_PAIR_TILE][..., :5], outs[plain[0]][..., :5]
             assert np.all(rel_l1(a, b)[[0, 1, 2, 4]] <= 1e-6), rel_l1(a, b)

@@ -1,8 +1,10 @@
 """Device arithmetic of the fast forms checked directly against the
-device's correctly rounded operations: the FP64 reciprocal (Newton-Raphson
-on a single-precision seed, with the division taken outside the seed's
-range) is within 1 ulp of 1.0 / x over random magnitudes from 1e-300 to
-1e300, both signs, and at the range edges, 0, inf and NaN."""
+device's correctly rounded operations: the FP64 reciprocal and square root
+(the hardware's approximations refined by Newton steps, with no branch;
+arguments near the ends of the exponent range scaled first) are within 1
+ulp of 1.0 / x and sqrt(x) over random magnitudes from 1e-300 to 1e300,
+both signs, the scaled ranges and subnormals, and at 0, inf and NaN; the
+default-mode chemistry's table-driven exponential and reciprocal likewise."""
 import ctypes
 
 import numpy as np
@@ -13,12 +15,17 @@ from evora_b200._native import lib
 pytestmark = pytest.mark.gpu
 
 
-def _rcp(x):
+def _fast(x):
     x = np.ascontiguousarray(x, dtype=np.float64)
-    out = np.empty(2 * x.size)
+    out = np.empty(4 * x.size)
     st = lib().evora_selftest_rcp(x.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p), x.size)
     assert st == 0
-    return out[:x.size], out[x.size:]
+    return out.reshape(4, x.size)
+
+
+def _rcp(x):
+    o = _fast(x)
+    return o[0], o[1]
 
 
 def test_rcp_fast_within_one_ulp(cuda_device):
@@ -26,11 +33,12 @@ def test_rcp_fast_within_one_ulp(cuda_device):
     mag = 10.0 ** rng.uniform(-300, 300, 1 << 20)
     x = mag * rng.choice([-1.0, 1.0], mag.size)
     edges = []
-    for e in (-126, 126):
+    for e in (-1022, -1000, 126, 1000, 1022):   # the scaled ranges' and the normal range's ends
         b = 2.0 ** e
         edges += [b, np.nextafter(b, 0), np.nextafter(b, np.inf), -b]
-    x = np.concatenate([x, edges, [1e-300, 1e300, -1e-300, -1e300, 5e-324, 1.7976931348623157e308,
-                                   1.0, -1.0, 3.0, 0.1, 1e-38, 1e38, 1e-37, 1e37]])
+    far = np.concatenate([10.0 ** rng.uniform(-323, -301, 1 << 12), 10.0 ** rng.uniform(301, 308, 1 << 12)])
+    x = np.concatenate([x, far, -far, edges, [1e-300, 1e300, -1e-300, -1e300, 5e-324, 1.7976931348623157e308,
+                                              1.0, -1.0, 3.0, 0.1, 1e-38, 1e38, 1e-37, 1e37]])
     fast, div = _rcp(x)
     with np.errstate(over="ignore", divide="ignore"):
         ref = 1.0 / x
@@ -48,6 +56,27 @@ def test_rcp_fast_specials(cuda_device):
     assert fast[0] == np.inf and fast[1] == -np.inf
     assert fast[2] == 0.0 and fast[3] == 0.0 and np.signbit(fast[3])
     assert np.isnan(fast[4])
+
+
+def test_sqrt_fast_within_one_ulp(cuda_device):
+    """The FP64 fast square root (approximate reciprocal square root, two
+    Newton steps and one correction, no branch) within 1 ulp of the
+    correctly rounded sqrt over random magnitudes from 1e-300 to 1e300, the
+    scaled ranges below 2^-1000 and above 2^1000, subnormals, and 0, -0,
+    inf, negative and NaN arguments."""
+    rng = np.random.default_rng(9)
+    x = np.concatenate([10.0 ** rng.uniform(-300, 300, 1 << 20), 10.0 ** rng.uniform(-323, -301, 1 << 12),
+                        10.0 ** rng.uniform(301, 308, 1 << 12),
+                        [5e-324, 2.2250738585072014e-308, 1.7976931348623157e308, 2.0 ** -1000, 2.0 ** 1000,
+                         np.nextafter(2.0 ** -1000, 0), np.nextafter(2.0 ** 1000, np.inf), 1.0, 2.0, 0.25]])
+    o = _fast(x)
+    fast, ref = o[2], o[3]
+    np.testing.assert_array_equal(ref, np.sqrt(x))   # the device's sqrt is correctly rounded
+    assert np.all(np.abs(fast - ref) <= np.spacing(ref))
+    with np.errstate(invalid="ignore"):
+        sp = _fast(np.array([0.0, -0.0, np.inf, -1.0, -np.inf, np.nan]))[2]
+    assert sp[0] == 0.0 and not np.signbit(sp[0]) and sp[1] == 0.0 and np.signbit(sp[1]) and sp[2] == np.inf
+    assert np.all(np.isnan(sp[3:]))
 
 
 def _chem_math(x):
