@@ -173,7 +173,7 @@ __device__ __forceinline__ void tube_run(const BatchArgs<T>& A, T* qs, T* w, int
             for (int f = 0; f < NF; ++f) qv[f] = qs[f * n + cc - 1];
             if (de) {
               unsigned e2 = 0;
-              prim(qv, wd, c, P, de, e2);
+              prim_k(qv, wd, c, P, de, e2);
             }
 #pragma unroll
             for (int f = 0; f < NF; ++f) qs[f * n + cc - 1] = qv[f] + dtdx * (flo[f] - fr[f]);

@@ -177,10 +177,9 @@ __device__ __forceinline__ void riemann_k(const T* wl, const T* wr, T* f, int so
 template <typename T>
 __device__ __forceinline__ void prim_k(T* q, T* w, const Gas<T>& c, const HydroParams& P, bool de, unsigned& err) {
   if constexpr (kFast && sizeof(T) == 8) {
-    if (!de) {
-      q2w_fast(q, w, c, err);
-      return;
-    }
+    if (de) q2w_de_fast(q, w, c, err);
+    else q2w_fast(q, w, c, err);
+    return;
   }
   prim(q, w, c, P, de, err);
 }
@@ -236,8 +235,8 @@ __device__ __forceinline__ void copy_async_wait() {
 
 // hydrostep per cell (timestep.f90:40-43): the signal speeds |u_d| + a of
 // a conserved state, in the working precision.  FP64: q2w and a = sqrt(g p
-// / rho) (in the fast form without dual energy: q2w_fast, the reciprocal
-// and square root of the fast forms).  FP32 form: its primitives (FP64 pressure recovery where kin >
+// / rho) (in the fast forms: q2w_fast or q2w_de_fast, the reciprocal and
+// square root of the fast forms).  FP32 form: its primitives (FP64 pressure recovery where kin >
 // E/2) and a in FP32; the maxima over cells and dt are formed in FP64 from
 // these exactly representable values.  The CFL kernel and the fused
 // update's reduction for the next step both call this, so either gives the
@@ -249,8 +248,9 @@ __device__ __forceinline__ void cfl_speeds(const T* qs, const HydroParams& P, bo
   for (int f = 0; f < NF; ++f) q[f] = qs[f];
   T a;
   if constexpr (sizeof(T) == 8) {
-    if (kFast && !de) {
-      q2w_fast(q, w, Gas<double>::make(P), err);
+    if (kFast) {
+      if (de) q2w_de_fast(q, w, Gas<double>::make(P), err);
+      else q2w_fast(q, w, Gas<double>::make(P), err);
       a = sqrt_fast(P.g * w[4] * rcp_fast(w[0]));
     } else {
       q2w(q, w, Gas<double>::make(P), de, err);
@@ -571,7 +571,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
       for (int f = 0; f < NF; ++f) qv[f] = sm.dq[f][tid];
       if (de) {
         unsigned e2 = 0;
-        prim(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
+        prim_k(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
       }
 #pragma unroll
       for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdx * (sm.fx[f][oj][oi] - sm.fx[f][oj][oi + 1]);
@@ -739,7 +739,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<T>& A, FusedSmem<T, N
         for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + idx);
         if (de) {
           unsigned e2 = 0;
-          prim(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
+          prim_k(qv, wdummy, c, P, de, e2);  // dual-energy resync of q (comp.f90:60-72)
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdx * (sm.fx[f][oj][oi] - sm.fx[f][oj][oi + 1]);
@@ -876,7 +876,7 @@ __device__ __forceinline__ void fused_cell1d(const FusedArgs<T>& A, int i) {
   for (int f = 0; f < NF; ++f) qv[f] = ld(A.qin + f * n + i);
   if (de) {
     unsigned e2 = 0;
-    prim(qv, wd, c, P, de, e2);
+    prim_k(qv, wd, c, P, de, e2);
   }
 #pragma unroll
   for (int f = 0; f < NF; ++f) A.qout[f * n + i] = qv[f] + dtdx * (flo[f] - fhi[f]);

@@ -452,7 +452,7 @@ __device__ __forceinline__ void tma_tile(const FusedArgs<T>& A, const TmaMap& ma
     for (int f = 0; f < NF; ++f) qv[f] = sm.dq[f][tid];
     if (de) {
       unsigned e2 = 0;
-      prim(qv, wdummy, c, P, de, e2);   // dual-energy resync of q (comp.f90:60-72)
+      prim_k(qv, wdummy, c, P, de, e2);   // dual-energy resync of q (comp.f90:60-72)
     }
 #pragma unroll
     for (int f = 0; f < NF; ++f) qv[f] = qv[f] + dtdx * (sm.fx[f][oj][oi] - sm.fx[f][oj][oi + 1]);

@@ -3,8 +3,9 @@
 A single grid is not decomposed (one grid per GPU; more GPUs run replicas).
 Independent tubes or requests shard by whole units: `shard_by_work` assigns
 each unit to a rank, largest estimated work first, always to the rank with
-the least work so far (LPT), so the ranks finish together; no data moves
-between ranks during the run.  The helpers below gather the per-rank
+the least work so far (LPT), so the ranks finish together; serving requests,
+which arrive over time, go one by one to the least-loaded rank
+(`assign_online`).  No data moves between ranks during the run.  The helpers below gather the per-rank
 results and reduce timings (max over ranks) with torch.distributed; they
 work with the NCCL backend on GPUs and with gloo on CPU (tests)."""
 from __future__ import annotations
@@ -44,6 +45,38 @@ def shard_by_work(work, world):
         shards[r].append(i)
         heapq.heappush(heap, (load + work[i], r))
     return [sorted(s) for s in shards]
+
+
+def request_work(shape, tend=1.0):
+    """Estimated work of a serving request on a state of `shape` (nz, ny,
+    nx, nf) run to time tend: cells x steps, the steps growing with the
+    largest edge length (a fixed CFL number over cells of size 1/n)."""
+    cells = int(np.prod(shape[:-1]))
+    return float(cells) * max(shape[:-1]) * float(tend)
+
+
+def assign_online(work, world):
+    """Per-request rank for requests arriving in order, each to the rank with
+    the least estimated work assigned so far (ties to the lowest rank): the
+    dispatch a front end makes without knowing later arrivals.  Deterministic,
+    so every rank computes the same assignment from the same request list."""
+    load = [0.0] * world
+    out = []
+    for w in work:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out.append(r)
+        load[r] += float(w)
+    return out
+
+
+def gather_objects(obj, rank, world):
+    """Every rank's `obj` on rank 0, in rank order (None elsewhere)."""
+    if world == 1:
+        return [obj]
+    import torch.distributed as dist
+    objs = [None] * world if rank == 0 else None
+    dist.gather_object(obj, objs, dst=0)
+    return objs
 
 
 def pack(lengths, q, indices):

@@ -75,3 +75,57 @@ def test_two_gloo_ranks_match_single_process(tmp_path):
     res = np.load(path)
     assert float(res["tmax"]) == 2.0
     np.testing.assert_array_equal(res["full"], ref)
+
+
+def test_assign_online_is_deterministic_and_balanced():
+    """Serving requests go, in arrival order, to the rank with the least
+    estimated work so far: every request has exactly one rank, every rank
+    computes the same assignment, and the loads end within the largest
+    single request of each other."""
+    rng = np.random.default_rng(3)
+    shapes = [(1, 1, int(n), 6) for n in rng.integers(128, 8193, 300)]
+    shapes += [(1, int(m), int(m), 6) for m in 16 * rng.integers(4, 65, 150)]
+    shapes += [(int(m), int(m), int(m), 6) for m in 16 * rng.integers(2, 9, 50)]
+    order = rng.permutation(len(shapes))
+    work = [sharding.request_work(shapes[i], 0.05) for i in order]
+    for world in (1, 2, 3, 8):
+        a = sharding.assign_online(work, world)
+        assert a == sharding.assign_online(list(work), world)
+        assert len(a) == len(work) and set(a) <= set(range(world))
+        load = np.zeros(world)
+        for w, r in zip(work, a):
+            load[r] += w
+        assert load.max() - load.min() <= max(work) + 1e-9
+    # cells x the largest edge (the steps to a fixed end time), x tend
+    assert sharding.request_work((1, 1, 4096, 6)) == 4096.0 * 4096
+    assert sharding.request_work((16, 16, 16, 6), 0.5) == 4096.0 * 16 * 0.5
+
+
+def _serving_worker(rank, world, port, work, result_path):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    owner = sharding.assign_online(work, world)
+    mine = [i for i, r in enumerate(owner) if r == rank]
+    parts = sharding.gather_objects((rank, mine, sum(work[i] for i in mine)), rank, world)
+    if rank == 0:
+        np.savez(result_path, ranks=[p[0] for p in parts], loads=[p[2] for p in parts],
+                 idx=np.concatenate([np.asarray(p[1], dtype=np.int64) for p in parts]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_serving_requests_split_over_two_gloo_ranks(tmp_path):
+    """Two gloo ranks assign the same request list independently and gather
+    their shares on rank 0: every request is served exactly once."""
+    rng = np.random.default_rng(4)
+    work = [float(w) for w in rng.uniform(1, 1000, 400)]
+    path = str(tmp_path / "serving.npz")
+    mp.spawn(_serving_worker, args=(2, _free_port(), work, path), nprocs=2, join=True)
+    r = np.load(path)
+    assert list(r["ranks"]) == [0, 1]
+    assert sorted(r["idx"].tolist()) == list(range(len(work)))
+    assert abs(r["loads"][0] - r["loads"][1]) <= max(work)
