@@ -13,8 +13,11 @@
 // thermal conduction (conduction = .true. with simplekappa = .true.) and,
 // with comoving coordinates (supercomoving = .true.), the expansion factor's
 // integration, the comoving units and the expansion terms run on the device
-// with each hydro step as in main.f90:119-185.  Runs with chemistry are
-// refused: the species network is not on the path this library implements.
+// with each hydro step as in main.f90:119-185.  With chemistry (the CIE
+// build: nq = 12, species n(H, H+, He, He+, He++, e-) in q(7:12)) the IC's
+// species come from initchem (main.f90:94), every step runs chem(q) and,
+// with cooldt, the cooling time step, and dumps and snapshots carry q(12);
+// the non-equilibrium build (noncie), which grids do not run, is refused.
 // With supercomoving, data/<k4>.000 and data/<k4>.units are written when a
 // step lands on dump_redshift(k4) (main.f90:197-202), and the cadence
 // variable is tsnap = a * nsnap.
@@ -211,12 +214,25 @@ int main(int argc, char** argv) {
     return 2;
   }
   (void)fb;
+  const bool chem = p.chemistry != 0;
+  const int nq = chem ? EVORA_NQ_CHEM : EVORA_NQ;
+  if (chem) {
+    // q(12): the IC's q(1:6), then initchem (main.f90:93-94) sets the
+    // equilibrium species through the drop-in layer
+    const size_t n = (size_t)p.nx * p.ny * p.nz;
+    std::vector<double> q12((size_t)EVORA_NQ_CHEM * n, 0.0);
+    for (size_t i = 0; i < n; ++i)
+      for (int f = 0; f < EVORA_NQ; ++f) q12[(size_t)EVORA_NQ_CHEM * i + f] = q[(size_t)EVORA_NQ * i + f];
+    if ((rc = evora_set_params(&p))) return fail("set_params", rc);
+    if ((rc = evora_initchem(q12.data()))) return fail("initchem", rc);
+    q.swap(q12);
+  }
   evora_units u;   // compunits at the start (main.f90:58-62)
   if ((rc = evora_compunits(&p, nullptr, &u))) return fail("compunits", rc);
   const bool comoving = p.supercomoving != 0;
   auto dump = [&](const char* name) {
     const std::string base = std::string("data/") + name;
-    int r = evora_write_dump((base + ".000").c_str(), q.data(), EVORA_NQ, p.nx, p.ny, p.nz, 1, p.nz);
+    int r = evora_write_dump((base + ".000").c_str(), q.data(), nq, p.nx, p.ny, p.nz, 1, p.nz);
     if (!r) r = evora_write_units((base + ".units").c_str(), &u);
     return r;
   };

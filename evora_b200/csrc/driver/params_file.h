@@ -312,14 +312,26 @@ inline evora_params hydro_params(const RunParams& r) {
   p.zstart = r["zstart"];
   p.zend = r["zend"];
   for (int i = 0; i < EVORA_NDUMP; ++i) p.dump_redshift[i] = r.dump_redshift[i];
+  p.chemistry = r.flag("chemistry");
+  p.noncie = r.flag("noncie");
+  p.cooling = r.flag("cooling");
+  p.background = r.flag("background");
+  p.bg = (int32_t)r["bg"];
+  p.cooldt = r.flag("cooldt");
+  p.j0 = r["j0"];
+  p.c_chem = r["c_chem"];
+  p.substep = r["substep"];
+  p.rhoh = r["rhoh"];
+  p.rhohe = r["rhohe"];
+  p.c_cooldt = r["c_cooldt"];
   return p;
 }
 
-// The parts of a run outside the hydro path that these drivers do not have.
+// The parts of a run these drivers do not have: the non-equilibrium
+// chemistry build (grids do not advect its 12 fields).
 inline std::string unsupported(const RunParams& r) {
   std::string s;
-  for (const char* k : {"chemistry"})
-    if (r.flag(k)) s += (s.empty() ? "" : ", ") + std::string(k);
+  if (r.flag("chemistry") && r.flag("noncie")) s += "noncie";
   if (!r.flag("hydro")) s += (s.empty() ? "" : ", ") + std::string("hydro = .false.");
   return s;
 }

@@ -108,6 +108,14 @@ double host_pressure(double* q, const HostGas& c, unsigned* err) {
 // press2temp without chemistry, comp.f90:87-102.
 double press2temp(double press, double rho, double temp0) { return press / rho * temp0; }
 
+// press2temp of a cell q(nq): with chemistry T = p / sum(n) temp0, n =
+// q(7:12) summed in element order, else p / rho temp0 (comp.f90:87-102).
+double cell_temp(double press, const double* q, bool chemistry, double temp0) {
+  if (!chemistry) return press2temp(press, q[0], temp0);
+  const double ns = q[6] + q[7] + q[8] + q[9] + q[10] + q[11];
+  return press / ns * temp0;
+}
+
 // compparameter's side effect on the domain bounds (parameter.f90:164-265):
 // a 1D run resets ymin, ymax, zmin, zmax to [0, dx], a 2D run zmin, zmax.
 struct Geometry {
@@ -146,16 +154,18 @@ std::string line_E(const double* v, int n, int w, int d) {
 }
 
 // ------------------------------------------------------------- snapshot --
-// Cell access for the snapshot writer: either a whole q(6, nx, ny, nz) or
-// the z = z1 plane plus the y = y1 plane (the cells on both live in the z
-// plane, so every cell has exactly one copy).
+// Cell access for the snapshot writer: either a whole q(nq, nx, ny, nz)
+// (nq = 12 with chemistry) or the z = z1 plane plus the y = y1 plane of
+// q(6, ...) (the cells on both live in the z plane, so every cell has
+// exactly one copy).
 struct CellView {
   double* q = nullptr;     // whole grid, or nullptr
   double* zp = nullptr;    // z plane: 6 * (ix + nx * iy)
   double* yp = nullptr;    // y plane: 6 * (ix + nx * iz)
   int nx = 0, ny = 0, z1 = 0, y1 = 0;
+  int nq = EVORA_NQ;       // values per cell of the whole grid
   double* at(int ix, int iy, int iz) const {   // 1-based
-    if (q) return q + (size_t)EVORA_NQ * ((ix - 1) + (size_t)nx * ((iy - 1) + (size_t)ny * (iz - 1)));
+    if (q) return q + (size_t)nq * ((ix - 1) + (size_t)nx * ((iy - 1) + (size_t)ny * (iz - 1)));
     if (iz == z1) return zp + (size_t)EVORA_NQ * ((ix - 1) + (size_t)nx * (iy - 1));
     return yp + (size_t)EVORA_NQ * ((ix - 1) + (size_t)nx * (iz - 1));
   }
@@ -170,10 +180,11 @@ int snapshot_text(const evora_params* p, const Geometry& G, const CellView& v, c
   (void)x1;
   const std::string name = ft::I0(k3, 3);
   unsigned err = 0;
+  const bool chem = p->chemistry != 0;
   auto row = [&](int ix, int iy, int iz, double* press, double* temp) {
     double* q = v.at(ix, iy, iz);
     *press = host_pressure(q, c, &err);
-    *temp = press2temp(*press, q[0], u->temp0);
+    *temp = cell_temp(*press, q, chem, u->temp0);
     return q;
   };
   if (what & EVORA_SNAP_CUT) {
@@ -450,7 +461,6 @@ int evora_read_units(const char* path, evora_units* u) {
 int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32_t k3, int32_t what,
                    const char* dir) {
   if (!p || !q || !u || k3 < 0) return EVORA_ERR_ARG;
-  if (p->chemistry) return EVORA_ERR_ARG;   // the writers take q(6, ...) and T without species
   evora::dropin_resident_write(q);
   Geometry G;
   int rc = geometry(p, &G);
@@ -459,6 +469,7 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
   v.q = q;
   v.nx = p->nx;
   v.ny = p->ny;
+  v.nq = p->chemistry ? EVORA_NQ_CHEM : EVORA_NQ;
   rc = snapshot_text(p, G, v, u, k3, what, dir);
   if (rc || !(what & EVORA_SNAP_BOV)) return rc;
   const std::string name = ft::I0(k3, 3);
@@ -469,10 +480,10 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
   std::vector<float> dens(n), temp(n);
   unsigned err = 0;
   for (size_t i = 0; i < n && !err; ++i) {
-    double* cell = q + EVORA_NQ * i;
+    double* cell = q + (size_t)v.nq * i;
     dens[i] = (float)cell[0];
     const double press = host_pressure(cell, c, &err);
-    temp[i] = (float)press2temp(press, cell[0], u->temp0);
+    temp[i] = (float)cell_temp(press, cell, p->chemistry != 0, u->temp0);
   }
   if (err) return (int)err;
   return bov_data(p, name, dens.data(), temp.data(), dir);
@@ -481,7 +492,15 @@ int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32
 int evora_grid_snapshot(evora_grid* g, const evora_units* u, int32_t k3, int32_t what, const char* dir) {
   if (!g || !u || k3 < 0) return EVORA_ERR_ARG;
   const evora_params* p = grid_params(g);
-  if (p->chemistry) return EVORA_ERR_ARG;   // temperatures without species
+  if (p->chemistry) {
+    // the temperatures read the species: the whole q(12) through the host
+    // writer; with dualenergy its resynchronised cells go back to the grid
+    std::vector<double> q((size_t)EVORA_NQ_CHEM * p->nx * p->ny * p->nz);
+    int rc = evora_grid_get_q(g, q.data());
+    if (!rc) rc = evora_snapshot(p, q.data(), u, k3, what, dir);
+    if (!rc && p->dualenergy) rc = evora_grid_set_q(g, q.data());
+    return rc;
+  }
   Geometry G;
   int rc = geometry(p, &G);
   if (rc) return rc;

@@ -115,9 +115,10 @@ typedef struct evora_params {
    * q(12, nx, ny, nz), q(7:12) = n(H, H+, He, He+, He++, e-) in equilibrium
    * (not advected: the CIE build's fluxes are nf = 6, global.f90:31-32).
    * The non-equilibrium build (noncie: ncie.f90's Patankar solver, the
-   * species advected, nf = 12, nw = 11) is accepted by evora_chem and
-   * evora_initchem only; grids and the routines that take w refuse it
-   * (EVORA_ERR_ARG).                                                         */
+   * species advected, nf = 12, nw = 11) is accepted by the drop-in
+   * routines (the hydro routines on the q(12)/w(11) layout, evora_chem,
+   * evora_initchem); grids, evora_hydrostep_noalloc and evora_coolstep
+   * refuse it (EVORA_ERR_ARG).                                               */
   int32_t chemistry;      /* Fortran logical                                 */
   int32_t noncie;         /* Fortran logical: non-equilibrium species (ncie) */
   int32_t cooling;        /* Fortran logical: radiative cooling (cie)         */

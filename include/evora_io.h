@@ -76,19 +76,21 @@ enum evora_snapshot_what {
   EVORA_SNAP_BOV = 4    /* <k3>.{dens,temp}.bov{,data}   snapshot.f90:225-228, 317-341, write.f90:66-104 */
 };
 
-/* snapshot(k3, q) (snapshot.f90:196-360) from a host q(6, nx, ny, nz) into
- * directory `dir` (the reference's "snap/").  Like the reference, pressure()
- * runs on every printed cell and, with dualenergy, resynchronises that
- * cell's E or S in q (comp.f90:60-69).  The .xz slice is opened in append
- * mode, as in the reference. */
+/* snapshot(k3, q) (snapshot.f90:196-360) from a host q(nq, nx, ny, nz) into
+ * directory `dir` (the reference's "snap/"); nq = 6, or 12 with chemistry,
+ * whose temperatures are p / sum(q(7:12)) temp0 (press2temp, comp.f90:
+ * 87-102).  Like the reference, pressure() runs on every printed cell and,
+ * with dualenergy, resynchronises that cell's E or S in q (comp.f90:60-69).
+ * The .xz slice is opened in append mode, as in the reference. */
 int evora_snapshot(const evora_params* p, double* q, const evora_units* u, int32_t k3, int32_t what,
                    const char* dir);
 
 /* The same from a grid's device-resident state, at the grid's time t:
  * gathers the z = max(nz/2,1) and y = max(ny/2,1) planes for cuts and
- * slices and computes the FP32 density and temperature bricks on the device;
- * with dualenergy the resynchronised cells are written back to the grid, as
- * the reference's in-place pressure() calls leave them. */
+ * slices and computes the FP32 density and temperature bricks on the device
+ * (with chemistry: the whole q(12) through the host writer); with
+ * dualenergy the resynchronised cells are written back to the grid, as the
+ * reference's in-place pressure() calls leave them. */
 int evora_grid_snapshot(evora_grid* g, const evora_units* u, int32_t k3, int32_t what, const char* dir);
 
 /* One plane of the grid's state in the reference layout (FP64, 6 values per

@@ -233,16 +233,23 @@ class Geometry:
 # ---------------------------------------------------------------- snapshot
 def snapshot_files(geo: Geometry, c: Gas, q: np.ndarray, u: dict, k3: int, cut=True, slice_=True,
                    bov=False) -> dict:
-    """snapshot.f90:196-360 -> {file name: bytes}; q (C shape (nz, ny, nx, 6))
-    is updated in place like the reference's."""
+    """snapshot.f90:196-360 -> {file name: bytes}; q (C shape (nz, ny, nx,
+    nq)) is updated in place like the reference's.  nq = 12 is the chemistry
+    build: T = p / sum(q(7:12)) temp0, summed in element order (press2temp,
+    comp.f90:87-102)."""
     nx, ny, nz = geo.nx, geo.ny, geo.nz
     y1, z1 = max(ny // 2, 1), max(nz // 2, 1)
     name = "%03d" % k3
     files = {}
 
+    chem = q.shape[-1] == 12
+
     def cell(ix, iy, iz):
         qq = q[iz - 1, iy - 1, ix - 1]
         press = pressure(qq, c)
+        if chem:
+            ns = qq[6] + qq[7] + qq[8] + qq[9] + qq[10] + qq[11]
+            return qq, press, press / ns * u["temp0"]
         return qq, press, press / qq[0] * u["temp0"]
 
     X = lambda ix: geo.x0 + (ix - 1) * geo.dx

@@ -151,3 +151,49 @@ def test_planes_round_trip(cuda_device, precision):
         np.testing.assert_array_equal(q2, expect)
         with pytest.raises(ev.EvoraError):
             eio.get_plane(grid, 3, 5)
+
+
+def test_driver_comoving_chemistry_run(cuda_device, tmp_path):
+    """The CIE build through the run driver (main.f90 with chemistry =
+    .true.): initchem sets the species of the IC (in.000 carries q(12), bit
+    for bit the oracle's), every step runs chem(q) with the sub-cycled
+    cooling, and out.000 matches the oracle's run to the chemistry tests'
+    tolerances; snapshot temperatures read the species."""
+    kw = dict(nx=256, ny=1, nz=1, boundtype=3, supercomoving=1, omega0=0.3, lambda0=0.7, hubble0=70.0, box=1.0,
+              zstart=10.0, zend=9.5, chemistry=1, cooling=1, g=5 / 3, cfl=0.4)
+    para = tmp_path / "chem"
+    para.write_text("comoving shock tube with chemistry\n$para\nnx = 256, ny = 1, nz = 1\nboundtype = 3\n"
+                    "supercomoving = .true., omega0 = 0.3, lambda0 = 0.7, hubble0 = 70.0, box = 1.0\n"
+                    "zstart = 10.0, zend = 9.5\nchemistry = .true., cooling = .true.\n"
+                    "g = 1.6666666666666667, cfl = 0.4\nnsnap = 2, cut = .true.\n/\n"
+                    "$ic_para\ndl = 1.0, dr = 0.5, ul = 0.0, ur = 0.0, pl = 1.0e-2, pr = 1.0e-3, x_diss = 0.5\n"
+                    "dir = 1\n/\n")
+    r = eio.run(para, tmp_path, "--strict", "--entropy")
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    o = Oracle(make_params(**kw))
+    q = o.ic_shocktube(1.0, 0.0, 1.0e-2, 0.5, 0.0, 1.0e-3, 0.5, 1)
+    assert q.shape == (1, 1, 256, 12)
+    o.initchem(q)
+    assert (tmp_path / "data" / "in.000").read_bytes() == orc.dump_bytes(q)
+    res = o.run(q, 10 ** 6)
+    assert res["status"] == 0 and not res["go"]
+    h, out = eio.read_dump(tmp_path / "data" / "out.000")
+    assert h == (12, 256, 1, 1, 1, 1)
+    # per field, the largest difference against the field's largest value
+    # (the transverse momenta are 0; the device's exp and pow enter the
+    # cooling, so the state is compared to the chemistry tests' tolerances)
+    rel = lambda a, b: np.max(np.abs(a - b), axis=(0, 1, 2)) / np.maximum(np.max(np.abs(b), axis=(0, 1, 2)), 1e-300)   # noqa: E731,E501
+    assert np.all(rel(out[..., :6], q[..., :6]) < 1e-9), rel(out[..., :6], q[..., :6])
+    assert np.all(rel(out[..., 6:], q[..., 6:]) < 1e-8), rel(out[..., 6:], q[..., 6:])
+    # snapshot 000 (tsnap = a nsnap passes no further integer before z =
+    # 9.5): T = p / sum(n) temp0 of in.000's cells, within the E16.6
+    # output (6 significant digits)
+    assert sorted(os.listdir(tmp_path / "snap")) == ["000.x"]
+    rows = np.loadtxt(tmp_path / "snap" / "000.x")
+    u = eio.read_units(tmp_path / "data" / "in.units")
+    cells = eio.read_dump(tmp_path / "data" / "in.000")[1][0, 0]
+    kin = 0.5 * cells[:, 1] ** 2 / cells[:, 0]
+    press = (5 / 3 - 1) * (cells[:, 4] - kin)
+    temp = press / cells[:, 6:12].sum(-1) * u.temp0
+    np.testing.assert_allclose(rows[:, 2], temp, rtol=1e-5)
+    np.testing.assert_allclose(rows[:, 1], cells[:, 0], rtol=1e-5)

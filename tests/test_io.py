@@ -135,6 +135,30 @@ def test_host_snapshot_matches_restatement(tmp_path, case, dualenergy):
         np.testing.assert_array_equal(out, q)
 
 
+@pytest.mark.parametrize("case", SNAP_CASES, ids=["1d", "2d", "3d"])
+def test_host_snapshot_with_chemistry_matches_restatement(tmp_path, case):
+    """The CIE build's q(12): temperatures p / sum(q(7:12)) temp0
+    (press2temp, comp.f90:87-102), cells read with the stride 12."""
+    g = float(np.float32(1.4))
+    p = ev.default_params(**case, chemistry=1)
+    q6 = random_state(p.nx, p.ny, p.nz, g, seed=5)
+    rng = np.random.default_rng(6)
+    q = np.concatenate([q6, rng.uniform(0.01, 1.0, q6.shape[:3] + (6,))], axis=-1)
+    u = eio.units_noncomoving(0.25, g)
+    out = eio.snapshot(p, q, u, 3, eio.SNAP_CUT | eio.SNAP_SLICE | eio.SNAP_BOV, tmp_path)
+    geo = orc.Geometry(p.nx, p.ny, p.nz, p.xmin, p.xmax, p.ymin, p.ymax, p.zmin, p.zmax)
+    files = orc.snapshot_files(geo, orc.Gas(g), q.copy(), orc.units_noncomoving(0.25, g), 3,
+                               cut=True, slice_=True, bov=True)
+    assert sorted(os.listdir(tmp_path)) == sorted(files)
+    for name, data in files.items():
+        assert (tmp_path / name).read_bytes() == data, name
+    np.testing.assert_array_equal(out, q)
+    # the species change the temperatures (against p / rho temp0)
+    plain = orc.snapshot_files(geo, orc.Gas(g), q6.copy(), orc.units_noncomoving(0.25, g), 3, cut=True,
+                               slice_=False, bov=False)
+    assert plain["003.x"] != files["003.x"]
+
+
 def test_xz_slice_appends_like_the_reference(tmp_path):
     p = ev.default_params(nx=4, ny=4, nz=2)
     q = random_state(4, 4, 2, p.g, seed=4)
@@ -226,8 +250,9 @@ def test_driver_reads_namelist_and_writes_parameter_copy(tmp_path, group):
 def test_driver_refuses_unknown_or_unsupported(tmp_path):
     r = run_print(para_file(tmp_path / "p1", "nx = 8, bogus = 3"))
     assert r.returncode != 0 and "bogus" in r.stderr
-    r = eio.run(para_file(tmp_path / "p2", "nx = 8, ny = 1, nz = 1\nchemistry = .true."), tmp_path)
-    assert r.returncode != 0 and "chemistry" in r.stderr
+    r = eio.run(para_file(tmp_path / "p2", "nx = 8, ny = 1, nz = 1\nchemistry = .true., noncie = .true."),
+                tmp_path)
+    assert r.returncode != 0 and "noncie" in r.stderr
     r = run_print(para_file(tmp_path / "p3", "nx = 8, dump_redshift = 3.0, x2.0"))
     assert r.returncode != 0 and "dump_redshift" in r.stderr
     r = eio.run(tmp_path / "missing", tmp_path)
