@@ -3,12 +3,18 @@
 // time loop with the state resident on the GPU and writes the reference's
 // output files.
 //
-//   evora_run <parameterfile> [--ic shocktube|kevinhelmholtz] [--fp32]
-//             [--strict] [--entropy] [--workdir DIR] [--print-params]
+//   evora_run <parameterfile> [--ic shocktube|kevinhelmholtz|dump:FILE]
+//             [--fp32] [--strict] [--entropy] [--workdir DIR]
+//             [--print-params]
 //
 // Input: namelist group para (parameter.f90:26-105) and, for the shocktube,
 // ic_para (ic/shocktube.f90:39-47).  The reference compiles one ic/<name>.f90
 // into the binary (object/Makefile:57-58); here --ic chooses at run time.
+// --ic dump:FILE reads the initial state from a dump in writedata's format
+// (write.f90:47-65; nn = 6, or 12 with the species of a chemistry run, the
+// whole grid in one file), the way ic/grafic.f90 reads an external initial
+// condition: the cosmological box's Zel'dovich IC (ic/cosmo.f90) is built
+// outside the driver and run through it.
 // Self-gravity (gravity = .true.), the temperature / Jeans pressure floors,
 // thermal conduction (conduction = .true. with simplekappa = .true.) and,
 // with comoving coordinates (supercomoving = .true.), the expansion factor's
@@ -135,7 +141,7 @@ int fail(const char* what, int rc) {
 int main(int argc, char** argv) {
   if (argc < 2) {
     std::fprintf(stderr,
-                 "usage: %s <parameterfile> [--ic shocktube|kevinhelmholtz] [--fp32] [--strict] [--entropy] "
+                 "usage: %s <parameterfile> [--ic shocktube|kevinhelmholtz|dump:FILE] [--fp32] [--strict] [--entropy] "
                  "[--workdir DIR] [--print-params]\n",
                  argv[0]);
     return 2;
@@ -207,16 +213,31 @@ int main(int argc, char** argv) {
 
   // ic(q) and the first dump (main.f90:80-97)
   std::vector<double> q;
+  const bool chem = p.chemistry != 0;
+  const int nq = chem ? EVORA_NQ_CHEM : EVORA_NQ;
+  bool have_species = false;   // the IC carries q(7:12)
   if (icname == "shocktube") ic_shocktube(p, d, icp, &q);
   else if (icname == "kevinhelmholtz") ic_kh(p, d, &q);
-  else {
+  else if (icname.rfind("dump:", 0) == 0) {
+    const std::string path = icname.substr(5);
+    int32_t h[6];
+    if ((rc = evora_read_dump_header(path.c_str(), h))) return fail("IC dump", rc);
+    if (!((h[0] == EVORA_NQ || (chem && h[0] == EVORA_NQ_CHEM)) && h[1] == p.nx && h[2] == p.ny && h[3] == p.nz &&
+          h[4] == 1 && h[5] == p.nz)) {
+      std::fprintf(stderr, "ERROR IC dump %s: nn,nx,ny,nz,lz,mz = %d,%d,%d,%d,%d,%d do not fit the run\n",
+                   path.c_str(), h[0], h[1], h[2], h[3], h[4], h[5]);
+      return 1;
+    }
+    std::vector<double> qd((size_t)h[0] * p.nx * p.ny * p.nz);
+    if ((rc = evora_read_dump(path.c_str(), h, qd.data(), (int64_t)qd.size()))) return fail("IC dump", rc);
+    have_species = h[0] == EVORA_NQ_CHEM;
+    q.swap(qd);
+  } else {
     std::fprintf(stderr, "unknown IC %s\n", icname.c_str());
     return 2;
   }
   (void)fb;
-  const bool chem = p.chemistry != 0;
-  const int nq = chem ? EVORA_NQ_CHEM : EVORA_NQ;
-  if (chem) {
+  if (chem && !have_species) {
     // q(12): the IC's q(1:6), then initchem (main.f90:93-94) sets the
     // equilibrium species through the drop-in layer
     const size_t n = (size_t)p.nx * p.ny * p.nz;

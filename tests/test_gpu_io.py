@@ -197,3 +197,56 @@ def test_driver_comoving_chemistry_run(cuda_device, tmp_path):
     temp = press / cells[:, 6:12].sum(-1) * u.temp0
     np.testing.assert_allclose(rows[:, 2], temp, rtol=1e-5)
     np.testing.assert_allclose(rows[:, 1], cells[:, 0], rtol=1e-5)
+
+
+COSMO_PARA = ("$para\nnx = 32, ny = 32, nz = 32, boundtype = 2, solver = 2, limiter = 1\n"
+              "g = 1.6666666666666667, cfl = 0.5\nsupercomoving = .true., gravity = .true.\n"
+              "omega0 = 0.3, lambda0 = 0.7, hubble0 = 70.0, box = 20.0, fb = 0.17, c_cosmo = 0.01\n"
+              "zstart = 50.0, zend = 46.0\ndualenergy = .true., de_thresh = 1.0e-3\n"
+              "chemistry = .true., cooling = .true.\n/\n")
+COSMO_KW = dict(nx=32, ny=32, nz=32, boundtype=2, solver=2, limiter=1, g=5 / 3, cfl=0.5, supercomoving=1, gravity=1,
+                omega0=0.3, lambda0=0.7, hubble0=70.0, box=20.0, fb=0.17, c_cosmo=0.01, zstart=50.0, zend=46.0,
+                dualenergy=1, de_thresh=1e-3, chemistry=1, cooling=1)
+
+
+def test_driver_cosmological_box_from_a_dump(cuda_device, tmp_path):
+    """The cosmological box (Zel'dovich IC, comoving gravity, dual energy,
+    CIE chemistry with cooling) through evora_run with --ic dump:FILE, the
+    way ic/grafic.f90 takes an external initial state: the driver's initchem
+    and its whole run equal the same run through the grid API bit for bit."""
+    p = ev.default_params(**COSMO_KW)
+    q = ev.ic.cosmo_zeldovich(p, seed=5, slope=-2.0, sigma=0.05, temp_k=100.0)   # q(12), species by initchem
+    assert q.shape == (32, 32, 32, 12)
+    # the dump carries q(1:6): the driver's initchem sets the species
+    eio.write_dump(tmp_path / "zeldovich.000", q[..., :6])
+    para = tmp_path / "cosmo"
+    para.write_text("cosmological box\n" + COSMO_PARA)
+    r = eio.run(para, tmp_path, "--ic", "dump:" + str(tmp_path / "zeldovich.000"))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    h, q_in = eio.read_dump(tmp_path / "data" / "in.000")
+    assert h == (12, 32, 32, 32, 1, 32)
+    np.testing.assert_array_equal(q_in, q)
+    with ev.Grid(p, ev.FP64) as g:
+        g.set_q(q)
+        steps = 0
+        while g.time()["go"] and steps < 100000:
+            g.step(1)
+            steps += 1
+        assert g.status() == 0 and steps > 5
+        q_grid = g.get_q()
+        s, _ = g.cosmo()
+    h, q_out = eio.read_dump(tmp_path / "data" / "out.000")
+    assert h == (12, 32, 32, 32, 1, 32)
+    np.testing.assert_array_equal(q_out, q_grid)
+    assert s["redshift"] <= 46.0
+    # the cold gas stays neutral; n(H) follows the density the run changed
+    assert not np.array_equal(q_out[..., 6], q[..., 6])
+    np.testing.assert_allclose(q_out[..., 6] / q_out[..., 0], q[..., 6] / q[..., 0], rtol=1e-12)
+
+
+def test_driver_refuses_a_dump_of_another_grid(cuda_device, tmp_path):
+    eio.write_dump(tmp_path / "bad.000", np.ones((4, 4, 4, 6)))
+    para = tmp_path / "cosmo"
+    para.write_text("cosmological box\n" + COSMO_PARA)
+    r = eio.run(para, tmp_path, "--ic", "dump:" + str(tmp_path / "bad.000"))
+    assert r.returncode != 0 and "do not fit" in r.stderr
