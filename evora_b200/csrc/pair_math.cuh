@@ -108,7 +108,7 @@ __device__ __forceinline__ void prim_p(const P2<S>* q, P2<S>* w, const Gas<S>& c
     if (hx || hy) {
       auto rec = [&](S q0, S q1, S q2, S q3, S q4) -> S {
         const double dm2 = ((double)q1 * q1) + ((double)q2 * q2) + ((double)q3 * q3);
-        return (S)(P.g1 * ((double)q4 - 0.5 * dm2 / (double)q0));
+        return (S)(P.g1 * ((double)q4 - 0.5 * dm2 * rcp_fast((double)q0)));
       };
       if (hx) press.x = rec(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x);
       if (hy) press.y = rec(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y);
