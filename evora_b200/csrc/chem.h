@@ -16,9 +16,11 @@ int chem_step(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double
 
 // The same on a grid of the default mode: fewer FP64 operations per cooling
 // sub-cycle (shared powers of T, a table-driven exponential, contracted
-// products), within a few ulp of chem_step per rate (chem_fast.cu).
+// products), within a few ulp of chem_step per rate (chem_fast.cu).  With
+// expand, each cell then takes the expansion terms of a comoving run
+// (expansion(q), cosmology.f90:53-72) in the same pass.
 int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
-                   cudaStream_t st);
+                   cudaStream_t st, bool expand = false);
 
 // coolstep (timestep.f90:106-143) part 1 on the state at the start of a
 // step (nf fields, f32 or f64) and its species: the smallest cooling time

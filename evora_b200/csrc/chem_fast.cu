@@ -176,6 +176,30 @@ template <class Exp, class Coef>
 struct CieFast {
   Exp ex;
   Coef kc;
+  // pressure() (comp.f90:45-85) with the fast forms: kin/E as kin (1/E),
+  // rho^(g-1) = exp((g-1) ln rho), the divisions as products with
+  // reciprocals; the same write-back of E or S
+  __device__ __forceinline__ double pressure(double* q, const Gas<double>& c, bool de, unsigned& err) const {
+    const double m2 = (q[1] * q[1]) + (q[2] * q[2]) + (q[3] * q[3]);
+    const double kin = 0.5 * m2 * rcp64(q[0]);
+    double press;
+    if (de) {
+      const double pg = ex(c.g1 * log(q[0]));
+      if (kin * rcp64(q[4]) > c.de_thresh1) {
+        press = q[5] * pg;
+        q[4] = kin + press * c.g1inv;
+      } else {
+        press = c.g1 * (q[4] - kin);
+        q[5] = press * rcp64(pg);
+      }
+    } else {
+      press = c.g1 * (q[4] - kin);
+    }
+    if (press <= 0.0) err |= EVORA_ERR_PRESSURE;
+    return press;
+  }
+  __device__ __forceinline__ double div_pow(double a, double x, double y) const { return a * rcp64(ex(y * log(x))); }
+  __device__ __forceinline__ double div(double a, double, double binv) const { return a * binv; }
   __device__ __forceinline__ void run(const ChemParams& C, const ChemCoef& k, double temp0, double dt, double rho,
                                       double& press, double* n, unsigned& err) const {
     const double nH = C.chiH * rho, nHe = C.chiHe * rho;
@@ -222,7 +246,7 @@ struct CieFast {
 template <typename T, int MINB, bool kTable, bool kSmemCoef>
 __global__ void __launch_bounds__(kChemThreads, MINB)
 k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P, const GridCtl* ctl,
-            unsigned* err) {
+            unsigned* err, bool expand) {
   if (ctl_skip(ctl)) return;
   __shared__ double tab[32];
   __shared__ double coef[2 * kNcool];
@@ -236,7 +260,7 @@ k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, 
   Coef kc;
   if constexpr (kSmemCoef) kc.c = coef;
   else kc.k = &ctl->coef;
-  chem_soa(q, n, nf, species, P, ctl, CieFast<Exp, Coef>{ex, kc}, err);
+  chem_soa(q, n, nf, species, P, ctl, CieFast<Exp, Coef>{ex, kc}, err, expand);
 }
 
 // The self-test of the error bounds over x[0..n): out[i] = Tang's exp(x[i]),
@@ -260,15 +284,15 @@ __global__ void k_math_selftest(const double* __restrict__ x, double* __restrict
 }  // namespace
 
 int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, double* species, GridCtl* ctl,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool expand) {
   const int64_t want = (n + kChemThreads - 1) / kChemThreads, cap = (int64_t)148 * kChemMinBlocks * 4;
   const int blocks = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
   if (f32)
     k_chem_fast<float, kChemMinBlocks, true, true>
-        <<<blocks, kChemThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err);
+        <<<blocks, kChemThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err, expand);
   else
     k_chem_fast<double, kChemMinBlocks, true, true>
-        <<<blocks, kChemThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err);
+        <<<blocks, kChemThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err, expand);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_cuda_error(e, "chem");

@@ -272,6 +272,12 @@ bool fused_expansion(const evora_grid* g) {
   return g->expansion && g->gravity && !g->floors && !g->conduction && !reference_backend(g);
 }
 
+// The expansion terms ride in the default mode's chem(q) pass: chem and the
+// expansion are adjacent in main.f90 (167, 178) when there is no conduction.
+bool chem_expansion(const evora_grid* g) {
+  return g->expansion && g->floors && !g->conduction && !(g->flags & EVORA_STRICT) && !reference_backend(g);
+}
+
 void drop_graphs(evora_grid* g) {
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   g->graphs.clear();
@@ -350,8 +356,11 @@ int enqueue_fused_step(evora_grid* g) {
   }
   if (g->floors) {
     // chem(q): the CIE species and cooling, and the pressure floors (main.f90:167)
-    auto* step = (g->flags & EVORA_STRICT) ? chem_step : chem_step_fast;
-    int rc = step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl, st);
+    int rc = (g->flags & EVORA_STRICT)
+                 ? chem_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->species,
+                             g->ctl, st)
+                 : chem_step_fast(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g),
+                                  g->species, g->ctl, st, chem_expansion(g));
     if (rc) return rc;
     g->launches += 1;
   }
@@ -361,7 +370,7 @@ int enqueue_fused_step(evora_grid* g) {
     if (rc) return rc;
     g->launches += 2;
   }
-  if (g->expansion && !fused_expansion(g)) {
+  if (g->expansion && !fused_expansion(g) && !chem_expansion(g)) {
     // expansion terms of E and S (main.f90:178)
     int rc = expansion_step(g->P, g->qbuf[g->cur ^ 1], g->precision == EVORA_FP32, g->nf, ncells(g), g->ctl, st);
     if (rc) return rc;
@@ -708,7 +717,8 @@ int graph_steps(evora_grid* g, int nsteps) {
       g->cur = start ^ (nsteps & 1);
       const bool fused = g->plan.cfl_fused != 0;
       g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + grav_launches(g) + (g->conduction ? 2 : 0) +
-                                       (g->floors ? 1 : 0) + (g->expansion && !fused_expansion(g) ? 1 : 0)) +
+                                       (g->floors ? 1 : 0) +
+                                       (g->expansion && !fused_expansion(g) && !chem_expansion(g) ? 1 : 0)) +
                      (fused && !fresh ? 1 : 0);
       g->cfl_fresh = fused;
     }
