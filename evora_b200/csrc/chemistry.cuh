@@ -122,29 +122,34 @@ __host__ __device__ inline double compbackground(int background, int bg, double 
 // exp(c ln T) from one logarithm (ln(T 1e-3) = ln T + ln 1e-3, ...): the
 // sub-cycled cooling evaluates this ~10 times per cell and step, and a power
 // costs about a logarithm plus an exponential; the results stay within a
-// few ulp of the direct powers.
+// few ulp of the direct powers.  kRefPow: the reference's own powers
+// (pow(T, -1.5), pow(T 1e-3, -0.2), ...), for the post-processor's host
+// state vector, whose text output is compared digit for digit.
+template <bool kRefPow = false>
 __host__ __device__ inline void comprates(double temp, const ChemCoef& k, int background, int cooling,
                                           double* chemrate, double* coolrate) {
-  const double lt = std::log(temp);
+  const double lt = kRefPow ? 0.0 : std::log(temp);
   const double temproot = std::sqrt(temp);
   const double tempinv = 1.0 / temp;
-  const double temp15 = std::exp(-1.5 * lt);
+  const double temp15 = kRefPow ? std::pow(temp, -1.5) : std::exp(-1.5 * lt);
   const double fec = 1.0 / (1.0 + std::sqrt(temp * 1e-5));
   const double fc1 = temproot * fec;
   const double e1 = std::exp(-((double)157809.1f * tempinv));
   const double e2 = std::exp(-((double)286335.4f * tempinv));
   const double e3 = std::exp(-((double)631515.0f * tempinv));
   const double ln1e3 = -6.907755278982137, ln1e6 = -13.815510557964274;   // ln 1e-3, ln 1e-6
-  const double fr = std::exp((double)(-0.2f) * (lt + ln1e3)) / (1.0 + std::exp((double)0.7f * (lt + ln1e6)));
+  const double fr = kRefPow ? std::pow(temp * 1e-3, (double)(-0.2f)) / (1.0 + std::pow(temp * 1e-6, (double)0.7f))
+                            : std::exp((double)(-0.2f) * (lt + ln1e3)) / (1.0 + std::exp((double)0.7f * (lt + ln1e6)));
   const double fr1 = fr / temproot;
   const double fr2 = fr * temproot;
   const float c3 = 0.3f * (-94000.0f);   // a product of two default reals
   const double edr = std::exp((double)(-470000.0f) * tempinv) * (1.0 + (double)c3 * tempinv);
+  const double p6353 = kRefPow ? std::pow(temp, (double)(-0.6353f)) : std::exp((double)(-0.6353f) * lt);
   chemrate[0] = k.c[0][0] * fc1 * e1;
   chemrate[1] = k.c[1][0] * fc1 * e2;
   chemrate[2] = k.c[2][0] * fc1 * e3;
   chemrate[3] = k.c[3][0] * fr1;
-  chemrate[4] = k.c[4][0] * std::exp((double)(-0.6353f) * lt) + k.c[6][0] * temp15 * edr;
+  chemrate[4] = k.c[4][0] * p6353 + k.c[6][0] * temp15 * edr;
   chemrate[5] = k.c[5][0] * fr1;
   if (background) {
     chemrate[6] = k.c[10][0];
@@ -154,15 +159,17 @@ __host__ __device__ inline void comprates(double temp, const ChemCoef& k, int ba
     chemrate[6] = chemrate[7] = chemrate[8] = 0.0;
   }
   if (cooling) {
+    const double p3647 = kRefPow ? std::pow(temp, (double)0.3647f) : std::exp((double)0.3647f * lt);
+    const double p397 = kRefPow ? std::pow(temp, (double)(-0.397f)) : std::exp((double)(-0.397f) * lt);
     coolrate[0] = k.c[0][1] * fc1 * e1;
     coolrate[1] = k.c[1][1] * fc1 * e2;
     coolrate[2] = k.c[2][1] * fc1 * e3;
     coolrate[3] = k.c[3][1] * fr2;
-    coolrate[4] = k.c[4][1] * std::exp((double)0.3647f * lt);
+    coolrate[4] = k.c[4][1] * p3647;
     coolrate[5] = k.c[5][1] * fr2;
     coolrate[6] = k.c[6][1] * temp15 * edr;
     coolrate[7] = k.c[7][1] * fec * std::exp((double)(-118348.0f) * tempinv);
-    coolrate[8] = k.c[8][1] * std::exp((double)(-0.397f) * lt) * fec * std::exp((double)(-473638.0f) * tempinv);
+    coolrate[8] = k.c[8][1] * p397 * fec * std::exp((double)(-473638.0f) * tempinv);
     coolrate[9] = k.c[9][1] * temproot;
     if (background) {
       coolrate[10] = k.c[10][1];

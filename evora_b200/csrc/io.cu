@@ -13,6 +13,7 @@
 
 #include "../../include/evora_gpu.h"
 #include "../../include/evora_io.h"
+#include "chemistry.cuh"
 #include "common.h"
 #include "cosmology.cuh"
 #include "fortran_fmt.h"
@@ -274,19 +275,60 @@ int bov_data(const evora_params* p, const std::string& name, const float* dens, 
 }
 
 // ------------------------------------------------------------------ post --
-// compstate(q, state), comp.f90:201-239, hydro build (nstate = 12).
-void compstate(double* q, const HostGas& c, double fb, const evora_units* u, double* state, unsigned* err) {
+// The chemistry the post-processor's state vector needs (post.f90:58-62):
+// chiH, chiHe, and compbackground + compcoef from the dump's unit file.
+struct PostChem {
+  bool on = false, cooling = false;
+  int background = 0;
+  double chiH = 0.0, chiHe = 0.0;
+  evora::ChemCoef k{};
+};
+
+PostChem post_chem(const evora_params* p, const evora_units* u) {
+  PostChem pc;
+  if (!p->chemistry) return pc;
+  pc.on = true;
+  pc.cooling = p->cooling != 0;
+  pc.background = p->background;
+  pc.chiH = p->rhoh / evora::kMH;
+  pc.chiHe = p->rhohe / evora::kMHe;
+  const double uv = evora::compbackground(p->background, p->bg, p->j0, u->redshift, u->cosmo, 0.0);
+  evora::compcoef(evora::ChemUnits{u->chem0, u->photo0, u->cool0, u->heat0}, uv, pc.k);
+  return pc;
+}
+
+// compstate(q, state), comp.f90:201-239: the hydro build's 12 values; with
+// chemistry (nstate = 26) also the species per density q(7:12)/rho, the
+// number densities q(7:12) number0 and, with cooling, Lambda and Gamma of
+// cool at the cell's T after cieabundance has put the cell's species in
+// equilibrium in q itself, as the reference's call does (its state(25:26)
+// are unset without cooling; here 0).
+void compstate(double* q, const HostGas& c, double fb, const evora_units* u, const PostChem& pc, double* state,
+               unsigned* err) {
   const double press = host_pressure(q, c, err);
-  const double temp = press2temp(press, q[0], u->temp0);
+  const double temp = cell_temp(press, q, pc.on, u->temp0);
   state[0] = q[0] / fb;
   for (int i = 1; i < 6; ++i) state[i] = q[i];
   state[6] = state[0] * u->density0;
   for (int i = 0; i < 3; ++i) state[7 + i] = q[1 + i] / state[0] * u->velocity0;
   state[10] = press * u->press0;
   state[11] = temp;
+  if (!pc.on) return;
+  for (int i = 6; i < 12; ++i) {
+    state[i + 6] = q[i] / state[0];
+    state[i + 12] = q[i] * u->number0;
+  }
+  state[24] = state[25] = 0.0;
+  if (pc.cooling) {
+    const double nH = pc.chiH * q[0], nHe = pc.chiHe * q[0];
+    double chemrate[evora::kNchem], coolrate[evora::kNcool];
+    evora::comprates<true>(temp, pc.k, pc.background, 1, chemrate, coolrate);
+    evora::cieabundance(nH, nHe, q + 6, chemrate, pc.background, pc.k.uv, *err);
+    evora::cool(q + 6, coolrate, pc.background, state[24], state[25]);
+  }
 }
 
-constexpr int kNstate = 12;
+constexpr int kNstate = 12, kNstateChem = 26;
 
 const char* const kStateNames[] = {"rho",     "rho u",   "rho v",   "rho w",    "E",      "S",     "rho_phys",
                                    "u",       "v",       "w",       "p",        "T",      "xi_HI", "xi_HII",
@@ -545,12 +587,15 @@ int evora_cuts_and_slices(const evora_params* p, double fb, const evora_units* u
   int rc = geometry(p, &G);
   if (rc) return rc;
   const HostGas c = host_gas(p, G);
+  const PostChem pc = post_chem(p, u);
+  const int nq = pc.on ? EVORA_NQ_CHEM : EVORA_NQ;
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   const double xmid = std::max(nx / 2, 1), ymid = std::max(ny / 2, 1), zmid = std::max(nz / 2, 1);
   const bool one = G.d.onedimension, two = G.d.twodimension;
   const bool cut_x = true, cut_y = !one, slice_xy = !one, cut_xy = !one && nx == ny;
   const bool cut_z = !one && !two, slice_xz = cut_z, slice_yz = cut_z, cut_xyz = cut_z && nx == ny && ny == nz;
-  const int nv = kNstate + 1, ns = kNstate + 2;
+  const int nstate = pc.on ? kNstateChem : kNstate;
+  const int nv = nstate + 1, ns = nstate + 2;
   std::vector<double> cx, cy, cz, cxy, cxyz, sxy, sxz, syz;
   // coordinates (post.f90:124-170): k - 0.5 in default real, sqrt(2.0) and
   // sqrt(3.0) of default reals
@@ -597,18 +642,18 @@ int evora_cuts_and_slices(const evora_params* p, double fb, const evora_units* u
     const std::string path = dir_join(datadir, std::string(infile) + "." + ft::I0(j, 3));
     int32_t h[6];
     if ((rc = evora_read_dump_header(path.c_str(), h))) return rc;
-    if (h[0] != EVORA_NQ || h[1] != nx || h[2] != ny || h[3] != nz || h[4] < 1 || h[5] < h[4] || h[5] > nz)
+    if (h[0] != nq || h[1] != nx || h[2] != ny || h[3] != nz || h[4] < 1 || h[5] < h[4] || h[5] > nz)
       return EVORA_ERR_ARG;
-    q.resize((size_t)EVORA_NQ * nx * ny * (h[5] - h[4] + 1));
+    q.resize((size_t)nq * nx * ny * (h[5] - h[4] + 1));
     if ((rc = evora_read_dump(path.c_str(), h, q.data(), (int64_t)q.size()))) return rc;
     const int lz = h[4];
     mz = h[5];
     for (int iz = lz; iz <= mz; ++iz)
       for (int iy = 1; iy <= ny; ++iy)
         for (int ix = 1; ix <= nx; ++ix) {
-          double* cell = &q[(size_t)EVORA_NQ * ((ix - 1) + (size_t)nx * ((iy - 1) + (size_t)ny * (iz - lz)))];
+          double* cell = &q[(size_t)nq * ((ix - 1) + (size_t)nx * ((iy - 1) + (size_t)ny * (iz - lz)))];
           auto st = [&](std::vector<double>& a, size_t idx, int off) {
-            compstate(cell, c, fb, u, &a[idx + off], &err);
+            compstate(cell, c, fb, u, pc, &a[idx + off], &err);
           };
           if (cut_x && iy == ymid && iz == zmid) st(cx, (size_t)nv * (ix - 1), 1);
           if (cut_y && ix == xmid && iz == zmid) st(cy, (size_t)nv * (iy - 1), 1);

@@ -103,12 +103,18 @@ int evora_grid_set_plane(evora_grid* g, int32_t axis, int32_t index, const doubl
 /* ---------------------------------------------------------- post-process -- */
 /* `post cs <infile>` (post.f90:85-246): reads <datadir>/<infile>.000,
  * .001, ... (the ranks' z slabs, until one ends at nz), computes the state
- * vector of comp.f90:201-239 (hydro build: 12 values) on the middle lines
- * and planes and writes <outdir>/<infile>.{x,y,z,xy,xyz}.cut and
- * .{xy,xz,yz}.slice as the reference does (including its writing of the
- * diagonal cut's data into the .xyz file, post.f90:228).  p gives the grid
- * and gas of the run (the reference rereads them from data/parameter), fb
- * the baryon fraction, u the unit scales of the dump (data/<infile>.units). */
+ * vector of comp.f90:201-239 on the middle lines and planes and writes
+ * <outdir>/<infile>.{x,y,z,xy,xyz}.cut and .{xy,xz,yz}.slice as the
+ * reference does (including its writing of the diagonal cut's data into the
+ * .xyz file, post.f90:228).  Hydro build: q(6) dumps, 12 values per cell.
+ * With chemistry (the CIE build): q(12) dumps, 26 values: also the species
+ * per density and the number densities and, with cooling, Lambda and Gamma
+ * from the rates at the cell's T (rates.f90's own powers), with the
+ * coefficients of compbackground and compcoef at the units of the dump
+ * (post.f90:58-62); cieabundance leaves the cell's species in equilibrium,
+ * as in the reference.  p gives the grid and gas of the run (the reference
+ * rereads them from data/parameter), fb the baryon fraction, u the unit
+ * scales of the dump (data/<infile>.units). */
 int evora_cuts_and_slices(const evora_params* p, double fb, const evora_units* u, const char* datadir,
                           const char* infile, const char* outdir);
 

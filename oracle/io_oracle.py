@@ -314,18 +314,193 @@ STATE_NAMES = ["rho", "rho u", "rho v", "rho w", "E", "S", "rho_phys", "u", "v",
                "n_HeIII", "n_e", "lambda", "gamma"]
 
 
-def compstate(qq: np.ndarray, c: Gas, fb: float, u: dict) -> list:
+# -------------------------------------- post: the chemistry's state vector
+# The CIE build's rates as post-processing evaluates them (rates.f90:26-189,
+# cie.f90:58-217, chemistry.f90:123-176), restated from the reference with
+# its own powers; default-real literals are single precision.
+NFLOOR, RATEFLOOR, CIE_TOL, CIE_NIT = 1.0e-40, 1.0e-40, 1e-10, 1000
+M_H, M_HE = f32(1.00794), f32(4.002602)
+
+
+def compbackground(background, bg, j0, z, cosmo, uv=0.0):
+    if not background:
+        return uv
+    if bg == 1:
+        return j0
+    if bg == 2:
+        if 3 < z < 6:
+            return j0 * 4.0 * cosmo
+        return j0 if 1 < z <= 3 else 0.0
+    if bg == 3:
+        if z > 8.0:
+            return 1e-5 * j0
+        if 6.0 < z <= 8.0:
+            return 0.5 * j0 * 10.0 ** ((-z + 6.0) * f32(0.35))
+        if 3.0 < z <= 6.0:
+            return j0 * 10.0 ** ((-z + 3.0) * f32(0.1))
+        if 1.0 < z <= 3.0:
+            return j0
+        return j0 * f32(0.1) * 10.0 ** z
+    return uv
+
+
+def compcoef(u: dict, uv: float):
+    """coef(13, 2) of rates.f90:26-78 from the unit file's chem0, photo0,
+    cool0, heat0."""
+    k = [[0.0, 0.0] for _ in range(13)]
+    c0, p0, k0, h0 = u["chem0"], u["photo0"], u["cool0"], u["heat0"]
+    k[0] = [c0 * 5.85e-11, k0 * 1.27e-21]
+    k[1] = [c0 * 2.38e-11, k0 * 9.38e-22]
+    k[2] = [c0 * 5.68e-12, k0 * 4.95e-22]
+    k[3] = [c0 * 8.4e-11, k0 * 8.7e-27]
+    k[4] = [c0 * 1.5e-10, k0 * 1.55e-26]
+    k[5] = [c0 * 3.36e-10, k0 * 3.48e-26]
+    k[6] = [c0 * 1.9e-3, k0 * 1.24e-13]
+    k[7] = [0.0, k0 * 7.5e-19]
+    k[8] = [0.0, k0 * 5.54e-17]
+    k[9] = [0.0, k0 * 1.42e-27 * 1.5]
+    k[10] = [p0 * 2.54e8 * uv, h0 * 2.54e8 * 7.75e-12 * uv]
+    k[11] = [p0 * 2.49e8 * uv, h0 * 2.49e8 * 2.19e-11 * uv]
+    k[12] = [p0 * 1.60e7 * uv, h0 * 1.60e7 * 3.10e-11 * uv]
+    return k
+
+
+def comprates(temp, k, background, cooling):
+    """rates.f90:80-158: chemical rates r[9], cooling rates cr[13]."""
+    troot, tinv, t15 = math.sqrt(temp), 1.0 / temp, temp ** -1.5
+    fec = 1.0 / (1.0 + math.sqrt(temp * 1e-5))
+    fc1 = troot * fec
+    e1 = math.exp(-(f32(157809.1) * tinv))
+    e2 = math.exp(-(f32(286335.4) * tinv))
+    e3 = math.exp(-(f32(631515.0) * tinv))
+    fr = (temp * 1e-3) ** f32(-0.2) / (1.0 + (temp * 1e-6) ** f32(0.7))
+    fr1, fr2 = fr / troot, fr * troot
+    c3 = f32(f32(0.3) * f32(-94000.0))
+    edr = math.exp(f32(-470000.0) * tinv) * (1.0 + c3 * tinv)
+    r = [k[0][0] * fc1 * e1, k[1][0] * fc1 * e2, k[2][0] * fc1 * e3, k[3][0] * fr1,
+         k[4][0] * temp ** f32(-0.6353) + k[6][0] * t15 * edr, k[5][0] * fr1]
+    r += [k[10][0], k[11][0], k[12][0]] if background else [0.0, 0.0, 0.0]
+    cr = None
+    if cooling:
+        cr = [k[0][1] * fc1 * e1, k[1][1] * fc1 * e2, k[2][1] * fc1 * e3, k[3][1] * fr2,
+              k[4][1] * temp ** f32(0.3647), k[5][1] * fr2, k[6][1] * t15 * edr,
+              k[7][1] * fec * math.exp(f32(-118348.0) * tinv),
+              k[8][1] * temp ** f32(-0.397) * fec * math.exp(f32(-473638.0) * tinv), k[9][1] * troot]
+        cr += [k[10][1], k[11][1], k[12][1]] if background else [0.0, 0.0, 0.0]
+    return r, cr
+
+
+def _cieions(nH, nHe, ne, r):
+    ion1, ion2, ion3 = r[0] * ne + r[6], r[1] * ne + r[7], r[2] * ne + r[8]
+    nHII = NFLOOR if ion1 < RATEFLOOR else nH / (1.0 + r[3] * ne / ion1)
+    if ion2 < RATEFLOOR:
+        return nHII, NFLOOR, NFLOOR
+    xi2 = r[4] * ne / ion2
+    if ion3 < RATEFLOOR:
+        return nHII, nHe / (1.0 + xi2), NFLOOR
+    xi3 = r[5] * ne / ion3
+    return nHII, nHe / (1.0 + xi2 + 1.0 / xi3), nHe / (1.0 + (xi2 + 1.0) * xi3)
+
+
+def _fne(nH, nHe, ne, r):
+    a, b, c = _cieions(nH, nHe, ne, r)
+    return a + b + 2 * c - ne
+
+
+def _rf_cie(nH, nHe, l, rr, r):
+    fl, fr, m = _fne(nH, nHe, l, r), _fne(nH, nHe, rr, r), 0.0
+    if fl * fr > 0.0:
+        raise ValueError("rf_cie: no root")
+    s = 0
+    for _ in range(CIE_NIT):
+        m = (fr * l - fl * rr) / (fr - fl)
+        if abs(rr - l) < CIE_TOL * abs(rr + l):
+            break
+        fm = _fne(nH, nHe, m, r)
+        if fm * fr > 0.0:
+            rr, fr = m, fm
+            if s == -1:
+                fl = fl * 0.5
+            s = -1
+        elif fl * fm > 0.0:
+            l, fl = m, fm
+            if s == 1:
+                fr = fr * 0.5
+            s = 1
+        else:
+            break
+    return m
+
+
+def cieabundance(nH, nHe, n, r, background, uv):
+    """cie.f90:58-112 with ncheck (chemistry.f90:159-176), n in place."""
+    if background and uv > 0.0:
+        ne = _rf_cie(nH, nHe, NFLOOR, nH + 2 * nHe, r)
+        a, b, c = _cieions(nH, nHe, ne, r)
+        n[:] = [nH - a, a, nHe - b - c, b, c, ne]
+        n[:] = [NFLOOR if NFLOOR > v else v for v in n]
+    else:
+        fH, fHe1, fHe2 = r[0] / r[3], r[1] / r[4], r[2] / r[5]
+        n0 = nH / (1.0 + fH)
+        n2 = nHe / (1.0 + fHe1 * (1.0 + fHe2))
+        n3 = n2 * fHe1
+        n4 = n3 * fHe2
+        n1 = n0 * fH
+        n[:] = [n0, n1, n2, n3, n4, n1 + n3 + 2 * n4]
+    for v in n[:5]:
+        if not (0.0 <= v <= 1e20):
+            raise ValueError("ncheck: abundance out of range")
+    n[:] = [NFLOOR if NFLOOR > v else v for v in n]
+
+
+def cool(n, cr, background):
+    """rates.f90:160-189: (Lambda, Gamma)."""
+    lam = (cr[0] * n[0] + cr[1] * n[2] + cr[2] * n[3] + cr[3] * n[1] + cr[4] * n[3] + cr[5] * n[4]
+           + cr[6] * n[3] + cr[7] * n[0] + cr[8] * n[3] + cr[9] * (n[1] + n[3] + 4.0 * n[4]))
+    gam = n[0] * cr[10] + n[2] * cr[11] + n[3] * cr[12] if background else 0.0
+    return lam * n[5], gam
+
+
+def post_chem(u: dict, cooling=True, background=0, bg=0, j0=1e-21, rhoh=None, rhohe=None) -> dict:
+    """post.f90:58-62: chiH, chiHe, compbackground and compcoef at the dump's
+    units."""
+    rhoh = f32(0.76) if rhoh is None else rhoh
+    rhohe = f32(0.24) if rhohe is None else rhohe
+    uv = compbackground(background, bg, j0, u["redshift"], u["cosmo"], 0.0)
+    return dict(cooling=cooling, background=background, chiH=rhoh / M_H, chiHe=rhohe / M_HE, k=compcoef(u, uv),
+                uv=uv)
+
+
+def compstate(qq: np.ndarray, c: Gas, fb: float, u: dict, chem: dict | None = None) -> list:
+    """comp.f90:201-239; with chem (the CIE build, qq of 12 values) the 26
+    entries, cieabundance leaving qq's species in equilibrium."""
     press = pressure(qq, c)
-    temp = press / qq[0] * u["temp0"]
+    if chem is None:
+        temp = press / qq[0] * u["temp0"]
+    else:
+        ns = qq[6] + qq[7] + qq[8] + qq[9] + qq[10] + qq[11]
+        temp = press / ns * u["temp0"]
     s1 = qq[0] / fb
     st = [s1] + [float(v) for v in qq[1:6]] + [s1 * u["density0"]]
     st += [qq[i] / s1 * u["velocity0"] for i in (1, 2, 3)]
     st += [press * u["press0"], temp]
-    return st
+    if chem is None:
+        return st
+    st += [qq[i] / s1 for i in range(6, 12)] + [qq[i] * u["number0"] for i in range(6, 12)]
+    lam = gam = 0.0
+    if chem["cooling"]:
+        nH, nHe = chem["chiH"] * qq[0], chem["chiHe"] * qq[0]
+        r, cr = comprates(temp, chem["k"], chem["background"], True)
+        n = [float(v) for v in qq[6:12]]
+        cieabundance(nH, nHe, n, r, chem["background"], chem["uv"])
+        qq[6:12] = n
+        lam, gam = cool(n, cr, chem["background"])
+    return st + [lam, gam]
 
 
-def cuts_and_slices_files(geo: Geometry, c: Gas, fb: float, u: dict, slabs, infile: str) -> dict:
-    """post cs: slabs = [(lz, q slab of C shape (mz-lz+1, ny, nx, 6)), ...]."""
+def cuts_and_slices_files(geo: Geometry, c: Gas, fb: float, u: dict, slabs, infile: str, chem=None) -> dict:
+    """post cs: slabs = [(lz, q slab of C shape (mz-lz+1, ny, nx, nq)), ...];
+    chem (post_chem) for the CIE build's q(12)."""
     nx, ny, nz = geo.nx, geo.ny, geo.nz
     xm, ym, zm = max(nx // 2, 1), max(ny // 2, 1), max(nz // 2, 1)
     one, two = geo.one, geo.two
@@ -351,21 +526,21 @@ def cuts_and_slices_files(geo: Geometry, c: Gas, fb: float, u: dict, slabs, infi
                 for ix in range(1, nx + 1):
                     qq = q[iz - lz, iy - 1, ix - 1]
                     if iy == ym and iz == zm:
-                        cx[ix - 1][1:] = compstate(qq, c, fb, u)
+                        cx[ix - 1][1:] = compstate(qq, c, fb, u, chem)
                     if cut_y and ix == xm and iz == zm:
-                        cy[iy - 1][1:] = compstate(qq, c, fb, u)
+                        cy[iy - 1][1:] = compstate(qq, c, fb, u, chem)
                     if cut_z and ix == xm and iy == ym:
-                        cz[iz - 1][1:] = compstate(qq, c, fb, u)
+                        cz[iz - 1][1:] = compstate(qq, c, fb, u, chem)
                     if cut_xy and iz == zm and ix == iy:
-                        cxy[ix - 1][1:] = compstate(qq, c, fb, u)
+                        cxy[ix - 1][1:] = compstate(qq, c, fb, u, chem)
                     if cut_xyz and ix == iy == iz:
-                        compstate(qq, c, fb, u)      # computed, then never written (post.f90:228)
+                        compstate(qq, c, fb, u, chem)      # computed, then never written (post.f90:228)
                     if slice_xy and iz == zm:
-                        sxy[(ix, iy)][2:] = compstate(qq, c, fb, u)
+                        sxy[(ix, iy)][2:] = compstate(qq, c, fb, u, chem)
                     if slice_xz and iy == ym:
-                        sxz[(ix, iz)][2:] = compstate(qq, c, fb, u)
+                        sxz[(ix, iz)][2:] = compstate(qq, c, fb, u, chem)
                     if slice_yz and ix == xm:
-                        syz[(iy, iz)][2:] = compstate(qq, c, fb, u)
+                        syz[(iy, iz)][2:] = compstate(qq, c, fb, u, chem)
     files = {}
     head_cut = "#" + "x".rjust(15) + "".join(h.rjust(16) for h in STATE_NAMES) + "\n"
     head_slice = "#" + "x".rjust(15) + "y".rjust(16) + "".join(h.rjust(16) for h in STATE_NAMES) + "\n"

@@ -197,6 +197,15 @@ def test_driver_comoving_chemistry_run(cuda_device, tmp_path):
     temp = press / cells[:, 6:12].sum(-1) * u.temp0
     np.testing.assert_allclose(rows[:, 2], temp, rtol=1e-5)
     np.testing.assert_allclose(rows[:, 1], cells[:, 0], rtol=1e-5)
+    # post cs on the q(12) dump: the 26-entry state vector per cell
+    r = eio.post("cs", "out", tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    cut = np.loadtxt(tmp_path / "out" / "out.x.cut")
+    assert cut.shape == (256, 27)
+    # (n number0) / (n / rho) / rho = number0 in every cell and species
+    ratio = cut[:, 19:25] / cut[:, 13:19] / cut[:, 1:2]
+    np.testing.assert_allclose(ratio, ratio[0, 0], rtol=1e-5)
+    assert np.all(cut[:, 25] > 0.0)   # Lambda of the cooling gas
 
 
 COSMO_PARA = ("$para\nnx = 32, ny = 32, nz = 32, boundtype = 2, solver = 2, limiter = 1\n"

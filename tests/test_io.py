@@ -211,6 +211,50 @@ def test_cuts_and_slices_match_restatement(tmp_path, case, slabs, dualenergy):
         assert (out / name).read_bytes() == blob, name
 
 
+@pytest.mark.parametrize("background", [0, 1], ids=["collisional", "uv-background"])
+def test_cuts_and_slices_with_chemistry_match_restatement(tmp_path, background):
+    """post cs on the CIE build's q(12) dumps: the 26-entry state vector
+    (species per density, number densities, Lambda and Gamma after
+    cieabundance at each cell's T, with a UV background through the
+    electron-density root) byte for byte against the restatement."""
+    import ctypes
+    from evora_b200 import _native
+    g = 5.0 / 3.0
+    kw = dict(nx=8, ny=6, nz=4, supercomoving=1, omega0=0.3, lambda0=0.7, hubble0=70.0, box=1.0, zstart=10.0,
+              chemistry=1, cooling=1, background=background, bg=3, j0=1e-21, g=g)
+    p = ev.default_params(**kw)
+    u = _native.EvoraUnits()
+    assert _native.lib().evora_compunits(ctypes.byref(p), None, ctypes.byref(u)) == 0
+    ud = {n: getattr(u, n) for n in orc.UNIT_NAMES}
+    rng = np.random.default_rng(8)
+    sh = (p.nz, p.ny, p.nx)
+    rho = rng.uniform(0.5, 2.0, sh)
+    vel = rng.uniform(-0.3, 0.3, sh + (3,))
+    n = rng.uniform(0.05, 1.0, sh + (6,)) * rho[..., None]
+    temp = 10.0 ** rng.uniform(3.7, 6.0, sh)
+    press = temp * n.sum(-1) / ud["temp0"]
+    q = np.empty(sh + (12,))
+    q[..., 0] = rho
+    q[..., 1:4] = rho[..., None] * vel
+    q[..., 4] = 0.5 * rho * (vel ** 2).sum(-1) + press / (g - 1)
+    q[..., 5] = press / rho ** (g - 1)
+    q[..., 6:] = n
+    data, out = tmp_path / "data", tmp_path / "out"
+    data.mkdir()
+    out.mkdir()
+    eio.write_dump(data / "out.000", q)
+    eio.cuts_and_slices(p, 1.0, u, data, "out", out)
+    geo = orc.Geometry(p.nx, p.ny, p.nz, p.xmin, p.xmax, p.ymin, p.ymax, p.zmin, p.zmax)
+    chem = orc.post_chem(ud, cooling=True, background=background, bg=3, j0=1e-21, rhoh=p.rhoh, rhohe=p.rhohe)
+    assert background == 0 or chem["uv"] > 0.0
+    files = orc.cuts_and_slices_files(geo, orc.Gas(g), 1.0, ud, [(1, q)], "out", chem=chem)
+    assert sorted(os.listdir(out)) == sorted(files)
+    for name, blob in files.items():
+        assert (out / name).read_bytes() == blob, name
+    row = (out / "out.x.cut").read_text().splitlines()[1].split()
+    assert len(row) == 27 and float(row[-2]) > 0.0   # x + 26 entries; Lambda of a cooling gas
+
+
 def test_cuts_and_slices_checks_dimensions(tmp_path):
     p = ev.default_params(nx=8, ny=1, nz=1)
     (tmp_path / "data").mkdir()
