@@ -118,6 +118,9 @@ __device__ __forceinline__ void pair_tile(const FusedArgs<S>& A, const TmaMap& m
   const Gas<S> c = Gas<S>::make(P);
   unsigned err = 0;
   const int64_t own = (int64_t)(Y0 + j) * nx + (X0 + p);
+  // tiles whose x/y halo lies inside the grid read every halo cell from the
+  // staged plane: no ghost map, no reflection (a block-uniform branch)
+  const bool edge = !(X0 >= 2 && X0 + TX + 2 <= nx && Y0 >= 2 && Y0 + TY + 2 <= ny);
 
   if (ctl_skip(A.ctl)) {
     for (int z = Z0; z < Z0 + ze; ++z) {
@@ -201,18 +204,26 @@ __device__ __forceinline__ void pair_tile(const FusedArgs<S>& A, const TmaMap& m
     for (int h = 0; h < HPT; ++h) {
       if (!h_on[h]) continue;
       V qv[5], wv[5];
+      if (edge) {
 #pragma unroll
-      for (int f = 0; f < 5; ++f) {
-        qv[f].x = h_g[h][0] >= 0 ? ld(plane + f * n + h_g[h][0]) : st[f * SPL + h_r[h][0]];
-        qv[f].y = h_g[h][1] >= 0 ? ld(plane + f * n + h_g[h][1]) : st[f * SPL + h_r[h][1]];
+        for (int f = 0; f < 5; ++f) {
+          qv[f].x = h_g[h][0] >= 0 ? ld(plane + f * n + h_g[h][0]) : st[f * SPL + h_r[h][0]];
+          qv[f].y = h_g[h][1] >= 0 ? ld(plane + f * n + h_g[h][1]) : st[f * SPL + h_r[h][1]];
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+          qv[f].x = st[f * SPL + h_r[h][0]];
+          qv[f].y = st[f * SPL + h_r[h][1]];
+        }
       }
       prim_p(qv, wv, c, P, err);
-      if (h_flip[h][0]) {
+      if (edge && h_flip[h][0]) {
         wv[1].x = -wv[1].x;
         wv[2].x = -wv[2].x;
         wv[3].x = -wv[3].x;
       }
-      if (h_flip[h][1]) {
+      if (edge && h_flip[h][1]) {
         wv[1].y = -wv[1].y;
         wv[2].y = -wv[2].y;
         wv[3].y = -wv[3].y;
