@@ -26,7 +26,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <type_traits>
 
 #include "../../include/evora_gpu.h"
 #include "chem.h"
@@ -60,11 +59,6 @@ __device__ __forceinline__ double rcp64(double x) {
   return e == e ? r : r0;
 }
 
-// The math library's exp.
-struct ExpLib {
-  __device__ __forceinline__ double operator()(double x) const { return exp(x); }
-};
-
 // The rate coefficients staged in shared memory (c[i][j] at 2 i + j), read
 // where they are used: a volatile load is not hoisted out of the sub-cycle
 // loop, so the 26 coefficients hold no registers across it.
@@ -75,12 +69,6 @@ struct CoefShared {
     asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(c + 2 * i + j)));
     return v;
   }
-};
-
-// The rate coefficients read from the step's ChemCoef.
-struct CoefRef {
-  const ChemCoef* k;
-  __device__ __forceinline__ double operator()(int i, int j) const { return k->c[i][j]; }
 };
 
 // comprates (rates.f90:80-158) at temperature temp (tempinv = 1/temp) with
@@ -238,12 +226,13 @@ struct CieFast {
   }
 };
 
-// chem(q) on the resident SoA state.  kTable: Tang's exponential (its table
-// staged in shared memory), else the math library's; kSmemCoef: the rate
-// coefficients read from shared memory where they are used (both measured
-// faster in the 256^3 cosmological box: with the library's exp the kernel
-// ran about 14 % slower, with the coefficients in registers about 5 %).
-template <typename T, int MINB, bool kTable, bool kSmemCoef>
+// chem(q) on the resident SoA state, with Tang's exponential (its table
+// staged in shared memory) and the rate coefficients read from shared
+// memory where they are used.  Both measured faster in the 256^3
+// cosmological box: with the library's exp the kernel ran about 14 % slower,
+// with the coefficients in registers about 5 %.  expand: the expansion
+// terms in the same pass.
+template <typename T, int MINB>
 __global__ void __launch_bounds__(kChemThreads, MINB)
 k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, HydroParams P, const GridCtl* ctl,
             unsigned* err, bool expand) {
@@ -253,14 +242,7 @@ k_chem_fast(T* __restrict__ q, int64_t n, int nf, double* __restrict__ species, 
   if (threadIdx.x < 32) tab[threadIdx.x] = kExp2Frac[threadIdx.x];
   if (threadIdx.x < 2 * kNcool) coef[threadIdx.x] = ctl->coef.c[threadIdx.x >> 1][threadIdx.x & 1];
   __syncthreads();
-  using Exp = typename std::conditional<kTable, ExpTable, ExpLib>::type;
-  using Coef = typename std::conditional<kSmemCoef, CoefShared, CoefRef>::type;
-  Exp ex;
-  if constexpr (kTable) ex.tab = tab;
-  Coef kc;
-  if constexpr (kSmemCoef) kc.c = coef;
-  else kc.k = &ctl->coef;
-  chem_soa(q, n, nf, species, P, ctl, CieFast<Exp, Coef>{ex, kc}, err, expand);
+  chem_soa(q, n, nf, species, P, ctl, CieFast<ExpTable, CoefShared>{ExpTable{tab}, CoefShared{coef}}, err, expand);
 }
 
 // The self-test of the error bounds over x[0..n): out[i] = Tang's exp(x[i]),
@@ -288,10 +270,10 @@ int chem_step_fast(const HydroParams& P, void* q, bool f32, int nf, int64_t n, d
   const int64_t want = (n + kChemThreads - 1) / kChemThreads, cap = (int64_t)148 * kChemMinBlocks * 4;
   const int blocks = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
   if (f32)
-    k_chem_fast<float, kChemMinBlocks, true, true>
+    k_chem_fast<float, kChemMinBlocks>
         <<<blocks, kChemThreads, 0, st>>>((float*)q, n, nf, species, P, ctl, &ctl->err, expand);
   else
-    k_chem_fast<double, kChemMinBlocks, true, true>
+    k_chem_fast<double, kChemMinBlocks>
         <<<blocks, kChemThreads, 0, st>>>((double*)q, n, nf, species, P, ctl, &ctl->err, expand);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

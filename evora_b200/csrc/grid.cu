@@ -61,6 +61,10 @@ struct evora_grid {
   // multi-step CUDA graphs, key = 4 * steps + 2 * (CFL maxima fresh) +
   // starting buffer
   std::map<long long, cudaGraphExec_t> graphs;
+  std::map<long long, int64_t> graph_launches;   // kernel launches per replay, by key
+  // the last enqueued step's closing control (step_end) is deferred into the
+  // next step's first control kernel or a flush
+  bool pending_end = false;
   // the previous update reduced the CFL maxima of the current state into
   // ctl->snext; any other change of the state clears this
   bool cfl_fresh = false;
@@ -205,6 +209,16 @@ __device__ __forceinline__ void step_end(GridCtl* ctl) {
 
 __global__ void k_step_end(GridCtl* ctl) { step_end(ctl); }
 
+// The control of consecutive fused steps in one launch: the previous step's
+// step_end (when end is set), then this step's step_begin with the maxima
+// the previous update reduced, and step_time -- the three single-thread
+// kernels' work in their order.
+__global__ void k_step_control(HydroParams P, GridCtl* ctl, int end) {
+  if (end) step_end(ctl);
+  step_begin(ctl, 1);
+  step_time(P, ctl);
+}
+
 // Control of a multi-grid step, one thread per grid: hydrostep part 2 and
 // updatetime (as k_step_begin + k_step_time), and after the update the step
 // count, the ping-pong parity and a compact status word.
@@ -281,6 +295,7 @@ bool chem_expansion(const evora_grid* g) {
 void drop_graphs(evora_grid* g) {
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   g->graphs.clear();
+  g->graph_launches.clear();
 }
 
 cudaEvent_t next_event(evora_grid* g) {
@@ -325,21 +340,41 @@ int enqueue_reference_step(evora_grid* g) {
   return 0;
 }
 
+// The deferred step_end of the last enqueued step, before the host reads
+// the control block or another kind of launch follows.
+void flush_step_end(evora_grid* g) {
+  if (!g->pending_end) return;
+  k_step_end<<<1, 1, 0, g->stream>>>(g->ctl);
+  g->launches += 1;
+  g->pending_end = false;
+}
+
 int enqueue_fused_step(evora_grid* g) {
   cudaStream_t st = g->stream;
   const bool use_next = g->cfl_fresh;
-  g->launches += use_next ? 4 : 5;
-  k_step_begin<<<1, 1, 0, st>>>(g->ctl, use_next ? 1 : 0);
-  mark(g);
-  if (!use_next) fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
-  if (g->P.cooldt) {
-    // coolstep (main.f90:120) on the state the step starts from
-    int rc = cool_step(g->P, g->qbuf[g->cur], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl, st);
-    if (rc) return rc;
-    g->launches += 1;
+  if (use_next && !g->P.cooldt) {
+    // the previous step's end, this step's begin and time in one launch
+    k_step_control<<<1, 1, 0, st>>>(g->P, g->ctl, g->pending_end ? 1 : 0);
+    g->pending_end = false;
+    g->launches += 2;   // the control kernel and the update
+    mark(g);
+    mark(g);
+  } else {
+    flush_step_end(g);
+    g->launches += use_next ? 3 : 4;
+    k_step_begin<<<1, 1, 0, st>>>(g->ctl, use_next ? 1 : 0);
+    mark(g);
+    if (!use_next) fused_cfl(g->plan, g->qbuf[g->cur], g->ctl, st);
+    if (g->P.cooldt) {
+      // coolstep (main.f90:120) on the state the step starts from
+      int rc =
+          cool_step(g->P, g->qbuf[g->cur], g->precision == EVORA_FP32, g->nf, ncells(g), g->species, g->ctl, st);
+      if (rc) return rc;
+      g->launches += 1;
+    }
+    mark(g);
+    k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
   }
-  mark(g);
-  k_step_time<<<1, 1, 0, st>>>(g->P, g->ctl);
   mark(g);
   fused_update(g->plan, g->qbuf[g->cur], g->qbuf[g->cur ^ 1], g->ctl, st);
   mark(g);
@@ -377,7 +412,7 @@ int enqueue_fused_step(evora_grid* g) {
     g->launches += 1;
   }
   mark(g);
-  k_step_end<<<1, 1, 0, st>>>(g->ctl);
+  g->pending_end = true;   // k_step_end, deferred (flush_step_end, k_step_control)
   CU(cudaGetLastError());
   // The swap is unconditional on the host; an inactive step copies q through
   // unchanged (fused_update does that when the step is inactive).
@@ -668,6 +703,8 @@ int evora_grid_step(evora_grid* g, int32_t nsteps, int32_t sync) {
     int rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
     if (rc) return rc;
   }
+  flush_step_end(g);
+  CU(cudaGetLastError());
   if (sync) return evora_grid_status(g);
   return 0;
 }
@@ -692,9 +729,12 @@ int graph_steps(evora_grid* g, int nsteps) {
       const int64_t launches0 = g->launches;
       for (int i = 0; i < nsteps && !rc; ++i)
         rc = reference_backend(g) ? enqueue_reference_step(g) : enqueue_fused_step(g);
+      if (!rc) flush_step_end(g);
       cudaError_t e = cudaStreamEndCapture(g->stream, &graph);
+      g->pending_end = false;
       g->cur = start;
       g->cfl_fresh = fresh;
+      const int64_t per_replay = g->launches - launches0;
       g->launches = launches0;
       if (rc) return rc;
       if (e != cudaSuccess) {
@@ -709,18 +749,13 @@ int graph_steps(evora_grid* g, int nsteps) {
         return EVORA_ERR_CUDA;
       }
       it = g->graphs.emplace(key, ex).first;
+      g->graph_launches[key] = per_replay;
     }
     CU(cudaGraphLaunch(it->second, g->stream));
-    if (reference_backend(g)) {
-      g->launches += (int64_t)nsteps * 10;
-    } else {
+    g->launches += g->graph_launches[key];   // the kernels the capture enqueued
+    if (!reference_backend(g)) {
       g->cur = start ^ (nsteps & 1);
-      const bool fused = g->plan.cfl_fused != 0;
-      g->launches += (int64_t)nsteps * ((fused ? 4 : 5) + grav_launches(g) + (g->conduction ? 2 : 0) +
-                                       (g->floors ? 1 : 0) +
-                                       (g->expansion && !fused_expansion(g) && !chem_expansion(g) ? 1 : 0)) +
-                     (fused && !fresh ? 1 : 0);
-      g->cfl_fresh = fused;
+      g->cfl_fresh = g->plan.cfl_fused != 0;
     }
   }
   return 0;

@@ -52,5 +52,7 @@ def test_launch_count_drops_cfl_kernel(cuda_device):
         g.set_timing(True)
         g.step(4)
         t = g.timing()
-    # step 1: begin, CFL, time, update, end; steps 2-4 without the CFL kernel
-    assert t["launches"] == 5 + 3 * 4
+    # step 1: begin, CFL, time, update; steps 2-4: one control kernel (the
+    # previous step's end, this step's begin and time) and the update; then
+    # the last step's end
+    assert t["launches"] == 4 + 3 * 2 + 1
