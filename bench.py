@@ -253,22 +253,31 @@ def time_dropin_resident(ev, q, mode, steps, warmup):
     resident mode: the state stays on the GPU between the calls, and
     evora_sync brings q back once at the end.  Returns (ms per step of the
     loop, ms of the final sync)."""
+    import ctypes
+    from evora_b200._native import lib
     p = kh_params(ev)
     sh = ev.shapes(p)
     w, evo, s = np.zeros(sh["w"]), np.zeros(sh["evo"]), np.zeros(sh["s"])
     qh = q.copy()
     di = ev.DropIn(p)
     di.set_resident(mode)
-    t, go = p.tstart, True
+    # the C ABI called as a Fortran main program calls it: the arrays' base
+    # addresses once, the scalars by reference
+    L = lib()
+    pw, pq, pevo, ps = (ctypes.c_void_p(a.ctypes.data) for a in (w, qh, evo, s))
+    dt, t = ctypes.c_double(0.0), ctypes.c_double(p.tstart)
+    go, dump, k = ctypes.c_int32(1), ctypes.c_int32(0), ctypes.c_int32(1)
 
     def step():
-        nonlocal t, go
-        di.primitive(w, qh)
-        di.bound(w)
-        dt = di.hydrostep(w, 1e99)
-        go, t, dt = di.updatetime(go, t, dt)
-        di.compevo(w, evo, s, dt)
-        di.sweep(w, qh, evo, s, dt)
+        rc = L.evora_primitive(pw, pq) | L.evora_bound(pw)
+        dt.value = 1e99
+        rc |= L.evora_hydrostep(pw, ctypes.byref(dt))
+        rc |= L.evora_updatetime(ctypes.byref(go), ctypes.byref(dump), ctypes.byref(k), ctypes.byref(t),
+                                 ctypes.byref(dt))
+        rc |= L.evora_compevo(pw, pevo, ps, dt.value)
+        rc |= L.evora_sweep(pw, pq, pevo, ps, dt.value)
+        if rc:
+            raise RuntimeError(f"drop-in step failed: status {rc}")
 
     try:
         for _ in range(warmup):

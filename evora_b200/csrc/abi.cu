@@ -421,6 +421,13 @@ int resident_bind(DropinState& S, const double* q) {
       S.rgrid = nullptr;
       return rc;
     }
+    // the FP32 form's fastest update where it takes the grid (a fixed
+    // choice, not timed, so that the results do not depend on a timing)
+    if (prec == EVORA_FP32 && !S.strict && (rc = evora_grid_set_tile(S.rgrid, EVORA_FP32_PAIR_TILE))) {
+      evora_grid_destroy(S.rgrid);
+      S.rgrid = nullptr;
+      return rc;
+    }
     S.rq = nullptr;
   }
   if (q != S.rq || S.rq_host_newer) {

@@ -30,7 +30,7 @@ STRICT = 2
 REFERENCE_KERNELS = 4
 # tile entry of the FP32 table that runs two cells per thread on packed FP32
 # pairs (its sums are associated differently from the other FP32 kernels)
-FP32_PAIR_TILE = 5
+FP32_PAIR_TILE = 5   # EVORA_FP32_PAIR_TILE
 # resident modes of the drop-in layer (evora_set_resident)
 RESIDENT_FP64 = 1
 RESIDENT_FP32 = 2

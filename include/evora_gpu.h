@@ -482,7 +482,11 @@ int evora_multigrid_status(evora_multigrid* m, evora_grid** grids, int32_t* go, 
  * ms_per_tile (optional, max_tiles entries) receives the timings. */
 int evora_grid_autotune(evora_grid* g, int32_t reps, int32_t* chosen, double* ms_per_tile,
                         int32_t max_tiles);
-/* Selects a tile shape by index (0 = the default). */
+/* Selects a tile shape by index (0 = the default); a shape that cannot run
+ * the grid falls back to 0.  EVORA_FP32_PAIR_TILE is the FP32 table's
+ * two-cells-per-thread kernel (packed f32x2; grids of whole 32x8 tiles with
+ * 5 fields, HLLC, minmod and the second-order scheme). */
+enum { EVORA_FP32_PAIR_TILE = 5 };
 int evora_grid_set_tile(evora_grid* g, int32_t tile);
 
 /* Kernel timing (no counterpart in the reference): when on, every step
