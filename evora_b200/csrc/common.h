@@ -59,6 +59,12 @@ const evora_params* grid_params(const evora_grid* g);
 int grid_cfl_maxima(evora_grid* g, double smax[3]);
 int grid_update_dt(evora_grid* g, double dt, bool sync);
 
+// evora_grid_set_q / evora_grid_get_q without their final wait: the copies
+// and conversions are only enqueued on the grid's stream.  q must stay valid
+// (set_q) and is complete (get_q) once that stream has been synchronised.
+int grid_set_q_async(evora_grid* g, const double* q);
+int grid_get_q_async(evora_grid* g, double* q);
+
 // Host arrays q bound to the resident mode's grid: before a routine that
 // reads q on the host, the newer device state is copied back
 // (dropin_resident_read); before one that also writes it, the device copy is

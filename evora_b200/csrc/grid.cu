@@ -53,6 +53,7 @@ struct evora_grid {
   int cur = 0;
   FusedPlan plan{};
   double* aos_stage = nullptr;  // device staging for q in reference layout
+  GridCtl ctl_init{};           // host source of the control block set_q uploads
   // kernel timing
   bool timing = false;
   std::vector<cudaEvent_t> events;  // 5 per timed step
@@ -489,6 +490,56 @@ void free_grid(evora_grid* g) {
 
 // Values per cell of q in the reference layout (12 with chemistry).
 int nq_of(const evora_grid* g) { return g->params.chemistry ? EVORA_NQ_CHEM : EVORA_NQ; }
+}  // namespace
+
+namespace evora {
+
+int grid_set_q_async(evora_grid* g, const double* q) {
+  int64_t nq;
+  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
+  const bool dev = is_device_pointer(q);
+  if (reference_backend(g)) {
+    CU(cudaMemcpyAsync(g->q_aos, q, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       g->stream));
+  } else {
+    const double* src = q;
+    if (!dev) {
+      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
+      CU(cudaMemcpyAsync(g->aos_stage, q, nq * 8, cudaMemcpyHostToDevice, g->stream));
+      src = g->aos_stage;
+    }
+    g->cur = 0;
+    fused_from_aos(g->plan, src, g->qbuf[0], g->stream, nq_of(g), g->species);
+  }
+  g->cfl_fresh = false;
+  if (g->multigrid) g->multigrid->dirty = true;   // its table entry (parity, maxima) changes
+  init_ctl(g, &g->ctl_init);
+  CU(cudaMemcpyAsync(g->ctl, &g->ctl_init, sizeof(GridCtl), cudaMemcpyHostToDevice, g->stream));
+  return 0;
+}
+
+int grid_get_q_async(evora_grid* g, double* q) {
+  int64_t nq;
+  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
+  const bool dev = is_device_pointer(q);
+  if (reference_backend(g)) {
+    CU(cudaMemcpyAsync(q, g->q_aos, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       g->stream));
+  } else {
+    double* dst = q;
+    if (!dev) {
+      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
+      dst = g->aos_stage;
+    }
+    fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream, nq_of(g), g->species);
+    if (!dev) CU(cudaMemcpyAsync(q, dst, nq * 8, cudaMemcpyDeviceToHost, g->stream));
+  }
+  return 0;
+}
+
+}  // namespace evora
+
+namespace {
 
 int create_grid(const evora_params* p, int32_t precision, int32_t flags, cudaStream_t astream, evora_grid** out);
 int graph_steps(evora_grid* g, int nsteps);
@@ -639,48 +690,16 @@ int evora_grid_set_stream(evora_grid* g, void* stream) {
 
 int evora_grid_set_q(evora_grid* g, const double* q) {
   if (!g || !q) return EVORA_ERR_ARG;
-  int64_t nq;
-  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
-  const bool dev = is_device_pointer(q);
-  if (reference_backend(g)) {
-    CU(cudaMemcpyAsync(g->q_aos, q, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                       g->stream));
-  } else {
-    const double* src = q;
-    if (!dev) {
-      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
-      CU(cudaMemcpyAsync(g->aos_stage, q, nq * 8, cudaMemcpyHostToDevice, g->stream));
-      src = g->aos_stage;
-    }
-    g->cur = 0;
-    fused_from_aos(g->plan, src, g->qbuf[0], g->stream, nq_of(g), g->species);
-  }
-  g->cfl_fresh = false;
-  if (g->multigrid) g->multigrid->dirty = true;   // its table entry (parity, maxima) changes
-  GridCtl c;
-  init_ctl(g, &c);
-  CU(cudaMemcpyAsync(g->ctl, &c, sizeof c, cudaMemcpyHostToDevice, g->stream));
+  int rc = grid_set_q_async(g, q);
+  if (rc) return rc;
   CU(cudaStreamSynchronize(g->stream));
   return 0;
 }
 
 int evora_grid_get_q(evora_grid* g, double* q) {
   if (!g || !q) return EVORA_ERR_ARG;
-  int64_t nq;
-  evora_array_sizes(&g->params, &nq, nullptr, nullptr, nullptr);
-  const bool dev = is_device_pointer(q);
-  if (reference_backend(g)) {
-    CU(cudaMemcpyAsync(q, g->q_aos, nq * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                       g->stream));
-  } else {
-    double* dst = q;
-    if (!dev) {
-      if (!g->aos_stage) CU(dalloc(g, (void**)&g->aos_stage, nq * 8));
-      dst = g->aos_stage;
-    }
-    fused_to_aos(g->plan, g->qbuf[g->cur], dst, g->stream, nq_of(g), g->species);
-    if (!dev) CU(cudaMemcpyAsync(q, dst, nq * 8, cudaMemcpyDeviceToHost, g->stream));
-  }
+  int rc = grid_get_q_async(g, q);
+  if (rc) return rc;
   CU(cudaStreamSynchronize(g->stream));
   return 0;
 }

@@ -19,18 +19,23 @@
 // time to solution (submit -> read back) is recorded.  A request's arithmetic
 // does not depend on what else is in flight.
 //
-// Single-threaded: one host thread drives a server.
+// One host thread drives a server; the server's own worker threads only
+// split large host copies (CopyPool).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <new>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "../../include/evora_gpu.h"
@@ -69,6 +74,7 @@ struct Request {
   long long off = 0;             // arena offset (tubes)
   evora_grid* grid = nullptr;    // 2D/3D
   bool batched = false;          // stepped by the server's multi-grid batch
+  bool uploading = false;        // admitted this round, its upload still in flight
   int stream = 0;                // index into the server's grid streams
   size_t bytes = 0;              // device footprint (grids)
   int64_t steps = 0;
@@ -77,6 +83,92 @@ struct Request {
   HostBuf result;                // read back state, released when delivered
   size_t result_n = 0;
   long long cells() const { return (long long)nx * ny * nz; }
+};
+
+// Large host copies (a request's state into the page-locked pool at submit,
+// a result out of it at delivery) split over worker threads: one core moves
+// a few GB/s, the host's memory system several times that.  The workers
+// start with the first large copy.  copy() returns when every worker has
+// finished its part of this copy, so none is still on an older one when
+// the next is posted.
+class CopyPool {
+ public:
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+
+  void copy(void* dst, const void* src, size_t bytes) {
+    if (bytes < kMinSplit || !start()) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      dst_ = static_cast<char*>(dst);
+      src_ = static_cast<const char*>(src);
+      bytes_ = bytes;
+      chunk_ = std::max<size_t>(kChunk, (bytes / (4 * (th_.size() + 1)) + 4095) & ~(size_t)4095);
+      next_.store(0);
+      finished_ = 0;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return finished_ == (int)th_.size(); });
+  }
+
+ private:
+  static constexpr size_t kMinSplit = 4u << 20;
+  static constexpr size_t kChunk = 1u << 20;
+
+  bool start() {
+    if (started_) return !th_.empty();
+    started_ = true;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int n = (int)std::min(8u, hw > 1 ? hw : 1u) - 1;   // the caller copies too
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { run(); });
+    return !th_.empty();
+  }
+
+  void work() {
+    for (;;) {
+      const size_t off = next_.fetch_add(1) * chunk_;
+      if (off >= bytes_) return;
+      std::memcpy(dst_ + off, src_ + off, std::min(chunk_, bytes_ - off));
+    }
+  }
+
+  void run() {
+    unsigned long seen = 0;
+    std::unique_lock<std::mutex> lk(m_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+      lk.unlock();
+      work();
+      lk.lock();
+      if (++finished_ == (int)th_.size()) done_.notify_one();
+    }
+  }
+
+  std::vector<std::thread> th_;
+  bool started_ = false;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  unsigned long gen_ = 0;
+  bool stop_ = false;
+  int finished_ = 0;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t bytes_ = 0, chunk_ = kChunk;
+  std::atomic<size_t> next_{0};
 };
 
 #define CU(call)                 \
@@ -118,6 +210,7 @@ struct evora_server {
   cudaStream_t rstream = nullptr;  // read-back of finished tubes
   std::vector<int> free_streams;   // indices of idle grid streams
   std::vector<Request*> to_free;   // grids read back, destroyed after the round
+  std::vector<Request*> uploads;   // grids admitted this round (uploads in flight)
   std::deque<int64_t> completed;   // ids finished since the last evora_server_completed
   std::vector<int64_t> slot_req; // slot -> request id (0 = free)
   std::vector<std::pair<long long, long long>> free_seg;  // (offset, length), sorted
@@ -137,6 +230,7 @@ struct evora_server {
   size_t fixed = 0;              // arena and staging
   // page-locked host buffers by size class (powers of two of doubles)
   std::map<int, std::vector<HostBuf>> free_bufs;
+  CopyPool copies;
   // host time per round phase: launch, read-back, admission, wait, free, detect
   double phase_s[6] = {0, 0, 0, 0, 0, 0};
   long long rounds = 0;
@@ -274,16 +368,20 @@ int admit(evora_server* s, Request& r) {
     if (rc) return rc == EVORA_ERR_NOMEM ? 1 : rc;
     s->free_streams.pop_back();
     r.stream = si;
-    rc = evora_grid_set_q(g, r.q0.p);
+    // enqueued only: the upload and conversion run on the grid's stream
+    // while the host admits the next requests; the grid joins the batch
+    // once the round's wait has seen them complete (join_uploads)
+    rc = grid_set_q_async(g, r.q0.p);
     if (rc) {
+      cudaStreamSynchronize(s->gstreams[si]);
       evora_grid_destroy(g);
       s->free_streams.push_back(si);
       return rc == EVORA_ERR_NOMEM ? 1 : rc;
     }
     r.grid = g;
     r.bytes = bytes;
-    r.batched = s->mg && evora_multigrid_add(s->mg, g) == 0;
-    if (r.batched) s->batched_grids++;
+    r.uploading = true;
+    s->uploads.push_back(&r);
     // time quantum: a round gives each grid about the same device time, so
     // its step count falls with its size (2^20 cell-updates per base step)
     const double quantum = (double)s->steps_per_tick * (double)(1 << 20);
@@ -291,8 +389,33 @@ int admit(evora_server* s, Request& r) {
     s->used += bytes;
   }
   r.state = REQ_RUNNING;
-  buf_put(s, r.q0);   // the upload has completed (both paths waited for it)
+  if (r.tube) buf_put(s, r.q0);   // the tube upload has completed (waited for above)
   return 0;
+}
+
+// Grids admitted this round: their uploads are complete once their streams
+// are; the host copies go back to the pool and the grids join the batch
+// (or step alone on their streams from the next round).
+int join_uploads(evora_server* s) {
+  for (Request* r : s->uploads) {
+    CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+    buf_put(s, r->q0);
+    r->uploading = false;
+    r->batched = s->mg && evora_multigrid_add(s->mg, r->grid) == 0;
+    if (r->batched) s->batched_grids++;
+  }
+  s->uploads.clear();
+  return 0;
+}
+
+// A grid that finished: its read-back (conversion to the reference layout
+// and the copy into a page-locked buffer) is enqueued on its stream at once
+// and collected in the next round.
+int start_readback(evora_server* s, Request& r) {
+  r.result_n = (size_t)EVORA_NQ * r.cells();
+  r.result = buf_get(s, r.result_n);
+  if (!r.result.p) return EVORA_ERR_NOMEM;
+  return grid_get_q_async(r.grid, r.result.p);
 }
 
 void finish(evora_server* s, Request& r, unsigned err) {
@@ -483,7 +606,7 @@ int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, dou
   const size_t nq = (size_t)EVORA_NQ * nx * ny * nz;
   r.q0 = buf_get(s, nq);
   if (!r.q0.p) return EVORA_ERR_NOMEM;
-  std::memcpy(r.q0.p, q0, nq * sizeof(double));
+  s->copies.copy(r.q0.p, q0, nq * sizeof(double));
   r.t_submit = s->now();
   if (s->first_submit < 0) s->first_submit = r.t_submit;
   if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) {   // could never fit
@@ -530,14 +653,15 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   }
   mark(0);
   // 3. while the GPU works: read back what finished in the previous round
+  //    (grids: collect the read-backs started when they finished)
   for (auto& kv : s->reqs) {
     Request& r = kv.second;
     if (r.state != REQ_FINISHING) continue;
-    r.result_n = (size_t)EVORA_NQ * r.cells();
-    r.result = buf_get(s, r.result_n);
-    if (!r.result.p) return EVORA_ERR_NOMEM;
     int rc = 0;
     if (r.tube) {
+      r.result_n = (size_t)EVORA_NQ * r.cells();
+      r.result = buf_get(s, r.result_n);
+      if (!r.result.p) return EVORA_ERR_NOMEM;
       tube_to_aos(s->q, s->stage2, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->rstream);
       CU(cudaMemcpyAsync(r.result.p, s->stage2, sizeof(double) * r.result_n, cudaMemcpyDeviceToHost,
                          s->rstream));
@@ -545,7 +669,7 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       free_segment(s, r.off, r.nx);
       s->slot_req[r.slot] = 0;
     } else {
-      rc = evora_grid_get_q(r.grid, r.result.p);
+      CU(cudaStreamSynchronize(s->gstreams[r.stream]));
       s->grid_cell_updates += (long long)r.steps * r.cells();
       s->to_free.push_back(&r);
     }
@@ -573,6 +697,10 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   CU(cudaStreamSynchronize(s->mstream));
   for (Request* r : grids)
     if (!r->batched) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+  {
+    int rc = join_uploads(s);
+    if (rc) return rc;
+  }
   mark(3);
   // 5. grids read back above can go now (their streams are idle)
   for (Request* r : s->to_free) {
@@ -622,6 +750,8 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       evora_multigrid_remove(s->mg, r->grid);
       r->batched = false;
       s->batched_grids--;
+      int rc2 = start_readback(s, *r);
+      if (rc2) return rc2;
     }
   }
   for (Request* r : grids) {
@@ -636,6 +766,8 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     r->steps = k;
     r->err = (unsigned)st;
     r->state = REQ_FINISHING;
+    rc = start_readback(s, *r);
+    if (rc) return rc;
   }
   mark(5);
   s->rounds++;
@@ -659,7 +791,7 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
   if (r.state != REQ_DONE && r.state != REQ_FAILED) return 0;
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (steps) *steps = r.steps;
-  if (q_out && r.result.p) std::memcpy(q_out, r.result.p, sizeof(double) * r.result_n);
+  if (q_out && r.result.p) s->copies.copy(q_out, r.result.p, sizeof(double) * r.result_n);
   const int err = (int)r.err;
   if (q_out) {   // delivered
     buf_put(s, r.result);
