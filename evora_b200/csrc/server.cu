@@ -697,10 +697,6 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   CU(cudaStreamSynchronize(s->mstream));
   for (Request* r : grids)
     if (!r->batched) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
-  {
-    int rc = join_uploads(s);
-    if (rc) return rc;
-  }
   mark(3);
   // 5. grids read back above can go now (their streams are idle)
   for (Request* r : s->to_free) {
@@ -767,6 +763,12 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     r->err = (unsigned)st;
     r->state = REQ_FINISHING;
     rc = start_readback(s, *r);
+    if (rc) return rc;
+  }
+  // grids admitted this round join the batch after its status was read (a
+  // batch changed since its last step reads each member's control block)
+  {
+    int rc = join_uploads(s);
     if (rc) return rc;
   }
   mark(5);
