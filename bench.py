@@ -791,25 +791,35 @@ def serving_requests(ev, n, seed=11):
     return reqs
 
 
-def serve(server, reqs, arrivals, keep=()):
+def serve(server, reqs, arrivals, keep=(), borrowed=True):
     """Submits requests at their arrival times (host clock) to the server and
-    ticks it until all are done.  Results are read into reused buffers, one
-    per shape; those of the requests in `keep` are kept.  Returns latencies by
-    kind, the wall time, cell-updates, rounds, mean round time, round phases
-    and the kept results."""
+    ticks it until all are done.  borrowed: each request's state is read, and
+    its result written into an array of its own, by the server's copy
+    threads while the device works (Server.submit_borrowed); else the state
+    is copied at submit and results are read into reused buffers, one per
+    shape.  The results of the requests in `keep` are kept.  Returns
+    latencies by kind, the wall time, cell-updates, rounds, mean round time,
+    round phases and the kept results."""
     lat = {"1d": [], "2d": [], "3d": []}
     kept, bufs = {}, {}
     cu0 = server.stats()["cell_updates"]
     ph0 = server.profile()
     t0 = time.perf_counter()
     nxt, done, ticks, tick_s, submit_s, deliver_s = 0, 0, 0, 0.0, 0.0, 0.0
+    slow = []   # (seconds, cells) per submit call
     ids = {}
     while done < len(reqs):
         now = time.perf_counter() - t0
         ts = time.perf_counter()
         while nxt < len(reqs) and arrivals[nxt] <= now:
             kind, q, tend = reqs[nxt]
-            ids[server.submit(q, tend, boundtype=1 if kind == "1d" else 2)] = nxt
+            bt = 1 if kind == "1d" else 2
+            t1 = time.perf_counter()
+            if borrowed:
+                ids[server.submit_borrowed(q, tend, boundtype=bt, out=np.empty(q.shape))] = nxt
+            else:
+                ids[server.submit(q, tend, boundtype=bt)] = nxt
+            slow.append((time.perf_counter() - t1, q.size // 6))
             nxt += 1
         tk = time.perf_counter()
         submit_s += tk - ts
@@ -820,7 +830,9 @@ def serve(server, reqs, arrivals, keep=()):
         for rid in server.completed():
             i = ids.pop(rid)
             shape = reqs[i][1].shape
-            if i in keep:
+            if borrowed:
+                out = None
+            elif i in keep:
                 out = np.empty(shape)
             else:
                 out = bufs.setdefault(shape, np.empty(shape))
@@ -835,8 +847,9 @@ def serve(server, reqs, arrivals, keep=()):
     wall = time.perf_counter() - t0
     ph = server.profile()
     phases = {k: ph[k] - ph0[k] for k in ph}
-    phases["submit"] = submit_s      # submit calls (host copy into the page-locked pool)
-    phases["deliver"] = deliver_s    # completed() and result() (host copy out of it)
+    phases["submit"] = submit_s      # submit calls (with borrowed=False: the copy into the page-locked pool)
+    phases["deliver"] = deliver_s    # completed() and result() (with borrowed=False: the copy out of it)
+    phases["submit_slowest_ms_cells"] = [[1e3 * t, c] for t, c in sorted(slow, reverse=True)[:4]]
     cu = server.stats()["cell_updates"] - cu0
     return lat, wall, cu, ticks, 1e3 * tick_s / max(1, ticks), phases, kept
 
@@ -865,7 +878,8 @@ def run_serving(args):
         barrier(world)
         lat, wall, cu, ticks, mround, phases, kept = serve(server, [reqs[i] for i in mine],
                                                            np.asarray(arrivals)[mine],
-                                                           keep={k for k, i in enumerate(mine) if i in keep})
+                                                           keep={k for k, i in enumerate(mine) if i in keep},
+                                                           borrowed=not args.copy_at_submit)
         kept = {mine[k]: v for k, v in kept.items()}
         parts = sharding.gather_objects((lat, wall, cu, ticks, mround, phases), rank, world)
         if rank != 0:
@@ -875,7 +889,9 @@ def run_serving(args):
         cu = sum(pt[2] for pt in parts)
         ticks = max(pt[3] for pt in parts)
         mround = max(pt[4] for pt in parts)
-        phases = {k: max(pt[5][k] for pt in parts) for k in parts[0][5]}
+        phases = {k: max(pt[5][k] for pt in parts) for k in parts[0][5] if k != "submit_slowest_ms_cells"}
+        phases["submit_slowest_ms_cells"] = sorted((x for pt in parts for x in pt[5]["submit_slowest_ms_cells"]),
+                                                   reverse=True)[:4]
         return lat, wall, cu, ticks, mround, phases, kept
 
     def summary(lat):
@@ -893,7 +909,7 @@ def run_serving(args):
     # as many requests as the burst below, so that the page-locked pool holds
     # the buffers a burst keeps at once (pinning memory is a one-time cost)
     warm = serving_requests(ev, args.nrequests, seed=10)
-    serve(server, warm, np.zeros(len(warm)))
+    serve(server, warm, np.zeros(len(warm)), borrowed=not args.copy_at_submit)
     if args.sustained:
         burst = serving_requests(ev, args.nrequests, seed=11)
         res = serve_sharded(burst, np.zeros(len(burst)))
@@ -946,6 +962,8 @@ def run_serving(args):
                                    "32^3-128^3, Poisson arrivals", "rate_per_s": rate,
                        "requests": len(reqs), "tick_steps": args.tick_steps, "hbm_budget_gb": 150,
                        "arrivals": "70% of the measured capacity" if args.sustained else "--rate",
+                       "host_copies": ("at submit and delivery on the driving thread" if args.copy_at_submit else
+                                       "borrowed arrays, copied by the server's threads while the device works"),
                        "parallelism": (f"requests dispatched to the least-loaded of {world} ranks on arrival, "
                                        "no exchange") if world > 1 else "single GPU"},
             "latency_s": summary(lat),
@@ -986,6 +1004,9 @@ def main():
     ap.add_argument("--tick-steps", type=int, default=32)
     ap.add_argument("--sustained", action="store_true",
                     help="serving: measure the capacity with a burst, then latency at 70%% of it")
+    ap.add_argument("--copy-at-submit", action="store_true",
+                    help="serving: copy each request's state at submit and its result at delivery on the "
+                         "driving thread (Server.submit) instead of the borrowed arrays of Server.submit_borrowed")
     ap.add_argument("--no-chemistry", action="store_true", help="cosmo: without the CIE chemistry and cooling")
     args = ap.parse_args()
     global NX, NY, NZ, AUTOTUNE, CHEMISTRY, WORKLOAD, TILES

@@ -238,6 +238,8 @@ def _declare_batch(L):
         "evora_server_destroy": ([G], c_int32),
         "evora_server_submit": ([G, c_int32, c_int32, c_int32, c_double, c_int32, c_void_p,
                                  ctypes.POINTER(c_int64)], c_int32),
+        "evora_server_submit_borrowed": ([G, c_int32, c_int32, c_int32, c_double, c_int32, c_void_p, c_void_p,
+                                          ctypes.POINTER(c_int64)], c_int32),
         "evora_server_tick": ([G, ctypes.POINTER(c_int32), ctypes.POINTER(c_int32)], c_int32),
         "evora_server_result": ([G, c_int64, c_void_p, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int32)],
                                 c_int32),

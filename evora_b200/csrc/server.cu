@@ -19,8 +19,15 @@
 // time to solution (submit -> read back) is recorded.  A request's arithmetic
 // does not depend on what else is in flight.
 //
+// Host copies: a request's state goes through a pool of page-locked buffers,
+// copied there at submit, or, for evora_server_submit_borrowed, by the
+// server's copy threads after submit (and the result likewise into the
+// caller's array), so that those copies overlap the device's rounds.  The
+// uploads, conversions and read-backs of a round are enqueued and waited for
+// once per round.
+//
 // One host thread drives a server; the server's own worker threads only
-// split large host copies (CopyPool).
+// run host copies of request states (Stager).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +39,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <numeric>
@@ -48,9 +56,17 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// REQ_FINISHING: done on the device, result not yet read back (reported as
-// running).
-enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3, REQ_FINISHING = 4 };
+// REQ_FINISHING: done on the device, result not yet read back;
+// REQ_DELIVERING: read back, being copied into a borrowed array (both
+// reported as running).
+enum ReqState {
+  REQ_PENDING = 0,
+  REQ_RUNNING = 1,
+  REQ_DONE = 2,
+  REQ_FAILED = 3,
+  REQ_FINISHING = 4,
+  REQ_DELIVERING = 5
+};
 
 // A host buffer of doubles from the server's pool of page-locked buffers
 // (so that uploads and read-backs are direct DMA), or pageable memory when
@@ -82,93 +98,123 @@ struct Request {
   unsigned err = 0;
   HostBuf result;                // read back state, released when delivered
   size_t result_n = 0;
+  // evora_server_submit_borrowed: the caller's arrays, and the chunks of the
+  // copy in flight (the initial state into q0, then the result into out)
+  const double* src = nullptr;
+  double* out = nullptr;
+  std::unique_ptr<std::atomic<int>> left;
   long long cells() const { return (long long)nx * ny * nz; }
 };
 
-// Large host copies (a request's state into the page-locked pool at submit,
-// a result out of it at delivery) split over worker threads: one core moves
-// a few GB/s, the host's memory system several times that.  The workers
-// start with the first large copy.  copy() returns when every worker has
-// finished its part of this copy, so none is still on an older one when
-// the next is posted.
-class CopyPool {
+// Host copies of request states (into the page-locked pool, and results
+// out of it) run on worker threads in 4 MB chunks: one core moves a few
+// GB/s, the host's memory system several times that.  post() queues a copy
+// and returns at once; *left counts its chunks still to copy (0: complete).
+// copy() posts and helps until its own copy is complete.  The workers start
+// with the first posted copy; stop() lets them finish every queued chunk.
+class Stager {
  public:
-  ~CopyPool() {
+  ~Stager() { stop(); }
+
+  void post(void* dst, const void* src, size_t bytes, std::atomic<int>* left) {
+    const size_t nchunks = bytes == 0 ? 1 : (bytes + kChunk - 1) / kChunk;
+    left->fetch_add((int)nchunks, std::memory_order_relaxed);
+    start();
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      for (size_t i = 0; i < nchunks; ++i) {
+        const size_t off = i * kChunk;
+        q_.push_back(Task{static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                          std::min(kChunk, bytes - std::min(bytes, off)), left});
+      }
+    }
+    cv_.notify_all();
+  }
+
+  void copy(void* dst, const void* src, size_t bytes) {
+    if (bytes < kMinSplit) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    std::atomic<int> left{0};
+    post(dst, src, bytes, &left);
+    std::unique_lock<std::mutex> lk(m_);
+    while (left.load(std::memory_order_acquire) > 0) {
+      if (!q_.empty()) {   // run queued chunks (FIFO) until this copy's are done
+        const Task t = q_.front();
+        q_.pop_front();
+        lk.unlock();
+        run(t);
+        lk.lock();
+        continue;
+      }
+      done_.wait(lk, [&] { return left.load(std::memory_order_acquire) == 0 || !q_.empty(); });
+    }
+  }
+
+  void stop() {
     {
       std::lock_guard<std::mutex> lk(m_);
       stop_ = true;
     }
     cv_.notify_all();
     for (auto& t : th_) t.join();
-  }
-
-  void copy(void* dst, const void* src, size_t bytes) {
-    if (bytes < kMinSplit || !start()) {
-      std::memcpy(dst, src, bytes);
-      return;
+    th_.clear();
+    // without workers (none could be started) the queue is run here
+    while (!q_.empty()) {
+      const Task t = q_.front();
+      q_.pop_front();
+      run(t);
     }
-    {
-      std::lock_guard<std::mutex> lk(m_);
-      dst_ = static_cast<char*>(dst);
-      src_ = static_cast<const char*>(src);
-      bytes_ = bytes;
-      chunk_ = std::max<size_t>(kChunk, (bytes / (4 * (th_.size() + 1)) + 4095) & ~(size_t)4095);
-      next_.store(0);
-      finished_ = 0;
-      ++gen_;
-    }
-    cv_.notify_all();
-    work();
-    std::unique_lock<std::mutex> lk(m_);
-    done_.wait(lk, [&] { return finished_ == (int)th_.size(); });
   }
 
  private:
   static constexpr size_t kMinSplit = 4u << 20;
-  static constexpr size_t kChunk = 1u << 20;
+  static constexpr size_t kChunk = 4u << 20;
+  struct Task {
+    char* dst;
+    const char* src;
+    size_t bytes;
+    std::atomic<int>* left;
+  };
 
-  bool start() {
-    if (started_) return !th_.empty();
+  void start() {
+    if (started_) return;
     started_ = true;
     const unsigned hw = std::thread::hardware_concurrency();
-    const int n = (int)std::min(8u, hw > 1 ? hw : 1u) - 1;   // the caller copies too
-    for (int i = 0; i < n; ++i) th_.emplace_back([this] { run(); });
-    return !th_.empty();
-  }
-
-  void work() {
-    for (;;) {
-      const size_t off = next_.fetch_add(1) * chunk_;
-      if (off >= bytes_) return;
-      std::memcpy(dst_ + off, src_ + off, std::min(chunk_, bytes_ - off));
+    const int n = (int)std::min(8u, hw > 1 ? hw : 2u);
+    try {
+      for (int i = 0; i < n; ++i) th_.emplace_back([this] { worker(); });
+    } catch (...) {   // no threads: copy() and stop() run the queue themselves
     }
   }
 
-  void run() {
-    unsigned long seen = 0;
+  void run(const Task& t) {
+    if (t.bytes) std::memcpy(t.dst, t.src, t.bytes);
+    if (t.left->fetch_sub(1, std::memory_order_acq_rel) == 1) {
+      std::lock_guard<std::mutex> lk(m_);
+      done_.notify_all();
+    }
+  }
+
+  void worker() {
     std::unique_lock<std::mutex> lk(m_);
     for (;;) {
-      cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
-      if (stop_) return;
-      seen = gen_;
+      cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+      if (q_.empty()) return;   // stopping, and every queued chunk is done
+      const Task t = q_.front();
+      q_.pop_front();
       lk.unlock();
-      work();
+      run(t);
       lk.lock();
-      if (++finished_ == (int)th_.size()) done_.notify_one();
     }
   }
 
   std::vector<std::thread> th_;
-  bool started_ = false;
+  bool started_ = false, stop_ = false;
   std::mutex m_;
   std::condition_variable cv_, done_;
-  unsigned long gen_ = 0;
-  bool stop_ = false;
-  int finished_ = 0;
-  char* dst_ = nullptr;
-  const char* src_ = nullptr;
-  size_t bytes_ = 0, chunk_ = kChunk;
-  std::atomic<size_t> next_{0};
+  std::deque<Task> q_;
 };
 
 #define CU(call)                 \
@@ -205,12 +251,21 @@ struct evora_server {
   int* head = nullptr;
   unsigned long long* cu = nullptr;
   void* gscratch = nullptr;
-  double* stage = nullptr;       // AoS staging of one tube (admission)
-  double* stage2 = nullptr;      // AoS staging of one tube (read-back)
+  // AoS staging of tubes (stage: the round's admissions, stage2: read-backs
+  // in flight), stage_cells cells each; the tubes' copies and conversions
+  // are enqueued on the read-back stream and waited for once per round
+  double* stage = nullptr;
+  double* stage2 = nullptr;
+  long long stage_cells = 0, stage_used = 0, stage2_used = 0;
+  std::vector<Request*> tube_uploads;  // tubes admitted this round
+  std::vector<Request*> tube_reads;    // tubes whose read-backs are in flight
+  std::deque<Request*> tube_waiting;   // finished tubes waiting for room in stage2
+  std::vector<TubeState> ts_host;      // host sources of the tube-table uploads, by slot
   cudaStream_t rstream = nullptr;  // read-back of finished tubes
   std::vector<int> free_streams;   // indices of idle grid streams
   std::vector<Request*> to_free;   // grids read back, destroyed after the round
   std::vector<Request*> uploads;   // grids admitted this round (uploads in flight)
+  std::vector<Request*> delivering;  // results being copied into borrowed arrays
   std::deque<int64_t> completed;   // ids finished since the last evora_server_completed
   std::vector<int64_t> slot_req; // slot -> request id (0 = free)
   std::vector<std::pair<long long, long long>> free_seg;  // (offset, length), sorted
@@ -230,7 +285,7 @@ struct evora_server {
   size_t fixed = 0;              // arena and staging
   // page-locked host buffers by size class (powers of two of doubles)
   std::map<int, std::vector<HostBuf>> free_bufs;
-  CopyPool copies;
+  Stager copies;
   // host time per round phase: launch, read-back, admission, wait, free, detect
   double phase_s[6] = {0, 0, 0, 0, 0, 0};
   long long rounds = 0;
@@ -244,10 +299,12 @@ namespace {
 HostBuf buf_get(evora_server* s, size_t n) {
   int cls = 10;
   while (((size_t)1 << cls) < n) ++cls;
-  auto& fl = s->free_bufs[cls];
-  if (!fl.empty()) {
-    HostBuf b = fl.back();
-    fl.pop_back();
+  // the smallest free buffer of this size class or a larger one (pinning new
+  // memory costs far more than holding a larger buffer for a while)
+  for (auto it = s->free_bufs.lower_bound(cls); it != s->free_bufs.end(); ++it) {
+    if (it->second.empty()) continue;
+    HostBuf b = it->second.back();
+    it->second.pop_back();
     return b;
   }
   HostBuf b;
@@ -315,6 +372,7 @@ size_t grid_bytes(const evora_server* s, long long cells) {
 
 int admit(evora_server* s, Request& r) {
   if (r.tube) {
+    if (s->stage_used + r.nx > s->stage_cells) return 1;   // the round's staging is full: next round
     int slot = -1;
     for (int i = 0; i < s->max_slots; ++i)
       if (s->slot_req[i] == 0) {
@@ -326,11 +384,14 @@ int admit(evora_server* s, Request& r) {
     r.slot = slot;
     r.off = off;
     s->slot_req[slot] = r.id;
-    // on the read-back stream: the running tube launch never touches a free
-    // slot or a free arena segment, so the upload overlaps it
-    CU(cudaMemcpyAsync(s->stage, r.q0.p, sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->rstream));
-    tube_from_aos(s->stage, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->rstream);
-    TubeState ts{};
+    // enqueued on the read-back stream (the running tube launch never
+    // touches a free slot or a free arena segment); waited for, and the host
+    // copy released, after the round (join_tube_uploads)
+    double* st = s->stage + (size_t)EVORA_NQ * s->stage_used;
+    CU(cudaMemcpyAsync(st, r.q0.p, sizeof(double) * EVORA_NQ * r.nx, cudaMemcpyHostToDevice, s->rstream));
+    tube_from_aos(st, s->q, s->precision == EVORA_FP32, s->arena, off, r.nx, s->nf, s->rstream);
+    TubeState& ts = s->ts_host[slot];
+    ts = TubeState{};
     ts.offset = off;
     ts.n = r.nx;
     ts.status = TUBE_RUNNING;
@@ -338,7 +399,8 @@ int admit(evora_server* s, Request& r) {
     ts.tend = r.tend;
     ts.bt = r.bt;
     CU(cudaMemcpyAsync(s->tubes + slot, &ts, sizeof ts, cudaMemcpyHostToDevice, s->rstream));
-    CU(cudaStreamSynchronize(s->rstream));
+    s->stage_used += r.nx;
+    s->tube_uploads.push_back(&r);
     s->active_tubes++;
     s->order_dirty = true;
   } else {
@@ -389,8 +451,47 @@ int admit(evora_server* s, Request& r) {
     s->used += bytes;
   }
   r.state = REQ_RUNNING;
-  if (r.tube) buf_put(s, r.q0);   // the tube upload has completed (waited for above)
   return 0;
+}
+
+// Tubes admitted this round: their uploads are complete once the read-back
+// stream is; their host copies go back to the pool.
+int join_tube_uploads(evora_server* s) {
+  if (s->tube_uploads.empty()) return 0;
+  CU(cudaStreamSynchronize(s->rstream));
+  for (Request* r : s->tube_uploads) buf_put(s, r->q0);
+  s->tube_uploads.clear();
+  s->stage_used = 0;
+  return 0;
+}
+
+// Finished tubes: conversion to the reference layout into stage2 and the
+// copy into a page-locked buffer, enqueued while the device is idle between
+// rounds (as many as stage2 holds) and collected in the next round.
+int issue_tube_reads(evora_server* s) {
+  while (!s->tube_waiting.empty()) {
+    Request& r = *s->tube_waiting.front();
+    if (s->stage2_used + r.nx > s->stage_cells) break;
+    r.result_n = (size_t)EVORA_NQ * r.cells();
+    r.result = buf_get(s, r.result_n);
+    if (!r.result.p) return EVORA_ERR_NOMEM;
+    double* st = s->stage2 + (size_t)EVORA_NQ * s->stage2_used;
+    tube_to_aos(s->q, st, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->rstream);
+    CU(cudaMemcpyAsync(r.result.p, st, sizeof(double) * r.result_n, cudaMemcpyDeviceToHost, s->rstream));
+    s->stage2_used += r.nx;
+    s->tube_reads.push_back(&r);
+    s->tube_waiting.pop_front();
+  }
+  return 0;
+}
+
+void finish(evora_server* s, Request& r, unsigned err) {
+  r.err = err;
+  r.state = err ? REQ_FAILED : REQ_DONE;
+  r.t_done = s->now();
+  s->last_done = r.t_done;
+  s->latencies.push_back(r.t_done - r.t_submit);
+  s->completed.push_back(r.id);
 }
 
 // Grids admitted this round: their uploads are complete once their streams
@@ -418,13 +519,72 @@ int start_readback(evora_server* s, Request& r) {
   return grid_get_q_async(r.grid, r.result.p);
 }
 
-void finish(evora_server* s, Request& r, unsigned err) {
-  r.err = err;
-  r.state = err ? REQ_FAILED : REQ_DONE;
-  r.t_done = s->now();
-  s->last_done = r.t_done;
-  s->latencies.push_back(r.t_done - r.t_submit);
-  s->completed.push_back(r.id);
+// A request's initial state: copied into the page-locked pool before
+// returning, or (borrowed) by the copy threads after it, the request
+// admissible once that copy is complete.
+int submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int32_t boundtype, const double* q0,
+           double* q_out, bool borrowed, int64_t* id) {
+  if (!s || !q0 || !id || nx < 2 || ny < 1 || nz < 1 || (nz > 1 && ny == 1)) return EVORA_ERR_ARG;
+  if (boundtype < 0 || boundtype > 3) return EVORA_ERR_ARG;
+  const bool tube = (ny == 1 && nz == 1);
+  if (tube && nx > s->max_tube) return EVORA_ERR_ARG;
+  Request r;
+  r.nx = nx;
+  r.ny = ny;
+  r.nz = nz;
+  if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) return EVORA_ERR_ARG;   // could never fit
+  r.id = s->next_id++;
+  r.tend = tend;
+  r.bt = boundtype;
+  r.tube = tube;
+  const size_t nq = (size_t)EVORA_NQ * nx * ny * nz;
+  r.q0 = buf_get(s, nq);
+  if (!r.q0.p) return EVORA_ERR_NOMEM;
+  if (borrowed) {
+    r.src = q0;
+    r.out = q_out;
+    r.left.reset(new (std::nothrow) std::atomic<int>(0));
+    if (!r.left) {
+      buf_put(s, r.q0);
+      return EVORA_ERR_NOMEM;
+    }
+    s->copies.post(r.q0.p, q0, nq * sizeof(double), r.left.get());
+  } else {
+    s->copies.copy(r.q0.p, q0, nq * sizeof(double));
+  }
+  r.t_submit = s->now();
+  if (s->first_submit < 0) s->first_submit = r.t_submit;
+  *id = r.id;
+  s->pending.push_back(r.id);
+  s->reqs.emplace(r.id, std::move(r));
+  return 0;
+}
+
+// A result read back into the page-locked pool: delivered now, or first
+// copied into the caller's borrowed array by the copy threads.
+void deliver(evora_server* s, Request& r, unsigned err) {
+  if (r.out && r.result.p) {
+    r.err = err;
+    r.state = REQ_DELIVERING;
+    s->copies.post(r.out, r.result.p, sizeof(double) * r.result_n, r.left.get());
+    s->delivering.push_back(&r);
+    return;
+  }
+  finish(s, r, err);
+}
+
+// Results whose copies into borrowed arrays are complete are finished.
+void collect_deliveries(evora_server* s) {
+  size_t k = 0;
+  for (Request* r : s->delivering) {
+    if (r->left->load(std::memory_order_acquire) > 0) {
+      s->delivering[k++] = r;
+      continue;
+    }
+    buf_put(s, r->result);
+    finish(s, *r, r->err);
+  }
+  s->delivering.resize(k);
 }
 
 int upload_order(evora_server* s) {
@@ -497,14 +657,20 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
   if (cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
   if (cudaStreamCreateWithFlags(&s->mstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
   if (evora_multigrid_create(precision, flags & ~EVORA_REFERENCE_KERNELS, s->mstream, &s->mg)) s->mg = nullptr;
-  if (cudaMalloc(&s->stage2, sizeof(double) * EVORA_NQ * max_tube_cells) != cudaSuccess) goto fail;
+  // tube staging: up to 64 tubes of the largest size per round, within a
+  // sixteenth of the budget
+  s->stage_cells = std::max<long long>(max_tube_cells,
+                                       std::min<long long>(64LL * max_tube_cells,
+                                                           (long long)(s->budget / 16 / (EVORA_NQ * sizeof(double)))));
+  s->ts_host.assign(max_tubes, TubeState{});
+  if (cudaMalloc(&s->stage2, sizeof(double) * EVORA_NQ * s->stage_cells) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->q, arena_bytes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->tubes, sizeof(TubeState) * max_tubes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->order, sizeof(int) * max_tubes) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->head, sizeof(int)) != cudaSuccess) goto fail;
   if (cudaMalloc(&s->cu, sizeof(unsigned long long)) != cudaSuccess) goto fail;
   if (cudaMemset(s->cu, 0, sizeof(unsigned long long)) != cudaSuccess) goto fail;
-  if (cudaMalloc(&s->stage, sizeof(double) * EVORA_NQ * max_tube_cells) != cudaSuccess) goto fail;
+  if (cudaMalloc(&s->stage, sizeof(double) * EVORA_NQ * s->stage_cells) != cudaSuccess) goto fail;
   {
     std::vector<TubeState> ts(max_tubes);
     for (auto& t : ts) {
@@ -548,7 +714,7 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
     }
     pl.gscratch = s->gscratch;
   }
-  s->used = arena_bytes + sizeof(double) * EVORA_NQ * max_tube_cells;
+  s->used = arena_bytes + 2 * sizeof(double) * EVORA_NQ * (size_t)s->stage_cells;
   s->fixed = s->used;
   if (s->used > s->budget) {
     evora_server_destroy(s);
@@ -564,6 +730,7 @@ fail:
 
 int evora_server_destroy(evora_server* s) {
   if (!s) return EVORA_ERR_ARG;
+  s->copies.stop();   // no copy into a buffer freed below is still queued
   cudaDeviceSynchronize();
   if (s->mg) evora_multigrid_destroy(s->mg);
   for (auto& kv : s->reqs) {
@@ -591,32 +758,12 @@ int evora_server_destroy(evora_server* s) {
 
 int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int32_t boundtype,
                         const double* q0, int64_t* id) {
-  if (!s || !q0 || !id || nx < 2 || ny < 1 || nz < 1 || (nz > 1 && ny == 1)) return EVORA_ERR_ARG;
-  if (boundtype < 0 || boundtype > 3) return EVORA_ERR_ARG;
-  const bool tube = (ny == 1 && nz == 1);
-  if (tube && nx > s->max_tube) return EVORA_ERR_ARG;
-  Request r;
-  r.id = s->next_id++;
-  r.nx = nx;
-  r.ny = ny;
-  r.nz = nz;
-  r.tend = tend;
-  r.bt = boundtype;
-  r.tube = tube;
-  const size_t nq = (size_t)EVORA_NQ * nx * ny * nz;
-  r.q0 = buf_get(s, nq);
-  if (!r.q0.p) return EVORA_ERR_NOMEM;
-  s->copies.copy(r.q0.p, q0, nq * sizeof(double));
-  r.t_submit = s->now();
-  if (s->first_submit < 0) s->first_submit = r.t_submit;
-  if (!tube && grid_bytes(s, r.cells()) > s->budget - s->fixed) {   // could never fit
-    buf_put(s, r.q0);
-    return EVORA_ERR_ARG;
-  }
-  *id = r.id;
-  s->pending.push_back(r.id);
-  s->reqs.emplace(r.id, std::move(r));
-  return 0;
+  return submit(s, nx, ny, nz, tend, boundtype, q0, nullptr, false, id);
+}
+
+int evora_server_submit_borrowed(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend,
+                                 int32_t boundtype, const double* q0, double* q_out, int64_t* id) {
+  return submit(s, nx, ny, nz, tend, boundtype, q0, q_out, true, id);
 }
 
 int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
@@ -652,39 +799,39 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     if (rc) return rc;
   }
   mark(0);
-  // 3. while the GPU works: read back what finished in the previous round
-  //    (grids: collect the read-backs started when they finished)
+  // 3. while the GPU works: collect the read-backs of what finished in the
+  //    previous round (enqueued when it was detected)
+  collect_deliveries(s);
+  if (!s->tube_reads.empty()) {
+    CU(cudaStreamSynchronize(s->rstream));
+    for (Request* r : s->tube_reads) {
+      free_segment(s, r->off, r->nx);
+      s->slot_req[r->slot] = 0;
+      deliver(s, *r, r->err);
+    }
+    s->tube_reads.clear();
+    s->stage2_used = 0;
+  }
   for (auto& kv : s->reqs) {
     Request& r = kv.second;
-    if (r.state != REQ_FINISHING) continue;
-    int rc = 0;
-    if (r.tube) {
-      r.result_n = (size_t)EVORA_NQ * r.cells();
-      r.result = buf_get(s, r.result_n);
-      if (!r.result.p) return EVORA_ERR_NOMEM;
-      tube_to_aos(s->q, s->stage2, s->precision == EVORA_FP32, s->arena, r.off, r.nx, s->nf, s->P.g1, s->rstream);
-      CU(cudaMemcpyAsync(r.result.p, s->stage2, sizeof(double) * r.result_n, cudaMemcpyDeviceToHost,
-                         s->rstream));
-      CU(cudaStreamSynchronize(s->rstream));
-      free_segment(s, r.off, r.nx);
-      s->slot_req[r.slot] = 0;
-    } else {
-      CU(cudaStreamSynchronize(s->gstreams[r.stream]));
-      s->grid_cell_updates += (long long)r.steps * r.cells();
-      s->to_free.push_back(&r);
-    }
-    finish(s, r, r.err | (unsigned)rc);
+    if (r.state != REQ_FINISHING || r.tube) continue;
+    CU(cudaStreamSynchronize(s->gstreams[r.stream]));
+    s->grid_cell_updates += (long long)r.steps * r.cells();
+    s->to_free.push_back(&r);
+    deliver(s, r, r.err);
   }
   mark(1);
   // 3b. admission, in arrival order, while memory and slots allow (host
   //     copies overlap the round); admitted work starts with the next round
   while (!s->pending.empty()) {
     Request& r = s->reqs[s->pending.front()];
+    if (r.left && r.left->load(std::memory_order_acquire) > 0) break;   // its state is still being copied
     int rc = admit(s, r);
     if (rc == 1) {
       bool idle = s->active_tubes == 0 && s->to_free.empty() && grids.empty();
       for (auto& kv : s->reqs)
-        idle = idle && kv.second.state != REQ_RUNNING && kv.second.state != REQ_FINISHING;
+        idle = idle && kv.second.state != REQ_RUNNING && kv.second.state != REQ_FINISHING &&
+               kv.second.state != REQ_DELIVERING;
       if (!idle) break;           // head of the queue waits for room
       rc = EVORA_ERR_NOMEM;       // nothing running and still no room: it never fits
     }
@@ -697,6 +844,10 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   CU(cudaStreamSynchronize(s->mstream));
   for (Request* r : grids)
     if (!r->batched) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+  {
+    int rc = join_tube_uploads(s);
+    if (rc) return rc;
+  }
   mark(3);
   // 5. grids read back above can go now (their streams are idle)
   for (Request* r : s->to_free) {
@@ -718,9 +869,14 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       r.steps = ts[i].k;
       r.err = ts[i].err;
       r.state = REQ_FINISHING;
+      s->tube_waiting.push_back(&r);
       s->active_tubes--;
       s->order_dirty = true;
     }
+  }
+  {
+    int rc = issue_tube_reads(s);
+    if (rc) return rc;
   }
   if (s->batched_grids > 0) {
     // one read of the batch's status words; finished grids leave the batch
@@ -771,10 +927,12 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     int rc = join_uploads(s);
     if (rc) return rc;
   }
+  collect_deliveries(s);
   mark(5);
   s->rounds++;
   int act = 0;
-  for (auto& kv : s->reqs) act += kv.second.state == REQ_RUNNING || kv.second.state == REQ_FINISHING;
+  for (auto& kv : s->reqs)
+    act += kv.second.state == REQ_RUNNING || kv.second.state == REQ_FINISHING || kv.second.state == REQ_DELIVERING;
   if (n_active) *n_active = act;
   if (n_pending) *n_pending = (int32_t)s->pending.size();
   return 0;
@@ -789,11 +947,13 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
     return EVORA_ERR_ARG;
   }
   Request& r = it->second;
-  if (state) *state = r.state == REQ_FINISHING ? REQ_RUNNING : r.state;
+  if (state) *state = r.state == REQ_FINISHING || r.state == REQ_DELIVERING ? REQ_RUNNING : r.state;
   if (r.state != REQ_DONE && r.state != REQ_FAILED) return 0;
   if (latency_s) *latency_s = r.t_done - r.t_submit;
   if (steps) *steps = r.steps;
   if (q_out && r.result.p) s->copies.copy(q_out, r.result.p, sizeof(double) * r.result_n);
+  else if (q_out && r.out && q_out != r.out && r.result_n)   // delivered into the borrowed array
+    s->copies.copy(q_out, r.out, sizeof(double) * r.result_n);
   const int err = (int)r.err;
   if (q_out) {   // delivered
     buf_put(s, r.result);

@@ -27,11 +27,13 @@ class Server:
               "server_create")
         self._h = h
         self.shapes = {}
+        self._borrowed = {}   # id -> (q0, out) arrays the server reads / writes after submit
 
     def close(self):
         if getattr(self, "_h", None):
             lib().evora_server_destroy(self._h)
             self._h = None
+        self._borrowed = {}
 
     def __del__(self):  # pragma: no cover
         try:
@@ -59,6 +61,29 @@ class Server:
         self.shapes[rid.value] = q0.shape
         return rid.value
 
+    def submit_borrowed(self, q0: np.ndarray, tend: float, boundtype: int = 0, out=None) -> int:
+        """As submit(), but the server's copy threads read q0 after the call
+        and, with `out` (float64, C-contiguous, q0's shape), write the result
+        into it before the request reports done, so the host copies overlap
+        the device's rounds.  The server keeps both arrays referenced until
+        result() delivers the request."""
+        q0 = np.ascontiguousarray(q0, dtype=np.float64)
+        if q0.ndim == 2:
+            nz, ny, nx = 1, 1, q0.shape[0]
+        else:
+            nz, ny, nx = q0.shape[:3]
+        if out is not None and (out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]
+                                or out.shape != q0.shape):
+            raise ValueError("out must be a C-contiguous float64 array of q0's shape")
+        rid = ctypes.c_int64()
+        check(lib().evora_server_submit_borrowed(self._h, nx, ny, nz, float(tend), int(boundtype),
+                                                 ctypes.c_void_p(q0.ctypes.data),
+                                                 None if out is None else ctypes.c_void_p(out.ctypes.data),
+                                                 ctypes.byref(rid)), "server_submit_borrowed")
+        self.shapes[rid.value] = q0.shape
+        self._borrowed[rid.value] = (q0, out)
+        return rid.value
+
     def tick(self):
         a, p = ctypes.c_int32(), ctypes.c_int32()
         check(lib().evora_server_tick(self._h, ctypes.byref(a), ctypes.byref(p)), "server_tick")
@@ -76,6 +101,8 @@ class Server:
         st = self.state(rid)
         if st not in (DONE, FAILED):
             return None
+        if out is None and rid in self._borrowed:
+            out = self._borrowed[rid][1]
         if out is not None:
             if out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or out.shape != tuple(self.shapes[rid]):
                 raise ValueError("out must be a C-contiguous float64 array of the request's shape")
@@ -86,6 +113,7 @@ class Server:
         err = lib().evora_server_result(self._h, int(rid), ctypes.c_void_p(q.ctypes.data), ctypes.byref(lat),
                                         ctypes.byref(steps), ctypes.byref(st2))
         del self.shapes[rid]
+        self._borrowed.pop(rid, None)
         return q, lat.value, steps.value, int(err)
 
     def stats(self):

@@ -567,6 +567,16 @@ int evora_server_destroy(evora_server* s);
  * server's for this request (0 keeps it).  EVORA_ERR_ARG if it can never fit. */
 int evora_server_submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int32_t boundtype,
                         const double* q0, int64_t* id);
+/* As evora_server_submit, without a copy before the call returns: the
+ * server's copy threads read q0 after it, so q0 must stay valid and
+ * unchanged until the request is no longer pending (evora_server_result
+ * reports it running, done or failed).  With q_out (the request's size in
+ * the reference layout) the result is copied into q_out before the request
+ * reports done or failed; q_out must stay valid until then, and
+ * evora_server_result with that same pointer delivers it without a copy.
+ * The host copies then overlap the device's rounds. */
+int evora_server_submit_borrowed(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend,
+                                 int32_t boundtype, const double* q0, double* q_out, int64_t* id);
 /* One scheduling round (admit, step, retire); reports active/pending counts. */
 int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending);
 /* state: 0 pending, 1 running, 2 done, 3 failed, -1 unknown id.  When done or

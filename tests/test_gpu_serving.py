@@ -34,13 +34,18 @@ def base(**kw):
     return ev.default_params(g=5 / 3, cfl=0.4, boundtype=2, tstart=0.0, **kw)
 
 
-def run_all(reqs, precision, flags=0, budget=150e9, spt=16, stagger=0):
+def run_all(reqs, precision, flags=0, budget=150e9, spt=16, stagger=0, borrowed=False):
+    """borrowed: Server.submit_borrowed, every other request with an output
+    array of its own (the others read back by result())."""
     out = {}
     with Server(base(), precision, flags, hbm_budget_bytes=budget, steps_per_tick=spt, max_tube_cells=1024,
                 max_tubes=64) as s:
         ids = []
         for i, (q, tend) in enumerate(reqs):
-            ids.append(s.submit(q, tend))
+            if borrowed:
+                ids.append(s.submit_borrowed(q, tend, out=np.full(q.shape, np.nan) if i % 2 == 0 else None))
+            else:
+                ids.append(s.submit(q, tend))
             for _ in range(stagger):
                 s.tick()
         for _ in range(100000):
@@ -88,3 +93,21 @@ def test_tight_budget_only_delays(cuda_device):
     tight, _ = run_all(reqs, ev.FP32, budget=2.5e6)     # one 3D grid at a time
     for i in roomy:
         np.testing.assert_array_equal(tight[i][0], roomy[i][0])
+
+
+def test_borrowed_arrays_equal_copies(cuda_device):
+    """Requests whose states the server's copy threads read after submit,
+    and whose results they write into the caller's arrays, give the results
+    of the copying submit bit for bit; the inputs are left unchanged.  The
+    512^2 request is copied in several chunks."""
+    reqs = mix(seed=4)
+    p = ev.default_params(nx=512, ny=512, nz=1, g=5 / 3)
+    reqs.insert(3, (ev.ic.kh2d(p), 0.002))
+    before = [q.copy() for q, _ in reqs]
+    copied, _ = run_all(reqs, ev.FP32, stagger=1)
+    lent, stats = run_all(reqs, ev.FP32, stagger=1, borrowed=True)
+    assert stats["completed"] == len(reqs)
+    for i in range(len(reqs)):
+        np.testing.assert_array_equal(reqs[i][0], before[i])
+        assert lent[i][3] == copied[i][3] == 0 and lent[i][2] == copied[i][2]
+        np.testing.assert_array_equal(lent[i][0], copied[i][0])
