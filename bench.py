@@ -906,9 +906,11 @@ def run_serving(args):
     # the mix warms it (graphs, page-locked buffers) and is not reported
     server = Server(ev.default_params(g=5.0 / 3.0, cfl=0.5, boundtype=1, tend=1.0), ev.FP32, 0,
                     hbm_budget_bytes=150e9, steps_per_tick=args.tick_steps, max_tube_cells=8192, max_tubes=4096)
-    # as many requests as the burst below, so that the page-locked pool holds
-    # the buffers a burst keeps at once (pinning memory is a one-time cost)
-    warm = serving_requests(ev, args.nrequests, seed=10)
+    # twice as many requests as the burst below, all at once, so that the
+    # page-locked pool holds the buffers a burst of the mix keeps at once
+    # (pinning memory is a service's one-time start-up cost: 54-111 ms per
+    # 128^3 state measured in a submit call)
+    warm = serving_requests(ev, 2 * args.nrequests, seed=10)
     serve(server, warm, np.zeros(len(warm)), borrowed=not args.copy_at_submit)
     if args.sustained:
         burst = serving_requests(ev, args.nrequests, seed=11)

@@ -246,6 +246,7 @@ def _declare_batch(L):
         "evora_server_stats": ([G, _dp, _dp, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64), _dp], c_int32),
         "evora_server_completed": ([G, ctypes.POINTER(c_int64), c_int32, ctypes.POINTER(c_int32)], c_int32),
         "evora_server_profile": ([G, _dp], c_int32),
+        "evora_server_device_ms": ([G, _dp, _dp], c_int32),
     }
     for name, (args, res) in sig.items():
         if hasattr(L, name):

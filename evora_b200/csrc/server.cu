@@ -288,6 +288,10 @@ struct evora_server {
   Stager copies;
   // host time per round phase: launch, read-back, admission, wait, free, detect
   double phase_s[6] = {0, 0, 0, 0, 0, 0};
+  // device time of the rounds' tube launches and multi-grid steps (events
+  // around them on their streams), ms
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double dev_ms[2] = {0.0, 0.0};
   long long rounds = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -538,6 +542,9 @@ int submit(evora_server* s, int32_t nx, int32_t ny, int32_t nz, double tend, int
   r.bt = boundtype;
   r.tube = tube;
   const size_t nq = (size_t)EVORA_NQ * nx * ny * nz;
+  // the page-locked buffer is taken here, on the driving thread: pinning new
+  // memory on a copy thread was measured to stall this thread's CUDA calls
+  // for longer than the pinning itself
   r.q0 = buf_get(s, nq);
   if (!r.q0.p) return EVORA_ERR_NOMEM;
   if (borrowed) {
@@ -655,6 +662,8 @@ int evora_server_create(const evora_params* base, int32_t precision, int32_t fla
     cudaGetLastError();
   }
   if (cudaStreamCreateWithFlags(&s->rstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
+  for (auto& e : s->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) goto fail;
   if (cudaStreamCreateWithFlags(&s->mstream, cudaStreamNonBlocking) != cudaSuccess) goto fail;
   if (evora_multigrid_create(precision, flags & ~EVORA_REFERENCE_KERNELS, s->mstream, &s->mg)) s->mg = nullptr;
   // tube staging: up to 64 tubes of the largest size per round, within a
@@ -749,6 +758,8 @@ int evora_server_destroy(evora_server* s) {
   cudaFree(s->stage);
   cudaFree(s->stage2);
   if (s->rstream) cudaStreamDestroy(s->rstream);
+  for (auto e : s->ev)
+    if (e) cudaEventDestroy(e);
   if (s->tstream) cudaStreamDestroy(s->tstream);
   if (s->mstream) cudaStreamDestroy(s->mstream);
   for (auto st : s->gstreams) cudaStreamDestroy(st);
@@ -781,10 +792,13 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
     int rc = upload_order(s);
     if (rc) return rc;
   }
+  const bool timed_tubes = s->plan.ntubes > 0 && s->ev[0];
   if (s->plan.ntubes > 0) {
+    if (timed_tubes) CU(cudaEventRecord(s->ev[0], s->tstream));
     CU(cudaMemsetAsync(s->head, 0, sizeof(int), s->tstream));
     s->launch(s->plan, s->q, s->tstream);
     CU(cudaGetLastError());
+    if (timed_tubes) CU(cudaEventRecord(s->ev[1], s->tstream));
   }
   std::vector<Request*> grids;
   for (auto& kv : s->reqs)
@@ -794,9 +808,12 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
       int rc = evora_grid_step(kv.second.grid, kv.second.round_steps, 0);
       if (rc) return rc;
     }
+  const bool timed_batch = s->batched_grids > 0 && s->ev[2];
   if (s->batched_grids > 0) {
+    if (timed_batch) CU(cudaEventRecord(s->ev[2], s->mstream));
     int rc = evora_multigrid_step(s->mg, s->steps_per_tick, 0);
     if (rc) return rc;
+    if (timed_batch) CU(cudaEventRecord(s->ev[3], s->mstream));
   }
   mark(0);
   // 3. while the GPU works: collect the read-backs of what finished in the
@@ -844,6 +861,12 @@ int evora_server_tick(evora_server* s, int32_t* n_active, int32_t* n_pending) {
   CU(cudaStreamSynchronize(s->mstream));
   for (Request* r : grids)
     if (!r->batched) CU(cudaStreamSynchronize(s->gstreams[r->stream]));
+  {
+    float ms = 0.f;
+    if (timed_tubes && cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) s->dev_ms[0] += ms;
+    if (timed_batch && cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]) == cudaSuccess) s->dev_ms[1] += ms;
+    cudaGetLastError();
+  }
   {
     int rc = join_tube_uploads(s);
     if (rc) return rc;
@@ -966,6 +989,13 @@ int evora_server_profile(evora_server* s, double out[7]) {
   if (!s || !out) return EVORA_ERR_ARG;
   for (int i = 0; i < 6; ++i) out[i] = s->phase_s[i];
   out[6] = (double)s->rounds;
+  return 0;
+}
+
+int evora_server_device_ms(evora_server* s, double* tube_ms, double* batch_ms) {
+  if (!s) return EVORA_ERR_ARG;
+  if (tube_ms) *tube_ms = s->dev_ms[0];
+  if (batch_ms) *batch_ms = s->dev_ms[1];
   return 0;
 }
 

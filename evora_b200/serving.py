@@ -132,10 +132,15 @@ class Server:
         return list(buf[:n.value])
 
     def profile(self):
-        """Host seconds per round phase and the number of rounds."""
+        """Host seconds per round phase, the number of rounds, and the device
+        seconds of the rounds' tube launches and multi-grid steps."""
         out = (ctypes.c_double * 7)()
         check(lib().evora_server_profile(self._h, out), "server_profile")
         names = ["launch", "readback", "admission", "wait", "free", "detect"]
         d = {n: out[i] for i, n in enumerate(names)}
         d["rounds"] = int(out[6])
+        tm, bm = ctypes.c_double(), ctypes.c_double()
+        check(lib().evora_server_device_ms(self._h, ctypes.byref(tm), ctypes.byref(bm)), "server_device_ms")
+        d["device_tubes"] = 1e-3 * tm.value
+        d["device_batch"] = 1e-3 * bm.value
         return d

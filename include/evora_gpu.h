@@ -588,6 +588,9 @@ int evora_server_result(evora_server* s, int64_t id, double* q_out, double* late
  * [2] admission, [3] waiting for the device, [4] freeing, [5] completion
  * checks; out[6] the number of rounds. */
 int evora_server_profile(evora_server* s, double out[7]);
+/* Device time so far of the rounds' tube launches and of the multi-grid
+ * batch's steps (CUDA events around them on their streams), ms. */
+int evora_server_device_ms(evora_server* s, double* tube_ms, double* batch_ms);
 /* Ids of requests finished (done or failed) since the last call, oldest
  * first, at most max_ids of them; *n receives the count. */
 int evora_server_completed(evora_server* s, int64_t* ids, int32_t max_ids, int32_t* n);
