@@ -33,6 +33,7 @@ struct BatchArgs {
   int budget;             // max steps per tube in this launch
   long long quantum;      // if > 0: a tube of n cells runs at most max(1, quantum / n) steps
   int cap;                // tubes with n <= cap live in shared memory
+  int capw;               // cap < n <= capw: w in shared memory, q in the scratch slot
   T* gscratch;            // per-CTA scratch for longer tubes: (NF + 5) * (nmax + 4) each
   int nmax;
   unsigned long long* cell_updates;  // running total
@@ -53,6 +54,7 @@ struct BatchPlan {
   int budget = 1;
   long long quantum = 0;
   int cap = 0;
+  int capw = 0;        // set with smem: the longest tube whose w fits the shared memory
   void* gscratch = nullptr;
   int nmax = 0;
   unsigned long long* cell_updates = nullptr;

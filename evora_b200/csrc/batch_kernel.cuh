@@ -18,8 +18,9 @@
 //            reference's pencil loop (muscl.f90:194-215): face states from
 //            the slopes and the predictor, one Riemann solve per interface,
 //            the flux of the previous interface carried, q updated in place.
-// A tube longer than the shared-memory capacity keeps q and w in a global
-// scratch slot of its CTA instead (same code, generic pointers).
+// A tube longer than the shared-memory capacity keeps q in a global scratch
+// slot of its CTA and w in shared memory while w alone fits, else both in
+// the slot (same code, generic pointers).
 #pragma once
 
 #include "batch.h"
@@ -229,6 +230,11 @@ __global__ void __launch_bounds__(NT) k_tubes(BatchArgs<T> A) {
     if (n <= A.cap) {
       qs = reinterpret_cast<T*>(sraw);
       w = qs + NF * A.cap;
+    } else if (n <= A.capw) {
+      // the primitives (read three times per cell and step by the sweeps)
+      // in shared memory, the state in the CTA's scratch slot
+      w = reinterpret_cast<T*>(sraw);
+      qs = A.gscratch + (size_t)blockIdx.x * (size_t)(NF + 5) * (A.nmax + 4);
     } else {
       qs = A.gscratch + (size_t)blockIdx.x * (size_t)(NF + 5) * (A.nmax + 4);
       w = qs + (size_t)NF * (A.nmax + 4);

@@ -358,6 +358,7 @@ void batch_launch(const BatchPlan& pl, void* q, cudaStream_t st) {
   A.budget = pl.budget;
   A.quantum = pl.quantum;
   A.cap = pl.cap;
+  A.capw = pl.capw;
   A.gscratch = (TT*)pl.gscratch;
   A.nmax = pl.nmax;
   A.cell_updates = pl.cell_updates;
@@ -368,6 +369,7 @@ template <int NF, int NT>
 BatchLaunch batch_pick_one(BatchPlan* pl) {
   pl->threads = NT;
   pl->smem = ((size_t)NF * pl->cap + 5 * ((size_t)pl->cap + 4)) * sizeof(TT);
+  pl->capw = std::max(pl->cap, (int)(pl->smem / (5 * sizeof(TT))) - 4);
   auto k = k_tubes<TT, NF, NT>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem);
   cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);

@@ -68,9 +68,12 @@ def test_batch_alone_equals_mix_and_graph_budget(cuda_device):
             np.testing.assert_array_equal(b.get_q(), mix[offs[i]:offs[i + 1]])
 
 
-def test_batch_long_tubes_from_global_memory(cuda_device):
+@pytest.mark.parametrize("ctas_per_sm,lengths", [
+    (8, [3000, 64, 5000, 1200]),   # shared capacity 333 cells: q and w in the scratch slot
+    (2, [3000, 64, 2000, 1200]),   # 1423 cells; 2000: w in shared memory, q in the slot (up to 2846)
+])
+def test_batch_long_tubes_from_global_memory(cuda_device, ctas_per_sm, lengths):
     kw = dict(g=1.4, cfl=0.8, boundtype=3, tend=0.01)
-    lengths = [3000, 64, 5000, 1200]
     p = ev.default_params(nx=max(lengths), ny=1, nz=1, **kw)
     qs = []
     for n in lengths:
@@ -78,7 +81,7 @@ def test_batch_long_tubes_from_global_memory(cuda_device):
         qs.append(ev.ic.shocktube(pt, ul=0.3).reshape(n, 6))
     q = np.ascontiguousarray(np.concatenate(qs))
     with ev.Batch(p, lengths, ev.FP64, ev.STRICT) as b:
-        b.configure(threads=256, ctas_per_sm=8)      # small shared capacity: long tubes go to global
+        b.configure(threads=256, ctas_per_sm=ctas_per_sm)   # small shared capacity: long tubes go to global
         b.set_q(q)
         assert b.run() == 0
         out = b.get_q()
