@@ -34,16 +34,13 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
-#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
-#include <mutex>
 #include <new>
 #include <numeric>
-#include <thread>
 #include <vector>
 
 #include "../../include/evora_gpu.h"
